@@ -1,0 +1,172 @@
+/*
+ * libwnfea_cuda -- C ABI of the B200 (sm_100a) C3D10 / co-rotational-beam solve path.
+ *
+ * Conventions (as the reference's ctypes bridge, wnfea/solver/fast_kernels.py:96-222, and
+ * its HIP C ABI, wnfea/solver/native/hip_kernels.cpp:1523-3164):
+ *   - every function returns int: 0 = OK, < 0 = argument/state error (WN_E* below),
+ *     > 0 = CUDA runtime error code; wn_last_error_string() describes the last failure
+ *     of the calling thread;
+ *   - opaque handles come from *_create and are released by *_destroy (cf. hip_amg_create
+ *     / hip_amg_destroy, hip_kernels.cpp:1891, 2541);
+ *   - plain entry points take HOST buffers and copy in and out (cf. hip_amg_solve_pcg,
+ *     hip_kernels.cpp:2491); *_device entry points take DEVICE pointers and a cudaStream_t
+ *     passed as uintptr_t (0 = legacy default stream) (cf. hip_amg_solve_pcg_device,
+ *     hip_kernels.cpp:2384);
+ *   - the library owns every device buffer inside a handle; caller buffers are borrowed
+ *     for the duration of a call.  A handle is not thread-safe: one stream per handle.
+ *   - sizes are int64_t, node / element indices int32_t, DOF layout node-major [ux,uy,uz].
+ * No entry point falls back to a CPU path: without a usable GPU they return an error.
+ */
+#ifndef WNFEA_CUDA_H
+#define WNFEA_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WN_OK 0
+#define WN_EINVAL (-1)
+#define WN_ESTATE (-2)
+#define WN_EMESH (-3)
+#define WN_EBREAKDOWN (-4)
+#define WN_ENOCONV (-5)
+#define WN_ENOTSPD (-6)
+#define WN_EALLOC (-7)
+#define WN_ETOOBIG (-8)
+
+/* ---------------------------------------------------------------------------------------
+ * Library
+ * ------------------------------------------------------------------------------------- */
+
+/* Message of the calling thread's last failure ("" if none).  Replaces the reference's
+ * bare integer codes (HIP_CHECK, hip_kernels.cpp:21-27). */
+const char* wn_last_error_string(void);
+
+/* Library version, e.g. 100 for 1.0.0. */
+int wn_version(void);
+
+/* ---------------------------------------------------------------------------------------
+ * C3D10 system handle: mesh + 3x3-block pattern + element->block map.
+ * Replaces the per-element COO template + scipy COO->CSR of assemble_c3d10_sparse_3dof
+ * (wnfea/solver/solid_solver.py:50-84) with a pattern built once.
+ * ------------------------------------------------------------------------------------- */
+
+/* nodes: n_nodes x 3 FP64 (host); conn: n_el x 10 int32 (host), C3D10 node order 4 corners
+ * + mid-edges 1-2, 2-3, 3-1, 1-4, 2-4, 3-4 (wnfea/elements/c3d10.py:52-58).
+ * Builds the sorted BSR3 pattern (block (i,j) iff nodes i, j share an element), the
+ * element->block map and the per-block gather lists, and uploads everything. */
+int wn_solid_create(int64_t n_nodes, int64_t n_el, const double* nodes, const int32_t* conn, void** out_handle);
+int wn_solid_destroy(void* h);
+/* n_nodes, n_el, nnzb (number of 3x3 blocks) */
+int wn_solid_info(void* h, int64_t* n_nodes, int64_t* n_el, int64_t* nnzb);
+/* Host copies: row_ptr (n_nodes+1), col_idx (nnzb). */
+int wn_solid_get_pattern(void* h, int32_t* row_ptr, int32_t* col_idx);
+/* Host copy of the element->block map: map[e*100 + 10a + b] = index of block
+ * (conn[e][a], conn[e][b]). */
+int wn_solid_get_map(void* h, int32_t* emap);
+/* Host-only pattern builder (no device work; usable without a GPU).  Call with
+ * col_idx == NULL to get *nnzb (and row_ptr if non-NULL); call again with col_idx
+ * (nnzb entries) and optionally emap (n_el*100) to fill them. */
+int wn_bsr3_pattern_host(int64_t n_nodes, int64_t n_el, const int32_t* conn, int64_t* nnzb, int32_t* row_ptr,
+                         int32_t* col_idx, int32_t* emap);
+/* Dirichlet mask over the 3*n_nodes DOFs (host, 1 = FIXED, NULL = none).  FIXED DOFs get
+ * zero rows/columns and diagonal 1 and a zero load (solid_solver.py:95-127). */
+int wn_solid_set_fixed(void* h, const uint8_t* fixed_mask);
+
+/* Assemble K = sum_e Ke (c3d10.py:219-249, solid_solver.py:26-129) into the handle's BSR3
+ * values (FP64, plus an FP32 copy for the mixed-precision solver), atomic-free through the
+ * element->block map; apply_bcs != 0 applies the Dirichlet mask in the same pass.
+ * props: n_el x 2 [E, nu] (host for wn_assemble_c3d10, device for the _device variant).
+ * Returns WN_EMESH if an element has det J <= 0 (c3d10.py:129-134). */
+int wn_assemble_c3d10(void* h, const double* props, int apply_bcs);
+int wn_assemble_c3d10_device(void* h, const double* d_props, int apply_bcs, uintptr_t stream);
+/* Host copy of the FP64 values: nnzb x 9 (row-major 3x3 blocks). */
+int wn_solid_get_values(void* h, double* values);
+/* Device pointers of the assembled values, pattern and Dirichlet mask (owned by h). */
+int wn_solid_device_arrays(void* h, const double** k64, const float** k32, const int32_t** row_ptr,
+                           const int32_t** col_idx, const uint8_t** fixed_mask);
+
+/* y = K x for the assembled matrix: precision 0 = FP64 values/accumulation, 1 = FP32
+ * values/accumulation (x, y are float then).  Device pointers. */
+int wn_spmv_solid_device(void* h, int precision, const void* x, void* y, uintptr_t stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Smoothed-aggregation AMG + PCG solver (no reference counterpart for C3D10: the reference's
+ * AMG, wnfea/solver/amg_preconditioner.py:147-661, aggregates 6-DOF beam nodes only).  The
+ * near-null space is the 6 rigid-body modes; coarse levels carry 6 DOFs per aggregate.
+ * ------------------------------------------------------------------------------------- */
+typedef struct wn_amg_params {
+  double strength_theta;   /* strong if |A_ij|_F >= theta sqrt(|A_ii|_F |A_jj|_F)      (0.08) */
+  int max_levels;          /* including the coarsest                                   (10)   */
+  int coarse_size;         /* stop coarsening at <= this many scalar DOFs               (1000) */
+  int smoother_degree;     /* Chebyshev degree per pre-/post-smoothing                  (2)    */
+  double cheb_lower;       /* lambda_min = cheb_lower * lambda_max                      (1/30) */
+  double cheb_safety;      /* lambda_max = cheb_safety * rho(D^-1 A) estimate          (1.1)  */
+  double prolong_omega;    /* P = (I - prolong_omega / rho * D^-1 A) P_tent             (4/3)  */
+  int smooth_prolongator;  /* 1 = smoothed aggregation, 0 = plain (tentative) aggregation      */
+  int power_iters;         /* power iterations for rho(D^-1 A)                          (15)   */
+} wn_amg_params;
+
+/* Defaults above. */
+int wn_amg_default_params(wn_amg_params* out);
+
+/* ---------------------------------------------------------------------------------------
+ * Generic block SpMV, y = alpha*A*x + beta*y (cf. hip_spmv_bsr6x6_fp32/_fp64,
+ * hip_kernels.cpp:2975-3087, whose CPU reference is bsr6x6_spmv_cpu, bsr_matrix.py:155-193).
+ * Block shapes (br x bc): 3x3, 6x6, 3x6, 6x3.  n_rows = number of block rows.
+ * ------------------------------------------------------------------------------------- */
+int wn_spmv_bsr_f64_device(int br, int bc, int64_t n_rows, const int32_t* row_ptr, const int32_t* col_idx,
+                           const double* values, const double* x, double* y, double alpha, double beta,
+                           uintptr_t stream);
+int wn_spmv_bsr_f32_device(int br, int bc, int64_t n_rows, const int32_t* row_ptr, const int32_t* col_idx,
+                           const float* values, const float* x, float* y, float alpha, float beta, uintptr_t stream);
+/* Host-buffer variant (allocates, copies, launches, copies back, frees) -- the calling
+ * convention of hip_spmv_bsr6x6_fp64 (hip_kernels.cpp:3032). n_cols = block columns. */
+int wn_spmv_bsr_f64(int br, int bc, int64_t n_rows, int64_t n_cols, int64_t nnzb, const int32_t* row_ptr,
+                    const int32_t* col_idx, const double* values, const double* x, double* y, double alpha,
+                    double beta);
+
+/* ---------------------------------------------------------------------------------------
+ * Element-level kernels
+ * ------------------------------------------------------------------------------------- */
+
+/* Ke (n_el x 30 x 30, row-major, DOF order node-major) of elements given by coordinates
+ * coords (n_el x 10 x 3) and props (n_el x 2) -- host buffers.  Batched form of
+ * element_stiffness_c3d10 (c3d10.py:219-249).  WN_EMESH on det J <= 0. */
+int wn_c3d10_element_stiffness(int64_t n_el, const double* coords, const double* props, double* Ke);
+
+/* Internal forces F_int = sum_e f_e(u) with f_e = sum_g w|J| B^T C B u_e (c3d10.py:252-283),
+ * atomic-free (node gather in element order).  Same argument list and U/F_int stride of 6
+ * as the reference's compute_c3d10_internal_forces_native (kernels.cpp:244-252); host
+ * buffers; F_int is accumulated into (the reference's += scatter). */
+int wn_c3d10_internal_forces(const double* nodes, const int32_t* solid_elements, const double* props, const double* U,
+                             double* F_int, int n_solids, int n_nodes);
+/* Handle variant on device pointers: f_int (3 n_nodes, overwritten) from u (3 n_nodes). */
+int wn_fint_c3d10_device(void* h, const double* d_u, double* d_fint, uintptr_t stream);
+
+/* Host-buffer variant of wn_fint_c3d10_device. */
+int wn_fint_c3d10(void* h, const double* u, double* fint);
+
+/* Stresses (compute_c3d10_stress_field, solid_solver.py:311-365): cell_sig n_el x 6
+ * [sxx,syy,szz,sxy,syz,szx] (mean of the 4 Gauss points), cell_vm n_el, nodal_vm n_nodes
+ * (unweighted mean over incident elements).  Uses the props of the last assembly. */
+int wn_stress_c3d10(void* h, const double* u, double* cell_sig, double* cell_vm, double* nodal_vm);
+int wn_stress_c3d10_device(void* h, const double* d_u, double* d_cell_sig, double* d_cell_vm, double* d_nodal_vm,
+                           uintptr_t stream);
+
+/* Compliance adjoint (no reference counterpart): for C = F^T u with K(E) u = F,
+ * grad_E[e] = dC/dE_e = -u_e^T Ke u_e / E_e (self-adjoint: reuses u, no extra solve) and
+ * grad_F = dC/dF = 2u on free DOFs, 0 on FIXED DOFs.  Either output may be NULL. */
+int wn_adjoint_compliance_device(void* h, const double* d_u, double* d_grad_E, double* d_grad_F, uintptr_t stream);
+int wn_adjoint_compliance(void* h, const double* u, double* grad_E, double* grad_F);
+
+/* Block until all work of the calling thread's device is done. */
+int wn_device_synchronize(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WNFEA_CUDA_H */

@@ -1,0 +1,29 @@
+"""wnfea_b200 -- B200-native (sm_100a) implementation of WNFEA's linear-elastic solve path.
+
+The public names follow the reference package ``wnfea`` (wnfea/__init__.py) for the C3D10
+solid and co-rotational beam path; every numerical kernel runs on the GPU through the C ABI
+of ``libwnfea_cuda.so`` (include/wnfea_cuda.h).
+"""
+
+from .model import (
+    DOFConstraint,
+    DOFType,
+    FEAModel,
+    LoadDef,
+    MaterialDef,
+    PropertyAssignment,
+    SectionDef,
+    SupportDef,
+    create_fixed_support,
+    create_rectangular_bar,
+)
+from .solid_solver import (
+    assemble_c3d10_sparse_3dof,
+    compute_c3d10_stress_field,
+)
+
+__all__ = [
+    "FEAModel", "MaterialDef", "SectionDef", "PropertyAssignment",
+    "SupportDef", "LoadDef", "DOFConstraint", "DOFType", "create_fixed_support", "create_rectangular_bar",
+    "assemble_c3d10_sparse_3dof", "compute_c3d10_stress_field",
+]

@@ -1,0 +1,108 @@
+"""ctypes binding of libwnfea_cuda.so (the C ABI in include/wnfea_cuda.h).
+
+Mirrors the reference's loader (``_get_hip_lib``, wnfea/solver/fast_kernels.py:96-222):
+argtypes/restype are declared once, and a non-zero status raises ``RuntimeError`` with the
+library's message (as fast_kernels.py:590-591, 660-661).  Unlike the reference there is no
+silent CPU fallback: a missing library raises at first use.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+_P = C.c_void_p
+_I = C.c_int
+_I64 = C.c_int64
+_D = C.c_double
+_F = C.c_float
+_U = C.c_uint64  # uintptr_t stream
+
+# name -> (restype, argtypes); must match include/wnfea_cuda.h
+SIGNATURES: dict[str, tuple] = {
+    "wn_last_error_string": (C.c_char_p, []),
+    "wn_version": (_I, []),
+    "wn_device_synchronize": (_I, []),
+    "wn_solid_create": (_I, [_I64, _I64, _P, _P, C.POINTER(_P)]),
+    "wn_solid_destroy": (_I, [_P]),
+    "wn_solid_info": (_I, [_P, C.POINTER(_I64), C.POINTER(_I64), C.POINTER(_I64)]),
+    "wn_solid_get_pattern": (_I, [_P, _P, _P]),
+    "wn_solid_get_map": (_I, [_P, _P]),
+    "wn_bsr3_pattern_host": (_I, [_I64, _I64, _P, C.POINTER(_I64), _P, _P, _P]),
+    "wn_solid_set_fixed": (_I, [_P, _P]),
+    "wn_assemble_c3d10": (_I, [_P, _P, _I]),
+    "wn_assemble_c3d10_device": (_I, [_P, _P, _I, _U]),
+    "wn_solid_get_values": (_I, [_P, _P]),
+    "wn_solid_device_arrays": (_I, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
+    "wn_spmv_solid_device": (_I, [_P, _I, _P, _P, _U]),
+    "wn_spmv_bsr_f64_device": (_I, [_I, _I, _I64, _P, _P, _P, _P, _P, _D, _D, _U]),
+    "wn_spmv_bsr_f32_device": (_I, [_I, _I, _I64, _P, _P, _P, _P, _P, _F, _F, _U]),
+    "wn_spmv_bsr_f64": (_I, [_I, _I, _I64, _I64, _I64, _P, _P, _P, _P, _P, _D, _D]),
+    "wn_c3d10_element_stiffness": (_I, [_I64, _P, _P, _P]),
+    "wn_c3d10_internal_forces": (_I, [_P, _P, _P, _P, _P, _I, _I]),
+    "wn_fint_c3d10_device": (_I, [_P, _P, _P, _U]),
+    "wn_fint_c3d10": (_I, [_P, _P, _P]),
+    "wn_stress_c3d10": (_I, [_P, _P, _P, _P, _P]),
+    "wn_stress_c3d10_device": (_I, [_P, _P, _P, _P, _P, _U]),
+    "wn_adjoint_compliance_device": (_I, [_P, _P, _P, _P, _U]),
+    "wn_adjoint_compliance": (_I, [_P, _P, _P, _P]),
+}
+
+LIB_PATH = Path(__file__).resolve().parent / "libwnfea_cuda.so"
+_LIB = None
+
+
+def lib():
+    """Load (once) and return the library; raises if it is missing or incomplete."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = Path(os.environ.get("WNFEA_CUDA_LIB", LIB_PATH))
+    if not path.exists():
+        raise RuntimeError(
+            f"libwnfea_cuda.so not found at {path}; build it with `python -m wnfea_b200.csrc.build` "
+            "(this package has no CPU fallback)"
+        )
+    handle = C.CDLL(str(path))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(handle, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = handle
+    return handle
+
+
+def last_error() -> str:
+    msg = lib().wn_last_error_string()
+    return msg.decode() if msg else ""
+
+
+class WnError(RuntimeError):
+    """A non-zero status from libwnfea_cuda."""
+
+    def __init__(self, fn: str, code: int, msg: str):
+        super().__init__(f"{fn} failed with status {code}: {msg}")
+        self.code = code
+
+
+def call(name: str, *args) -> None:
+    rc = getattr(lib(), name)(*args)
+    if rc != 0:
+        raise WnError(name, rc, last_error())
+
+
+def ptr(a: np.ndarray | None):
+    """Host pointer of a C-contiguous array (None -> NULL)."""
+    if a is None:
+        return None
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def dptr(t) -> int | None:
+    """Device pointer of a torch tensor (None -> NULL)."""
+    return None if t is None else t.data_ptr()

@@ -1,0 +1,131 @@
+// Device-resident AMG hierarchy and solver workspace.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <memory>
+#include <vector>
+
+#include "amg_setup.h"
+#include "device_array.h"
+
+namespace wn {
+
+struct DevBsr {
+  int br = 0, bc = 0;
+  int64_t n_rows = 0, n_cols = 0, nnzb = 0;
+  DArray<int32_t> rp, ci;
+  DArray<double> v64;
+  DArray<float> v32;
+  int upload(const HostBsr& h);
+};
+
+// work vectors of one level in one precision
+template <typename T>
+struct LevelVecs {
+  DArray<T> b, x, x2, r, d, d2, res;
+  int alloc(int64_t n) {
+    WN_CHECK(b.alloc(n));
+    WN_CHECK(x.alloc(n));
+    WN_CHECK(x2.alloc(n));
+    WN_CHECK(r.alloc(n));
+    WN_CHECK(d.alloc(n));
+    WN_CHECK(d2.alloc(n));
+    WN_CHECK(res.alloc(n));
+    return 0;
+  }
+};
+
+struct DevLevel {
+  int bs = 3;
+  int64_t n_nodes = 0;
+  // A: level 0 borrows the system's matrix; coarser levels own theirs
+  const int32_t* a_rp = nullptr;
+  const int32_t* a_ci = nullptr;
+  const double* a64 = nullptr;
+  const float* a32 = nullptr;
+  DevBsr A;
+  DArray<double> dinv64;
+  DArray<float> dinv32;
+  double rho = 0.0;
+  double inv_theta = 0.0;
+  std::vector<double> c1, c2;  // Chebyshev step coefficients k = 1..deg-1
+  DevBsr P, R;
+  LevelVecs<double> v64;
+  LevelVecs<float> v32;
+};
+
+struct AmgHierarchy {
+  HostHierarchy host;  // kept for export to tests / diagnostics
+  std::vector<DevLevel> levels;
+  int64_t n_coarse = 0;
+  DArray<double> coarse_inv;
+  DArray<double> cb64, cx64;  // coarsest rhs / solution (FP64 path)
+  DArray<float> cb32, cx32;   // (FP32 path)
+  int degree = 2;
+  double setup_seconds = 0.0;
+};
+
+// PCG scalars shared between kernels (device)
+struct PcgScalars {
+  double rz[2];    // r.z of the last two iterations (parity-indexed)
+  double bnorm2;   // ||b||^2
+  double tol2;     // (rtol ||b||)^2
+  double rr;       // ||r||^2 of the last check
+  double alpha;
+  int done;
+  int iters;
+  int status;
+  int pad;
+};
+
+template <typename T>
+struct PcgVecs {
+  DArray<T> x, r, z, p0, p1, q;
+  int alloc(int64_t n) {
+    WN_CHECK(x.alloc(n));
+    WN_CHECK(r.alloc(n));
+    WN_CHECK(z.alloc(n));
+    WN_CHECK(p0.alloc(n));
+    WN_CHECK(p1.alloc(n));
+    WN_CHECK(q.alloc(n));
+    return 0;
+  }
+};
+
+struct GraphCache {
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t stream = nullptr;
+  int64_t key = -1;
+  ~GraphCache() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+  void reset() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    key = -1;
+  }
+};
+
+struct SolverWork {
+  int64_t n = 0;  // scalar DOFs
+  static constexpr int kParts = 148 * 4;  // CTAs of every partial-producing kernel
+  DArray<double> partA, partB, partC;
+  DArray<PcgScalars> scal;   // [0] = FP64 / inner solve, [1] = outer refinement
+  DArray<double> u64, r64, Fd;  // outer refinement (mixed) vectors
+  DArray<double> dinv64;      // Jacobi (point) of the fine matrix
+  DArray<float> dinv32;
+  PcgVecs<double> p64;
+  PcgVecs<float> p32;
+  // graphs: [precision][kind] kind 0 = init, 1 = chunk of iterations
+  GraphCache graphs[2][2];
+  int64_t launches = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  ~SolverWork() {
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+  }
+};
+
+}  // namespace wn

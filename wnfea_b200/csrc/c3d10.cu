@@ -1,0 +1,360 @@
+// C3D10 element kernels for sm_100a:
+//   * stiffness of every element (upper-triangle 3x3 blocks) into a scratch buffer,
+//   * atomic-free gather of those blocks into the BSR3 matrix through the element->block
+//     map's inverse, with Dirichlet rows/columns applied in the same pass,
+//   * matrix-free internal force / strain energy (adjoint) and Gauss-point stresses.
+//
+// Element math restates wnfea/elements/c3d10.py:219-318.  Ke entries use the isotropic
+// closed form K_ab[i][j] = sum_g w|J| (lam a_i b_j + mu a_j b_i + mu delta_ij a.b) with
+// a = dN_a/dx, b = dN_b/dx, which equals (B^T C B)[3a+i][3b+j] of c3d10.py:244-246; only
+// a <= b is computed and K_ba = K_ab^T, so Ke is exactly symmetric as after
+// c3d10.py:248.
+#include <algorithm>
+
+#include "c3d10.cuh"
+#include "common.cuh"
+#include "kernels.h"
+
+namespace wn {
+
+// (a, b) of upper-triangle index t (inverse of tri_index)
+__constant__ unsigned char c_tri_a[55];
+__constant__ unsigned char c_tri_b[55];
+
+static int ensure_tri_tables() {
+  static thread_local int done_dev = -1;
+  int dev = 0;
+  WN_CUDA(cudaGetDevice(&dev));
+  if (done_dev == dev) return 0;
+  unsigned char ta[55], tb[55];
+  int t = 0;
+  for (int a = 0; a < 10; ++a)
+    for (int b = a; b < 10; ++b) {
+      ta[t] = (unsigned char)a;
+      tb[t] = (unsigned char)b;
+      ++t;
+    }
+  WN_CUDA(cudaMemcpyToSymbol(c_tri_a, ta, sizeof(ta)));
+  WN_CUDA(cudaMemcpyToSymbol(c_tri_b, tb, sizeof(tb)));
+  done_dev = dev;
+  return 0;
+}
+
+constexpr int KE_TILE = 16;      // elements per CTA
+constexpr int KE_THREADS = 256;  // threads per CTA
+
+// Stage one element's coordinates: X[a][j] = nodes[conn[e][a]][j].
+__device__ __forceinline__ void load_coords(const double* __restrict__ nodes, const int32_t* __restrict__ conn,
+                                            int64_t e, double X[10][3]) {
+#pragma unroll
+  for (int a = 0; a < 10; ++a) {
+    const int64_t n = conn[e * 10 + a];
+    X[a][0] = nodes[n * 3 + 0];
+    X[a][1] = nodes[n * 3 + 1];
+    X[a][2] = nodes[n * 3 + 2];
+  }
+}
+
+// Ke upper triangle of elements [0, n_el): out[(e * 55 + t) * 9 + 3 i + j].
+// Phase 1: one thread per (element, Gauss point) computes dN/dx and w|J| into shared
+// memory.  Phase 2: all threads produce the 495 block entries of the tile's elements,
+// written contiguously.  An element with det J <= 0 raises bit 0 of *flags.
+__global__ void __launch_bounds__(KE_THREADS) ke_upper_kernel(int64_t n_el, const double* __restrict__ nodes,
+                                                              const int32_t* __restrict__ conn,
+                                                              const double* __restrict__ props,
+                                                              double* __restrict__ out, int* __restrict__ flags) {
+  __shared__ double s_dn[KE_TILE][4][3][10];
+  __shared__ double s_w[KE_TILE][4];
+  __shared__ double s_lam[KE_TILE], s_mu[KE_TILE];
+  for (int64_t tile = blockIdx.x; tile * KE_TILE < n_el; tile += gridDim.x) {
+    const int64_t e0 = tile * KE_TILE;
+    const int ne = (int)((n_el - e0) < KE_TILE ? (n_el - e0) : KE_TILE);
+    if (threadIdx.x < KE_TILE * 4) {
+      const int le = threadIdx.x >> 2, g = threadIdx.x & 3;
+      if (le < ne) {
+        double X[10][3];
+        load_coords(nodes, conn, e0 + le, X);
+        double dndx[3][10];
+        const double det = gp_cartesian(g, X, dndx);
+        if (!(det > 0.0)) flags[0] = 1;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int a = 0; a < 10; ++a) s_dn[le][g][i][a] = dndx[i][a];
+        s_w[le][g] = kWeight * det;
+        if (g == 0) {
+          double lam, mu;
+          lame(props[(e0 + le) * 2], props[(e0 + le) * 2 + 1], lam, mu);
+          s_lam[le] = lam;
+          s_mu[le] = mu;
+        }
+      }
+    }
+    __syncthreads();
+    const int n_out = ne * 495;
+    double* dst = out + e0 * 495;
+    for (int o = threadIdx.x; o < n_out; o += KE_THREADS) {
+      const int le = o / 495;
+      const int rem = o - le * 495;
+      const int t = rem / 9;
+      const int ij = rem - t * 9;
+      const int i = ij / 3, j = ij - (ij / 3) * 3;
+      const int a = c_tri_a[t], b = c_tri_b[t];
+      const double lam = s_lam[le], mu = s_mu[le];
+      double acc = 0.0;
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {
+        const double ai = s_dn[le][g][i][a], bj = s_dn[le][g][j][b];
+        const double aj = s_dn[le][g][j][a], bi = s_dn[le][g][i][b];
+        double v = lam * ai * bj + mu * aj * bi;
+        if (i == j) {
+          const double dot = s_dn[le][g][0][a] * s_dn[le][g][0][b] + s_dn[le][g][1][a] * s_dn[le][g][1][b] +
+                             s_dn[le][g][2][a] * s_dn[le][g][2][b];
+          v += mu * dot;
+        }
+        acc += s_w[le][g] * v;
+      }
+      dst[o] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+// Gather-assemble: one thread per matrix entry.  K[b][k] = sum over the block's gather list
+// (fixed (element, a, b) order) of the stored element block, transposed when a > b.
+// Dirichlet: an entry in a fixed row or column becomes 1 on the diagonal, 0 elsewhere
+// (solid_solver.py:105-125).  Writes FP64 values and, if k32 != nullptr, an FP32 copy.
+__global__ void gather_assemble_kernel(int64_t nnzb, const int32_t* __restrict__ gptr,
+                                       const int32_t* __restrict__ gsrc, const double* __restrict__ ke,
+                                       const int32_t* __restrict__ block_row, const int32_t* __restrict__ col_idx,
+                                       const uint8_t* __restrict__ fixed, double* __restrict__ k64,
+                                       float* __restrict__ k32) {
+  const int64_t total = nnzb * 9;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = t / 9;
+    const int k = (int)(t - b * 9);
+    const int i = k / 3, j = k - (k / 3) * 3;
+    const int kt = j * 3 + i;
+    const int32_t s = gptr[b], e = gptr[b + 1];
+    double acc = 0.0;
+    for (int32_t q = s; q < e; ++q) {
+      const int32_t src = gsrc[q];
+      const int64_t blk = src >> 1;
+      acc += ke[blk * 9 + ((src & 1) ? kt : k)];
+    }
+    if (fixed) {
+      const int64_t rdof = (int64_t)block_row[b] * 3 + i;
+      const int64_t cdof = (int64_t)col_idx[b] * 3 + j;
+      if (fixed[rdof] | fixed[cdof]) acc = (rdof == cdof) ? 1.0 : 0.0;
+    }
+    k64[t] = acc;
+    if (k32) k32[t] = (float)acc;
+  }
+}
+
+// Matrix-free element forces f_e = Ke u_e (= sum_g w|J| B^T C B u_e, c3d10.py:252-283) for
+// DOF stride `stride` (3 for the solid path, 6 for the reference's mixed-DOF layout of
+// kernels.cpp:244-376).  If fe_out: writes f_e (n_el x 30).  If energy_out: writes
+// u_e . f_e per element.  If grad_e: writes -u_e . f_e / E_e (compliance adjoint).
+__global__ void element_force_kernel(int64_t n_el, const double* __restrict__ nodes, const int32_t* __restrict__ conn,
+                                     const double* __restrict__ props, const double* __restrict__ u, int stride,
+                                     double* __restrict__ fe_out, double* __restrict__ energy_out,
+                                     double* __restrict__ grad_e, int* __restrict__ flags) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n_el; e += (int64_t)gridDim.x * blockDim.x) {
+    double X[10][3], ue[10][3];
+    load_coords(nodes, conn, e, X);
+#pragma unroll
+    for (int a = 0; a < 10; ++a) {
+      const int64_t n = conn[e * 10 + a];
+      ue[a][0] = u[n * stride + 0];
+      ue[a][1] = u[n * stride + 1];
+      ue[a][2] = u[n * stride + 2];
+    }
+    const double E = props[e * 2], nu = props[e * 2 + 1];
+    const double f = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    const double c11 = f * (1.0 - nu), c12 = f * nu, G = E / (2.0 * (1.0 + nu));
+    double fe[10][3];
+#pragma unroll
+    for (int a = 0; a < 10; ++a) fe[a][0] = fe[a][1] = fe[a][2] = 0.0;
+    bool bad = false;
+#pragma unroll 1
+    for (int g = 0; g < 4; ++g) {
+      double d[3][10];
+      const double det = gp_cartesian(g, X, d);
+      if (!(det > 0.0)) bad = true;
+      double eps[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int a = 0; a < 10; ++a) {
+        eps[0] += d[0][a] * ue[a][0];
+        eps[1] += d[1][a] * ue[a][1];
+        eps[2] += d[2][a] * ue[a][2];
+        eps[3] += d[1][a] * ue[a][0] + d[0][a] * ue[a][1];
+        eps[4] += d[2][a] * ue[a][1] + d[1][a] * ue[a][2];
+        eps[5] += d[2][a] * ue[a][0] + d[0][a] * ue[a][2];
+      }
+      const double s0 = c11 * eps[0] + c12 * eps[1] + c12 * eps[2];
+      const double s1 = c12 * eps[0] + c11 * eps[1] + c12 * eps[2];
+      const double s2 = c12 * eps[0] + c12 * eps[1] + c11 * eps[2];
+      const double s3 = G * eps[3], s4 = G * eps[4], s5 = G * eps[5];
+      const double w = kWeight * det;
+#pragma unroll
+      for (int a = 0; a < 10; ++a) {
+        fe[a][0] += w * (d[0][a] * s0 + d[1][a] * s3 + d[2][a] * s5);
+        fe[a][1] += w * (d[1][a] * s1 + d[0][a] * s3 + d[2][a] * s4);
+        fe[a][2] += w * (d[2][a] * s2 + d[1][a] * s4 + d[0][a] * s5);
+      }
+    }
+    if (bad) flags[0] = 1;
+    if (fe_out) {
+#pragma unroll
+      for (int a = 0; a < 10; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) fe_out[e * 30 + a * 3 + c] = fe[a][c];
+    }
+    if (energy_out || grad_e) {
+      double en = 0.0;
+#pragma unroll
+      for (int a = 0; a < 10; ++a) en += ue[a][0] * fe[a][0] + ue[a][1] * fe[a][1] + ue[a][2] * fe[a][2];
+      if (energy_out) energy_out[e] = en;
+      if (grad_e) grad_e[e] = -en / E;
+    }
+  }
+}
+
+// Node gather of element vectors: out[n * stride + c] (+)= sum over the node's incident
+// (element, local node) pairs, in ascending element order, of fe[e][a][c].  Atomic-free.
+__global__ void node_gather_kernel(int64_t n_nodes, const int64_t* __restrict__ inc_ptr,
+                                   const int32_t* __restrict__ inc_ea, const double* __restrict__ fe, int stride,
+                                   int accumulate, double* __restrict__ out) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_nodes * 3;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t n = t / 3;
+    const int c = (int)(t - n * 3);
+    double s = 0.0;
+    for (int64_t q = inc_ptr[n]; q < inc_ptr[n + 1]; ++q) s += fe[(int64_t)inc_ea[q] * 3 + c];
+    if (accumulate)
+      out[n * stride + c] += s;
+    else
+      out[n * stride + c] = s;
+  }
+}
+
+// Cell stresses: mean of the 4 Gauss-point stresses [sxx, syy, szz, sxy, syz, szx] and the
+// mean Gauss-point von Mises (solid_solver.py:341-350, c3d10.py:286-318).
+__global__ void stress_kernel(int64_t n_el, const double* __restrict__ nodes, const int32_t* __restrict__ conn,
+                              const double* __restrict__ props, const double* __restrict__ u,
+                              double* __restrict__ cell_sig, double* __restrict__ cell_vm) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n_el; e += (int64_t)gridDim.x * blockDim.x) {
+    double X[10][3], ue[10][3];
+    load_coords(nodes, conn, e, X);
+#pragma unroll
+    for (int a = 0; a < 10; ++a) {
+      const int64_t n = conn[e * 10 + a];
+      ue[a][0] = u[n * 3 + 0];
+      ue[a][1] = u[n * 3 + 1];
+      ue[a][2] = u[n * 3 + 2];
+    }
+    const double E = props[e * 2], nu = props[e * 2 + 1];
+    const double f = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    const double c11 = f * (1.0 - nu), c12 = f * nu, G = E / (2.0 * (1.0 + nu));
+    double ssum[6] = {0, 0, 0, 0, 0, 0};
+    double vmsum = 0.0;
+#pragma unroll 1
+    for (int g = 0; g < 4; ++g) {
+      double d[3][10];
+      gp_cartesian(g, X, d);
+      double eps[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int a = 0; a < 10; ++a) {
+        eps[0] += d[0][a] * ue[a][0];
+        eps[1] += d[1][a] * ue[a][1];
+        eps[2] += d[2][a] * ue[a][2];
+        eps[3] += d[1][a] * ue[a][0] + d[0][a] * ue[a][1];
+        eps[4] += d[2][a] * ue[a][1] + d[1][a] * ue[a][2];
+        eps[5] += d[2][a] * ue[a][0] + d[0][a] * ue[a][2];
+      }
+      const double s[6] = {c11 * eps[0] + c12 * eps[1] + c12 * eps[2], c12 * eps[0] + c11 * eps[1] + c12 * eps[2],
+                           c12 * eps[0] + c12 * eps[1] + c11 * eps[2], G * eps[3], G * eps[4], G * eps[5]};
+#pragma unroll
+      for (int k = 0; k < 6; ++k) ssum[k] += s[k];
+      const double a0 = s[0] - s[1], a1 = s[1] - s[2], a2 = s[2] - s[0];
+      vmsum += sqrt(0.5 * (a0 * a0 + a1 * a1 + a2 * a2 + 6.0 * (s[3] * s[3] + s[4] * s[4] + s[5] * s[5])));
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) cell_sig[e * 6 + k] = ssum[k] / 4.0;
+    cell_vm[e] = vmsum / 4.0;
+  }
+}
+
+// Nodal von Mises = unweighted mean of incident cells' von Mises (solid_solver.py:352-363).
+__global__ void nodal_average_kernel(int64_t n_nodes, const int64_t* __restrict__ inc_ptr,
+                                     const int32_t* __restrict__ inc_ea, const double* __restrict__ cell_vm,
+                                     double* __restrict__ nodal) {
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < n_nodes; n += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = inc_ptr[n], e = inc_ptr[n + 1];
+    double acc = 0.0;
+    for (int64_t q = s; q < e; ++q) acc += cell_vm[inc_ea[q] / 10];
+    nodal[n] = (e > s) ? acc / (double)(e - s) : 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------------------
+int launch_ke_upper(int64_t n_el, const double* nodes, const int32_t* conn, const double* props, double* out,
+                    int* flags, cudaStream_t st) {
+  WN_CHECK(ensure_tri_tables());
+  if (n_el == 0) return 0;
+  const int64_t tiles = (n_el + KE_TILE - 1) / KE_TILE;
+  const int grid = (int)std::min<int64_t>(tiles, (int64_t)kNumSMs * 8);
+  ke_upper_kernel<<<grid, KE_THREADS, 0, st>>>(n_el, nodes, conn, props, out, flags);
+  WN_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int launch_gather_assemble(int64_t nnzb, const int32_t* gptr, const int32_t* gsrc, const double* ke,
+                           const int32_t* block_row, const int32_t* col_idx, const uint8_t* fixed, double* k64,
+                           float* k32, cudaStream_t st) {
+  if (nnzb == 0) return 0;
+  const int grid = grid_for(nnzb * 9, 1, 256, 32);
+  gather_assemble_kernel<<<grid, 256, 0, st>>>(nnzb, gptr, gsrc, ke, block_row, col_idx, fixed, k64, k32);
+  WN_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int launch_element_force(int64_t n_el, const double* nodes, const int32_t* conn, const double* props,
+                         const double* u, int stride, double* fe_out, double* energy_out, double* grad_e,
+                         int* flags, cudaStream_t st) {
+  if (n_el == 0) return 0;
+  const int grid = grid_for(n_el, 1, 128, 16);
+  element_force_kernel<<<grid, 128, 0, st>>>(n_el, nodes, conn, props, u, stride, fe_out, energy_out, grad_e, flags);
+  WN_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int launch_node_gather(int64_t n_nodes, const int64_t* inc_ptr, const int32_t* inc_ea, const double* fe, int stride,
+                       int accumulate, double* out, cudaStream_t st) {
+  if (n_nodes == 0) return 0;
+  const int grid = grid_for(n_nodes * 3, 1, 256, 16);
+  node_gather_kernel<<<grid, 256, 0, st>>>(n_nodes, inc_ptr, inc_ea, fe, stride, accumulate, out);
+  WN_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int launch_stress(int64_t n_el, int64_t n_nodes, const double* nodes, const int32_t* conn, const double* props,
+                  const double* u, const int64_t* inc_ptr, const int32_t* inc_ea, double* cell_sig, double* cell_vm,
+                  double* nodal_vm, cudaStream_t st) {
+  if (n_el > 0) {
+    const int grid = grid_for(n_el, 1, 128, 16);
+    stress_kernel<<<grid, 128, 0, st>>>(n_el, nodes, conn, props, u, cell_sig, cell_vm);
+    WN_CUDA(cudaGetLastError());
+  }
+  if (n_nodes > 0) {
+    const int grid = grid_for(n_nodes, 1, 256, 16);
+    nodal_average_kernel<<<grid, 256, 0, st>>>(n_nodes, inc_ptr, inc_ea, cell_vm, nodal_vm);
+    WN_CUDA(cudaGetLastError());
+  }
+  return 0;
+}
+
+}  // namespace wn

@@ -1,0 +1,442 @@
+// extern "C" boundary of libwnfea_cuda: handle management, assembly, SpMV and element-level
+// entry points (declared in include/wnfea_cuda.h).
+#include <cstdarg>
+#include <cstring>
+#include <string>
+
+#include "wnfea_cuda.h"
+#include "common.cuh"
+#include "amg.h"
+#include "kernels.h"
+#include "solid.h"
+
+namespace wn {
+
+static thread_local std::string g_last_error;
+
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+}
+const char* last_error() { return g_last_error.c_str(); }
+
+__global__ void grad_f_kernel(int64_t n, const double* __restrict__ u, const uint8_t* __restrict__ fixed,
+                              double* __restrict__ g) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    g[i] = (fixed && fixed[i]) ? 0.0 : 2.0 * u[i];
+}
+
+static Solid* as_solid(void* h) { return reinterpret_cast<Solid*>(h); }
+
+static int select_device(Solid* s) {
+  WN_CUDA(cudaSetDevice(s->device));
+  return 0;
+}
+
+static int read_flag(Solid* s, cudaStream_t st, int* value) {
+  WN_CUDA(cudaMemcpyAsync(value, s->flags.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  WN_CUDA(cudaStreamSynchronize(st));
+  return 0;
+}
+
+}  // namespace wn
+
+using namespace wn;
+
+extern "C" {
+
+const char* wn_last_error_string(void) { return wn::last_error(); }
+
+int wn_version(void) { return 100; }
+
+int wn_device_synchronize(void) {
+  WN_CUDA(cudaDeviceSynchronize());
+  return 0;
+}
+
+int wn_solid_create(int64_t n_nodes, int64_t n_el, const double* nodes, const int32_t* conn, void** out_handle) {
+  WN_REQUIRE(out_handle && nodes && (conn || n_el == 0), WN_EINVAL, "wn_solid_create: null argument");
+  WN_REQUIRE(n_nodes > 0 && n_el >= 0, WN_EINVAL, "wn_solid_create: bad sizes n_nodes=%lld n_el=%lld",
+             (long long)n_nodes, (long long)n_el);
+  WN_REQUIRE(n_nodes < (int64_t)INT32_MAX / 6, WN_ETOOBIG, "wn_solid_create: too many nodes");
+  *out_handle = nullptr;
+  int dev = 0;
+  WN_CUDA(cudaGetDevice(&dev));
+  Bsr3Pattern pat;
+  int rc = build_bsr3_pattern(n_nodes, n_el, conn, pat);
+  WN_REQUIRE(rc != -3, WN_EMESH, "wn_solid_create: element node index out of range [0, %lld)", (long long)n_nodes);
+  WN_REQUIRE(rc != -8, WN_ETOOBIG, "wn_solid_create: mesh too large for 32-bit block indices");
+  WN_REQUIRE(rc == 0, WN_EINVAL, "wn_solid_create: pattern construction failed (%d)", rc);
+  auto* s = new Solid();
+  s->device = dev;
+  s->n_nodes = n_nodes;
+  s->n_el = n_el;
+  s->nnzb = pat.nnzb;
+  s->h_nodes.assign(nodes, nodes + n_nodes * 3);
+  int st = 0;
+  st = st ? st : s->nodes.upload(nodes, n_nodes * 3);
+  st = st ? st : s->conn.upload(conn, n_el * 10);
+  st = st ? st : s->row_ptr.upload(pat.row_ptr);
+  st = st ? st : s->col_idx.upload(pat.col_idx);
+  st = st ? st : s->block_row.upload(pat.block_row);
+  st = st ? st : s->diag_block.upload(pat.diag_block);
+  st = st ? st : s->emap.upload(pat.emap);
+  st = st ? st : s->gptr.upload(pat.gather_ptr);
+  st = st ? st : s->gsrc.upload(pat.gather_src);
+  st = st ? st : s->inc_ptr.upload(pat.inc_ptr);
+  st = st ? st : s->inc_ea.upload(pat.inc_ea);
+  st = st ? st : s->flags.alloc(16);
+  st = st ? st : s->flags.zero();
+  st = st ? st : s->fixed.alloc(n_nodes * 3);
+  st = st ? st : s->fixed.zero();
+  if (st == 0) {
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+      set_error("wn_solid_create: %s", cudaGetErrorString(e));
+      st = (int)e;
+    }
+  }
+  if (st != 0) {
+    delete s;
+    return st;
+  }
+  s->h_row_ptr = std::move(pat.row_ptr);
+  s->h_col_idx = std::move(pat.col_idx);
+  s->h_diag_block = std::move(pat.diag_block);
+  s->h_fixed.assign(n_nodes * 3, 0);
+  *out_handle = s;
+  return 0;
+}
+
+int wn_bsr3_pattern_host(int64_t n_nodes, int64_t n_el, const int32_t* conn, int64_t* nnzb, int32_t* row_ptr,
+                         int32_t* col_idx, int32_t* emap) {
+  WN_REQUIRE(nnzb && (conn || n_el == 0) && n_nodes > 0 && n_el >= 0, WN_EINVAL, "wn_bsr3_pattern_host: bad argument");
+  Bsr3Pattern pat;
+  int rc = build_bsr3_pattern(n_nodes, n_el, conn, pat);
+  WN_REQUIRE(rc != -3, WN_EMESH, "wn_bsr3_pattern_host: element node index out of range");
+  WN_REQUIRE(rc != -8, WN_ETOOBIG, "wn_bsr3_pattern_host: mesh too large for 32-bit block indices");
+  WN_REQUIRE(rc == 0, WN_EINVAL, "wn_bsr3_pattern_host: failed (%d)", rc);
+  *nnzb = pat.nnzb;
+  if (row_ptr) memcpy(row_ptr, pat.row_ptr.data(), sizeof(int32_t) * (n_nodes + 1));
+  if (col_idx) memcpy(col_idx, pat.col_idx.data(), sizeof(int32_t) * pat.nnzb);
+  if (col_idx && emap) memcpy(emap, pat.emap.data(), sizeof(int32_t) * n_el * 100);
+  return 0;
+}
+
+int wn_solid_destroy(void* h) {
+  if (!h) return 0;
+  Solid* s = as_solid(h);
+  cudaSetDevice(s->device);
+  delete s;
+  return 0;
+}
+
+int wn_solid_info(void* h, int64_t* n_nodes, int64_t* n_el, int64_t* nnzb) {
+  WN_REQUIRE(h, WN_EINVAL, "wn_solid_info: null handle");
+  Solid* s = as_solid(h);
+  if (n_nodes) *n_nodes = s->n_nodes;
+  if (n_el) *n_el = s->n_el;
+  if (nnzb) *nnzb = s->nnzb;
+  return 0;
+}
+
+int wn_solid_get_pattern(void* h, int32_t* row_ptr, int32_t* col_idx) {
+  WN_REQUIRE(h, WN_EINVAL, "wn_solid_get_pattern: null handle");
+  Solid* s = as_solid(h);
+  if (row_ptr) memcpy(row_ptr, s->h_row_ptr.data(), sizeof(int32_t) * (s->n_nodes + 1));
+  if (col_idx) memcpy(col_idx, s->h_col_idx.data(), sizeof(int32_t) * s->nnzb);
+  return 0;
+}
+
+int wn_solid_get_map(void* h, int32_t* emap) {
+  WN_REQUIRE(h && emap, WN_EINVAL, "wn_solid_get_map: null argument");
+  Solid* s = as_solid(h);
+  WN_CHECK(select_device(s));
+  WN_CUDA(cudaMemcpy(emap, s->emap.p, s->emap.bytes(), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int wn_solid_set_fixed(void* h, const uint8_t* fixed_mask) {
+  WN_REQUIRE(h, WN_EINVAL, "wn_solid_set_fixed: null handle");
+  Solid* s = as_solid(h);
+  WN_CHECK(select_device(s));
+  if (fixed_mask) {
+    for (int64_t i = 0; i < s->n_nodes * 3; ++i) s->h_fixed[i] = fixed_mask[i] ? 1 : 0;
+  } else {
+    std::fill(s->h_fixed.begin(), s->h_fixed.end(), 0);
+  }
+  WN_CUDA(cudaMemcpy(s->fixed.p, s->h_fixed.data(), s->h_fixed.size(), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int wn_assemble_c3d10_device(void* h, const double* d_props, int apply_bcs, uintptr_t stream) {
+  WN_REQUIRE(h && (d_props || as_solid(h)->n_el == 0), WN_EINVAL, "wn_assemble_c3d10: null argument");
+  Solid* s = as_solid(h);
+  WN_CHECK(select_device(s));
+  cudaStream_t st = (cudaStream_t)stream;
+  WN_CHECK(s->props.alloc(s->n_el * 2));
+  if (s->n_el) WN_CUDA(cudaMemcpyAsync(s->props.p, d_props, s->props.bytes(), cudaMemcpyDeviceToDevice, st));
+  WN_CHECK(s->ke.alloc(s->n_el * 55 * 9));
+  WN_CHECK(s->k64.alloc(s->nnzb * 9));
+  WN_CHECK(s->k32.alloc(s->nnzb * 9));
+  WN_CUDA(cudaMemsetAsync(s->flags.p, 0, sizeof(int), st));
+  WN_CHECK(launch_ke_upper(s->n_el, s->nodes.p, s->conn.p, s->props.p, s->ke.p, s->flags.p, st));
+  WN_CHECK(launch_gather_assemble(s->nnzb, s->gptr.p, s->gsrc.p, s->ke.p, s->block_row.p, s->col_idx.p,
+                                  apply_bcs ? s->fixed.p : nullptr, s->k64.p, s->k32.p, st));
+  int flag = 0;
+  WN_CHECK(read_flag(s, st, &flag));
+  WN_REQUIRE(flag == 0, WN_EMESH, "wn_assemble_c3d10: non-positive Jacobian determinant in a C3D10 element");
+  s->assembled = true;
+  s->bcs_applied = apply_bcs != 0;
+  return 0;
+}
+
+int wn_assemble_c3d10(void* h, const double* props, int apply_bcs) {
+  WN_REQUIRE(h && (props || as_solid(h)->n_el == 0), WN_EINVAL, "wn_assemble_c3d10: null argument");
+  Solid* s = as_solid(h);
+  WN_CHECK(select_device(s));
+  DArray<double> d;
+  WN_CHECK(d.upload(props, s->n_el * 2));
+  return wn_assemble_c3d10_device(h, d.p, apply_bcs, 0);
+}
+
+int wn_solid_get_values(void* h, double* values) {
+  WN_REQUIRE(h && values, WN_EINVAL, "wn_solid_get_values: null argument");
+  Solid* s = as_solid(h);
+  WN_REQUIRE(s->assembled, WN_ESTATE, "wn_solid_get_values: not assembled");
+  WN_CHECK(select_device(s));
+  WN_CUDA(cudaMemcpy(values, s->k64.p, s->k64.bytes(), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int wn_solid_device_arrays(void* h, const double** k64, const float** k32, const int32_t** row_ptr,
+                           const int32_t** col_idx, const uint8_t** fixed_mask) {
+  WN_REQUIRE(h, WN_EINVAL, "wn_solid_device_arrays: null handle");
+  Solid* s = as_solid(h);
+  if (k64) *k64 = s->k64.p;
+  if (k32) *k32 = s->k32.p;
+  if (row_ptr) *row_ptr = s->row_ptr.p;
+  if (col_idx) *col_idx = s->col_idx.p;
+  if (fixed_mask) *fixed_mask = s->fixed.p;
+  return 0;
+}
+
+int wn_spmv_solid_device(void* h, int precision, const void* x, void* y, uintptr_t stream) {
+  WN_REQUIRE(h && x && y, WN_EINVAL, "wn_spmv_solid_device: null argument");
+  Solid* s = as_solid(h);
+  WN_REQUIRE(s->assembled, WN_ESTATE, "wn_spmv_solid_device: not assembled");
+  WN_CHECK(select_device(s));
+  if (precision == 0)
+    return launch_bsr_spmv_f64(3, 3, s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, (const double*)x, (double*)y,
+                               1.0, 0.0, (cudaStream_t)stream);
+  if (precision == 1)
+    return launch_bsr_spmv_f32(3, 3, s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k32.p, (const float*)x, (float*)y,
+                               1.0f, 0.0f, (cudaStream_t)stream);
+  set_error("wn_spmv_solid_device: precision must be 0 (FP64) or 1 (FP32)");
+  return WN_EINVAL;
+}
+
+int wn_spmv_bsr_f64_device(int br, int bc, int64_t n_rows, const int32_t* row_ptr, const int32_t* col_idx,
+                           const double* values, const double* x, double* y, double alpha, double beta,
+                           uintptr_t stream) {
+  WN_REQUIRE(n_rows >= 0 && (n_rows == 0 || (row_ptr && col_idx && values && x && y)), WN_EINVAL,
+             "wn_spmv_bsr_f64_device: null argument");
+  return launch_bsr_spmv_f64(br, bc, n_rows, row_ptr, col_idx, values, x, y, alpha, beta, (cudaStream_t)stream);
+}
+
+int wn_spmv_bsr_f32_device(int br, int bc, int64_t n_rows, const int32_t* row_ptr, const int32_t* col_idx,
+                           const float* values, const float* x, float* y, float alpha, float beta, uintptr_t stream) {
+  WN_REQUIRE(n_rows >= 0 && (n_rows == 0 || (row_ptr && col_idx && values && x && y)), WN_EINVAL,
+             "wn_spmv_bsr_f32_device: null argument");
+  return launch_bsr_spmv_f32(br, bc, n_rows, row_ptr, col_idx, values, x, y, alpha, beta, (cudaStream_t)stream);
+}
+
+int wn_spmv_bsr_f64(int br, int bc, int64_t n_rows, int64_t n_cols, int64_t nnzb, const int32_t* row_ptr,
+                    const int32_t* col_idx, const double* values, const double* x, double* y, double alpha,
+                    double beta) {
+  WN_REQUIRE(row_ptr && col_idx && values && x && y, WN_EINVAL, "wn_spmv_bsr_f64: null argument");
+  WN_REQUIRE(n_rows >= 0 && n_cols >= 0 && nnzb >= 0, WN_EINVAL, "wn_spmv_bsr_f64: negative size");
+  WN_REQUIRE(row_ptr[n_rows] == nnzb, WN_EINVAL, "wn_spmv_bsr_f64: row_ptr[n_rows] != nnzb");
+  for (int64_t k = 0; k < nnzb; ++k)
+    WN_REQUIRE(col_idx[k] >= 0 && col_idx[k] < n_cols, WN_EINVAL, "wn_spmv_bsr_f64: column index out of range");
+  DArray<int32_t> rp, ci;
+  DArray<double> v, dx, dy;
+  WN_CHECK(rp.upload(row_ptr, n_rows + 1));
+  WN_CHECK(ci.upload(col_idx, nnzb));
+  WN_CHECK(v.upload(values, nnzb * br * bc));
+  WN_CHECK(dx.upload(x, n_cols * bc));
+  WN_CHECK(dy.upload(y, n_rows * br));
+  WN_CHECK(launch_bsr_spmv_f64(br, bc, n_rows, rp.p, ci.p, v.p, dx.p, dy.p, alpha, beta, 0));
+  WN_CUDA(cudaMemcpy(y, dy.p, dy.bytes(), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int wn_c3d10_element_stiffness(int64_t n_el, const double* coords, const double* props, double* Ke) {
+  WN_REQUIRE(n_el >= 0 && (n_el == 0 || (coords && props && Ke)), WN_EINVAL,
+             "wn_c3d10_element_stiffness: null argument");
+  if (n_el == 0) return 0;
+  // each element gets its own 10 nodes: nodes = coords, conn[e][a] = 10 e + a
+  std::vector<int32_t> conn(n_el * 10);
+  for (int64_t k = 0; k < n_el * 10; ++k) conn[k] = (int32_t)k;
+  DArray<double> dn, dp, dke;
+  DArray<int32_t> dc;
+  DArray<int> flags;
+  WN_CHECK(dn.upload(coords, n_el * 30));
+  WN_CHECK(dp.upload(props, n_el * 2));
+  WN_CHECK(dc.upload(conn));
+  WN_CHECK(dke.alloc(n_el * 55 * 9));
+  WN_CHECK(flags.alloc(1));
+  WN_CHECK(flags.zero());
+  WN_CHECK(launch_ke_upper(n_el, dn.p, dc.p, dp.p, dke.p, flags.p, 0));
+  std::vector<double> up(n_el * 55 * 9);
+  int flag = 0;
+  WN_CUDA(cudaMemcpy(up.data(), dke.p, dke.bytes(), cudaMemcpyDeviceToHost));
+  WN_CUDA(cudaMemcpy(&flag, flags.p, sizeof(int), cudaMemcpyDeviceToHost));
+  WN_REQUIRE(flag == 0, WN_EMESH, "wn_c3d10_element_stiffness: non-positive Jacobian determinant");
+  for (int64_t e = 0; e < n_el; ++e) {
+    double* K = Ke + e * 900;
+    for (int a = 0; a < 10; ++a)
+      for (int b = a; b < 10; ++b) {
+        const double* blk = up.data() + (e * 55 + tri_index(a, b)) * 9;
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) {
+            K[(3 * a + i) * 30 + 3 * b + j] = blk[i * 3 + j];
+            K[(3 * b + j) * 30 + 3 * a + i] = blk[i * 3 + j];
+          }
+      }
+  }
+  return 0;
+}
+
+int wn_c3d10_internal_forces(const double* nodes, const int32_t* solid_elements, const double* props, const double* U,
+                             double* F_int, int n_solids, int n_nodes) {
+  WN_REQUIRE(nodes && U && F_int && n_nodes > 0 && n_solids >= 0, WN_EINVAL,
+             "wn_c3d10_internal_forces: bad argument");
+  if (n_solids == 0) return 0;
+  WN_REQUIRE(solid_elements && props, WN_EINVAL, "wn_c3d10_internal_forces: null argument");
+  Bsr3Pattern pat;
+  // only the node incidence is needed; build it directly
+  std::vector<int64_t> inc_ptr(n_nodes + 1, 0);
+  for (int64_t k = 0; k < (int64_t)n_solids * 10; ++k) {
+    WN_REQUIRE(solid_elements[k] >= 0 && solid_elements[k] < n_nodes, WN_EMESH,
+               "wn_c3d10_internal_forces: node index out of range");
+    inc_ptr[solid_elements[k] + 1]++;
+  }
+  for (int i = 0; i < n_nodes; ++i) inc_ptr[i + 1] += inc_ptr[i];
+  std::vector<int32_t> inc((int64_t)n_solids * 10);
+  {
+    std::vector<int64_t> pos(inc_ptr.begin(), inc_ptr.end() - 1);
+    for (int64_t e = 0; e < n_solids; ++e)
+      for (int a = 0; a < 10; ++a) inc[pos[solid_elements[e * 10 + a]]++] = (int32_t)(e * 10 + a);
+  }
+  DArray<double> dn, dp, du, dfe, df;
+  DArray<int32_t> dc, dinc;
+  DArray<int64_t> dptr;
+  DArray<int> flags;
+  WN_CHECK(dn.upload(nodes, (int64_t)n_nodes * 3));
+  WN_CHECK(dc.upload(solid_elements, (int64_t)n_solids * 10));
+  WN_CHECK(dp.upload(props, (int64_t)n_solids * 2));
+  WN_CHECK(du.upload(U, (int64_t)n_nodes * 6));
+  WN_CHECK(df.upload(F_int, (int64_t)n_nodes * 6));
+  WN_CHECK(dptr.upload(inc_ptr));
+  WN_CHECK(dinc.upload(inc));
+  WN_CHECK(dfe.alloc((int64_t)n_solids * 30));
+  WN_CHECK(flags.alloc(1));
+  WN_CHECK(flags.zero());
+  WN_CHECK(launch_element_force(n_solids, dn.p, dc.p, dp.p, du.p, 6, dfe.p, nullptr, nullptr, flags.p, 0));
+  WN_CHECK(launch_node_gather(n_nodes, dptr.p, dinc.p, dfe.p, 6, 1, df.p, 0));
+  WN_CUDA(cudaMemcpy(F_int, df.p, df.bytes(), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int wn_fint_c3d10_device(void* h, const double* d_u, double* d_fint, uintptr_t stream) {
+  WN_REQUIRE(h && d_u && d_fint, WN_EINVAL, "wn_fint_c3d10_device: null argument");
+  Solid* s = as_solid(h);
+  WN_REQUIRE(s->props.n == s->n_el * 2, WN_ESTATE, "wn_fint_c3d10_device: no material properties (assemble first)");
+  WN_CHECK(select_device(s));
+  cudaStream_t st = (cudaStream_t)stream;
+  WN_CHECK(s->fe.alloc(s->n_el * 30));
+  WN_CHECK(launch_element_force(s->n_el, s->nodes.p, s->conn.p, s->props.p, d_u, 3, s->fe.p, nullptr, nullptr,
+                                s->flags.p, st));
+  WN_CHECK(launch_node_gather(s->n_nodes, s->inc_ptr.p, s->inc_ea.p, s->fe.p, 3, 0, d_fint, st));
+  return 0;
+}
+
+int wn_fint_c3d10(void* h, const double* u, double* fint) {
+  WN_REQUIRE(h && u && fint, WN_EINVAL, "wn_fint_c3d10: null argument");
+  Solid* s = as_solid(h);
+  WN_CHECK(select_device(s));
+  DArray<double> du, df;
+  WN_CHECK(du.upload(u, s->n_nodes * 3));
+  WN_CHECK(df.alloc(s->n_nodes * 3));
+  WN_CHECK(wn_fint_c3d10_device(h, du.p, df.p, 0));
+  WN_CUDA(cudaMemcpy(fint, df.p, df.bytes(), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int wn_stress_c3d10_device(void* h, const double* d_u, double* d_cell_sig, double* d_cell_vm, double* d_nodal_vm,
+                           uintptr_t stream) {
+  WN_REQUIRE(h && d_u && d_cell_sig && d_cell_vm && d_nodal_vm, WN_EINVAL, "wn_stress_c3d10_device: null argument");
+  Solid* s = as_solid(h);
+  WN_REQUIRE(s->props.n == s->n_el * 2, WN_ESTATE, "wn_stress_c3d10_device: no material properties");
+  WN_CHECK(select_device(s));
+  return launch_stress(s->n_el, s->n_nodes, s->nodes.p, s->conn.p, s->props.p, d_u, s->inc_ptr.p, s->inc_ea.p,
+                       d_cell_sig, d_cell_vm, d_nodal_vm, (cudaStream_t)stream);
+}
+
+int wn_stress_c3d10(void* h, const double* u, double* cell_sig, double* cell_vm, double* nodal_vm) {
+  WN_REQUIRE(h && u && cell_sig && cell_vm && nodal_vm, WN_EINVAL, "wn_stress_c3d10: null argument");
+  Solid* s = as_solid(h);
+  WN_CHECK(select_device(s));
+  DArray<double> du, dsig, dvm, dnv;
+  WN_CHECK(du.upload(u, s->n_nodes * 3));
+  WN_CHECK(dsig.alloc(s->n_el * 6));
+  WN_CHECK(dvm.alloc(s->n_el));
+  WN_CHECK(dnv.alloc(s->n_nodes));
+  WN_CHECK(wn_stress_c3d10_device(h, du.p, dsig.p, dvm.p, dnv.p, 0));
+  WN_CUDA(cudaMemcpy(cell_sig, dsig.p, dsig.bytes(), cudaMemcpyDeviceToHost));
+  WN_CUDA(cudaMemcpy(cell_vm, dvm.p, dvm.bytes(), cudaMemcpyDeviceToHost));
+  WN_CUDA(cudaMemcpy(nodal_vm, dnv.p, dnv.bytes(), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int wn_adjoint_compliance_device(void* h, const double* d_u, double* d_grad_E, double* d_grad_F, uintptr_t stream) {
+  WN_REQUIRE(h && d_u, WN_EINVAL, "wn_adjoint_compliance_device: null argument");
+  Solid* s = as_solid(h);
+  WN_REQUIRE(s->props.n == s->n_el * 2, WN_ESTATE, "wn_adjoint_compliance_device: no material properties");
+  WN_CHECK(select_device(s));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (d_grad_E)
+    WN_CHECK(launch_element_force(s->n_el, s->nodes.p, s->conn.p, s->props.p, d_u, 3, nullptr, nullptr, d_grad_E,
+                                  s->flags.p, st));
+  if (d_grad_F) {
+    const int64_t n = s->n_nodes * 3;
+    grad_f_kernel<<<grid_for(n, 1, 256, 8), 256, 0, st>>>(n, d_u, s->bcs_applied ? s->fixed.p : nullptr, d_grad_F);
+    WN_CUDA(cudaGetLastError());
+  }
+  return 0;
+}
+
+int wn_adjoint_compliance(void* h, const double* u, double* grad_E, double* grad_F) {
+  WN_REQUIRE(h && u, WN_EINVAL, "wn_adjoint_compliance: null argument");
+  Solid* s = as_solid(h);
+  WN_CHECK(select_device(s));
+  DArray<double> du, dge, dgf;
+  WN_CHECK(du.upload(u, s->n_nodes * 3));
+  if (grad_E) WN_CHECK(dge.alloc(s->n_el));
+  if (grad_F) WN_CHECK(dgf.alloc(s->n_nodes * 3));
+  WN_CHECK(wn_adjoint_compliance_device(h, du.p, dge.p, dgf.p, 0));
+  if (grad_E) WN_CUDA(cudaMemcpy(grad_E, dge.p, dge.bytes(), cudaMemcpyDeviceToHost));
+  if (grad_F) WN_CUDA(cudaMemcpy(grad_F, dgf.p, dgf.bytes(), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+}  // extern "C"
+
+namespace wn {
+Solid::~Solid() = default;
+}

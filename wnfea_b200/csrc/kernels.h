@@ -1,0 +1,31 @@
+// Host-side launchers of the sm_100a kernels (internal; the public boundary is
+// include/wnfea_cuda.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace wn {
+
+// c3d10.cu
+int launch_ke_upper(int64_t n_el, const double* nodes, const int32_t* conn, const double* props, double* out,
+                    int* flags, cudaStream_t st);
+int launch_gather_assemble(int64_t nnzb, const int32_t* gptr, const int32_t* gsrc, const double* ke,
+                           const int32_t* block_row, const int32_t* col_idx, const uint8_t* fixed, double* k64,
+                           float* k32, cudaStream_t st);
+int launch_element_force(int64_t n_el, const double* nodes, const int32_t* conn, const double* props,
+                         const double* u, int stride, double* fe_out, double* energy_out, double* grad_e,
+                         int* flags, cudaStream_t st);
+int launch_node_gather(int64_t n_nodes, const int64_t* inc_ptr, const int32_t* inc_ea, const double* fe, int stride,
+                       int accumulate, double* out, cudaStream_t st);
+int launch_stress(int64_t n_el, int64_t n_nodes, const double* nodes, const int32_t* conn, const double* props,
+                  const double* u, const int64_t* inc_ptr, const int32_t* inc_ea, double* cell_sig, double* cell_vm,
+                  double* nodal_vm, cudaStream_t st);
+
+// spmv.cu
+int launch_bsr_spmv_f64(int br, int bc, int64_t n_rows, const int32_t* rp, const int32_t* ci, const double* v,
+                        const double* x, double* y, double alpha, double beta, cudaStream_t st);
+int launch_bsr_spmv_f32(int br, int bc, int64_t n_rows, const int32_t* rp, const int32_t* ci, const float* v,
+                        const float* x, float* y, float alpha, float beta, cudaStream_t st);
+
+}  // namespace wn

@@ -1,0 +1,137 @@
+// Host-side construction of the 3x3-block (BSR3) sparsity pattern of a C3D10 mesh, the
+// element -> block map and its inverse (the per-block gather lists used by the atomic-free
+// assembly kernel).
+//
+// The reference assembles scalar COO triplets from a 30-DOF node-major template and lets
+// scipy sum duplicates (wnfea/solver/solid_solver.py:50-84).  Here the node graph is built
+// once: block (i, j) exists iff nodes i and j share an element, columns sorted within each
+// row.  Its 3x3 expansion is exactly the reference CSR pattern before BCs.  The map
+// emap[e][10a+b] gives the block index of (conn[e][a], conn[e][b]); the gather list of a
+// block holds its contributions ordered by (element, a, b), which fixes the summation
+// order of every matrix entry and makes assembly bit-reproducible.
+#include "pattern.h"
+
+#include <algorithm>
+#include <thread>
+#include <vector>
+
+namespace wn {
+
+static void parallel_for(int64_t n, int nthreads, const std::function<void(int64_t, int64_t)>& fn) {
+  if (nthreads <= 1 || n < 4096) {
+    fn(0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  int64_t chunk = (n + nthreads - 1) / nthreads;
+  for (int t = 0; t < nthreads; ++t) {
+    int64_t a = t * chunk, b = std::min(n, a + chunk);
+    if (a >= b) break;
+    th.emplace_back(fn, a, b);
+  }
+  for (auto& x : th) x.join();
+}
+
+int host_threads() {
+  unsigned h = std::thread::hardware_concurrency();
+  if (h == 0) h = 1;
+  if (h > 32) h = 32;
+  return (int)h;
+}
+
+int build_bsr3_pattern(int64_t n_nodes, int64_t n_el, const int32_t* conn, Bsr3Pattern& out) {
+  if (n_nodes <= 0 || n_el < 0) return -1;
+  for (int64_t k = 0; k < n_el * 10; ++k)
+    if (conn[k] < 0 || conn[k] >= n_nodes) return -3;
+  if (n_el * 110 >= (int64_t)INT32_MAX) return -8;
+  const int nth = host_threads();
+
+  // node -> incident (element, local node) pairs e * 10 + a, elements ascending
+  std::vector<int64_t>& inc_ptr = out.inc_ptr;
+  inc_ptr.assign(n_nodes + 1, 0);
+  for (int64_t k = 0; k < n_el * 10; ++k) inc_ptr[conn[k] + 1]++;
+  for (int64_t i = 0; i < n_nodes; ++i) inc_ptr[i + 1] += inc_ptr[i];
+  std::vector<int32_t>& inc = out.inc_ea;
+  inc.resize(n_el * 10);
+  {
+    std::vector<int64_t> pos(inc_ptr.begin(), inc_ptr.end() - 1);
+    for (int64_t e = 0; e < n_el; ++e)
+      for (int a = 0; a < 10; ++a) inc[pos[conn[e * 10 + a]]++] = (int32_t)(e * 10 + a);
+  }
+
+  // row i columns = sorted unique nodes of incident elements
+  std::vector<std::vector<int32_t>> rows(n_nodes);
+  parallel_for(n_nodes, nth, [&](int64_t a, int64_t b) {
+    std::vector<int32_t> buf;
+    for (int64_t i = a; i < b; ++i) {
+      buf.clear();
+      for (int64_t k = inc_ptr[i]; k < inc_ptr[i + 1]; ++k) {
+        const int32_t* c = conn + (int64_t)(inc[k] / 10) * 10;
+        buf.insert(buf.end(), c, c + 10);
+      }
+      if (buf.empty()) buf.push_back((int32_t)i);  // isolated node: keep a diagonal block
+      std::sort(buf.begin(), buf.end());
+      buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
+      rows[i] = buf;
+    }
+  });
+  out.n_nodes = n_nodes;
+  out.row_ptr.assign(n_nodes + 1, 0);
+  for (int64_t i = 0; i < n_nodes; ++i) out.row_ptr[i + 1] = out.row_ptr[i] + (int32_t)rows[i].size();
+  const int64_t nnzb = out.row_ptr[n_nodes];
+  if (nnzb >= (int64_t)INT32_MAX) return -8;
+  out.nnzb = nnzb;
+  out.col_idx.resize(nnzb);
+  out.block_row.resize(nnzb);
+  out.diag_block.resize(n_nodes);
+  parallel_for(n_nodes, nth, [&](int64_t a, int64_t b) {
+    for (int64_t i = a; i < b; ++i) {
+      int32_t p = out.row_ptr[i];
+      for (size_t k = 0; k < rows[i].size(); ++k) {
+        out.col_idx[p + k] = rows[i][k];
+        out.block_row[p + k] = (int32_t)i;
+        if (rows[i][k] == i) out.diag_block[i] = p + (int32_t)k;
+      }
+      std::vector<int32_t>().swap(rows[i]);
+    }
+  });
+
+  // element -> block map by binary search in the sorted row
+  out.emap.resize(n_el * 100);
+  parallel_for(n_el, nth, [&](int64_t a, int64_t b) {
+    for (int64_t e = a; e < b; ++e) {
+      const int32_t* c = conn + e * 10;
+      for (int ia = 0; ia < 10; ++ia) {
+        const int32_t r = c[ia];
+        const int32_t* beg = out.col_idx.data() + out.row_ptr[r];
+        const int32_t* end = out.col_idx.data() + out.row_ptr[r + 1];
+        for (int ib = 0; ib < 10; ++ib) {
+          const int32_t* f = std::lower_bound(beg, end, c[ib]);
+          out.emap[e * 100 + ia * 10 + ib] = (int32_t)(f - out.col_idx.data());
+        }
+      }
+    }
+  });
+
+  // inverse map: per block, contributions in (element, a, b) order.  A contribution names a
+  // stored upper-triangle element block (tri index of (min(a,b), max(a,b))) and whether it
+  // is used transposed (a > b): src = (e * 55 + tri) * 2 + transposed.
+  out.gather_ptr.assign(nnzb + 1, 0);
+  for (int64_t k = 0; k < n_el * 100; ++k) out.gather_ptr[out.emap[k] + 1]++;
+  for (int64_t k = 0; k < nnzb; ++k) out.gather_ptr[k + 1] += out.gather_ptr[k];
+  out.gather_src.resize(n_el * 100);
+  {
+    std::vector<int32_t> pos(out.gather_ptr.begin(), out.gather_ptr.end() - 1);
+    for (int64_t e = 0; e < n_el; ++e)
+      for (int ia = 0; ia < 10; ++ia)
+        for (int ib = 0; ib < 10; ++ib) {
+          const int lo = ia < ib ? ia : ib, hi = ia < ib ? ib : ia;
+          const int tri = tri_index(lo, hi);
+          const int32_t blk = out.emap[e * 100 + ia * 10 + ib];
+          out.gather_src[pos[blk]++] = (int32_t)((e * 55 + tri) * 2 + (ia > ib ? 1 : 0));
+        }
+  }
+  return 0;
+}
+
+}  // namespace wn

@@ -1,0 +1,48 @@
+// The device-resident C3D10 system behind an opaque C-ABI handle: mesh, BSR3 pattern,
+// element -> block map and gather lists, assembled FP64 / FP32 values, Dirichlet mask, the
+// AMG hierarchy and the solver workspace.
+#pragma once
+
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "device_array.h"
+#include "pattern.h"
+
+namespace wn {
+
+struct AmgHierarchy;  // amg.h
+struct SolverWork;    // solver.cu
+
+struct Solid {
+  int device = 0;
+  int64_t n_nodes = 0, n_el = 0, nnzb = 0;
+  // host copies kept for the CSR/BSR export and the AMG setup
+  std::vector<int32_t> h_row_ptr, h_col_idx, h_diag_block;
+  std::vector<double> h_nodes;
+  std::vector<uint8_t> h_fixed;
+  // device mesh
+  DArray<double> nodes;     // n_nodes x 3
+  DArray<int32_t> conn;     // n_el x 10
+  DArray<double> props;     // n_el x 2  [E, nu]
+  // pattern + maps
+  DArray<int32_t> row_ptr, col_idx, block_row, diag_block;
+  DArray<int32_t> emap, gptr, gsrc;
+  DArray<int64_t> inc_ptr;
+  DArray<int32_t> inc_ea;
+  // values
+  DArray<uint8_t> fixed;    // 3 n_nodes (0/1)
+  DArray<double> k64;       // nnzb x 9
+  DArray<float> k32;        // nnzb x 9
+  DArray<double> ke;        // scratch: n_el x 55 x 9 element blocks
+  DArray<double> fe;        // scratch: n_el x 30 element forces
+  DArray<int> flags;        // device status words
+  bool assembled = false;
+  bool bcs_applied = false;
+  std::unique_ptr<AmgHierarchy> amg;
+  std::unique_ptr<SolverWork> work;
+  ~Solid();
+};
+
+}  // namespace wn

@@ -1,0 +1,62 @@
+// Stand-alone BSR SpMV kernels y = alpha * A x + beta * y for the block shapes of the solve
+// path (3x3 solid, 6x6 beam / coarse levels, 3x6 prolongation, 6x3 restriction), FP64
+// values with FP64 accumulation and FP32 values with FP32 accumulation.  One warp per
+// block row, grid sized to whole waves of the 148 SMs (grid-stride over rows).
+#include "common.cuh"
+#include "kernels.h"
+#include "spmv.cuh"
+
+namespace wn {
+
+template <int BR, int BC, typename T>
+__global__ void __launch_bounds__(256) bsr_spmv_kernel(int64_t n_rows, const int32_t* __restrict__ row_ptr,
+                                                       const int32_t* __restrict__ col_idx, const T* __restrict__ vals,
+                                                       const T* __restrict__ x, T* __restrict__ y, T alpha, T beta) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t row = warp; row < n_rows; row += nwarps) {
+    T acc[BR];
+    warp_block_row<BR, BC, T, T>(row_ptr, col_idx, vals, row, XLoad<T, T>{x}, acc, lane);
+    if (lane < BR) {
+      T v = acc[0];
+#pragma unroll
+      for (int r = 1; r < BR; ++r)
+        if (lane == r) v = acc[r];
+      const int64_t o = row * BR + lane;
+      y[o] = (beta == T(0)) ? alpha * v : alpha * v + beta * y[o];
+    }
+  }
+}
+
+template <int BR, int BC, typename T>
+static int launch(int64_t n_rows, const int32_t* rp, const int32_t* ci, const T* v, const T* x, T* y, T a, T b,
+                  cudaStream_t st) {
+  if (n_rows == 0) return 0;
+  const int grid = grid_for(n_rows, 32, 256, 16);
+  bsr_spmv_kernel<BR, BC, T><<<grid, 256, 0, st>>>(n_rows, rp, ci, v, x, y, a, b);
+  WN_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int launch_bsr_spmv_f64(int br, int bc, int64_t n_rows, const int32_t* rp, const int32_t* ci, const double* v,
+                        const double* x, double* y, double alpha, double beta, cudaStream_t st) {
+  if (br == 3 && bc == 3) return launch<3, 3, double>(n_rows, rp, ci, v, x, y, alpha, beta, st);
+  if (br == 6 && bc == 6) return launch<6, 6, double>(n_rows, rp, ci, v, x, y, alpha, beta, st);
+  if (br == 3 && bc == 6) return launch<3, 6, double>(n_rows, rp, ci, v, x, y, alpha, beta, st);
+  if (br == 6 && bc == 3) return launch<6, 3, double>(n_rows, rp, ci, v, x, y, alpha, beta, st);
+  set_error("unsupported block shape %dx%d", br, bc);
+  return WN_EINVAL;
+}
+
+int launch_bsr_spmv_f32(int br, int bc, int64_t n_rows, const int32_t* rp, const int32_t* ci, const float* v,
+                        const float* x, float* y, float alpha, float beta, cudaStream_t st) {
+  if (br == 3 && bc == 3) return launch<3, 3, float>(n_rows, rp, ci, v, x, y, alpha, beta, st);
+  if (br == 6 && bc == 6) return launch<6, 6, float>(n_rows, rp, ci, v, x, y, alpha, beta, st);
+  if (br == 3 && bc == 6) return launch<3, 6, float>(n_rows, rp, ci, v, x, y, alpha, beta, st);
+  if (br == 6 && bc == 3) return launch<6, 3, float>(n_rows, rp, ci, v, x, y, alpha, beta, st);
+  set_error("unsupported block shape %dx%d", br, bc);
+  return WN_EINVAL;
+}
+
+}  // namespace wn

@@ -1,0 +1,162 @@
+"""Device-resident C3D10 system (handle around ``wn_solid_*``) and the BSR3 matrix object.
+
+``SolidSystem`` owns one library handle: the mesh, the 3x3-block pattern, the element ->
+block map, the assembled FP64/FP32 values and the Dirichlet mask, all on the GPU.
+``BSR3Matrix`` is what ``assemble_c3d10_sparse_3dof`` returns in place of the reference's
+scipy CSR (solid_solver.py:26-129): it keeps ``.shape``/``.nnz`` and converts with
+``.tocsr()`` / ``.to_bsr()`` for comparisons with scipy.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib
+from ._lib import call, ptr
+
+
+class SolidSystem:
+    """One C3D10 mesh on the GPU (nodes (N,3) float64, conn (M,10) int)."""
+
+    def __init__(self, nodes: np.ndarray, conn: np.ndarray):
+        self.nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        self.conn = np.ascontiguousarray(conn, dtype=np.int32)
+        if self.nodes.ndim != 2 or self.nodes.shape[1] != 3:
+            raise ValueError("nodes must have shape (N, 3)")
+        if self.conn.ndim != 2 or self.conn.shape[1] != 10:
+            raise ValueError("conn must have shape (M, 10)")
+        h = C.c_void_p()
+        call("wn_solid_create", len(self.nodes), len(self.conn), ptr(self.nodes), ptr(self.conn), C.byref(h))
+        self._h = h
+        n, m, b = C.c_int64(), C.c_int64(), C.c_int64()
+        call("wn_solid_info", self._h, C.byref(n), C.byref(m), C.byref(b))
+        self.n_nodes, self.n_el, self.nnzb = n.value, m.value, b.value
+        self.fixed_mask = np.zeros(3 * self.n_nodes, dtype=np.uint8)
+        self.props: np.ndarray | None = None
+        self.bcs_applied = False
+        self._solver = None
+
+    # -- lifetime -------------------------------------------------------------------------
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            try:
+                if self._solver is not None:
+                    self._solver.close()
+                    self._solver = None
+                _lib.lib().wn_solid_destroy(self._h)
+            finally:
+                self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- pattern ----------------------------------------------------------------------------
+    def pattern(self) -> tuple[np.ndarray, np.ndarray]:
+        rp = np.empty(self.n_nodes + 1, dtype=np.int32)
+        ci = np.empty(self.nnzb, dtype=np.int32)
+        call("wn_solid_get_pattern", self._h, ptr(rp), ptr(ci))
+        return rp, ci
+
+    def element_map(self) -> np.ndarray:
+        m = np.empty((self.n_el, 100), dtype=np.int32)
+        call("wn_solid_get_map", self._h, ptr(m))
+        return m
+
+    # -- assembly ---------------------------------------------------------------------------
+    def set_fixed(self, fixed_dofs) -> None:
+        mask = np.zeros(3 * self.n_nodes, dtype=np.uint8)
+        if fixed_dofs is not None and len(fixed_dofs):
+            mask[np.asarray(fixed_dofs, dtype=np.int64)] = 1
+        self.fixed_mask = mask
+        call("wn_solid_set_fixed", self._h, ptr(mask))
+
+    def assemble(self, props: np.ndarray, apply_bcs: bool = True) -> None:
+        props = np.ascontiguousarray(props, dtype=np.float64)
+        if props.shape != (self.n_el, 2):
+            raise ValueError(f"props must have shape ({self.n_el}, 2)")
+        call("wn_assemble_c3d10", self._h, ptr(props), int(bool(apply_bcs)))
+        self.props = props
+        self.bcs_applied = bool(apply_bcs)
+        if self._solver is not None:
+            self._solver.invalidate()
+
+    def values(self) -> np.ndarray:
+        v = np.empty((self.nnzb, 3, 3), dtype=np.float64)
+        call("wn_solid_get_values", self._h, ptr(v))
+        return v
+
+    # -- element-level operators --------------------------------------------------------------
+    def internal_forces(self, u: np.ndarray) -> np.ndarray:
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        f = np.empty(3 * self.n_nodes)
+        call("wn_fint_c3d10", self._h, ptr(u), ptr(f))
+        return f
+
+    def stress_field(self, u: np.ndarray):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        sig = np.empty((self.n_el, 6))
+        vm = np.empty(self.n_el)
+        nvm = np.empty(self.n_nodes)
+        call("wn_stress_c3d10", self._h, ptr(u), ptr(sig), ptr(vm), ptr(nvm))
+        return sig, vm, nvm
+
+    def compliance_gradient(self, u: np.ndarray):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        gE = np.empty(self.n_el)
+        gF = np.empty(3 * self.n_nodes)
+        call("wn_adjoint_compliance", self._h, ptr(u), ptr(gE), ptr(gF))
+        return gE, gF
+
+
+class BSR3Matrix:
+    """The assembled stiffness matrix, resident on the GPU in 3x3-block BSR form."""
+
+    def __init__(self, system: SolidSystem):
+        self.system = system
+
+    @property
+    def shape(self) -> tuple[int, int]:
+        n = 3 * self.system.n_nodes
+        return (n, n)
+
+    @property
+    def nnz_blocks(self) -> int:
+        return self.system.nnzb
+
+    @property
+    def nnz(self) -> int:
+        """Stored scalar entries (9 per block, Dirichlet zeros included)."""
+        return 9 * self.system.nnzb
+
+    @property
+    def dtype(self):
+        return np.dtype(np.float64)
+
+    def to_bsr(self) -> sp.bsr_matrix:
+        rp, ci = self.system.pattern()
+        return sp.bsr_matrix((self.system.values(), ci, rp), shape=self.shape)
+
+    def tocsr(self) -> sp.csr_matrix:
+        """Scalar CSR; with BCs applied, explicit zeros are dropped as eliminate_zeros does
+        (solid_solver.py:127)."""
+        K = self.to_bsr().tocsr()
+        K.sort_indices()
+        if self.system.bcs_applied:
+            K.eliminate_zeros()
+        return K
+
+    def diagonal(self) -> np.ndarray:
+        return self.tocsr().diagonal()
+
+    def __matmul__(self, x):
+        return self.system.matvec(np.asarray(x, dtype=np.float64))
