@@ -112,6 +112,75 @@ typedef struct wn_amg_params {
 /* Defaults above. */
 int wn_amg_default_params(wn_amg_params* out);
 
+/* Build the hierarchy of the assembled matrix of h (host setup in C++, FP64, then upload of
+ * FP64 and FP32 copies).  params NULL = defaults.  Re-run after every re-assembly. */
+int wn_amg_setup(void* h, const wn_amg_params* params);
+
+/* One V-cycle z = M^-1 r at the finest level (precision 0: double r/z, 1: float r/z).
+ * Device pointers (the preconditioner apply of hip_amg_apply_vcycle_device,
+ * hip_kernels.cpp:2080-2340). */
+int wn_amg_vcycle_device(void* h, int precision, const void* d_r, void* d_z, uintptr_t stream);
+
+/* Hierarchy shape: *n_levels counts the coarsest (dense) level; per level l < n_levels-1:
+ * bs[l] DOFs per node, n_nodes[l], nnzb[l] blocks of A_l (arrays of 16, may be NULL). */
+int wn_amg_info(void* h, int* n_levels, int* bs, int64_t* n_nodes, int64_t* nnzb, int64_t* n_coarse,
+                double* setup_seconds);
+
+/* Host copy of a hierarchy matrix: which = 0 (A_l, l >= 1), 1 (P_l), 2 (R_l = P_l^T).
+ * Call with rp == NULL to get the sizes, then with buffers (rp: n_rows+1, ci: nnzb,
+ * v: nnzb*br*bc). */
+int wn_amg_level_matrix(void* h, int level, int which, int* br, int* bc, int64_t* n_rows, int64_t* n_cols,
+                        int64_t* nnzb, int32_t* rp, int32_t* ci, double* v);
+/* Level data: rho (spectral radius estimate of D^-1 A_l) and 1/diag(A_l) (n_nodes*bs). */
+int wn_amg_level_data(void* h, int level, double* rho, double* dinv);
+/* Coarsest level: dense A_c and A_c^-1 (n_coarse^2 each, row-major, may be NULL). */
+int wn_amg_coarse(void* h, int64_t* n_coarse, double* Ac, double* Ac_inv);
+
+/* Host-only setup (no GPU needed): same algorithm on a caller-supplied BSR3 matrix;
+ * returns a host hierarchy handle usable with the three export calls above. */
+int wn_amg_setup_host(int64_t n_nodes, const int32_t* row_ptr, const int32_t* col_idx, const double* values,
+                      const double* coords, const uint8_t* fixed_mask, const wn_amg_params* params, void** out);
+int wn_amg_host_destroy(void* hier);
+/* Exports of a host-only hierarchy (as wn_amg_level_matrix / _level_data / _coarse);
+ * wn_amg_host_level_data with level == -1 returns the number of levels with a prolongator
+ * in *n_nodes. */
+int wn_amg_host_level_matrix(void* hier, int level, int which, int* br, int* bc, int64_t* n_rows, int64_t* n_cols,
+                             int64_t* nnzb, int32_t* rp, int32_t* ci, double* v);
+int wn_amg_host_level_data(void* hier, int level, double* rho, double* dinv, int64_t* n_nodes, int* bs);
+int wn_amg_host_coarse(void* hier, int64_t* n_coarse, double* Ac, double* Ac_inv);
+
+/* PCG solve of K u = F (solid_solver.py:197-308; GPU-resident like hip_amg_solve_pcg,
+ * hip_kernels.cpp:2384-2517). */
+typedef struct wn_solve_params {
+  double rtol;        /* stop when ||F - K u|| <= rtol ||F||                          */
+  int max_iter;       /* total PCG iterations (inner iterations for mixed)            */
+  int precond;        /* 0 none, 1 point Jacobi (solid_solver.py:228-236), 2 AMG      */
+  int precision;      /* 0 FP64 throughout; 1 FP32 inner PCG + AMG inside FP64
+                         iterative refinement (solid_solver.py:271-300)                */
+  double inner_rtol;  /* mixed: inner relative tolerance (<= 0: max(1e-4, rtol))      */
+  int max_outer;      /* mixed: refinement steps (<= 0: 10)                           */
+  int chunk;          /* iterations per CUDA-graph replay / host convergence check    */
+  int use_graph;      /* 1 = replay captured chunks as a CUDA graph                   */
+} wn_solve_params;
+
+typedef struct wn_solve_stats {
+  int iterations;        /* PCG iterations (sum of inner iterations for mixed)      */
+  int outer_iterations;  /* refinement steps (0 for FP64)                            */
+  int status;            /* 0 converged, WN_ENOCONV, WN_EBREAKDOWN                   */
+  int n_levels;          /* AMG levels including the coarsest (0 without AMG)        */
+  double rel_res;        /* final true ||F - K u|| / ||F|| (FP64 matrix)             */
+  double solve_seconds;  /* device time of the solve (CUDA events)                   */
+  double setup_seconds;  /* wall time of the last AMG setup                          */
+  int64_t kernel_launches; /* kernels issued by the solve (graph replays counted per kernel) */
+} wn_solve_stats;
+
+/* Device pointers F, u (3 n_nodes).  Returns 0 even when not converged: check
+ * stats->status.  Builds the AMG hierarchy with defaults if precond == 2 and none exists. */
+int wn_solve_device(void* h, const double* d_F, double* d_u, const wn_solve_params* params, wn_solve_stats* stats,
+                    uintptr_t stream);
+/* Host buffers F, u (copies in and out). */
+int wn_solve(void* h, const double* F, double* u, const wn_solve_params* params, wn_solve_stats* stats);
+
 /* ---------------------------------------------------------------------------------------
  * Generic block SpMV, y = alpha*A*x + beta*y (cf. hip_spmv_bsr6x6_fp32/_fp64,
  * hip_kernels.cpp:2975-3087, whose CPU reference is bsr6x6_spmv_cpu, bsr_matrix.py:155-193).

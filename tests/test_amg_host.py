@@ -1,0 +1,92 @@
+"""The library's host AMG setup (C++) checked on the CPU against scipy, and the oracle's
+V-cycle/PCG with that hierarchy against the direct solution.  No GPU needed."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+from scipy.sparse.linalg import spsolve
+
+from oracle import amg as oamg
+from oracle import solid
+from wnfea_b200.amg import AMGParams, setup_host
+from wnfea_b200.mesh import generate_c3d10_ibeam_structured, generate_c3d10_kuhn_block
+from wnfea_b200.model import solid_element_props, solid_fixed_dofs, solid_load_vector
+
+
+def _system(which):
+    if which == "c1":
+        m, _ = generate_c3d10_kuhn_block()
+    else:
+        m, _ = generate_c3d10_ibeam_structured(n_slices=12, length=4.0 * 12 / 315, seed=3)
+    K, F, fixed = solid.assemble(m.mesh_nodes, m.solid_elements, solid_element_props(m), solid_load_vector(m),
+                                 solid_fixed_dofs(m), apply_bcs=False)
+    mask = np.zeros(K.shape[0], dtype=np.uint8)
+    mask[fixed] = 1
+    # BCs without eliminate_zeros: keep the 3x3 block pattern
+    n = K.shape[0]
+    row = np.repeat(np.arange(n), np.diff(K.indptr))
+    mr, mc = mask[row].astype(bool), mask[K.indices].astype(bool)
+    K.data[(mr | mc) & (row != K.indices)] = 0.0
+    K.data[mr & (row == K.indices)] = 1.0
+    F[mask.astype(bool)] = 0.0
+    return m, K, F, mask
+
+
+@pytest.fixture(scope="module", params=["c1", "ibeam"])
+def case(request):
+    m, K, F, mask = _system(request.param)
+    H = setup_host(sp.bsr_matrix(K, blocksize=(3, 3)), m.mesh_nodes, mask, AMGParams(coarse_size=300))
+    return m, K, F, mask, H
+
+
+def test_hierarchy_is_galerkin(case):
+    m, K, F, mask, H = case
+    A = K
+    assert len(H.levels) >= 1
+    for lvl, L in enumerate(H.levels):
+        P, R = L.P.tocsr(), L.R.tocsr()
+        assert abs(R - P.T).max() == 0.0  # R = P^T exactly
+        Ac = (R @ A @ P).toarray()
+        nxt = H.levels[lvl + 1].A.toarray() if lvl + 1 < len(H.levels) else H.coarse_A
+        scale = np.abs(Ac).max()
+        np.testing.assert_allclose(nxt, 0.5 * (Ac + Ac.T), rtol=0, atol=1e-12 * scale)
+        np.testing.assert_array_equal(nxt, nxt.T)
+        d = A.diagonal()
+        np.testing.assert_allclose(L.dinv, 1.0 / d, rtol=1e-15)
+        A = sp.csr_matrix(nxt)
+
+
+def test_spectral_radius_estimate(case):
+    m, K, F, mask, H = case
+    from scipy.sparse.linalg import eigsh
+
+    d = K.diagonal()
+    Ds = sp.diags(1 / np.sqrt(d))
+    lam = eigsh(Ds @ K @ Ds, k=1, which="LA", return_eigenvectors=False)[0]
+    rho = H.levels[0].rho
+    assert 0.7 * lam <= rho <= lam * (1 + 1e-9)
+
+
+def test_coarse_inverse(case):
+    *_, H = case
+    np.testing.assert_allclose(H.coarse_inv @ H.coarse_A, np.eye(len(H.coarse_A)), atol=1e-8)
+
+
+def test_oracle_pcg_with_hierarchy_converges(case):
+    m, K, F, mask, H = case
+    u_ref = spsolve(K.tocsc(), F)
+    x, its = oamg.pcg(K, F, lambda r: oamg.vcycle(K, H, r), rtol=1e-10, max_iter=300)
+    assert its < 80, its
+    assert np.linalg.norm(x - u_ref) / np.linalg.norm(u_ref) < 1e-8
+
+
+def test_setup_is_deterministic():
+    m, K, F, mask = _system("c1")
+    Kb = sp.bsr_matrix(K, blocksize=(3, 3))
+    H1 = setup_host(Kb, m.mesh_nodes, mask, AMGParams(coarse_size=300))
+    H2 = setup_host(Kb, m.mesh_nodes, mask, AMGParams(coarse_size=300))
+    for a, b in zip(H1.levels, H2.levels):
+        assert np.array_equal(a.P.data, b.P.data) and a.rho == b.rho
+    assert np.array_equal(H1.coarse_inv, H2.coarse_inv)

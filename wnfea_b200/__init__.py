@@ -17,13 +17,17 @@ from .model import (
     create_fixed_support,
     create_rectangular_bar,
 )
+from .mixed_precision import FULL_FP64, MIXED_FP32, TRI_PRECISION, PrecisionConfig
 from .solid_solver import (
     assemble_c3d10_sparse_3dof,
     compute_c3d10_stress_field,
+    solve_c3d10_pcg,
+    solve_c3d10_system,
 )
 
 __all__ = [
     "FEAModel", "MaterialDef", "SectionDef", "PropertyAssignment",
     "SupportDef", "LoadDef", "DOFConstraint", "DOFType", "create_fixed_support", "create_rectangular_bar",
-    "assemble_c3d10_sparse_3dof", "compute_c3d10_stress_field",
+    "assemble_c3d10_sparse_3dof", "compute_c3d10_stress_field", "solve_c3d10_pcg", "solve_c3d10_system",
+    "PrecisionConfig", "MIXED_FP32", "FULL_FP64", "TRI_PRECISION",
 ]

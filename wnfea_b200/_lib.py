@@ -21,6 +21,56 @@ _D = C.c_double
 _F = C.c_float
 _U = C.c_uint64  # uintptr_t stream
 
+class AmgParams(C.Structure):
+    """wn_amg_params"""
+
+    _fields_ = [
+        ("strength_theta", C.c_double),
+        ("max_levels", C.c_int),
+        ("coarse_size", C.c_int),
+        ("smoother_degree", C.c_int),
+        ("cheb_lower", C.c_double),
+        ("cheb_safety", C.c_double),
+        ("prolong_omega", C.c_double),
+        ("smooth_prolongator", C.c_int),
+        ("power_iters", C.c_int),
+    ]
+
+
+class SolveParams(C.Structure):
+    """wn_solve_params"""
+
+    _fields_ = [
+        ("rtol", C.c_double),
+        ("max_iter", C.c_int),
+        ("precond", C.c_int),
+        ("precision", C.c_int),
+        ("inner_rtol", C.c_double),
+        ("max_outer", C.c_int),
+        ("chunk", C.c_int),
+        ("use_graph", C.c_int),
+    ]
+
+
+class SolveStats(C.Structure):
+    """wn_solve_stats"""
+
+    _fields_ = [
+        ("iterations", C.c_int),
+        ("outer_iterations", C.c_int),
+        ("status", C.c_int),
+        ("n_levels", C.c_int),
+        ("rel_res", C.c_double),
+        ("solve_seconds", C.c_double),
+        ("setup_seconds", C.c_double),
+        ("kernel_launches", C.c_int64),
+    ]
+
+
+_PI = C.POINTER(C.c_int)
+_PI64 = C.POINTER(C.c_int64)
+_PD = C.POINTER(C.c_double)
+
 # name -> (restype, argtypes); must match include/wnfea_cuda.h
 SIGNATURES: dict[str, tuple] = {
     "wn_last_error_string": (C.c_char_p, []),
@@ -49,6 +99,20 @@ SIGNATURES: dict[str, tuple] = {
     "wn_stress_c3d10_device": (_I, [_P, _P, _P, _P, _P, _U]),
     "wn_adjoint_compliance_device": (_I, [_P, _P, _P, _P, _U]),
     "wn_adjoint_compliance": (_I, [_P, _P, _P, _P]),
+    "wn_amg_default_params": (_I, [C.POINTER(AmgParams)]),
+    "wn_amg_setup": (_I, [_P, C.POINTER(AmgParams)]),
+    "wn_amg_vcycle_device": (_I, [_P, _I, _P, _P, _U]),
+    "wn_amg_info": (_I, [_P, _PI, _PI, _PI64, _PI64, _PI64, _PD]),
+    "wn_amg_level_matrix": (_I, [_P, _I, _I, _PI, _PI, _PI64, _PI64, _PI64, _P, _P, _P]),
+    "wn_amg_level_data": (_I, [_P, _I, _PD, _P]),
+    "wn_amg_coarse": (_I, [_P, _PI64, _P, _P]),
+    "wn_amg_setup_host": (_I, [_I64, _P, _P, _P, _P, _P, C.POINTER(AmgParams), C.POINTER(_P)]),
+    "wn_amg_host_destroy": (_I, [_P]),
+    "wn_amg_host_level_matrix": (_I, [_P, _I, _I, _PI, _PI, _PI64, _PI64, _PI64, _P, _P, _P]),
+    "wn_amg_host_level_data": (_I, [_P, _I, _PD, _P, _PI64, _PI]),
+    "wn_amg_host_coarse": (_I, [_P, _PI64, _P, _P]),
+    "wn_solve_device": (_I, [_P, _P, _P, C.POINTER(SolveParams), C.POINTER(SolveStats), _U]),
+    "wn_solve": (_I, [_P, _P, _P, C.POINTER(SolveParams), C.POINTER(SolveStats)]),
 }
 
 LIB_PATH = Path(__file__).resolve().parent / "libwnfea_cuda.so"

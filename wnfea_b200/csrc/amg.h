@@ -77,7 +77,7 @@ struct PcgScalars {
   int done;
   int iters;
   int status;
-  int pad;
+  int max_iter;
 };
 
 template <typename T>
@@ -98,6 +98,7 @@ struct GraphCache {
   cudaGraphExec_t exec = nullptr;
   cudaStream_t stream = nullptr;
   int64_t key = -1;
+  int64_t kernels = 0;  // kernels per replay
   ~GraphCache() {
     if (exec) cudaGraphExecDestroy(exec);
   }
@@ -113,18 +114,23 @@ struct SolverWork {
   static constexpr int kParts = 148 * 4;  // CTAs of every partial-producing kernel
   DArray<double> partA, partB, partC;
   DArray<PcgScalars> scal;   // [0] = FP64 / inner solve, [1] = outer refinement
-  DArray<double> u64, r64, Fd;  // outer refinement (mixed) vectors
+  DArray<double> u64, r64;  // outer refinement vectors
+  DArray<float> r32;
   DArray<double> dinv64;      // Jacobi (point) of the fine matrix
   DArray<float> dinv32;
   PcgVecs<double> p64;
   PcgVecs<float> p32;
-  // graphs: [precision][kind] kind 0 = init, 1 = chunk of iterations
-  GraphCache graphs[2][2];
+  // captured chunk graphs: [mode 0 fp64 / 1 mixed / 2 fp32][preconditioner 0 none / 1 jacobi / 2 amg]
+  GraphCache graphs[3][3];
   int64_t launches = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaStream_t own = nullptr;  // used when the caller passes the legacy default stream
   ~SolverWork() {
+    for (auto& a : graphs)
+      for (auto& g : a) g.reset();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (own) cudaStreamDestroy(own);
   }
 };
 

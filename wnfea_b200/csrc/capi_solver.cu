@@ -1,0 +1,186 @@
+// extern "C" boundary of the AMG setup and the PCG / mixed-precision solver.
+#include <cstring>
+
+#include "amg.h"
+#include "common.cuh"
+#include "solid.h"
+#include "solver.h"
+#include "wnfea_cuda.h"
+
+using namespace wn;
+
+namespace {
+
+struct HostAmgHandle {
+  HostHierarchy h;
+};
+
+// a hierarchy handle may be a Solid (device + host copy) or a host-only handle; the caller
+// says which by the entry point used.  Solid handles carry the hierarchy in s->amg->host.
+HostHierarchy* host_of_solid(void* h) {
+  Solid* s = reinterpret_cast<Solid*>(h);
+  return s->amg ? &s->amg->host : nullptr;
+}
+
+int export_matrix(HostHierarchy* H, int level, int which, int* br, int* bc, int64_t* n_rows, int64_t* n_cols,
+                  int64_t* nnzb, int32_t* rp, int32_t* ci, double* v) {
+  WN_REQUIRE(H, WN_ESTATE, "wn_amg_level_matrix: no hierarchy");
+  WN_REQUIRE(level >= 0 && level < (int)H->levels.size(), WN_EINVAL, "wn_amg_level_matrix: level out of range");
+  WN_REQUIRE(which >= 0 && which <= 2, WN_EINVAL, "wn_amg_level_matrix: which in {0,1,2}");
+  WN_REQUIRE(!(which == 0 && level == 0), WN_EINVAL, "wn_amg_level_matrix: A_0 is the assembled matrix");
+  const HostLevel& L = H->levels[level];
+  const HostBsr& M = which == 0 ? L.A : (which == 1 ? L.P : L.R);
+  if (br) *br = M.br;
+  if (bc) *bc = M.bc;
+  if (n_rows) *n_rows = M.n_rows;
+  if (n_cols) *n_cols = M.n_cols;
+  if (nnzb) *nnzb = M.nnzb();
+  if (rp) memcpy(rp, M.rp.data(), sizeof(int32_t) * M.rp.size());
+  if (ci) memcpy(ci, M.ci.data(), sizeof(int32_t) * M.ci.size());
+  if (v) memcpy(v, M.v.data(), sizeof(double) * M.v.size());
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wn_amg_default_params(wn_amg_params* out) {
+  WN_REQUIRE(out, WN_EINVAL, "wn_amg_default_params: null argument");
+  *out = amg_default_params();
+  return 0;
+}
+
+int wn_amg_setup(void* h, const wn_amg_params* params) {
+  WN_REQUIRE(h, WN_EINVAL, "wn_amg_setup: null handle");
+  Solid* s = reinterpret_cast<Solid*>(h);
+  WN_CUDA(cudaSetDevice(s->device));
+  return solver_setup(s, params ? *params : amg_default_params());
+}
+
+int wn_amg_vcycle_device(void* h, int precision, const void* d_r, void* d_z, uintptr_t stream) {
+  WN_REQUIRE(h && d_r && d_z && (precision == 0 || precision == 1), WN_EINVAL, "wn_amg_vcycle_device: bad argument");
+  Solid* s = reinterpret_cast<Solid*>(h);
+  WN_CUDA(cudaSetDevice(s->device));
+  return amg_vcycle(s, precision, d_r, d_z, (cudaStream_t)stream);
+}
+
+int wn_amg_info(void* h, int* n_levels, int* bs, int64_t* n_nodes, int64_t* nnzb, int64_t* n_coarse,
+                double* setup_seconds) {
+  WN_REQUIRE(h, WN_EINVAL, "wn_amg_info: null handle");
+  Solid* s = reinterpret_cast<Solid*>(h);
+  WN_REQUIRE(s->amg, WN_ESTATE, "wn_amg_info: no hierarchy");
+  const HostHierarchy& H = s->amg->host;
+  const int L = (int)H.levels.size();
+  if (n_levels) *n_levels = L + 1;
+  for (int l = 0; l < L && l < 16; ++l) {
+    if (bs) bs[l] = H.levels[l].bs;
+    if (n_nodes) n_nodes[l] = H.levels[l].n_nodes;
+    if (nnzb) nnzb[l] = l == 0 ? s->nnzb : H.levels[l].A.nnzb();
+  }
+  if (n_coarse) *n_coarse = H.n_coarse;
+  if (setup_seconds) *setup_seconds = s->amg->setup_seconds;
+  return 0;
+}
+
+int wn_amg_level_matrix(void* h, int level, int which, int* br, int* bc, int64_t* n_rows, int64_t* n_cols,
+                        int64_t* nnzb, int32_t* rp, int32_t* ci, double* v) {
+  WN_REQUIRE(h, WN_EINVAL, "wn_amg_level_matrix: null handle");
+  HostHierarchy* H = reinterpret_cast<Solid*>(h)->amg ? host_of_solid(h) : nullptr;
+  return export_matrix(H, level, which, br, bc, n_rows, n_cols, nnzb, rp, ci, v);
+}
+
+int wn_amg_level_data(void* h, int level, double* rho, double* dinv) {
+  WN_REQUIRE(h, WN_EINVAL, "wn_amg_level_data: null handle");
+  HostHierarchy* H = host_of_solid(h);
+  WN_REQUIRE(H && level >= 0 && level < (int)H->levels.size(), WN_EINVAL, "wn_amg_level_data: bad level");
+  const HostLevel& L = H->levels[level];
+  if (rho) *rho = L.rho;
+  if (dinv) memcpy(dinv, L.dinv.data(), sizeof(double) * L.dinv.size());
+  return 0;
+}
+
+int wn_amg_coarse(void* h, int64_t* n_coarse, double* Ac, double* Ac_inv) {
+  WN_REQUIRE(h, WN_EINVAL, "wn_amg_coarse: null handle");
+  HostHierarchy* H = host_of_solid(h);
+  WN_REQUIRE(H, WN_ESTATE, "wn_amg_coarse: no hierarchy");
+  if (n_coarse) *n_coarse = H->n_coarse;
+  if (Ac) memcpy(Ac, H->coarse_A.data(), sizeof(double) * H->coarse_A.size());
+  if (Ac_inv) memcpy(Ac_inv, H->coarse_inv.data(), sizeof(double) * H->coarse_inv.size());
+  return 0;
+}
+
+int wn_amg_setup_host(int64_t n_nodes, const int32_t* row_ptr, const int32_t* col_idx, const double* values,
+                      const double* coords, const uint8_t* fixed_mask, const wn_amg_params* params, void** out) {
+  WN_REQUIRE(out && row_ptr && col_idx && values && coords && n_nodes > 0, WN_EINVAL,
+             "wn_amg_setup_host: bad argument");
+  auto* hh = new HostAmgHandle();
+  int rc = amg_build(params ? *params : amg_default_params(), n_nodes, row_ptr, col_idx, values, coords, fixed_mask,
+                     hh->h);
+  if (rc != 0) {
+    delete hh;
+    return rc;
+  }
+  *out = hh;
+  return 0;
+}
+
+int wn_amg_host_destroy(void* hier) {
+  delete reinterpret_cast<HostAmgHandle*>(hier);
+  return 0;
+}
+
+int wn_amg_host_level_matrix(void* hier, int level, int which, int* br, int* bc, int64_t* n_rows, int64_t* n_cols,
+                             int64_t* nnzb, int32_t* rp, int32_t* ci, double* v) {
+  WN_REQUIRE(hier, WN_EINVAL, "wn_amg_host_level_matrix: null handle");
+  return export_matrix(&reinterpret_cast<HostAmgHandle*>(hier)->h, level, which, br, bc, n_rows, n_cols, nnzb, rp,
+                       ci, v);
+}
+
+int wn_amg_host_level_data(void* hier, int level, double* rho, double* dinv, int64_t* n_nodes, int* bs) {
+  WN_REQUIRE(hier, WN_EINVAL, "wn_amg_host_level_data: null handle");
+  HostHierarchy& H = reinterpret_cast<HostAmgHandle*>(hier)->h;
+  if (level == -1) {  // number of levels with P (coarsest excluded)
+    if (n_nodes) *n_nodes = (int64_t)H.levels.size();
+    return 0;
+  }
+  WN_REQUIRE(level >= 0 && level < (int)H.levels.size(), WN_EINVAL, "wn_amg_host_level_data: bad level");
+  const HostLevel& L = H.levels[level];
+  if (rho) *rho = L.rho;
+  if (dinv) memcpy(dinv, L.dinv.data(), sizeof(double) * L.dinv.size());
+  if (n_nodes) *n_nodes = L.n_nodes;
+  if (bs) *bs = L.bs;
+  return 0;
+}
+
+int wn_amg_host_coarse(void* hier, int64_t* n_coarse, double* Ac, double* Ac_inv) {
+  WN_REQUIRE(hier, WN_EINVAL, "wn_amg_host_coarse: null handle");
+  HostHierarchy& H = reinterpret_cast<HostAmgHandle*>(hier)->h;
+  if (n_coarse) *n_coarse = H.n_coarse;
+  if (Ac) memcpy(Ac, H.coarse_A.data(), sizeof(double) * H.coarse_A.size());
+  if (Ac_inv) memcpy(Ac_inv, H.coarse_inv.data(), sizeof(double) * H.coarse_inv.size());
+  return 0;
+}
+
+int wn_solve_device(void* h, const double* d_F, double* d_u, const wn_solve_params* params, wn_solve_stats* stats,
+                    uintptr_t stream) {
+  WN_REQUIRE(h && d_F && d_u && params, WN_EINVAL, "wn_solve_device: null argument");
+  Solid* s = reinterpret_cast<Solid*>(h);
+  WN_CUDA(cudaSetDevice(s->device));
+  return solver_solve(s, d_F, d_u, *params, stats, (cudaStream_t)stream);
+}
+
+int wn_solve(void* h, const double* F, double* u, const wn_solve_params* params, wn_solve_stats* stats) {
+  WN_REQUIRE(h && F && u && params, WN_EINVAL, "wn_solve: null argument");
+  Solid* s = reinterpret_cast<Solid*>(h);
+  WN_CUDA(cudaSetDevice(s->device));
+  const int64_t n = s->n_nodes * 3;
+  DArray<double> dF, du;
+  WN_CHECK(dF.upload(F, n));
+  WN_CHECK(du.alloc(n));
+  WN_CHECK(solver_solve(s, dF.p, du.p, *params, stats, 0));
+  WN_CUDA(cudaMemcpy(u, du.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+}  // extern "C"

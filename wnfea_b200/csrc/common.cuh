@@ -48,6 +48,7 @@ namespace wn {
 constexpr int kWarp = 32;
 constexpr int kNumSMs = 148;  // B200; grids are sized in multiples of this
 
+#if defined(__CUDACC__)
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -75,6 +76,8 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   __syncthreads();
   return r;
 }
+
+#endif  // __CUDACC__
 
 inline int grid_for(int64_t work_items, int threads_per_item_group, int block, int max_waves = 16) {
   int64_t blocks = (work_items * threads_per_item_group + block - 1) / block;

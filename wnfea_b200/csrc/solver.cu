@@ -18,6 +18,7 @@
 //   * mixed precision: FP32 matrix / V-cycle / vectors with FP32 accumulation inside an
 //     FP64 refinement loop whose residual r = F - K u uses the FP64 matrix.
 #include <chrono>
+#include <type_traits>
 #include <cmath>
 #include <cstring>
 
@@ -233,22 +234,25 @@ __global__ void __launch_bounds__(kThreads) k_coarse(int64_t n, const double* __
 // PCG kernels
 // ---------------------------------------------------------------------------------------
 
-// r = b, x = 0, partC = b . b ; (+ zero-RHS handling in k_init_scalars)
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_init_vecs(int64_t n, const T* __restrict__ b, T* __restrict__ x,
-                                                        T* __restrict__ r, double* __restrict__ partC) {
+// r = b, x = 0, rm = (TM) b (if rm != null), partC = b . b (zero-RHS handling in k_init_scalars)
+template <typename TK, typename TM>
+__global__ void __launch_bounds__(kThreads) k_init_vecs(int64_t n, const TK* __restrict__ b, TK* __restrict__ x,
+                                                        TK* __restrict__ r, TM* __restrict__ rm,
+                                                        double* __restrict__ partC) {
   __shared__ double sh[kThreads / 32];
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const T v = b[i];
+    const TK v = b[i];
     r[i] = v;
-    x[i] = T(0);
+    x[i] = TK(0);
+    if (rm) rm[i] = (TM)v;
     s += (double)v * (double)v;
   }
   write_part(s, partC, sh);
 }
 
-__global__ void k_init_scalars(PcgScalars* S, const double* __restrict__ partC, int nparts, double rtol) {
+__global__ void k_init_scalars(PcgScalars* S, const double* __restrict__ partC, int nparts, double rtol,
+                               int max_iter) {
   __shared__ double sh[kThreads / 32];
   const double bb = reduce_parts(partC, nparts, sh);
   if (threadIdx.x == 0) {
@@ -259,6 +263,7 @@ __global__ void k_init_scalars(PcgScalars* S, const double* __restrict__ partC, 
     S->alpha = 0.0;
     S->iters = 0;
     S->status = 0;
+    S->max_iter = max_iter;
     S->done = (bb == 0.0 || !isfinite(bb)) ? 1 : 0;
     if (!isfinite(bb)) S->status = WN_EBREAKDOWN;
   }
@@ -281,28 +286,37 @@ __global__ void __launch_bounds__(kThreads) k_prec_vec(int64_t n, const T* __res
   write_part(s, partA, sh);
 }
 
+template <typename TK, typename TM>
+struct XPNew2 {  // p_j = z_j + beta p_old_j, z in the preconditioner's precision
+  const TM* __restrict__ z;
+  const TK* __restrict__ p;
+  TK beta;
+  __device__ __forceinline__ TK operator()(int64_t j) const { return (TK)z[j] + beta * p[j]; }
+};
+
 // iteration k: rz = sum(partA); beta = rz / rz_prev (0 at k = 0); p_new = z + beta p_old;
 // q = A p_new; partB = p_new . q.  Parity par = k & 1 selects the p buffers and rz slot.
-template <int BS, typename T>
+// TK: Krylov vectors / matrix precision; TM: preconditioner output precision.
+template <int BS, typename TK, typename TM>
 __global__ void __launch_bounds__(kThreads) k_spmv_dot(int64_t n_rows, const int32_t* __restrict__ rp,
-                                                       const int32_t* __restrict__ ci, const T* __restrict__ av,
-                                                       const T* __restrict__ z, const T* __restrict__ p_old,
-                                                       T* __restrict__ p_new, T* __restrict__ q,
+                                                       const int32_t* __restrict__ ci, const TK* __restrict__ av,
+                                                       const TM* __restrict__ z, const TK* __restrict__ p_old,
+                                                       TK* __restrict__ p_new, TK* __restrict__ q,
                                                        const double* __restrict__ partA, double* __restrict__ partB,
                                                        int nparts, int first, int par, PcgScalars* __restrict__ S) {
   __shared__ double sh[kThreads / 32];
   if (S->done) return;
   const double rz = reduce_parts(partA, nparts, sh);
   const double rz_prev = S->rz[par ^ 1];
-  const T beta = first ? T(0) : (T)(rz / rz_prev);
+  const TK beta = first ? TK(0) : (TK)(rz / rz_prev);
   double dot = 0.0;
   WARP_ROW_LOOP(n_rows) {
-    T acc[BS];
-    warp_block_row<BS, BS, T, T>(rp, ci, av, row, XPNew<T>{z, p_old, beta}, acc, lane);
+    TK acc[BS];
+    warp_block_row<BS, BS, TK, TK>(rp, ci, av, row, XPNew2<TK, TM>{z, p_old, beta}, acc, lane);
     if (lane < BS) {
       const int64_t i = row * BS + lane;
-      const T pi = z[i] + beta * p_old[i];
-      const T qi = pick<BS>(acc, lane);
+      const TK pi = (TK)z[i] + beta * p_old[i];
+      const TK qi = pick<BS>(acc, lane);
       p_new[i] = pi;
       q[i] = qi;
       dot += (double)pi * (double)qi;
@@ -312,12 +326,13 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dot(int64_t n_rows, const int
   if (blockIdx.x == 0 && threadIdx.x == 0) S->rz[par] = rz;
 }
 
-// alpha = rz / (p . q); x += alpha p; r -= alpha q; partC = r . r
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_update(int64_t n, T* __restrict__ x, T* __restrict__ r,
-                                                     const T* __restrict__ p, const T* __restrict__ q,
-                                                     const double* __restrict__ partB, double* __restrict__ partC,
-                                                     int nparts, int par, PcgScalars* __restrict__ S) {
+// alpha = rz / (p . q); x += alpha p; r -= alpha q; rm = (TM) r (if rm != null); partC = r . r
+template <typename TK, typename TM>
+__global__ void __launch_bounds__(kThreads) k_update(int64_t n, TK* __restrict__ x, TK* __restrict__ r,
+                                                     TM* __restrict__ rm, const TK* __restrict__ p,
+                                                     const TK* __restrict__ q, const double* __restrict__ partB,
+                                                     double* __restrict__ partC, int nparts, int par,
+                                                     PcgScalars* __restrict__ S) {
   __shared__ double sh[kThreads / 32];
   if (S->done) return;
   const double gamma = reduce_parts(partB, nparts, sh);
@@ -329,36 +344,56 @@ __global__ void __launch_bounds__(kThreads) k_update(int64_t n, T* __restrict__ 
     }
     return;
   }
-  const T a = (T)alpha;
+  const TK a = (TK)alpha;
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     x[i] += a * p[i];
-    const T ri = r[i] - a * q[i];
+    const TK ri = r[i] - a * q[i];
     r[i] = ri;
+    if (rm) rm[i] = (TM)ri;
     s += (double)ri * (double)ri;
   }
   write_part(s, partC, sh);
   if (blockIdx.x == 0 && threadIdx.x == 0) S->alpha = alpha;
 }
 
-// convergence test after iteration k (one CTA)
-__global__ void k_check(PcgScalars* S, const double* __restrict__ partC, int nparts, int k, int max_iter) {
+// convergence test after an iteration (one CTA); the iteration count lives on the device so
+// that a captured chunk of iterations can be replayed any number of times
+__global__ void k_check(PcgScalars* S, const double* __restrict__ partC, int nparts) {
   __shared__ double sh[kThreads / 32];
   if (S->done) return;
   const double rr = reduce_parts(partC, nparts, sh);
   if (threadIdx.x == 0) {
+    const int it = S->iters + 1;
     S->rr = rr;
-    S->iters = k + 1;
+    S->iters = it;
     if (!isfinite(rr)) {
       S->status = WN_EBREAKDOWN;
       S->done = 1;
     } else if (rr <= S->tol2) {
       S->done = 1;
-    } else if (k + 1 >= max_iter) {
+    } else if (it >= S->max_iter) {
       S->status = WN_ENOCONV;
       S->done = 1;
     }
   }
+}
+
+// S->rr = sum(partC) (one CTA)
+__global__ void k_reduce_rr(PcgScalars* S, const double* __restrict__ partC, int nparts) {
+  __shared__ double sh[kThreads / 32];
+  const double rr = reduce_parts(partC, nparts, sh);
+  if (threadIdx.x == 0) S->rr = rr;
+}
+
+// partials of x . x
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_dot_self(int64_t n, const T* __restrict__ x, double* __restrict__ part) {
+  __shared__ double sh[kThreads / 32];
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    s += (double)x[i] * (double)x[i];
+  write_part(s, part, sh);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -387,8 +422,9 @@ __global__ void __launch_bounds__(kThreads) k_outer_residual(int64_t n_rows, con
   write_part(s, partC, sh);
 }
 
-// u64 += (double) dx32
-__global__ void k_accumulate(int64_t n, double* __restrict__ u, const float* __restrict__ dx) {
+// u64 += (double) dx
+template <typename T>
+__global__ void k_accumulate(int64_t n, double* __restrict__ u, const T* __restrict__ dx) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     u[i] += (double)dx[i];
 }
@@ -499,7 +535,6 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
     DevLevel* Ln = lvl + 1 < nlev ? &H.levels[lvl + 1] : nullptr;
     T* bc = Ln ? Prec<T>::vecs(*Ln).b.p : Prec<T>::cb(H);
     T* xc = Ln ? Prec<T>::vecs(*Ln).x2.p : Prec<T>::cx(H);
-    if (deg == 0) xc = Ln ? Prec<T>::vecs(*Ln).x.p : xc;
     k_level_spmv<6, BS, T><<<rows_grid(L.R.n_rows), kThreads, 0, st>>>(L.R.n_rows, L.R.rp.p, L.R.ci.p,
                                                                         Prec<T>::Rv(L), V.res.p, bc, 0, S);
     W.launches++;
@@ -544,44 +579,74 @@ static int apply_prec(Solid* s, SolverWork& W, int precond, const T* r, T* z, co
   return 0;
 }
 
-// one PCG iteration k (parity k & 1)
-template <typename T>
-static int pcg_iteration(Solid* s, SolverWork& W, int precond, int k, int max_iter, PcgScalars* S, cudaStream_t st) {
-  PcgVecs<T>& P = Prec<T>::pcg(W);
-  const int par = k & 1;
-  T* p_new = par ? P.p1.p : P.p0.p;
-  T* p_old = par ? P.p0.p : P.p1.p;
-  const int32_t* rp = s->row_ptr.p;
-  const int32_t* ci = s->col_idx.p;
-  const T* av = Prec<T>::A0(s);
-  k_spmv_dot<3, T><<<SolverWork::kParts, kThreads, 0, st>>>(s->n_nodes, rp, ci, av, P.z.p, p_old, p_new, P.q.p,
-                                                            W.partA.p, W.partB.p, SolverWork::kParts, k == 0, par, S);
-  k_update<T><<<SolverWork::kParts, kThreads, 0, st>>>(W.n, P.x.p, P.r.p, p_new, P.q.p, W.partB.p, W.partC.p,
-                                                       SolverWork::kParts, par, S);
-  k_check<<<1, kThreads, 0, st>>>(S, W.partC.p, SolverWork::kParts, k, max_iter);
-  W.launches += 3;
-  WN_CUDA(cudaGetLastError());
-  return apply_prec<T>(s, W, precond, P.r.p, P.z.p, S, st);
+// PCG buffers of one precision pairing: Krylov vectors / matrix in TK, preconditioner in TM
+template <typename TK, typename TM>
+struct PcgBufs {
+  TK *x, *r, *p0, *p1, *q;
+  TM *z, *rm;  // rm: r in TM for the preconditioner (nullptr when TK == TM: r is used)
+  const TK* A;
+};
+
+template <typename TK, typename TM>
+static PcgBufs<TK, TM> pcg_bufs(Solid* s, SolverWork& W);
+template <>
+PcgBufs<double, double> pcg_bufs(Solid* s, SolverWork& W) {
+  return {W.p64.x.p, W.p64.r.p, W.p64.p0.p, W.p64.p1.p, W.p64.q.p, W.p64.z.p, nullptr, s->k64.p};
+}
+template <>
+PcgBufs<double, float> pcg_bufs(Solid* s, SolverWork& W) {
+  return {W.p64.x.p, W.p64.r.p, W.p64.p0.p, W.p64.p1.p, W.p64.q.p, W.p32.z.p, W.p32.r.p, s->k64.p};
+}
+template <>
+PcgBufs<float, float> pcg_bufs(Solid* s, SolverWork& W) {
+  return {W.p32.x.p, W.p32.r.p, W.p32.p0.p, W.p32.p1.p, W.p32.q.p, W.p32.z.p, nullptr, s->k32.p};
 }
 
-// PCG on the fine matrix in precision T: solves A x = b (b, x are the PcgVecs' r/x after
-// init).  Iterations are replayed through a CUDA graph of `chunk` iterations.
-template <typename T>
-static int pcg_solve(Solid* s, SolverWork& W, int pi, const T* b, double rtol, int max_iter, int precond, int chunk,
-                     int use_graph, PcgScalars* S, cudaStream_t st, PcgScalars* hS) {
-  PcgVecs<T>& P = Prec<T>::pcg(W);
-  k_init_vecs<T><<<SolverWork::kParts, kThreads, 0, st>>>(W.n, b, P.x.p, P.r.p, W.partC.p);
-  k_init_scalars<<<1, kThreads, 0, st>>>(S, W.partC.p, SolverWork::kParts, rtol);
+template <typename TK, typename TM>
+static const TM* prec_input(const PcgBufs<TK, TM>& B) {
+  if constexpr (std::is_same<TK, TM>::value)
+    return B.r;
+  else
+    return B.rm;
+}
+
+// one PCG iteration k (parity k & 1)
+template <typename TK, typename TM>
+static int pcg_iteration(Solid* s, SolverWork& W, int precond, int k, PcgScalars* S, cudaStream_t st) {
+  PcgBufs<TK, TM> B = pcg_bufs<TK, TM>(s, W);
+  const int par = k & 1;
+  TK* p_new = par ? B.p1 : B.p0;
+  TK* p_old = par ? B.p0 : B.p1;
+  k_spmv_dot<3, TK, TM><<<SolverWork::kParts, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, B.A, B.z,
+                                                                 p_old, p_new, B.q, W.partA.p, W.partB.p,
+                                                                 SolverWork::kParts, k == 0, par, S);
+  k_update<TK, TM><<<SolverWork::kParts, kThreads, 0, st>>>(W.n, B.x, B.r, B.rm, p_new, B.q, W.partB.p, W.partC.p,
+                                                            SolverWork::kParts, par, S);
+  k_check<<<1, kThreads, 0, st>>>(S, W.partC.p, SolverWork::kParts);
+  W.launches += 3;
+  WN_CUDA(cudaGetLastError());
+  return apply_prec<TM>(s, W, precond, prec_input(B), B.z, S, st);
+}
+
+// PCG on the fine matrix: solves A x = b from x = 0 to ||r|| <= rtol ||b||.  The first chunk
+// of iterations is issued directly (iteration 0 forms p = z); later chunks replay one
+// captured CUDA graph.  mode indexes the graph cache (0 fp64, 1 mixed, 2 fp32).
+template <typename TK, typename TM>
+static int pcg_solve(Solid* s, SolverWork& W, int mode, const TK* b, double rtol, int max_iter, int precond,
+                     int chunk, int use_graph, PcgScalars* S, cudaStream_t st, PcgScalars* hS) {
+  PcgBufs<TK, TM> B = pcg_bufs<TK, TM>(s, W);
+  WN_CUDA(cudaMemsetAsync(B.p0, 0, W.n * sizeof(TK), st));  // iteration 0: p = z + 0 * p_old
+  WN_CUDA(cudaMemsetAsync(B.p1, 0, W.n * sizeof(TK), st));
+  k_init_vecs<TK, TM><<<SolverWork::kParts, kThreads, 0, st>>>(W.n, b, B.x, B.r, B.rm, W.partC.p);
+  k_init_scalars<<<1, kThreads, 0, st>>>(S, W.partC.p, SolverWork::kParts, rtol, max_iter);
   W.launches += 2;
   WN_CUDA(cudaGetLastError());
-  WN_CHECK(apply_prec<T>(s, W, precond, P.r.p, P.z.p, S, st));
-  chunk = std::max(2, chunk + (chunk & 1));  // even: parity pattern repeats per chunk
-  GraphCache& G = W.graphs[pi][1];
-  const int64_t key = ((int64_t)precond << 40) ^ ((int64_t)chunk << 20) ^ (int64_t)max_iter;
-  int k0 = 0;
-  // the first chunk is issued directly (iteration 0 uses beta = 0)
-  for (int k = 0; k < chunk && k < max_iter; ++k) WN_CHECK(pcg_iteration<T>(s, W, precond, k, max_iter, S, st));
-  k0 = chunk;
+  WN_CHECK(apply_prec<TM>(s, W, precond, prec_input(B), B.z, S, st));
+  chunk = std::max(2, chunk + (chunk & 1));  // even: the parity pattern repeats per chunk
+  GraphCache& G = W.graphs[mode][precond];
+  const int64_t key = chunk;
+  for (int k = 0; k < chunk && k < max_iter; ++k) WN_CHECK((pcg_iteration<TK, TM>(s, W, precond, k, S, st)));
+  int k0 = chunk;
   while (true) {
     WN_CUDA(cudaMemcpyAsync(hS, S, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
     WN_CUDA(cudaStreamSynchronize(st));
@@ -590,12 +655,12 @@ static int pcg_solve(Solid* s, SolverWork& W, int pi, const T* b, double rtol, i
       if (G.key != key || G.stream != st || !G.exec) {
         G.reset();
         cudaGraph_t graph;
+        const int64_t before = W.launches;
         WN_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         int rc = 0;
-        // iteration indices inside the graph are relative: k_check uses k for the iteration
-        // count, so the graph is captured for "k0 = chunk" and the host re-launches it with
-        // the count advanced by the kernels themselves (S->iters); max_iter bounds it.
-        for (int k = 0; k < chunk && rc == 0; ++k) rc = pcg_iteration<T>(s, W, precond, chunk + k, max_iter, S, st);
+        // the iteration count and max_iter live on the device (k_check) and the chunk is
+        // even, so one captured chunk serves every later chunk
+        for (int k = 0; k < chunk && rc == 0; ++k) rc = pcg_iteration<TK, TM>(s, W, precond, chunk + k, S, st);
         cudaError_t e = cudaStreamEndCapture(st, &graph);
         WN_CHECK(rc);
         WN_CUDA(e);
@@ -604,14 +669,275 @@ static int pcg_solve(Solid* s, SolverWork& W, int pi, const T* b, double rtol, i
         WN_CUDA(e);
         G.key = key;
         G.stream = st;
+        G.kernels = W.launches - before;
+        W.launches = before;
       }
       WN_CUDA(cudaGraphLaunch(G.exec, st));
+      W.launches += G.kernels;
     } else {
-      for (int k = 0; k < chunk; ++k) WN_CHECK(pcg_iteration<T>(s, W, precond, k0 + k, max_iter, S, st));
+      for (int k = 0; k < chunk; ++k) WN_CHECK((pcg_iteration<TK, TM>(s, W, precond, k0 + k, S, st)));
     }
     k0 += chunk;
   }
   return 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// setup: host hierarchy -> device
+// ---------------------------------------------------------------------------------------
+int DevBsr::upload(const HostBsr& h) {
+  br = h.br;
+  bc = h.bc;
+  n_rows = h.n_rows;
+  n_cols = h.n_cols;
+  nnzb = h.nnzb();
+  WN_CHECK(rp.upload(h.rp));
+  WN_CHECK(ci.upload(h.ci));
+  WN_CHECK(v64.upload(h.v));
+  std::vector<float> f(h.v.begin(), h.v.end());
+  WN_CHECK(v32.upload(f));
+  return 0;
+}
+
+static void cheb_coefficients(const wn_amg_params& prm, DevLevel& L) {
+  const double lmax = prm.cheb_safety * L.rho;
+  const double lmin = prm.cheb_lower * lmax;
+  const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
+  const double sigma = theta / delta;
+  double rho_old = 1.0 / sigma;
+  L.inv_theta = 1.0 / theta;
+  L.c1.clear();
+  L.c2.clear();
+  for (int k = 1; k < prm.smoother_degree; ++k) {
+    const double rho_new = 1.0 / (2.0 * sigma - rho_old);
+    L.c1.push_back(rho_new * rho_old);
+    L.c2.push_back(2.0 * rho_new / delta);
+    rho_old = rho_new;
+  }
+}
+
+static int ensure_work(Solid* s) {
+  if (!s->work) s->work.reset(new SolverWork());
+  SolverWork& W = *s->work;
+  const int64_t n = s->n_nodes * 3;
+  if (W.n != n) {
+    W.n = n;
+    WN_CHECK(W.p64.alloc(n));
+    WN_CHECK(W.p32.alloc(n));
+    WN_CHECK(W.u64.alloc(n));
+    WN_CHECK(W.r64.alloc(n));
+    WN_CHECK(W.r32.alloc(n));
+    WN_CHECK(W.dinv64.alloc(n));
+    WN_CHECK(W.dinv32.alloc(n));
+    for (auto& a : W.graphs)
+      for (auto& g : a) g.reset();
+  }
+  WN_CHECK(W.partA.alloc(SolverWork::kParts));
+  WN_CHECK(W.partB.alloc(SolverWork::kParts));
+  WN_CHECK(W.partC.alloc(SolverWork::kParts));
+  WN_CHECK(W.scal.alloc(2));
+  if (!W.ev0) {
+    WN_CUDA(cudaEventCreate(&W.ev0));
+    WN_CUDA(cudaEventCreate(&W.ev1));
+  }
+  return 0;
+}
+
+int solver_setup(Solid* s, const wn_amg_params& prm) {
+  WN_REQUIRE(s->assembled, WN_ESTATE, "AMG setup: matrix not assembled");
+  WN_REQUIRE(prm.smoother_degree >= 1 && prm.smoother_degree <= 8, WN_EINVAL, "AMG setup: smoother_degree in [1, 8]");
+  WN_REQUIRE(prm.max_levels >= 1 && prm.max_levels <= 16, WN_EINVAL, "AMG setup: max_levels in [1, 16]");
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<double> vals(s->nnzb * 9);
+  WN_CUDA(cudaMemcpy(vals.data(), s->k64.p, vals.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  std::unique_ptr<AmgHierarchy> H(new AmgHierarchy());
+  const uint8_t* fixed = s->bcs_applied ? s->h_fixed.data() : nullptr;
+  WN_CHECK(amg_build(prm, s->n_nodes, s->h_row_ptr.data(), s->h_col_idx.data(), vals.data(), s->h_nodes.data(),
+                     fixed, H->host));
+  H->degree = prm.smoother_degree;
+  H->levels.resize(H->host.levels.size());
+  for (size_t l = 0; l < H->host.levels.size(); ++l) {
+    const HostLevel& h = H->host.levels[l];
+    DevLevel& L = H->levels[l];
+    L.bs = h.bs;
+    L.n_nodes = h.n_nodes;
+    if (l == 0) {
+      L.a_rp = s->row_ptr.p;
+      L.a_ci = s->col_idx.p;
+    } else {
+      WN_CHECK(L.A.upload(h.A));
+    }
+    WN_CHECK(L.dinv64.upload(h.dinv));
+    std::vector<float> f(h.dinv.begin(), h.dinv.end());
+    WN_CHECK(L.dinv32.upload(f));
+    L.rho = h.rho;
+    cheb_coefficients(prm, L);
+    WN_CHECK(L.P.upload(h.P));
+    WN_CHECK(L.R.upload(h.R));
+    WN_CHECK(L.v64.alloc(h.n_nodes * h.bs));
+    WN_CHECK(L.v32.alloc(h.n_nodes * h.bs));
+  }
+  H->n_coarse = H->host.n_coarse;
+  WN_CHECK(H->coarse_inv.upload(H->host.coarse_inv));
+  WN_CHECK(H->cb64.alloc(H->n_coarse));
+  WN_CHECK(H->cx64.alloc(H->n_coarse));
+  WN_CHECK(H->cb32.alloc(H->n_coarse));
+  WN_CHECK(H->cx32.alloc(H->n_coarse));
+  WN_CUDA(cudaDeviceSynchronize());
+  H->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  s->amg = std::move(H);
+  WN_CHECK(ensure_work(s));
+  for (auto& a : s->work->graphs)
+    for (auto& g : a) g.reset();
+  return 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// solve
+// ---------------------------------------------------------------------------------------
+static int true_residual(Solid* s, SolverWork& W, const double* F, const double* u, float* r32, cudaStream_t st,
+                         double* rr) {
+  k_outer_residual<<<SolverWork::kParts, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, F, u,
+                                                            W.r64.p, r32, W.partC.p);
+  k_reduce_rr<<<1, kThreads, 0, st>>>(W.scal.p + 1, W.partC.p, SolverWork::kParts);
+  W.launches += 2;
+  WN_CUDA(cudaGetLastError());
+  PcgScalars h;
+  WN_CUDA(cudaMemcpyAsync(&h, W.scal.p + 1, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+  WN_CUDA(cudaStreamSynchronize(st));
+  *rr = h.rr;
+  return 0;
+}
+
+// Outer loop common to all modes: u = 0; r = F - K u (FP64); while ||r|| > rtol ||F||: solve
+// K d = r approximately with the inner PCG, u += d, recompute the FP64 residual.
+//   mode 0 (fp64):  inner PCG FP64 (matrix, vectors, V-cycle), target 0.5 rtol ||F|| / ||r||
+//   mode 1 (mixed): inner PCG FP64 with an FP32 AMG V-cycle (FP32 values, vectors and
+//                   accumulation; FP64 coarsest inverse), same target
+//   mode 2 (fp32 IR): inner PCG entirely FP32 (FP32 K SpMV) to max(inner_rtol, target);
+//                   the classic iterative refinement of solid_solver.py:271-300
+// FP64 dot products everywhere.  The FP64 loop makes the stopping test the true residual.
+template <typename TK, typename TM>
+static int outer_loop(Solid* s, SolverWork& W, int mode, const double* F, double fnorm, const wn_solve_params& prm,
+                      int chunk, cudaStream_t st, int* total_iters, int* outer, int* status, double* rr) {
+  const int64_t n = W.n;
+  const int max_outer = prm.max_outer > 0 ? prm.max_outer : 10;
+  PcgScalars hS{};
+  WN_CUDA(cudaMemsetAsync(W.u64.p, 0, n * sizeof(double), st));
+  WN_CUDA(cudaMemcpyAsync(W.r64.p, F, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  *rr = fnorm * fnorm;
+  bool first = true;
+  while (true) {
+    if (!first) WN_CHECK(true_residual(s, W, F, W.u64.p, mode == 2 ? W.r32.p : nullptr, st, rr));
+    const double rn = std::sqrt(*rr);
+    if (!std::isfinite(*rr)) {
+      *status = WN_EBREAKDOWN;
+      break;
+    }
+    if (rn <= prm.rtol * fnorm) break;
+    if (*outer >= max_outer || *total_iters >= prm.max_iter) {
+      *status = WN_ENOCONV;
+      break;
+    }
+    double target = std::min(0.5, 0.5 * prm.rtol * fnorm / rn);
+    if (mode == 2) {
+      const double inner = prm.inner_rtol > 0.0 ? prm.inner_rtol : 1e-4;
+      target = std::max(target, inner);
+      if (first) {  // r32 = (float) F
+        WN_CHECK(true_residual(s, W, F, W.u64.p, W.r32.p, st, rr));
+      }
+    }
+    first = false;
+    const TK* b;
+    if constexpr (std::is_same<TK, float>::value)
+      b = W.r32.p;
+    else
+      b = W.r64.p;
+    WN_CHECK((pcg_solve<TK, TM>(s, W, mode, b, target, prm.max_iter - *total_iters, prm.precond, chunk,
+                                prm.use_graph, W.scal.p, st, &hS)));
+    *total_iters += hS.iters;
+    ++*outer;
+    if (hS.status == WN_EBREAKDOWN) {
+      *status = WN_EBREAKDOWN;
+      break;
+    }
+    PcgBufs<TK, TM> B = pcg_bufs<TK, TM>(s, W);
+    k_accumulate<TK><<<vec_grid(n), kThreads, 0, st>>>(n, W.u64.p, B.x);
+    W.launches++;
+    WN_CUDA(cudaGetLastError());
+  }
+  return 0;
+}
+
+int solver_solve(Solid* s, const double* F, double* u, const wn_solve_params& prm, wn_solve_stats* stats,
+                 cudaStream_t st) {
+  WN_REQUIRE(s->assembled, WN_ESTATE, "solve: matrix not assembled");
+  WN_REQUIRE(prm.precond >= 0 && prm.precond <= 2, WN_EINVAL, "solve: precond must be 0 (none), 1 (jacobi), 2 (amg)");
+  WN_REQUIRE(prm.precision >= 0 && prm.precision <= 2, WN_EINVAL,
+             "solve: precision must be 0 (fp64), 1 (mixed: fp32 AMG in fp64 PCG) or 2 (fp32 PCG in fp64 refinement)");
+  WN_REQUIRE(prm.max_iter > 0 && prm.rtol > 0.0, WN_EINVAL, "solve: max_iter > 0 and rtol > 0 required");
+  if (prm.precond == 2 && !s->amg) WN_CHECK(solver_setup(s, amg_default_params()));
+  WN_CHECK(ensure_work(s));
+  SolverWork& W = *s->work;
+  W.launches = 0;
+  if (st == 0) {  // stream capture is not allowed on the legacy default stream
+    if (!W.own) WN_CUDA(cudaStreamCreate(&W.own));  // blocking: ordered with stream 0
+    st = W.own;
+  }
+  const int64_t n = W.n;
+  const int chunk = prm.chunk > 0 ? prm.chunk : 8;
+  PcgScalars hS{};
+  k_fill_dinv<<<vec_grid(n), kThreads, 0, st>>>(s->n_nodes, s->diag_block.p, s->k64.p, W.dinv64.p, W.dinv32.p);
+  W.launches++;
+  WN_CUDA(cudaEventRecord(W.ev0, st));
+  k_dot_self<double><<<SolverWork::kParts, kThreads, 0, st>>>(n, F, W.partC.p);
+  k_reduce_rr<<<1, kThreads, 0, st>>>(W.scal.p + 1, W.partC.p, SolverWork::kParts);
+  W.launches += 2;
+  WN_CUDA(cudaMemcpyAsync(&hS, W.scal.p + 1, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+  WN_CUDA(cudaStreamSynchronize(st));
+  const double fnorm = std::sqrt(hS.rr);
+  int total_iters = 0, outer = 0, status = 0;
+  double rr = 0.0;
+  if (fnorm == 0.0) {
+    WN_CUDA(cudaMemsetAsync(u, 0, n * sizeof(double), st));
+  } else if (!std::isfinite(fnorm)) {
+    status = WN_EBREAKDOWN;
+    rr = hS.rr;
+    WN_CUDA(cudaMemsetAsync(u, 0, n * sizeof(double), st));
+  } else {
+    if (prm.precision == 0)
+      WN_CHECK((outer_loop<double, double>(s, W, 0, F, fnorm, prm, chunk, st, &total_iters, &outer, &status, &rr)));
+    else if (prm.precision == 1)
+      WN_CHECK((outer_loop<double, float>(s, W, 1, F, fnorm, prm, chunk, st, &total_iters, &outer, &status, &rr)));
+    else
+      WN_CHECK((outer_loop<float, float>(s, W, 2, F, fnorm, prm, chunk, st, &total_iters, &outer, &status, &rr)));
+    WN_CUDA(cudaMemcpyAsync(u, W.u64.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  }
+  WN_CUDA(cudaEventRecord(W.ev1, st));
+  WN_CUDA(cudaEventSynchronize(W.ev1));
+  float ms = 0.f;
+  WN_CUDA(cudaEventElapsedTime(&ms, W.ev0, W.ev1));
+  if (stats) {
+    stats->iterations = total_iters;
+    stats->outer_iterations = outer;
+    stats->status = status;
+    stats->rel_res = fnorm > 0.0 ? std::sqrt(rr) / fnorm : 0.0;
+    stats->solve_seconds = ms * 1e-3;
+    stats->kernel_launches = W.launches;
+    stats->setup_seconds = s->amg ? s->amg->setup_seconds : 0.0;
+    stats->n_levels = s->amg ? (int)s->amg->levels.size() + 1 : 0;
+  }
+  return 0;
+}
+
+int amg_vcycle(Solid* s, int precision, const void* r, void* z, cudaStream_t st) {
+  WN_REQUIRE(s->amg, WN_ESTATE, "vcycle: no AMG hierarchy (call wn_amg_setup)");
+  WN_CHECK(ensure_work(s));
+  SolverWork& W = *s->work;
+  WN_CUDA(cudaMemsetAsync(W.scal.p, 0, sizeof(PcgScalars), st));  // done = 0
+  if (precision == 0)
+    return vcycle<double>(s, *s->amg, W, 0, (const double*)r, (double*)z, nullptr, W.scal.p, st);
+  return vcycle<float>(s, *s->amg, W, 0, (const float*)r, (float*)z, nullptr, W.scal.p, st);
 }
 
 }  // namespace wn

@@ -54,6 +54,93 @@ def assemble_c3d10_sparse_3dof(model: FEAModel, apply_bcs: bool = True):
     return BSR3Matrix(system), F, fixed
 
 
+_PRECOND = {"none": 0, "jacobi": 1, "amg": 2}
+_PRECISION = {"fp64": 0, "mixed_fp32": 1, "mixed_fp32_ir": 2}
+
+
+def solve_c3d10_pcg(
+    K: BSR3Matrix,
+    F: np.ndarray,
+    rtol: float = 1e-6,
+    max_iter: int = 2000,
+    preconditioner: str = "amg",
+    precision: str = "fp64",
+    amg_params=None,
+    inner_rtol: float = 0.0,
+    chunk: int = 8,
+):
+    """PCG on the GPU -> (u, iterations, final_rel_res, solve_time_sec) (solid_solver.py:197-308).
+
+    ``preconditioner``: "amg" (smoothed aggregation, default), "jacobi" (point Jacobi, the
+    reference's default) or "none".  ``precision``:
+
+    * "fp64"          -- FP64 matrix, vectors, V-cycle;
+    * "mixed_fp32"    -- FP64 PCG (FP64 SpMV, vectors, dots) preconditioned by an FP32 AMG
+                         V-cycle (FP32 values, vectors and accumulation; FP64 coarsest
+                         inverse), inside the FP64 true-residual loop;
+    * "mixed_fp32_ir" -- the reference's mixed mode (:271-300): FP32 PCG (FP32 SpMV) inside
+                         FP64 iterative refinement.  Converges slowly once cond(K) * 6e-8
+                         approaches 1 (an FP32 SpMV cannot resolve smooth displacement
+                         fields: K u cancels ~8 digits per row); fine for small meshes.
+
+    All modes stop on the true FP64 residual ||F - K u|| <= rtol ||F||.  The returned
+    iteration count is the real one (the reference stores scipy's ``info`` there,
+    :288-291).
+    """
+    if preconditioner not in _PRECOND:
+        raise ValueError(f"preconditioner must be one of {sorted(_PRECOND)}, got {preconditioner!r}")
+    if precision not in _PRECISION:
+        raise ValueError(f"precision must be one of {sorted(_PRECISION)}, got {precision!r}")
+    t0 = time.perf_counter()
+    system = K.system
+    if preconditioner == "amg" and (amg_params is not None or not system.amg_ready):
+        system.amg_setup(amg_params)
+    u, st = system.solve(F, rtol=rtol, max_iter=max_iter, precond=_PRECOND[preconditioner],
+                         precision=_PRECISION[precision], inner_rtol=inner_rtol, chunk=chunk)
+    if st["status"] == -4:
+        raise RuntimeError("PCG breakdown (p^T K p <= 0 or non-finite): matrix not SPD?")
+    K.last_stats = st
+    return u, st["iterations"], st["rel_res"], time.perf_counter() - t0
+
+
+def solve_c3d10_system(
+    K: BSR3Matrix,
+    F: np.ndarray,
+    method: str = "auto",
+    rtol: float = 1e-6,
+    max_iter: int = 2000,
+    preconditioner: str = "amg",
+    precision: str = "fp64",
+):
+    """Unified solve -> (u, stats) (solid_solver.py:132-194).
+
+    ``method``: "pcg" (GPU PCG), "auto" (the same: the GPU path has no size threshold), or
+    "direct" -- the reference's SuperLU branch (:164-183) has no GPU counterpart here and
+    raises.  Stats keep the reference's keys (method, iterations, solve_time_sec, rel_res)
+    and add outer_iters, dof_per_s, setup_time_sec and levels.
+    """
+    if method == "direct":
+        raise NotImplementedError("direct sparse factorisation is not part of the GPU path; use method='pcg'")
+    if method not in ("auto", "pcg"):
+        raise ValueError(f"method must be 'auto', 'pcg' or 'direct', got {method!r}")
+    u, iters, rel, secs = solve_c3d10_pcg(K, F, rtol=rtol, max_iter=max_iter, preconditioner=preconditioner,
+                                          precision=precision)
+    st = K.last_stats
+    stats = {
+        "method": f"pcg_{preconditioner}_{precision}",
+        "iterations": iters,
+        "solve_time_sec": secs,
+        "rel_res": rel,
+        "outer_iters": st["outer_iterations"],
+        "device_solve_sec": st["solve_seconds"],
+        "setup_time_sec": st["setup_seconds"],
+        "levels": st["n_levels"],
+        "status": st["status"],
+        "dof_per_s": K.shape[0] / st["solve_seconds"] if st["solve_seconds"] > 0 else float("inf"),
+    }
+    return u, stats
+
+
 def compute_c3d10_stress_field(model: FEAModel, u_3dof: np.ndarray):
     """Cell stresses (M, 6), cell von Mises (M,), nodal von Mises (N,) on the GPU."""
     system = solid_system(model)

@@ -37,7 +37,7 @@ class SolidSystem:
         self.fixed_mask = np.zeros(3 * self.n_nodes, dtype=np.uint8)
         self.props: np.ndarray | None = None
         self.bcs_applied = False
-        self._solver = None
+        self.amg_ready = False
 
     # -- lifetime -------------------------------------------------------------------------
     @property
@@ -47,9 +47,6 @@ class SolidSystem:
     def close(self):
         if getattr(self, "_h", None):
             try:
-                if self._solver is not None:
-                    self._solver.close()
-                    self._solver = None
                 _lib.lib().wn_solid_destroy(self._h)
             finally:
                 self._h = None
@@ -87,8 +84,34 @@ class SolidSystem:
         call("wn_assemble_c3d10", self._h, ptr(props), int(bool(apply_bcs)))
         self.props = props
         self.bcs_applied = bool(apply_bcs)
-        if self._solver is not None:
-            self._solver.invalidate()
+        self.amg_ready = False
+
+    # -- solver -------------------------------------------------------------------------------
+    def amg_setup(self, params=None) -> None:
+        from .amg import AMGParams
+
+        prm = (params or AMGParams()).to_c()
+        call("wn_amg_setup", self._h, C.byref(prm))
+        self.amg_ready = True
+
+    def solve(self, F: np.ndarray, rtol: float = 1e-8, max_iter: int = 2000, precond: int = 2,
+              precision: int = 0, inner_rtol: float = 0.0, max_outer: int = 10, chunk: int = 8,
+              use_graph: bool = True):
+        """Solve K u = F on the GPU (host buffers); returns (u, stats dict)."""
+        F = np.ascontiguousarray(F, dtype=np.float64)
+        u = np.empty_like(F)
+        prm = _lib.SolveParams(rtol, max_iter, precond, precision, inner_rtol, max_outer, chunk, int(use_graph))
+        st = _lib.SolveStats()
+        call("wn_solve", self._h, ptr(F), ptr(u), C.byref(prm), C.byref(st))
+        return u, {f: getattr(st, f) for f, _ in _lib.SolveStats._fields_}
+
+    def matvec(self, x: np.ndarray) -> np.ndarray:
+        rp, ci = self.pattern()
+        v = self.values()
+        y = np.zeros(3 * self.n_nodes)
+        call("wn_spmv_bsr_f64", 3, 3, self.n_nodes, self.n_nodes, self.nnzb, ptr(rp), ptr(ci), ptr(v),
+             ptr(np.ascontiguousarray(x, dtype=np.float64)), ptr(y), 1.0, 0.0)
+        return y
 
     def values(self) -> np.ndarray:
         v = np.empty((self.nnzb, 3, 3), dtype=np.float64)
