@@ -206,6 +206,26 @@ int wn_spmv_bsr_f64(int br, int bc, int64_t n_rows, int64_t n_cols, int64_t nnzb
  * element_stiffness_c3d10 (c3d10.py:219-249).  WN_EMESH on det J <= 0. */
 int wn_c3d10_element_stiffness(int64_t n_el, const double* coords, const double* props, double* Ke);
 
+/* Element stiffness for callers that must not allocate device memory (no counterpart in the
+ * reference).  Code whose device memory belongs to another allocator -- a framework's caching
+ * allocator, or a pool sized once at start-up -- cannot let a library call cudaMalloc behind
+ * its back (the allocation can fail or fragment the pool), and latency-bound loops cannot
+ * absorb the device-wide synchronisation of cudaFree.  wn_c3d10_element_stiffness allocates
+ * on every call; this variant takes device pointers from the caller -- nodes (n_nodes x 3),
+ * conn (n_el x 10), props (n_el x 2), Ke out (n_el x 30 x 30) -- and keeps its scratch (the
+ * upper-triangle blocks of each element plus a status word) in a fixed device array that
+ * every GPU loading the library holds until exit (about 8.1 MB).  It calls no cudaMalloc,
+ * cudaFree or allocating library routine.
+ *   - n_el > WN_NOALLOC_MAX_ELEMENTS returns WN_ETOOBIG (split the batch);
+ *   - the first call on a device looks up the scratch address and loads the element
+ *     kernel's constant tables: make that first call before any stream capture;
+ *   - all calls share the scratch, so calls that overlap on the GPU (other streams, other
+ *     threads) race: serialise them;
+ *   - the call synchronises `stream` to report WN_EMESH for det J <= 0. */
+#define WN_NOALLOC_MAX_ELEMENTS 2048
+int wn_c3d10_element_stiffness_noalloc(int64_t n_el, const double* d_nodes, const int32_t* d_conn,
+                                       const double* d_props, double* d_Ke, uintptr_t stream);
+
 /* Internal forces F_int = sum_e f_e(u) with f_e = sum_g w|J| B^T C B u_e (c3d10.py:252-283),
  * atomic-free (node gather in element order).  Same argument list and U/F_int stride of 6
  * as the reference's compute_c3d10_internal_forces_native (kernels.cpp:244-252); host
