@@ -59,7 +59,50 @@ def parse():
     ap.add_argument("--cpu-iters", type=int, default=12, help="scipy cg iterations in the CPU sample")
     ap.add_argument("--skip-jacobi", action="store_true", help="do not measure the Jacobi iteration count")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--only", choices=["solve-mixed", "solve-fp64", "spmv32", "spmv64"], default=None,
+                    help="profiling mode: run only this operation (warmup + steps times) and print its time")
     return ap.parse_args()
+
+
+def run_only(args):
+    """Profiling mode used by the ncu recipes in profiles/: one operation, nothing else."""
+    import torch
+
+    from wnfea_b200 import _lib
+    from wnfea_b200.solid_solver import assemble_c3d10_sparse_3dof
+
+    m, meta = build_model(args.slices)
+    K, F_np, _ = assemble_c3d10_sparse_3dof(m)
+    s = K.system
+    st = torch.cuda.current_stream().cuda_stream
+    n = 3 * s.n_nodes
+    if args.only.startswith("solve"):
+        s.amg_setup()
+        F = torch.from_numpy(F_np).cuda()
+        u = torch.empty_like(F)
+        prec = 1 if args.only == "solve-mixed" else 0
+
+        def op():
+            prm = _lib.SolveParams(1e-8, 2000, 2, prec, 0.0, 10, 8, 1)
+            stt = _lib.SolveStats()
+            _lib.call("wn_solve_device", s.handle, F.data_ptr(), u.data_ptr(), prm, stt, st)
+    else:
+        prec = 1 if args.only == "spmv32" else 0
+        dt = torch.float32 if prec else torch.float64
+        x = torch.randn(n, dtype=torch.float64, device="cuda").to(dt)
+        y = torch.empty_like(x)
+
+        def op():
+            _lib.call("wn_spmv_solid_device", s.handle, prec, x.data_ptr(), y.data_ptr(), st)
+    for _ in range(args.warmup):
+        op()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        op()
+    torch.cuda.synchronize()
+    print(json.dumps({"only": args.only, "ms_per_op": (time.perf_counter() - t0) * 1e3 / args.steps,
+                      "elements": meta["n_elements"], "nnz_blocks": s.nnzb}))
 
 
 def build_model(slices):
@@ -397,7 +440,9 @@ def run_ours(args):
 
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.only:
+        run_only(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -84,7 +84,9 @@ int wn_assemble_c3d10(void* h, const double* props, int apply_bcs);
 int wn_assemble_c3d10_device(void* h, const double* d_props, int apply_bcs, uintptr_t stream);
 /* Host copy of the FP64 values: nnzb x 9 (row-major 3x3 blocks). */
 int wn_solid_get_values(void* h, double* values);
-/* Device pointers of the assembled values, pattern and Dirichlet mask (owned by h). */
+/* Device pointers of the assembled values, pattern and Dirichlet mask (owned by h).  The
+ * device values are component-major: entry (i, j) of block b at k64[(3 i + j) * nnzb + b]
+ * (wn_solid_get_values returns row-major blocks). */
 int wn_solid_device_arrays(void* h, const double** k64, const float** k32, const int32_t** row_ptr,
                            const int32_t** col_idx, const uint8_t** fixed_mask);
 

@@ -111,7 +111,10 @@ struct GraphCache {
 
 struct SolverWork {
   int64_t n = 0;  // scalar DOFs
-  static constexpr int kParts = 148 * 4;  // CTAs of every partial-producing kernel
+  static constexpr int kMaxParts = 148 * 16;
+  // number of valid partials in partA / partB / partC: the grid of the kernel that last
+  // wrote them (host-side bookkeeping, baked into captured graphs in launch order)
+  int npA = 0, npB = 0, npC = 0;
   DArray<double> partA, partB, partC;
   DArray<PcgScalars> scal;   // [0] = FP64 / inner solve, [1] = outer refinement
   DArray<double> u64, r64;  // outer refinement vectors

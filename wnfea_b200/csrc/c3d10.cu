@@ -120,35 +120,47 @@ __global__ void __launch_bounds__(KE_THREADS) ke_upper_kernel(int64_t n_el, cons
   }
 }
 
-// Gather-assemble: one thread per matrix entry.  K[b][k] = sum over the block's gather list
-// (fixed (element, a, b) order) of the stored element block, transposed when a > b.
-// Dirichlet: an entry in a fixed row or column becomes 1 on the diagonal, 0 elsewhere
-// (solid_solver.py:105-125).  Writes FP64 values and, if k32 != nullptr, an FP32 copy.
+// Gather-assemble: one thread per 3x3 block.  K[b] = sum over the block's gather list (fixed
+// (element, a, b) order) of the stored element block, transposed when a > b.  Dirichlet: an
+// entry in a fixed row or column becomes 1 on the diagonal, 0 elsewhere
+// (solid_solver.py:105-125).  Output is component-major (entry k of block b at k * nnzb + b)
+// in FP64 and, if k32 != nullptr, FP32 -- consecutive threads write consecutive addresses.
 __global__ void gather_assemble_kernel(int64_t nnzb, const int32_t* __restrict__ gptr,
                                        const int32_t* __restrict__ gsrc, const double* __restrict__ ke,
                                        const int32_t* __restrict__ block_row, const int32_t* __restrict__ col_idx,
                                        const uint8_t* __restrict__ fixed, double* __restrict__ k64,
                                        float* __restrict__ k32) {
-  const int64_t total = nnzb * 9;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t b = t / 9;
-    const int k = (int)(t - b * 9);
-    const int i = k / 3, j = k - (k / 3) * 3;
-    const int kt = j * 3 + i;
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < nnzb; b += (int64_t)gridDim.x * blockDim.x) {
+    double acc[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) acc[k] = 0.0;
     const int32_t s = gptr[b], e = gptr[b + 1];
-    double acc = 0.0;
     for (int32_t q = s; q < e; ++q) {
       const int32_t src = gsrc[q];
-      const int64_t blk = src >> 1;
-      acc += ke[blk * 9 + ((src & 1) ? kt : k)];
+      const double* blk = ke + (int64_t)(src >> 1) * 9;
+      if (src & 1) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) acc[i * 3 + j] += blk[j * 3 + i];
+      } else {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) acc[k] += blk[k];
+      }
     }
     if (fixed) {
-      const int64_t rdof = (int64_t)block_row[b] * 3 + i;
-      const int64_t cdof = (int64_t)col_idx[b] * 3 + j;
-      if (fixed[rdof] | fixed[cdof]) acc = (rdof == cdof) ? 1.0 : 0.0;
+      const int64_t r0 = (int64_t)block_row[b] * 3, c0 = (int64_t)col_idx[b] * 3;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          if (fixed[r0 + i] | fixed[c0 + j]) acc[i * 3 + j] = (r0 + i == c0 + j) ? 1.0 : 0.0;
     }
-    k64[t] = acc;
-    if (k32) k32[t] = (float)acc;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      k64[k * nnzb + b] = acc[k];
+      if (k32) k32[k * nnzb + b] = (float)acc[k];
+    }
   }
 }
 
@@ -316,7 +328,7 @@ int launch_gather_assemble(int64_t nnzb, const int32_t* gptr, const int32_t* gsr
                            const int32_t* block_row, const int32_t* col_idx, const uint8_t* fixed, double* k64,
                            float* k32, cudaStream_t st) {
   if (nnzb == 0) return 0;
-  const int grid = grid_for(nnzb * 9, 1, 256, 32);
+  const int grid = grid_for(nnzb, 1, 256, 16);
   gather_assemble_kernel<<<grid, 256, 0, st>>>(nnzb, gptr, gsrc, ke, block_row, col_idx, fixed, k64, k32);
   WN_CUDA(cudaGetLastError());
   return 0;

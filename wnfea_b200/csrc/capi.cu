@@ -2,6 +2,8 @@
 // entry points (declared in include/wnfea_cuda.h).
 #include <cstdarg>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 
 #include "wnfea_cuda.h"
@@ -23,6 +25,19 @@ void set_error(const char* fmt, ...) {
   g_last_error = buf;
 }
 const char* last_error() { return g_last_error.c_str(); }
+
+int occupancy_per_sm(const void* kernel, int threads) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  auto key = std::make_pair(kernel, threads);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0) != cudaSuccess || n < 1) n = 1;
+  cache[key] = n;
+  return n;
+}
 
 __global__ void grad_f_kernel(int64_t n, const double* __restrict__ u, const uint8_t* __restrict__ fixed,
                               double* __restrict__ g) {
@@ -209,7 +224,11 @@ int wn_solid_get_values(void* h, double* values) {
   Solid* s = as_solid(h);
   WN_REQUIRE(s->assembled, WN_ESTATE, "wn_solid_get_values: not assembled");
   WN_CHECK(select_device(s));
-  WN_CUDA(cudaMemcpy(values, s->k64.p, s->k64.bytes(), cudaMemcpyDeviceToHost));
+  // device values are component-major (9 arrays of nnzb); return row-major blocks
+  std::vector<double> soa(s->nnzb * 9);
+  WN_CUDA(cudaMemcpy(soa.data(), s->k64.p, s->k64.bytes(), cudaMemcpyDeviceToHost));
+  for (int64_t b = 0; b < s->nnzb; ++b)
+    for (int k = 0; k < 9; ++k) values[b * 9 + k] = soa[k * s->nnzb + b];
   return 0;
 }
 
@@ -231,11 +250,11 @@ int wn_spmv_solid_device(void* h, int precision, const void* x, void* y, uintptr
   WN_REQUIRE(s->assembled, WN_ESTATE, "wn_spmv_solid_device: not assembled");
   WN_CHECK(select_device(s));
   if (precision == 0)
-    return launch_bsr_spmv_f64(3, 3, s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, (const double*)x, (double*)y,
-                               1.0, 0.0, (cudaStream_t)stream);
+    return launch_solid_spmv_f64(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, s->nnzb, (const double*)x,
+                                 (double*)y, (cudaStream_t)stream);
   if (precision == 1)
-    return launch_bsr_spmv_f32(3, 3, s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k32.p, (const float*)x, (float*)y,
-                               1.0f, 0.0f, (cudaStream_t)stream);
+    return launch_solid_spmv_f32(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k32.p, s->nnzb, (const float*)x,
+                                 (float*)y, (cudaStream_t)stream);
   set_error("wn_spmv_solid_device: precision must be 0 (FP64) or 1 (FP32)");
   return WN_EINVAL;
 }

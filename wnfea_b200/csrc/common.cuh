@@ -77,6 +77,18 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return r;
 }
 
+// Grid of at most one full wave: blocks resident on all SMs at once for `kernel` with
+// `threads` threads per CTA (occupancy queried once per kernel), capped by the work.
+int occupancy_per_sm(const void* kernel, int threads);  // cached per (kernel, threads), capi.cu
+
+template <typename K>
+inline int resident_grid(K kernel, int threads, int64_t work_ctas) {
+  const int per_sm = occupancy_per_sm(reinterpret_cast<const void*>(kernel), threads);
+  int64_t g = (int64_t)kNumSMs * per_sm;
+  if (work_ctas < g) g = work_ctas;
+  return g < 1 ? 1 : (int)g;
+}
+
 #endif  // __CUDACC__
 
 inline int grid_for(int64_t work_items, int threads_per_item_group, int block, int max_waves = 16) {

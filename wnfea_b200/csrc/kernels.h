@@ -22,10 +22,15 @@ int launch_stress(int64_t n_el, int64_t n_nodes, const double* nodes, const int3
                   const double* u, const int64_t* inc_ptr, const int32_t* inc_ea, double* cell_sig, double* cell_vm,
                   double* nodal_vm, cudaStream_t st);
 
-// spmv.cu
+// spmv.cu -- generic matrices are block-contiguous (AoS); the assembled fine-level matrix
+// of a solid handle is component-major (SoA, stride nnzb)
 int launch_bsr_spmv_f64(int br, int bc, int64_t n_rows, const int32_t* rp, const int32_t* ci, const double* v,
                         const double* x, double* y, double alpha, double beta, cudaStream_t st);
 int launch_bsr_spmv_f32(int br, int bc, int64_t n_rows, const int32_t* rp, const int32_t* ci, const float* v,
                         const float* x, float* y, float alpha, float beta, cudaStream_t st);
+int launch_solid_spmv_f64(int64_t n_rows, const int32_t* rp, const int32_t* ci, const double* v, int64_t nnzb,
+                          const double* x, double* y, cudaStream_t st);
+int launch_solid_spmv_f32(int64_t n_rows, const int32_t* rp, const int32_t* ci, const float* v, int64_t nnzb,
+                          const float* x, float* y, cudaStream_t st);
 
 }  // namespace wn

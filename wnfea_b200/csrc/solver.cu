@@ -35,6 +35,8 @@ namespace wn {
 // reductions shared by the PCG kernels
 // ---------------------------------------------------------------------------------------
 constexpr int kThreads = 256;
+// Row kernels are register-limited: ask for 6 resident CTAs per SM (<= 42 registers).
+constexpr int kMinBlocks = 6;
 
 // all threads of the CTA get the fixed-order sum of part[0..n)
 __device__ __forceinline__ double reduce_parts(const double* __restrict__ part, int n, double* sh) {
@@ -71,6 +73,31 @@ struct XPNew {  // p_j = z_j + beta p_old_j
   __device__ __forceinline__ T operator()(int64_t j) const { return z[j] + beta * p[j]; }
 };
 
+// the fine level (3x3 blocks, the assembled matrix) is component-major; coarse levels are
+// block-contiguous
+template <int BS>
+struct LayoutOf {
+  static constexpr Layout value = (BS == 3) ? kSoA : kAoS;
+};
+
+// lanes per block row: 16 for the fine 3x3 level (rows of ~25 blocks: two rows per warp keep
+// more loads in flight), a full warp for the 6x6 coarse levels
+template <int BS>
+struct GroupOf {
+  static constexpr int value = (BS == 3) ? 16 : 32;
+};
+
+// Row loop for groups of G lanes: defines `lane` (index inside the group), `row` and needs
+// `const bool active = row < n_rows;` in the body (all lanes stay in the loop for the
+// group shuffles).
+#define GROUP_ROW_LOOP(n_rows, G)                                                              \
+  const int lane = (threadIdx.x & 31) % (G);                                                   \
+  const int grp_ = (threadIdx.x & 31) / (G);                                                   \
+  const int64_t warp0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;                 \
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;                               \
+  for (int64_t rb_ = warp0, row = warp0 * (32 / (G)) + grp_; rb_ * (32 / (G)) < (n_rows);      \
+       rb_ += nwarps, row = rb_ * (32 / (G)) + grp_)
+
 #define WARP_ROW_LOOP(n_rows)                                                   \
   const int lane = threadIdx.x & 31;                                            \
   const int64_t warp0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;  \
@@ -93,17 +120,19 @@ __device__ __forceinline__ T pick(const T (&acc)[BS], int lane) {
 // First pre-smoothing step from x = 0.  deg == 1: x = d0, res = b - A x (fused residual).
 // deg >= 2: second Chebyshev step: r1 = D^-1 (b - A d0), d1 = c1 d0 + c2 r1, x = d0 + d1.
 template <int BS, typename T>
-__global__ void __launch_bounds__(kThreads) k_pre_first(int64_t n_rows, const int32_t* __restrict__ rp,
-                                                        const int32_t* __restrict__ ci, const T* __restrict__ av,
+__global__ void __launch_bounds__(kThreads, (BS == 3) ? kMinBlocks : 1) k_pre_first(int64_t n_rows, const int32_t* __restrict__ rp,
+                                                        const int32_t* __restrict__ ci, const T* __restrict__ av, int64_t stride,
                                                         const T* __restrict__ b, const T* __restrict__ dinv,
                                                         T inv_theta, int deg, T c1, T c2, T* __restrict__ x,
                                                         T* __restrict__ r, T* __restrict__ d, T* __restrict__ res,
                                                         const PcgScalars* __restrict__ S) {
   if (S->done) return;
-  WARP_ROW_LOOP(n_rows) {
+  GROUP_ROW_LOOP(n_rows, GroupOf<BS>::value) {
+    const bool active = row < n_rows;
     T acc[BS];
-    warp_block_row<BS, BS, T, T>(rp, ci, av, row, XD0<T>{b, dinv, inv_theta}, acc, lane);
-    if (lane < BS) {
+    group_block_row<BS, BS, GroupOf<BS>::value, LayoutOf<BS>::value, T, T>(rp, ci, av, stride, row, active,
+        XD0<T>{b, dinv, inv_theta}, acc, lane);
+    if (active && lane < BS) {
       const int64_t i = row * BS + lane;
       const T t = pick<BS>(acc, lane);
       const T bi = b[i], di = dinv[i];
@@ -125,8 +154,8 @@ __global__ void __launch_bounds__(kThreads) k_pre_first(int64_t n_rows, const in
 // Chebyshev step k >= 1: r -= D^-1 A d_in; d_out = c1 d_in + c2 r; x += d_out.
 // If part != nullptr: also the partial of b . x (the PCG's r . z at the finest level).
 template <int BS, typename T>
-__global__ void __launch_bounds__(kThreads) k_cheb_step(int64_t n_rows, const int32_t* __restrict__ rp,
-                                                        const int32_t* __restrict__ ci, const T* __restrict__ av,
+__global__ void __launch_bounds__(kThreads, (BS == 3) ? kMinBlocks : 1) k_cheb_step(int64_t n_rows, const int32_t* __restrict__ rp,
+                                                        const int32_t* __restrict__ ci, const T* __restrict__ av, int64_t stride,
                                                         const T* __restrict__ dinv, const T* __restrict__ d_in,
                                                         T* __restrict__ d_out, T* __restrict__ r, T* __restrict__ x,
                                                         T c1, T c2, const T* __restrict__ b, double* __restrict__ part,
@@ -134,10 +163,12 @@ __global__ void __launch_bounds__(kThreads) k_cheb_step(int64_t n_rows, const in
   __shared__ double sh[kThreads / 32];
   if (S->done) return;
   double dot = 0.0;
-  WARP_ROW_LOOP(n_rows) {
+  GROUP_ROW_LOOP(n_rows, GroupOf<BS>::value) {
+    const bool active = row < n_rows;
     T acc[BS];
-    warp_block_row<BS, BS, T, T>(rp, ci, av, row, XLoad<T, T>{d_in}, acc, lane);
-    if (lane < BS) {
+    group_block_row<BS, BS, GroupOf<BS>::value, LayoutOf<BS>::value, T, T>(rp, ci, av, stride, row, active,
+        XLoad<T, T>{d_in}, acc, lane);
+    if (active && lane < BS) {
       const int64_t i = row * BS + lane;
       const T ri = r[i] - dinv[i] * pick<BS>(acc, lane);
       const T dn = c1 * d_in[i] + c2 * ri;
@@ -153,44 +184,75 @@ __global__ void __launch_bounds__(kThreads) k_cheb_step(int64_t n_rows, const in
 
 // res = b - A x
 template <int BS, typename T>
-__global__ void __launch_bounds__(kThreads) k_residual(int64_t n_rows, const int32_t* __restrict__ rp,
-                                                       const int32_t* __restrict__ ci, const T* __restrict__ av,
+__global__ void __launch_bounds__(kThreads, (BS == 3) ? kMinBlocks : 1) k_residual(int64_t n_rows, const int32_t* __restrict__ rp,
+                                                       const int32_t* __restrict__ ci, const T* __restrict__ av, int64_t stride,
                                                        const T* __restrict__ b, const T* __restrict__ x,
                                                        T* __restrict__ res, const PcgScalars* __restrict__ S) {
   if (S->done) return;
-  WARP_ROW_LOOP(n_rows) {
+  GROUP_ROW_LOOP(n_rows, GroupOf<BS>::value) {
+    const bool active = row < n_rows;
     T acc[BS];
-    warp_block_row<BS, BS, T, T>(rp, ci, av, row, XLoad<T, T>{x}, acc, lane);
-    if (lane < BS) {
+    group_block_row<BS, BS, GroupOf<BS>::value, LayoutOf<BS>::value, T, T>(rp, ci, av, stride, row, active,
+        XLoad<T, T>{x}, acc, lane);
+    if (active && lane < BS) {
       const int64_t i = row * BS + lane;
       res[i] = b[i] - pick<BS>(acc, lane);
     }
   }
 }
 
-// y = A x (accumulate = 0) or y += A x (accumulate = 1) for a BR x BC block matrix
-template <int BR, int BC, typename T>
+// y = A x (accumulate = 0) or y += A x (accumulate = 1) for a BR x BC block-contiguous
+// matrix; G lanes per block row (32 / G rows per warp) so that short rows (the prolongators)
+// still fill the warp.
+template <int BR, int BC, int G, typename T>
 __global__ void __launch_bounds__(kThreads) k_level_spmv(int64_t n_rows, const int32_t* __restrict__ rp,
                                                          const int32_t* __restrict__ ci, const T* __restrict__ av,
                                                          const T* __restrict__ x, T* __restrict__ y, int accumulate,
                                                          const PcgScalars* __restrict__ S) {
   if (S->done) return;
-  WARP_ROW_LOOP(n_rows) {
+  constexpr int RPW = 32 / G;
+  const int lane = threadIdx.x & 31;
+  const int gl = lane % G, grp = lane / G;
+  const int64_t warp0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t rb = warp0; rb * RPW < n_rows; rb += nwarps) {
+    const int64_t row = rb * RPW + grp;
+    const bool active = row < n_rows;
     T acc[BR];
-    warp_block_row<BR, BC, T, T>(rp, ci, av, row, XLoad<T, T>{x}, acc, lane);
-    if (lane < BR) {
-      const int64_t i = row * BR + lane;
-      const T v = pick<BR>(acc, lane);
+    group_block_row<BR, BC, G, kAoS, T, T>(rp, ci, av, 0, row, active, XLoad<T, T>{x}, acc, gl);
+    if (active && gl < BR) {
+      const int64_t i = row * BR + gl;
+      const T v = pick<BR>(acc, gl);
       y[i] = accumulate ? y[i] + v : v;
     }
+  }
+}
+
+// launch k_level_spmv with a group size matched to the mean row length
+template <int BR, int BC, typename T>
+static void level_spmv(const DevBsr& M, const T* vals, const T* x, T* y, int accumulate, const PcgScalars* S,
+                       cudaStream_t st) {
+  const double avg = M.n_rows ? (double)M.nnzb / (double)M.n_rows : 0.0;
+  if (avg >= 24.0) {
+    auto k = k_level_spmv<BR, BC, 32, T>;
+    k<<<resident_grid(k, kThreads, (M.n_rows * 32 + kThreads - 1) / kThreads), kThreads, 0, st>>>(
+        M.n_rows, M.rp.p, M.ci.p, vals, x, y, accumulate, S);
+  } else if (avg >= 12.0) {
+    auto k = k_level_spmv<BR, BC, 16, T>;
+    k<<<resident_grid(k, kThreads, (M.n_rows * 16 + kThreads - 1) / kThreads), kThreads, 0, st>>>(
+        M.n_rows, M.rp.p, M.ci.p, vals, x, y, accumulate, S);
+  } else {
+    auto k = k_level_spmv<BR, BC, 8, T>;
+    k<<<resident_grid(k, kThreads, (M.n_rows * 8 + kThreads - 1) / kThreads), kThreads, 0, st>>>(
+        M.n_rows, M.rp.p, M.ci.p, vals, x, y, accumulate, S);
   }
 }
 
 // First post-smoothing step from a nonzero x: r0 = D^-1 (b - A x), d0 = r0 / theta,
 // x2 = x + d0 (x2 is a separate buffer: x is still read by neighbouring rows).
 template <int BS, typename T>
-__global__ void __launch_bounds__(kThreads) k_post_first(int64_t n_rows, const int32_t* __restrict__ rp,
-                                                         const int32_t* __restrict__ ci, const T* __restrict__ av,
+__global__ void __launch_bounds__(kThreads, (BS == 3) ? kMinBlocks : 1) k_post_first(int64_t n_rows, const int32_t* __restrict__ rp,
+                                                         const int32_t* __restrict__ ci, const T* __restrict__ av, int64_t stride,
                                                          const T* __restrict__ b, const T* __restrict__ dinv,
                                                          T inv_theta, const T* __restrict__ x, T* __restrict__ x2,
                                                          T* __restrict__ r, T* __restrict__ d, double* __restrict__ part,
@@ -198,10 +260,12 @@ __global__ void __launch_bounds__(kThreads) k_post_first(int64_t n_rows, const i
   __shared__ double sh[kThreads / 32];
   if (S->done) return;
   double dot = 0.0;
-  WARP_ROW_LOOP(n_rows) {
+  GROUP_ROW_LOOP(n_rows, GroupOf<BS>::value) {
+    const bool active = row < n_rows;
     T acc[BS];
-    warp_block_row<BS, BS, T, T>(rp, ci, av, row, XLoad<T, T>{x}, acc, lane);
-    if (lane < BS) {
+    group_block_row<BS, BS, GroupOf<BS>::value, LayoutOf<BS>::value, T, T>(rp, ci, av, stride, row, active,
+        XLoad<T, T>{x}, acc, lane);
+    if (active && lane < BS) {
       const int64_t i = row * BS + lane;
       const T r0 = dinv[i] * (b[i] - pick<BS>(acc, lane));
       const T d0 = r0 * inv_theta;
@@ -298,8 +362,8 @@ struct XPNew2 {  // p_j = z_j + beta p_old_j, z in the preconditioner's precisio
 // q = A p_new; partB = p_new . q.  Parity par = k & 1 selects the p buffers and rz slot.
 // TK: Krylov vectors / matrix precision; TM: preconditioner output precision.
 template <int BS, typename TK, typename TM>
-__global__ void __launch_bounds__(kThreads) k_spmv_dot(int64_t n_rows, const int32_t* __restrict__ rp,
-                                                       const int32_t* __restrict__ ci, const TK* __restrict__ av,
+__global__ void __launch_bounds__(kThreads, (BS == 3) ? kMinBlocks : 1) k_spmv_dot(int64_t n_rows, const int32_t* __restrict__ rp,
+                                                       const int32_t* __restrict__ ci, const TK* __restrict__ av, int64_t stride,
                                                        const TM* __restrict__ z, const TK* __restrict__ p_old,
                                                        TK* __restrict__ p_new, TK* __restrict__ q,
                                                        const double* __restrict__ partA, double* __restrict__ partB,
@@ -310,10 +374,12 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dot(int64_t n_rows, const int
   const double rz_prev = S->rz[par ^ 1];
   const TK beta = first ? TK(0) : (TK)(rz / rz_prev);
   double dot = 0.0;
-  WARP_ROW_LOOP(n_rows) {
+  GROUP_ROW_LOOP(n_rows, GroupOf<BS>::value) {
+    const bool active = row < n_rows;
     TK acc[BS];
-    warp_block_row<BS, BS, TK, TK>(rp, ci, av, row, XPNew2<TK, TM>{z, p_old, beta}, acc, lane);
-    if (lane < BS) {
+    group_block_row<BS, BS, GroupOf<BS>::value, LayoutOf<BS>::value, TK, TK>(rp, ci, av, stride, row, active,
+        XPNew2<TK, TM>{z, p_old, beta}, acc, lane);
+    if (active && lane < BS) {
       const int64_t i = row * BS + lane;
       const TK pi = (TK)z[i] + beta * p_old[i];
       const TK qi = pick<BS>(acc, lane);
@@ -401,17 +467,19 @@ __global__ void __launch_bounds__(kThreads) k_dot_self(int64_t n, const T* __res
 // ---------------------------------------------------------------------------------------
 
 // r64 = F - K64 u64, r32 = (float) r64, partC = r64 . r64
-__global__ void __launch_bounds__(kThreads) k_outer_residual(int64_t n_rows, const int32_t* __restrict__ rp,
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_outer_residual(int64_t n_rows, const int32_t* __restrict__ rp,
                                                              const int32_t* __restrict__ ci,
-                                                             const double* __restrict__ av, const double* __restrict__ F,
+                                                             const double* __restrict__ av, int64_t stride, const double* __restrict__ F,
                                                              const double* __restrict__ u, double* __restrict__ r64,
                                                              float* __restrict__ r32, double* __restrict__ partC) {
   __shared__ double sh[kThreads / 32];
   double s = 0.0;
-  WARP_ROW_LOOP(n_rows) {
+  GROUP_ROW_LOOP(n_rows, 16) {
+    const bool active = row < n_rows;
     double acc[3];
-    warp_block_row<3, 3, double, double>(rp, ci, av, row, XLoad<double, double>{u}, acc, lane);
-    if (lane < 3) {
+    group_block_row<3, 3, 16, kSoA, double, double>(rp, ci, av, stride, row, active, XLoad<double, double>{u}, acc,
+                                                    lane);
+    if (active && lane < 3) {
       const int64_t i = row * 3 + lane;
       const double ri = F[i] - pick<3>(acc, lane);
       r64[i] = ri;
@@ -429,13 +497,14 @@ __global__ void k_accumulate(int64_t n, double* __restrict__ u, const T* __restr
     u[i] += (double)dx[i];
 }
 
-__global__ void k_fill_dinv(int64_t n_rows, const int32_t* __restrict__ diag_block, const double* __restrict__ k64,
+__global__ void k_fill_dinv(int64_t n_rows, int64_t nnzb, const int32_t* __restrict__ diag_block,
+                            const double* __restrict__ k64,
                             double* __restrict__ d64, float* __restrict__ d32) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_rows * 3;
        t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t row = t / 3;
     const int c = (int)(t - row * 3);
-    const double dv = k64[(int64_t)diag_block[row] * 9 + c * 4];
+    const double dv = k64[(int64_t)(c * 4) * nnzb + diag_block[row]];  // component-major values
     const double inv = (fabs(dv) > 1e-12) ? 1.0 / dv : 1.0;  // solid_solver.py:230
     d64[t] = inv;
     d32[t] = (float)inv;
@@ -497,7 +566,8 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
                   const PcgScalars* S, cudaStream_t st) {
   const int nlev = (int)H.levels.size();
   if (lvl == nlev) {  // coarsest
-    k_coarse<T><<<rows_grid(H.n_coarse), kThreads, 0, st>>>(H.n_coarse, H.coarse_inv.p, b, out, S);
+    k_coarse<T><<<resident_grid(k_coarse<T>, kThreads, (H.n_coarse * 32 + kThreads - 1) / kThreads), kThreads, 0,
+                  st>>>(H.n_coarse, H.coarse_inv.p, b, out, S);
     W.launches++;
     return 0;
   }
@@ -507,52 +577,58 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
   const T* dinv = Prec<T>::dinv(L);
   const int deg = H.degree;
   const T it = (T)L.inv_theta;
-  const int g = rows_grid(nr);
+  const int64_t sd = (lvl == 0) ? s->nnzb : 0;  // component stride of the fine matrix
+  const int64_t work = (nr * 32 + kThreads - 1) / kThreads;
   auto run = [&](auto bs_tag) -> int {
     constexpr int BS = decltype(bs_tag)::value;
+    auto rg = [&](auto kern) { return resident_grid(kern, kThreads, work); };
     const int32_t* rp;
     const int32_t* ci;
     const T* av;
     level_A<BS, T>(s, L, lvl, rp, ci, av);
     // pre-smoothing (+ residual)
     const T c1 = deg >= 2 ? (T)L.c1[0] : T(0), c2 = deg >= 2 ? (T)L.c2[0] : T(0);
-    k_pre_first<BS, T><<<g, kThreads, 0, st>>>(nr, rp, ci, av, b, dinv, it, deg, c1, c2, V.x.p, V.r.p, V.d.p,
-                                               V.res.p, S);
+    k_pre_first<BS, T><<<rg(k_pre_first<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, deg, c1, c2,
+                                                                    V.x.p, V.r.p, V.d.p, V.res.p, S);
     W.launches++;
     T* din = V.d.p;
     T* dout = V.d2.p;
     for (int k = 2; k < deg; ++k) {
-      k_cheb_step<BS, T><<<g, kThreads, 0, st>>>(nr, rp, ci, av, dinv, din, dout, V.r.p, V.x.p, (T)L.c1[k - 1],
-                                                 (T)L.c2[k - 1], b, nullptr, S);
+      k_cheb_step<BS, T><<<rg(k_cheb_step<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout, V.r.p,
+                                                                      V.x.p, (T)L.c1[k - 1], (T)L.c2[k - 1], b,
+                                                                      nullptr, S);
       W.launches++;
       std::swap(din, dout);
     }
     if (deg >= 2) {
-      k_residual<BS, T><<<g, kThreads, 0, st>>>(nr, rp, ci, av, b, V.x.p, V.res.p, S);
+      k_residual<BS, T><<<rg(k_residual<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, V.x.p, V.res.p, S);
       W.launches++;
     }
     // restriction b_c = R res
     DevLevel* Ln = lvl + 1 < nlev ? &H.levels[lvl + 1] : nullptr;
     T* bc = Ln ? Prec<T>::vecs(*Ln).b.p : Prec<T>::cb(H);
     T* xc = Ln ? Prec<T>::vecs(*Ln).x2.p : Prec<T>::cx(H);
-    k_level_spmv<6, BS, T><<<rows_grid(L.R.n_rows), kThreads, 0, st>>>(L.R.n_rows, L.R.rp.p, L.R.ci.p,
-                                                                        Prec<T>::Rv(L), V.res.p, bc, 0, S);
+    level_spmv<6, BS, T>(L.R, Prec<T>::Rv(L), V.res.p, bc, 0, S, st);
     W.launches++;
     WN_CHECK(vcycle<T>(s, H, W, lvl + 1, bc, xc, nullptr, S, st));
     // prolongation x += P x_c
-    k_level_spmv<BS, 6, T><<<g, kThreads, 0, st>>>(nr, L.P.rp.p, L.P.ci.p, Prec<T>::Pv(L), xc, V.x.p, 1, S);
+    level_spmv<BS, 6, T>(L.P, Prec<T>::Pv(L), xc, V.x.p, 1, S, st);
     W.launches++;
     // post-smoothing: result in `out`
     double* part_last = (deg == 1) ? part : nullptr;
-    k_post_first<BS, T><<<(part_last ? SolverWork::kParts : g), kThreads, 0, st>>>(nr, rp, ci, av, b, dinv, it, V.x.p,
-                                                                                   out, V.r.p, V.d.p, part_last, S);
+    const int gpf = rg(k_post_first<BS, T>);
+    if (part_last) W.npA = gpf;
+    k_post_first<BS, T><<<gpf, kThreads, 0, st>>>(
+        nr, rp, ci, av, sd, b, dinv, it, V.x.p, out, V.r.p, V.d.p, part_last, S);
     W.launches++;
     din = V.d.p;
     dout = V.d2.p;
     for (int k = 1; k < deg; ++k) {
       double* pk = (k == deg - 1) ? part : nullptr;
-      k_cheb_step<BS, T><<<(pk ? SolverWork::kParts : g), kThreads, 0, st>>>(
-          nr, rp, ci, av, dinv, din, dout, V.r.p, out, (T)L.c1[k - 1], (T)L.c2[k - 1], b, pk, S);
+      const int gcs = rg(k_cheb_step<BS, T>);
+      if (pk) W.npA = gcs;
+      k_cheb_step<BS, T><<<gcs, kThreads, 0, st>>>(
+          nr, rp, ci, av, sd, dinv, din, dout, V.r.p, out, (T)L.c1[k - 1], (T)L.c2[k - 1], b, pk, S);
       W.launches++;
       std::swap(din, dout);
     }
@@ -572,7 +648,9 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
 template <typename T>
 static int apply_prec(Solid* s, SolverWork& W, int precond, const T* r, T* z, const PcgScalars* S, cudaStream_t st) {
   if (precond == 2) return vcycle<T>(s, *s->amg, W, 0, r, z, W.partA.p, S, st);
-  k_prec_vec<T><<<SolverWork::kParts, kThreads, 0, st>>>(W.n, r, Prec<T>::fine_dinv(W), precond == 1 ? 1 : 0, z,
+  const int gp = resident_grid(k_prec_vec<T>, kThreads, (W.n + kThreads - 1) / kThreads);
+  W.npA = gp;
+  k_prec_vec<T><<<gp, kThreads, 0, st>>>(W.n, r, Prec<T>::fine_dinv(W), precond == 1 ? 1 : 0, z,
                                                          W.partA.p, S);
   W.launches++;
   WN_CUDA(cudaGetLastError());
@@ -617,12 +695,15 @@ static int pcg_iteration(Solid* s, SolverWork& W, int precond, int k, PcgScalars
   const int par = k & 1;
   TK* p_new = par ? B.p1 : B.p0;
   TK* p_old = par ? B.p0 : B.p1;
-  k_spmv_dot<3, TK, TM><<<SolverWork::kParts, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, B.A, B.z,
+  const int gsd = resident_grid(k_spmv_dot<3, TK, TM>, kThreads, (s->n_nodes * 32 + kThreads - 1) / kThreads);
+  const int gup = resident_grid(k_update<TK, TM>, kThreads, (W.n + kThreads - 1) / kThreads);
+  k_spmv_dot<3, TK, TM><<<gsd, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, B.A, s->nnzb, B.z,
                                                                  p_old, p_new, B.q, W.partA.p, W.partB.p,
-                                                                 SolverWork::kParts, k == 0, par, S);
-  k_update<TK, TM><<<SolverWork::kParts, kThreads, 0, st>>>(W.n, B.x, B.r, B.rm, p_new, B.q, W.partB.p, W.partC.p,
-                                                            SolverWork::kParts, par, S);
-  k_check<<<1, kThreads, 0, st>>>(S, W.partC.p, SolverWork::kParts);
+                                                                 W.npA, k == 0, par, S);
+  W.npB = gsd;
+  k_update<TK, TM><<<gup, kThreads, 0, st>>>(W.n, B.x, B.r, B.rm, p_new, B.q, W.partB.p, W.partC.p, W.npB, par, S);
+  W.npC = gup;
+  k_check<<<1, kThreads, 0, st>>>(S, W.partC.p, W.npC);
   W.launches += 3;
   WN_CUDA(cudaGetLastError());
   return apply_prec<TM>(s, W, precond, prec_input(B), B.z, S, st);
@@ -637,8 +718,9 @@ static int pcg_solve(Solid* s, SolverWork& W, int mode, const TK* b, double rtol
   PcgBufs<TK, TM> B = pcg_bufs<TK, TM>(s, W);
   WN_CUDA(cudaMemsetAsync(B.p0, 0, W.n * sizeof(TK), st));  // iteration 0: p = z + 0 * p_old
   WN_CUDA(cudaMemsetAsync(B.p1, 0, W.n * sizeof(TK), st));
-  k_init_vecs<TK, TM><<<SolverWork::kParts, kThreads, 0, st>>>(W.n, b, B.x, B.r, B.rm, W.partC.p);
-  k_init_scalars<<<1, kThreads, 0, st>>>(S, W.partC.p, SolverWork::kParts, rtol, max_iter);
+  W.npC = resident_grid(k_init_vecs<TK, TM>, kThreads, (W.n + kThreads - 1) / kThreads);
+  k_init_vecs<TK, TM><<<W.npC, kThreads, 0, st>>>(W.n, b, B.x, B.r, B.rm, W.partC.p);
+  k_init_scalars<<<1, kThreads, 0, st>>>(S, W.partC.p, W.npC, rtol, max_iter);
   W.launches += 2;
   WN_CUDA(cudaGetLastError());
   WN_CHECK(apply_prec<TM>(s, W, precond, prec_input(B), B.z, S, st));
@@ -732,9 +814,9 @@ static int ensure_work(Solid* s) {
     for (auto& a : W.graphs)
       for (auto& g : a) g.reset();
   }
-  WN_CHECK(W.partA.alloc(SolverWork::kParts));
-  WN_CHECK(W.partB.alloc(SolverWork::kParts));
-  WN_CHECK(W.partC.alloc(SolverWork::kParts));
+  WN_CHECK(W.partA.alloc(SolverWork::kMaxParts));
+  WN_CHECK(W.partB.alloc(SolverWork::kMaxParts));
+  WN_CHECK(W.partC.alloc(SolverWork::kMaxParts));
   WN_CHECK(W.scal.alloc(2));
   if (!W.ev0) {
     WN_CUDA(cudaEventCreate(&W.ev0));
@@ -748,8 +830,11 @@ int solver_setup(Solid* s, const wn_amg_params& prm) {
   WN_REQUIRE(prm.smoother_degree >= 1 && prm.smoother_degree <= 8, WN_EINVAL, "AMG setup: smoother_degree in [1, 8]");
   WN_REQUIRE(prm.max_levels >= 1 && prm.max_levels <= 16, WN_EINVAL, "AMG setup: max_levels in [1, 16]");
   const auto t0 = std::chrono::steady_clock::now();
-  std::vector<double> vals(s->nnzb * 9);
-  WN_CUDA(cudaMemcpy(vals.data(), s->k64.p, vals.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  std::vector<double> soa(s->nnzb * 9), vals(s->nnzb * 9);
+  WN_CUDA(cudaMemcpy(soa.data(), s->k64.p, soa.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int64_t b = 0; b < s->nnzb; ++b)  // component-major on the device -> row-major blocks
+    for (int k = 0; k < 9; ++k) vals[b * 9 + k] = soa[k * s->nnzb + b];
+  std::vector<double>().swap(soa);
   std::unique_ptr<AmgHierarchy> H(new AmgHierarchy());
   const uint8_t* fixed = s->bcs_applied ? s->h_fixed.data() : nullptr;
   WN_CHECK(amg_build(prm, s->n_nodes, s->h_row_ptr.data(), s->h_col_idx.data(), vals.data(), s->h_nodes.data(),
@@ -797,9 +882,10 @@ int solver_setup(Solid* s, const wn_amg_params& prm) {
 // ---------------------------------------------------------------------------------------
 static int true_residual(Solid* s, SolverWork& W, const double* F, const double* u, float* r32, cudaStream_t st,
                          double* rr) {
-  k_outer_residual<<<SolverWork::kParts, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, F, u,
+  W.npC = resident_grid(k_outer_residual, kThreads, (s->n_nodes * 32 + kThreads - 1) / kThreads);
+  k_outer_residual<<<W.npC, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, s->nnzb, F, u,
                                                             W.r64.p, r32, W.partC.p);
-  k_reduce_rr<<<1, kThreads, 0, st>>>(W.scal.p + 1, W.partC.p, SolverWork::kParts);
+  k_reduce_rr<<<1, kThreads, 0, st>>>(W.scal.p + 1, W.partC.p, W.npC);
   W.launches += 2;
   WN_CUDA(cudaGetLastError());
   PcgScalars h;
@@ -887,11 +973,13 @@ int solver_solve(Solid* s, const double* F, double* u, const wn_solve_params& pr
   const int64_t n = W.n;
   const int chunk = prm.chunk > 0 ? prm.chunk : 8;
   PcgScalars hS{};
-  k_fill_dinv<<<vec_grid(n), kThreads, 0, st>>>(s->n_nodes, s->diag_block.p, s->k64.p, W.dinv64.p, W.dinv32.p);
+  k_fill_dinv<<<vec_grid(n), kThreads, 0, st>>>(s->n_nodes, s->nnzb, s->diag_block.p, s->k64.p, W.dinv64.p,
+                                                 W.dinv32.p);
   W.launches++;
   WN_CUDA(cudaEventRecord(W.ev0, st));
-  k_dot_self<double><<<SolverWork::kParts, kThreads, 0, st>>>(n, F, W.partC.p);
-  k_reduce_rr<<<1, kThreads, 0, st>>>(W.scal.p + 1, W.partC.p, SolverWork::kParts);
+  W.npC = resident_grid(k_dot_self<double>, kThreads, (n + kThreads - 1) / kThreads);
+  k_dot_self<double><<<W.npC, kThreads, 0, st>>>(n, F, W.partC.p);
+  k_reduce_rr<<<1, kThreads, 0, st>>>(W.scal.p + 1, W.partC.p, W.npC);
   W.launches += 2;
   WN_CUDA(cudaMemcpyAsync(&hS, W.scal.p + 1, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
   WN_CUDA(cudaStreamSynchronize(st));

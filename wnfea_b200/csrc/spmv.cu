@@ -1,42 +1,57 @@
 // Stand-alone BSR SpMV kernels y = alpha * A x + beta * y for the block shapes of the solve
 // path (3x3 solid, 6x6 beam / coarse levels, 3x6 prolongation, 6x3 restriction), FP64
 // values with FP64 accumulation and FP32 values with FP32 accumulation.  One warp per
-// block row, grid sized to whole waves of the 148 SMs (grid-stride over rows).
+// block row (16 lanes for the 3x3 fine matrix), one resident wave of CTAs (grid-stride).
 #include "common.cuh"
 #include "kernels.h"
 #include "spmv.cuh"
 
 namespace wn {
 
-template <int BR, int BC, typename T>
+template <int BR, int BC, int G, Layout L, typename T>
 __global__ void __launch_bounds__(256) bsr_spmv_kernel(int64_t n_rows, const int32_t* __restrict__ row_ptr,
                                                        const int32_t* __restrict__ col_idx, const T* __restrict__ vals,
-                                                       const T* __restrict__ x, T* __restrict__ y, T alpha, T beta) {
-  const int lane = threadIdx.x & 31;
+                                                       int64_t stride, const T* __restrict__ x, T* __restrict__ y,
+                                                       T alpha, T beta) {
+  constexpr int RPW = 32 / G;  // block rows per warp
+  const int gl = (threadIdx.x & 31) % G, grp = (threadIdx.x & 31) / G;
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t row = warp; row < n_rows; row += nwarps) {
+  for (int64_t rb = warp; rb * RPW < n_rows; rb += nwarps) {
+    const int64_t row = rb * RPW + grp;
+    const bool active = row < n_rows;
     T acc[BR];
-    warp_block_row<BR, BC, T, T>(row_ptr, col_idx, vals, row, XLoad<T, T>{x}, acc, lane);
-    if (lane < BR) {
+    group_block_row<BR, BC, G, L, T, T>(row_ptr, col_idx, vals, stride, row, active, XLoad<T, T>{x}, acc, gl);
+    if (active && gl < BR) {
       T v = acc[0];
 #pragma unroll
       for (int r = 1; r < BR; ++r)
-        if (lane == r) v = acc[r];
-      const int64_t o = row * BR + lane;
+        if (gl == r) v = acc[r];
+      const int64_t o = row * BR + gl;
       y[o] = (beta == T(0)) ? alpha * v : alpha * v + beta * y[o];
     }
   }
 }
 
-template <int BR, int BC, typename T>
+// G = 16 lanes per row for the 3x3 fine matrix (rows of ~25 blocks), a full warp otherwise
+template <int BR, int BC, typename T, Layout L = kAoS, int G = 32>
 static int launch(int64_t n_rows, const int32_t* rp, const int32_t* ci, const T* v, const T* x, T* y, T a, T b,
-                  cudaStream_t st) {
+                  cudaStream_t st, int64_t stride = 0) {
   if (n_rows == 0) return 0;
-  const int grid = grid_for(n_rows, 32, 256, 16);
-  bsr_spmv_kernel<BR, BC, T><<<grid, 256, 0, st>>>(n_rows, rp, ci, v, x, y, a, b);
+  const int grid = resident_grid(bsr_spmv_kernel<BR, BC, G, L, T>, 256, (n_rows * G + 255) / 256);
+  bsr_spmv_kernel<BR, BC, G, L, T><<<grid, 256, 0, st>>>(n_rows, rp, ci, v, stride, x, y, a, b);
   WN_CUDA(cudaGetLastError());
   return 0;
+}
+
+int launch_solid_spmv_f64(int64_t n_rows, const int32_t* rp, const int32_t* ci, const double* v, int64_t nnzb,
+                          const double* x, double* y, cudaStream_t st) {
+  return launch<3, 3, double, kSoA, 16>(n_rows, rp, ci, v, x, y, 1.0, 0.0, st, nnzb);
+}
+
+int launch_solid_spmv_f32(int64_t n_rows, const int32_t* rp, const int32_t* ci, const float* v, int64_t nnzb,
+                          const float* x, float* y, cudaStream_t st) {
+  return launch<3, 3, float, kSoA, 16>(n_rows, rp, ci, v, x, y, 1.0f, 0.0f, st, nnzb);
 }
 
 int launch_bsr_spmv_f64(int br, int bc, int64_t n_rows, const int32_t* rp, const int32_t* ci, const double* v,
