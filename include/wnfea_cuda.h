@@ -253,6 +253,47 @@ int wn_stress_c3d10_device(void* h, const double* d_u, double* d_cell_sig, doubl
 int wn_adjoint_compliance_device(void* h, const double* d_u, double* d_grad_E, double* d_grad_F, uintptr_t stream);
 int wn_adjoint_compliance(void* h, const double* u, double* grad_E, double* grad_F);
 
+/* ---------------------------------------------------------------------------------------
+ * Co-rotational 3D beam frames (6 DOFs per node [ux, uy, uz, rx, ry, rz]).
+ * Element data as prepare_batch_data builds it (wnfea/solver/fast_kernels.py:263-306):
+ * elements n_el x 2, props n_el x 6 [E, G, A, Iy, Iz, J], e_ref n_el x 9 (reference triad
+ * rows e1, e2, e3), L0 n_el.
+ * ------------------------------------------------------------------------------------- */
+
+/* F_int += f_int(U) -- same argument list as the reference's
+ * compute_beam_internal_forces_native (wnfea/solver/native/kernels.cpp:19-29); host
+ * buffers, computed on the GPU with an atomic-free node gather. */
+int wn_beam_internal_forces(const double* nodes, const int32_t* elements, const double* props, const double* e_ref,
+                            const double* L0_arr, const double* U, double* F_int, int n_elements, int n_nodes);
+
+/* Frame handle: element data on the device plus the 6x6-block pattern of the tangent (block
+ * (i, j) iff i == j or a beam joins i and j) and its gather lists. */
+int wn_beam_create(int64_t n_nodes, int64_t n_el, const double* nodes, const int32_t* elements, const double* props,
+                   const double* e_ref, const double* L0, void** out);
+int wn_beam_destroy(void* h);
+int wn_beam_info(void* h, int64_t* n_nodes, int64_t* n_el, int64_t* nnzb);
+int wn_beam_get_pattern(void* h, int32_t* row_ptr, int32_t* col_idx);
+/* Dirichlet mask over the 6 n DOFs (1 = constrained; NULL clears). */
+int wn_beam_set_fixed(void* h, const uint8_t* fixed_mask);
+/* f_int(U) into fint (6 n, overwritten; NULL to skip) and, if assemble_tangent, the
+ * consistent tangent K_t = d f_int / d U (exact derivative of the force code, not a finite
+ * difference; cf. the JFNK operator, wnfea/solver/jfnk_operator.py:98-134) into the
+ * handle's BSR6 values; apply_bcs != 0 turns constrained rows/columns into identity. */
+int wn_beam_evaluate_device(void* h, const double* d_U, double* d_fint, int assemble_tangent, int apply_bcs,
+                            uintptr_t stream);
+int wn_beam_evaluate(void* h, const double* U, double* fint, int assemble_tangent, int apply_bcs);
+/* Host copy of the tangent values: nnzb x 36, row-major 6x6 blocks. */
+int wn_beam_get_tangent(void* h, double* values);
+/* Solve K_t x = b (K_t is not symmetric away from U = 0).  method 1: dense LU with partial
+ * pivoting on one CTA (frames up to WN_BEAM_DENSE_MAX DOFs); 2: BiCGStab preconditioned by
+ * the inverse 6x6 diagonal blocks (rtol, max_iter); 0: dense when it fits, else BiCGStab.
+ * Returns WN_ENOCONV / WN_EBREAKDOWN (singular) as status; rel_res = ||b - K x|| / ||b||. */
+#define WN_BEAM_DENSE_MAX 3072
+int wn_beam_solve_device(void* h, const double* d_b, double* d_x, int method, double rtol, int max_iter, int* iters,
+                         double* rel_res, uintptr_t stream);
+int wn_beam_solve(void* h, const double* rhs, double* x, int method, double rtol, int max_iter, int* iters,
+                  double* rel_res);
+
 /* Block until all work of the calling thread's device is done. */
 int wn_device_synchronize(void);
 

@@ -17,6 +17,14 @@ from .model import (
     create_fixed_support,
     create_rectangular_bar,
 )
+from .autograd import Compliance, ComplianceProblem
+from .beam import (
+    BeamFrame,
+    NonLinearConvergenceError,
+    compute_internal_forces_fast,
+    prepare_batch_data,
+    solve_nonlinear_jfnk,
+)
 from .mixed_precision import FULL_FP64, MIXED_FP32, TRI_PRECISION, PrecisionConfig
 from .solid_solver import (
     assemble_c3d10_sparse_3dof,
@@ -30,4 +38,6 @@ __all__ = [
     "SupportDef", "LoadDef", "DOFConstraint", "DOFType", "create_fixed_support", "create_rectangular_bar",
     "assemble_c3d10_sparse_3dof", "compute_c3d10_stress_field", "solve_c3d10_pcg", "solve_c3d10_system",
     "PrecisionConfig", "MIXED_FP32", "FULL_FP64", "TRI_PRECISION",
+    "compute_internal_forces_fast", "prepare_batch_data", "solve_nonlinear_jfnk", "NonLinearConvergenceError",
+    "BeamFrame", "ComplianceProblem", "Compliance",
 ]

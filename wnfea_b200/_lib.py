@@ -114,6 +114,17 @@ SIGNATURES: dict[str, tuple] = {
     "wn_amg_host_coarse": (_I, [_P, _PI64, _P, _P]),
     "wn_solve_device": (_I, [_P, _P, _P, C.POINTER(SolveParams), C.POINTER(SolveStats), _U]),
     "wn_solve": (_I, [_P, _P, _P, C.POINTER(SolveParams), C.POINTER(SolveStats)]),
+    "wn_beam_internal_forces": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I]),
+    "wn_beam_create": (_I, [_I64, _I64, _P, _P, _P, _P, _P, C.POINTER(_P)]),
+    "wn_beam_destroy": (_I, [_P]),
+    "wn_beam_info": (_I, [_P, _PI64, _PI64, _PI64]),
+    "wn_beam_get_pattern": (_I, [_P, _P, _P]),
+    "wn_beam_set_fixed": (_I, [_P, _P]),
+    "wn_beam_evaluate_device": (_I, [_P, _P, _P, _I, _I, _U]),
+    "wn_beam_evaluate": (_I, [_P, _P, _P, _I, _I]),
+    "wn_beam_get_tangent": (_I, [_P, _P]),
+    "wn_beam_solve_device": (_I, [_P, _P, _P, _I, _D, _I, _PI, _PD, _U]),
+    "wn_beam_solve": (_I, [_P, _P, _P, _I, _D, _I, _PI, _PD]),
 }
 
 LIB_PATH = Path(__file__).resolve().parent / "libwnfea_cuda.so"

@@ -574,7 +574,9 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
   DevLevel& L = H.levels[lvl];
   LevelVecs<T>& V = Prec<T>::vecs(L);
   const int64_t nr = L.n_nodes;
-  const T* dinv = Prec<T>::dinv(L);
+  // level 0: 1/diag of the current matrix (refreshed per solve), so a hierarchy kept across
+  // re-assemblies still smooths with the right diagonal
+  const T* dinv = (lvl == 0) ? Prec<T>::fine_dinv(W) : Prec<T>::dinv(L);
   const int deg = H.degree;
   const T it = (T)L.inv_theta;
   const int64_t sd = (lvl == 0) ? s->nnzb : 0;  // component stride of the fine matrix
@@ -1022,6 +1024,8 @@ int amg_vcycle(Solid* s, int precision, const void* r, void* z, cudaStream_t st)
   WN_REQUIRE(s->amg, WN_ESTATE, "vcycle: no AMG hierarchy (call wn_amg_setup)");
   WN_CHECK(ensure_work(s));
   SolverWork& W = *s->work;
+  k_fill_dinv<<<vec_grid(W.n), kThreads, 0, st>>>(s->n_nodes, s->nnzb, s->diag_block.p, s->k64.p, W.dinv64.p,
+                                                  W.dinv32.p);
   WN_CUDA(cudaMemsetAsync(W.scal.p, 0, sizeof(PcgScalars), st));  // done = 0
   if (precision == 0)
     return vcycle<double>(s, *s->amg, W, 0, (const double*)r, (double*)z, nullptr, W.scal.p, st);

@@ -263,3 +263,58 @@ def generate_c3d10_ibeam_structured(
         "tip_nodes_loaded": int(tip.sum()),
     }
     return model, meta
+
+
+# face corner triples of a C3D10 (local indices) and their mid-edge nodes
+_FACES = (((0, 1, 2), (4, 5, 6)), ((0, 1, 3), (4, 8, 7)), ((1, 2, 3), (5, 9, 8)), ((0, 2, 3), (6, 9, 7)))
+
+
+def face_pressure_loads(coords: np.ndarray, conn: np.ndarray, axis: int, value: float, pressure: float,
+                        tol: float = 1e-9) -> np.ndarray:
+    """Consistent nodal forces (n, 3) of a uniform pressure on the element faces lying in the
+    plane coords[:, axis] == value, pushing towards -axis for pressure > 0.
+
+    A flat quadratic (6-node) triangle of area A under uniform traction t carries 0 at its
+    corners and t A / 3 at each mid-edge node (the integrals of the quadratic triangle's
+    shape functions).
+    """
+    F = np.zeros((len(coords), 3))
+    on = np.abs(coords[:, axis] - value) <= tol * max(1.0, abs(value))
+    for corners, mids in _FACES:
+        c = conn[:, corners]
+        sel = on[c].all(axis=1)
+        if not sel.any():
+            continue
+        p = coords[c[sel]]
+        area = 0.5 * np.linalg.norm(np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]), axis=1)
+        m = conn[sel][:, mids]
+        np.add.at(F[:, axis], m.ravel(), np.repeat(-pressure * area / 3.0, 3))
+    return F
+
+
+def generate_c3d10_pressure_block(
+    length: float = 2.0,
+    width: float = 1.0,
+    height: float = 0.5,
+    nx: int = 60,
+    ny: int = 30,
+    nz: int = 15,
+    e_min: float = 1e9,
+    e_max: float = 210e9,
+    nu: float = 0.3,
+    pressure: float = 10e3,
+    seed: int = 0,
+) -> tuple[FEAModel, dict]:
+    """Kuhn block (6 tets per hex) with per-element E log-uniform in [e_min, e_max] (seeded),
+    the z = 0 face clamped and a uniform pressure on the z = height face, applied as
+    consistent quadratic-face nodal loads.  60 x 30 x 15 hexes give 162,000 elements."""
+    model, meta = generate_c3d10_kuhn_block(length, width, height, nx, ny, nz, E=e_max, nu=nu, tip_force=None,
+                                            clamp="z0")
+    rng = np.random.default_rng(seed)
+    E = np.exp(rng.uniform(np.log(e_min), np.log(e_max), size=len(model.solid_elements)))
+    model.solid_props = np.column_stack([E, np.full_like(E, nu)])
+    F = face_pressure_loads(model.mesh_nodes, model.solid_elements, 2, height, pressure)
+    model.loads = [LoadDef(node_id=int(i), is_geometry_node=False, fx=F[i, 0], fy=F[i, 1], fz=F[i, 2])
+                   for i in np.nonzero(np.abs(F).sum(axis=1))[0]]
+    meta["total_load"] = float(F[:, 2].sum())
+    return model, meta
