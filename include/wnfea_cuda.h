@@ -183,6 +183,19 @@ int wn_solve_device(void* h, const double* d_F, double* d_u, const wn_solve_para
 /* Host buffers F, u (copies in and out). */
 int wn_solve(void* h, const double* F, double* u, const wn_solve_params* params, wn_solve_stats* stats);
 
+/* Multi-right-hand-side solve (no reference counterpart: the reference solves load cases one
+ * solve_c3d10_pcg call at a time, solid_solver.py:197-308).  F, U: row-major n x n_rhs
+ * (n = 3 n_nodes, load case j in column j).  Cases are solved in batches of 32 sharing every
+ * matrix read; each case keeps its own PCG recurrence and stops at its own
+ * ||F_j - K U_j|| <= rtol ||F_j|| (FP64 true residual).  precision 0: FP64 V-cycle; 1: FP32
+ * V-cycle inside the FP64 PCG.  stats: iterations = batched iterations summed over batches,
+ * status = worst case, rel_res = largest case residual.  case_iters / case_rel_res: optional
+ * host arrays of n_rhs entries. */
+int wn_solve_multi_device(void* h, int n_rhs, const double* d_F, double* d_U, const wn_solve_params* params,
+                          wn_solve_stats* stats, int* case_iters, double* case_rel_res, uintptr_t stream);
+int wn_solve_multi(void* h, int n_rhs, const double* F, double* U, const wn_solve_params* params,
+                   wn_solve_stats* stats, int* case_iters, double* case_rel_res);
+
 /* ---------------------------------------------------------------------------------------
  * Generic block SpMV, y = alpha*A*x + beta*y (cf. hip_spmv_bsr6x6_fp32/_fp64,
  * hip_kernels.cpp:2975-3087, whose CPU reference is bsr6x6_spmv_cpu, bsr_matrix.py:155-193).

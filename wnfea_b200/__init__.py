@@ -29,6 +29,7 @@ from .mixed_precision import FULL_FP64, MIXED_FP32, TRI_PRECISION, PrecisionConf
 from .solid_solver import (
     assemble_c3d10_sparse_3dof,
     compute_c3d10_stress_field,
+    solve_c3d10_multi,
     solve_c3d10_pcg,
     solve_c3d10_system,
 )
@@ -37,6 +38,7 @@ __all__ = [
     "FEAModel", "MaterialDef", "SectionDef", "PropertyAssignment",
     "SupportDef", "LoadDef", "DOFConstraint", "DOFType", "create_fixed_support", "create_rectangular_bar",
     "assemble_c3d10_sparse_3dof", "compute_c3d10_stress_field", "solve_c3d10_pcg", "solve_c3d10_system",
+    "solve_c3d10_multi",
     "PrecisionConfig", "MIXED_FP32", "FULL_FP64", "TRI_PRECISION",
     "compute_internal_forces_fast", "prepare_batch_data", "solve_nonlinear_jfnk", "NonLinearConvergenceError",
     "BeamFrame", "ComplianceProblem", "Compliance",

@@ -65,6 +65,7 @@ struct AmgHierarchy {
   DArray<float> cb32, cx32;   // (FP32 path)
   int degree = 2;
   double setup_seconds = 0.0;
+  uint64_t id = 0;  // unique per setup (workspaces sized for a hierarchy compare it)
 };
 
 // PCG scalars shared between kernels (device)

@@ -9,6 +9,7 @@
 #include "wnfea_cuda.h"
 #include "common.cuh"
 #include "amg.h"
+#include "block.h"
 #include "kernels.h"
 #include "solid.h"
 

@@ -183,4 +183,27 @@ int wn_solve(void* h, const double* F, double* u, const wn_solve_params* params,
   return 0;
 }
 
+int wn_solve_multi_device(void* h, int n_rhs, const double* d_F, double* d_U, const wn_solve_params* params,
+                          wn_solve_stats* stats, int* case_iters, double* case_rel_res, uintptr_t stream) {
+  WN_REQUIRE(h && params && n_rhs >= 0 && (n_rhs == 0 || (d_F && d_U)), WN_EINVAL,
+             "wn_solve_multi_device: bad argument");
+  Solid* s = reinterpret_cast<Solid*>(h);
+  WN_CUDA(cudaSetDevice(s->device));
+  return solver_solve_multi(s, n_rhs, d_F, d_U, *params, stats, case_iters, case_rel_res, (cudaStream_t)stream);
+}
+
+int wn_solve_multi(void* h, int n_rhs, const double* F, double* U, const wn_solve_params* params,
+                   wn_solve_stats* stats, int* case_iters, double* case_rel_res) {
+  WN_REQUIRE(h && params && n_rhs >= 0 && (n_rhs == 0 || (F && U)), WN_EINVAL, "wn_solve_multi: bad argument");
+  Solid* s = reinterpret_cast<Solid*>(h);
+  WN_CUDA(cudaSetDevice(s->device));
+  const int64_t n = s->n_nodes * 3 * (int64_t)n_rhs;
+  DArray<double> dF, dU;
+  WN_CHECK(dF.upload(F, n));
+  WN_CHECK(dU.alloc(n));
+  WN_CHECK(solver_solve_multi(s, n_rhs, dF.p, dU.p, *params, stats, case_iters, case_rel_res, 0));
+  if (n) WN_CUDA(cudaMemcpy(U, dU.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
 }  // extern "C"

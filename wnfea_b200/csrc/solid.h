@@ -14,6 +14,7 @@ namespace wn {
 
 struct AmgHierarchy;  // amg.h
 struct SolverWork;    // solver.cu
+struct BlockWork;     // block.h
 
 struct Solid {
   int device = 0;
@@ -42,6 +43,7 @@ struct Solid {
   bool bcs_applied = false;
   std::unique_ptr<AmgHierarchy> amg;
   std::unique_ptr<SolverWork> work;
+  std::unique_ptr<BlockWork> bwork;
   ~Solid();
 };
 

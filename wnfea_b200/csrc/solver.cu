@@ -842,6 +842,8 @@ int solver_setup(Solid* s, const wn_amg_params& prm) {
   WN_CHECK(amg_build(prm, s->n_nodes, s->h_row_ptr.data(), s->h_col_idx.data(), vals.data(), s->h_nodes.data(),
                      fixed, H->host));
   H->degree = prm.smoother_degree;
+  static uint64_t next_id = 0;
+  H->id = ++next_id;
   H->levels.resize(H->host.levels.size());
   for (size_t l = 0; l < H->host.levels.size(); ++l) {
     const HostLevel& h = H->host.levels[l];

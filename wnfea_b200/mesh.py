@@ -265,6 +265,23 @@ def generate_c3d10_ibeam_structured(
     return model, meta
 
 
+def tip_load_cases(coords: np.ndarray, n_cases: int = 32, seed: int = 0, f_min: float = 1e4, f_max: float = 1e5,
+                   axis: int = 0) -> np.ndarray:
+    """Seeded batch of tip load cases (3 n_nodes, n_cases): case j is a total force of magnitude
+    U[f_min, f_max] along a direction uniform on the unit sphere (a normalised Gaussian),
+    shared equally over the nodes of the far end (coords[:, axis] == max)."""
+    rng = np.random.default_rng(seed)
+    d = rng.standard_normal((n_cases, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    mag = rng.uniform(f_min, f_max, size=n_cases)
+    x = coords[:, axis]
+    tip = np.flatnonzero(x >= x.max() - 1e-9 * max(1.0, abs(x.max())))
+    F = np.zeros((3 * len(coords), n_cases))
+    for c in range(3):
+        F[3 * tip + c, :] = (d[:, c] * mag / len(tip))[None, :]
+    return F
+
+
 # face corner triples of a C3D10 (local indices) and their mid-edge nodes
 _FACES = (((0, 1, 2), (4, 5, 6)), ((0, 1, 3), (4, 8, 7)), ((1, 2, 3), (5, 9, 8)), ((0, 2, 3), (6, 9, 7)))
 

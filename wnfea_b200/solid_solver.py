@@ -103,6 +103,39 @@ def solve_c3d10_pcg(
     return u, st["iterations"], st["rel_res"], time.perf_counter() - t0
 
 
+def solve_c3d10_multi(
+    K: BSR3Matrix,
+    F: np.ndarray,
+    rtol: float = 1e-8,
+    max_iter: int = 2000,
+    preconditioner: str = "amg",
+    precision: str = "mixed_fp32",
+    amg_params=None,
+    chunk: int = 8,
+):
+    """Several load cases at once -> (U, stats); F is (n, k), one load case per column.
+
+    No reference counterpart: the reference runs solve_c3d10_pcg once per load case
+    (solid_solver.py:197-308).  Here the cases go through the GPU in batches of 32 that share
+    every matrix read, each case with its own PCG recurrence and its own stopping test on the
+    FP64 true residual.  ``precision``: "fp64" or "mixed_fp32" (FP32 V-cycle in FP64 PCG).
+    stats adds ``case_iterations`` and ``case_rel_res`` (arrays of k).
+    """
+    if preconditioner not in _PRECOND:
+        raise ValueError(f"preconditioner must be one of {sorted(_PRECOND)}, got {preconditioner!r}")
+    if precision not in ("fp64", "mixed_fp32"):
+        raise ValueError(f"precision must be 'fp64' or 'mixed_fp32' for several load cases, got {precision!r}")
+    system = K.system
+    if preconditioner == "amg" and (amg_params is not None or not system.amg_ready):
+        system.amg_setup(amg_params)
+    U, st = system.solve_multi(F, rtol=rtol, max_iter=max_iter, precond=_PRECOND[preconditioner],
+                               precision=_PRECISION[precision], chunk=chunk)
+    if st["status"] == -4:
+        raise RuntimeError("PCG breakdown (p^T K p <= 0 or non-finite): matrix not SPD?")
+    K.last_stats = st
+    return U, st
+
+
 def solve_c3d10_system(
     K: BSR3Matrix,
     F: np.ndarray,

@@ -105,6 +105,41 @@ class SolidSystem:
         call("wn_solve", self._h, ptr(F), ptr(u), C.byref(prm), C.byref(st))
         return u, {f: getattr(st, f) for f, _ in _lib.SolveStats._fields_}
 
+    def solve_multi(self, F: np.ndarray, rtol: float = 1e-8, max_iter: int = 2000, precond: int = 2,
+                    precision: int = 1, max_outer: int = 10, chunk: int = 8, use_graph: bool = True):
+        """Solve K U = F for the load cases in the columns of F (n x k, host) in batches of 32
+        sharing every matrix read; returns (U, stats dict with per-case 'case_iterations' and
+        'case_rel_res')."""
+        F = np.ascontiguousarray(F, dtype=np.float64)
+        if F.ndim == 1:
+            F = F[:, None]
+        k = F.shape[1]
+        U = np.empty_like(F)
+        prm = _lib.SolveParams(rtol, max_iter, precond, precision, 0.0, max_outer, chunk, int(use_graph))
+        st = _lib.SolveStats()
+        its = np.zeros(k, dtype=np.int32)
+        rel = np.zeros(k)
+        call("wn_solve_multi", self._h, k, ptr(F), ptr(U), C.byref(prm), C.byref(st), ptr(its), ptr(rel))
+        out = {f: getattr(st, f) for f, _ in _lib.SolveStats._fields_}
+        out["case_iterations"] = its
+        out["case_rel_res"] = rel
+        return U, out
+
+    def solve_multi_device(self, F, U, rtol: float = 1e-8, max_iter: int = 2000, precond: int = 2,
+                           precision: int = 1, max_outer: int = 10, chunk: int = 8, stream: int = 0):
+        """Device-pointer variant: F, U are CUDA tensors of shape (n, k), row-major, float64."""
+        k = int(F.shape[1])
+        prm = _lib.SolveParams(rtol, max_iter, precond, precision, 0.0, max_outer, chunk, 1)
+        st = _lib.SolveStats()
+        its = np.zeros(k, dtype=np.int32)
+        rel = np.zeros(k)
+        call("wn_solve_multi_device", self._h, k, _lib.dptr(F), _lib.dptr(U), C.byref(prm), C.byref(st), ptr(its),
+             ptr(rel), stream)
+        out = {f: getattr(st, f) for f, _ in _lib.SolveStats._fields_}
+        out["case_iterations"] = its
+        out["case_rel_res"] = rel
+        return out
+
     def matvec(self, x: np.ndarray) -> np.ndarray:
         rp, ci = self.pattern()
         v = self.values()
