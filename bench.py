@@ -59,7 +59,8 @@ def parse():
     ap.add_argument("--cpu-iters", type=int, default=12, help="scipy cg iterations in the CPU sample")
     ap.add_argument("--skip-jacobi", action="store_true", help="do not measure the Jacobi iteration count")
     ap.add_argument("--skip-cpu", action="store_true")
-    ap.add_argument("--only", choices=["solve-mixed", "solve-fp64", "spmv32", "spmv64"], default=None,
+    ap.add_argument("--cases", type=int, default=32, help="load cases of the batched (multi-RHS) solve")
+    ap.add_argument("--only", choices=["solve-mixed", "solve-fp64", "solve-multi", "spmv32", "spmv64"], default=None,
                     help="profiling mode: run only this operation (warmup + steps times) and print its time")
     return ap.parse_args()
 
@@ -76,7 +77,17 @@ def run_only(args):
     s = K.system
     st = torch.cuda.current_stream().cuda_stream
     n = 3 * s.n_nodes
-    if args.only.startswith("solve"):
+    if args.only == "solve-multi":
+        from wnfea_b200.mesh import tip_load_cases
+
+        s.amg_setup()
+        Fm = torch.from_numpy(tip_load_cases(m.mesh_nodes, n_cases=args.cases, seed=0)).cuda()
+        Um = torch.empty_like(Fm)
+        info = {}
+
+        def op():
+            info.update(s.solve_multi_device(Fm, Um, rtol=1e-8, precision=1, stream=st))
+    elif args.only.startswith("solve"):
         s.amg_setup()
         F = torch.from_numpy(F_np).cuda()
         u = torch.empty_like(F)
@@ -101,8 +112,14 @@ def run_only(args):
     for _ in range(args.steps):
         op()
     torch.cuda.synchronize()
-    print(json.dumps({"only": args.only, "ms_per_op": (time.perf_counter() - t0) * 1e3 / args.steps,
-                      "elements": meta["n_elements"], "nnz_blocks": s.nnzb}))
+    out = {"only": args.only, "ms_per_op": (time.perf_counter() - t0) * 1e3 / args.steps,
+           "elements": meta["n_elements"], "nnz_blocks": s.nnzb}
+    if args.only == "solve-multi":
+        out.update({"cases": args.cases, "iterations": info["iterations"], "outer": info["outer_iterations"],
+                    "status": info["status"], "max_rel_res": info["rel_res"],
+                    "device_ms": info["solve_seconds"] * 1e3,
+                    "case_iterations": [int(v) for v in info["case_iterations"]]})
+    print(json.dumps(out))
 
 
 def build_model(slices):

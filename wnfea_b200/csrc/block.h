@@ -58,8 +58,8 @@ struct BlockWork {
   DArray<BlockScalars> scal;           // [0] inner PCG, [1] outer column norms
   DArray<double> rtol_cols;            // kBatch inner targets
   std::vector<double> h_rtol;
-  // outer refinement (FP64): F, U, R = F - K U
-  DArray<double> F, U, R;
+  // outer refinement: F, U = U + Ulo (double-double), R = F - K U
+  DArray<double> F, U, Ulo, R;
   // Krylov vectors (FP64)
   DArray<double> x, r, p0, p1, q;
   // 1 / diag of the fine matrix (refreshed per solve)

@@ -33,27 +33,66 @@ constexpr int kThreads = 256;
 constexpr int kRowsPerWarp = 4;  // 8 lanes per block row
 
 // ---------------------------------------------------------------------------------------
-// 4-case vectors
+// case ownership and 4-case vectors
 // ---------------------------------------------------------------------------------------
+// Lane l (0..7) of an 8-lane group owns four of the 32 load cases of a DOF row.  The map is
+// chosen per kernel by the type M of its widest vectors so that every vector load is one
+// coalesced 16-byte-per-lane access:
+//   M = float : cases 4l .. 4l+3             (one float4 of a float row)
+//   M = double: cases 2l, 2l+1, 16+2l, 17+2l (two double2 of a double row, each contiguous
+//                                             over the 8 lanes)
 template <typename T>
 struct C4 {
   T v[4];
 };
-__device__ __forceinline__ C4<float> ld4(const float* __restrict__ p) {
-  const float4 a = *reinterpret_cast<const float4*>(p);
-  return {{a.x, a.y, a.z, a.w}};
+template <typename M>
+__device__ __forceinline__ int case_of(int l, int k) {
+  if constexpr (sizeof(M) == 4)
+    return 4 * l + k;
+  else
+    return (k < 2) ? 2 * l + k : 16 + 2 * l + (k - 2);
 }
-__device__ __forceinline__ C4<double> ld4(const double* __restrict__ p) {
-  const double2 a = reinterpret_cast<const double2*>(p)[0];
-  const double2 b = reinterpret_cast<const double2*>(p)[1];
-  return {{a.x, a.y, b.x, b.y}};
+template <typename M>
+__device__ __forceinline__ C4<float> ldc(const float* __restrict__ row, int l) {
+  if constexpr (sizeof(M) == 4) {
+    const float4 a = *reinterpret_cast<const float4*>(row + 4 * l);
+    return {{a.x, a.y, a.z, a.w}};
+  } else {
+    const float2 a = *reinterpret_cast<const float2*>(row + 2 * l);
+    const float2 b = *reinterpret_cast<const float2*>(row + 16 + 2 * l);
+    return {{a.x, a.y, b.x, b.y}};
+  }
 }
-__device__ __forceinline__ void st4(float* p, const C4<float>& v) {
-  *reinterpret_cast<float4*>(p) = make_float4(v.v[0], v.v[1], v.v[2], v.v[3]);
+template <typename M>
+__device__ __forceinline__ C4<double> ldc(const double* __restrict__ row, int l) {
+  if constexpr (sizeof(M) == 4) {
+    const double2 a = *reinterpret_cast<const double2*>(row + 4 * l);
+    const double2 b = *reinterpret_cast<const double2*>(row + 4 * l + 2);
+    return {{a.x, a.y, b.x, b.y}};
+  } else {
+    const double2 a = *reinterpret_cast<const double2*>(row + 2 * l);
+    const double2 b = *reinterpret_cast<const double2*>(row + 16 + 2 * l);
+    return {{a.x, a.y, b.x, b.y}};
+  }
 }
-__device__ __forceinline__ void st4(double* p, const C4<double>& v) {
-  reinterpret_cast<double2*>(p)[0] = make_double2(v.v[0], v.v[1]);
-  reinterpret_cast<double2*>(p)[1] = make_double2(v.v[2], v.v[3]);
+template <typename M>
+__device__ __forceinline__ void stc(float* row, int l, const C4<float>& v) {
+  if constexpr (sizeof(M) == 4) {
+    *reinterpret_cast<float4*>(row + 4 * l) = make_float4(v.v[0], v.v[1], v.v[2], v.v[3]);
+  } else {
+    *reinterpret_cast<float2*>(row + 2 * l) = make_float2(v.v[0], v.v[1]);
+    *reinterpret_cast<float2*>(row + 16 + 2 * l) = make_float2(v.v[2], v.v[3]);
+  }
+}
+template <typename M>
+__device__ __forceinline__ void stc(double* row, int l, const C4<double>& v) {
+  if constexpr (sizeof(M) == 4) {
+    reinterpret_cast<double2*>(row + 4 * l)[0] = make_double2(v.v[0], v.v[1]);
+    reinterpret_cast<double2*>(row + 4 * l)[1] = make_double2(v.v[2], v.v[3]);
+  } else {
+    *reinterpret_cast<double2*>(row + 2 * l) = make_double2(v.v[0], v.v[1]);
+    *reinterpret_cast<double2*>(row + 16 + 2 * l) = make_double2(v.v[2], v.v[3]);
+  }
 }
 template <typename TO, typename TI>
 __device__ __forceinline__ C4<TO> cvt4(const C4<TI>& a) {
@@ -61,27 +100,40 @@ __device__ __forceinline__ C4<TO> cvt4(const C4<TI>& a) {
 }
 
 // ---------------------------------------------------------------------------------------
-// row loop and per-case reductions
+// loops and per-case reductions
 // ---------------------------------------------------------------------------------------
-// Defines c0 (first load case of this lane) and loops `row` over the block rows of this
-// group.  Lanes leave the loop independently (no shuffles inside).
-#define BATCH_ROW_LOOP(n_rows)                                                           \
-  const int c0 = (threadIdx.x & 7) * 4;                                                  \
-  const int64_t warp0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;           \
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;                         \
-  for (int64_t row = warp0 * kRowsPerWarp + ((threadIdx.x & 31) >> 3); row < (n_rows);   \
-       row += nwarps * kRowsPerWarp)
+// Defines l (lane in the 8-lane group), `row` (the block row of this group) and loops over
+// groups of 4 consecutive rows per warp.  The loop bound is warp-uniform so that all 32 lanes
+// reach the row product's shuffles; a body may `continue` once the row product is done.
+#define BATCH_ROW_LOOP(n_rows)                                                               \
+  const int l = threadIdx.x & 7;                                                             \
+  const int64_t warp0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;               \
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;                             \
+  for (int64_t rb_ = warp0, row = warp0 * kRowsPerWarp + ((threadIdx.x & 31) >> 3);          \
+       rb_ * kRowsPerWarp < (n_rows);                                                         \
+       rb_ += nwarps, row = rb_ * kRowsPerWarp + ((threadIdx.x & 31) >> 3))
 
-// Element loop over an n x kBatch vector in 4-case quads: defines c0 and the quad index t
-// (elements 4t..4t+3, DOF 4t / kBatch).  The grid stride is a multiple of 8 quads, so a
-// thread always sees the same four cases.
-#define BATCH_QUAD_LOOP(n)                                                                     \
-  const int c0 = (threadIdx.x & 7) * 4;                                                        \
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < (n) * (kBatch / 4);     \
-       t += (int64_t)gridDim.x * blockDim.x)
+// The same with a team of S groups (S = 1 or 4) per row: 4 / S rows per warp; `lead` is true
+// in the team's first group, which alone runs the epilogue.
+#define BATCH_TEAM_LOOP(n_rows, S)                                                            \
+  const int l = threadIdx.x & 7;                                                             \
+  const bool lead = (((threadIdx.x & 31) >> 3) % (S)) == 0;                                  \
+  const int64_t warp0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;               \
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;                             \
+  for (int64_t rb_ = warp0, row = warp0 * (kRowsPerWarp / (S)) + ((threadIdx.x & 31) >> 3) / (S); \
+       rb_ * (kRowsPerWarp / (S)) < (n_rows);                                                 \
+       rb_ += nwarps, row = rb_ * (kRowsPerWarp / (S)) + ((threadIdx.x & 31) >> 3) / (S))
 
-// CTA partials of the four per-lane case sums d[0..3] (cases c0..c0+3 with c0 = (lane & 7) * 4)
-// into part[blockIdx.x * kBatch + case], in a fixed order.  All threads of the CTA call it.
+// Loop over the DOF rows i of n x kBatch vectors, 8 lanes per row; defines l.  The grid
+// stride is a multiple of 8 lanes, so a thread always owns the same four cases.
+#define BATCH_DOF_LOOP(n)                                                                      \
+  const int l = threadIdx.x & 7;                                                               \
+  for (int64_t t_ = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, i = t_ >> 3; t_ < (n) * 8; \
+       t_ += (int64_t)gridDim.x * blockDim.x, i = t_ >> 3)
+
+// CTA partials of the four per-lane case sums d[0..3] (cases case_of<M>(l, k)) into
+// part[blockIdx.x * kBatch + case], in a fixed order.  All threads of the CTA call it.
+template <typename M>
 __device__ __forceinline__ void write_case_parts(double (&d)[4], double* __restrict__ part) {
   __shared__ double sh[kThreads / 32][kBatch];
 #pragma unroll
@@ -92,7 +144,7 @@ __device__ __forceinline__ void write_case_parts(double (&d)[4], double* __restr
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (lane < 8)
 #pragma unroll
-    for (int k = 0; k < 4; ++k) sh[w][lane * 4 + k] = d[k];
+    for (int k = 0; k < 4; ++k) sh[w][case_of<M>(lane, k)] = d[k];
   __syncthreads();
   if (threadIdx.x < kBatch) {
     double s = 0.0;
@@ -116,77 +168,227 @@ __device__ __forceinline__ double reduce_case_parts(const double* __restrict__ p
   return t;
 }
 
+template <typename M>
+__device__ __forceinline__ C4<double> case_scalars(const double* __restrict__ v, int l) {
+  return {{v[case_of<M>(l, 0)], v[case_of<M>(l, 1)], v[case_of<M>(l, 2)], v[case_of<M>(l, 3)]}};
+}
+
 // ---------------------------------------------------------------------------------------
-// batched block-row product: acc[r][k] = sum_q A(row, q)[r][c] * x(col_q, c)[case c0 + k]
+// x functors of the batched row product: value of DOF i for this lane's cases
 // ---------------------------------------------------------------------------------------
-template <typename T>
+template <typename T, typename M>
 struct BLoad {
   const T* __restrict__ x;
-  __device__ __forceinline__ C4<T> operator()(int64_t i, int c0) const { return ld4(x + i * kBatch + c0); }
+  __device__ __forceinline__ C4<T> operator()(int64_t i, int l) const { return ldc<M>(x + i * kBatch, l); }
 };
-template <typename T>
+template <typename T, typename M>
 struct BD0 {  // first Chebyshev step from zero: dinv_i b_i / theta
   const T* __restrict__ b;
   const T* __restrict__ dinv;
   T inv_theta;
-  __device__ __forceinline__ C4<T> operator()(int64_t i, int c0) const {
-    C4<T> v = ld4(b + i * kBatch + c0);
+  __device__ __forceinline__ C4<T> operator()(int64_t i, int l) const {
+    C4<T> v = ldc<M>(b + i * kBatch, l);
     const T di = dinv[i];
 #pragma unroll
     for (int k = 0; k < 4; ++k) v.v[k] = di * v.v[k] * inv_theta;
     return v;
   }
 };
-template <typename TK, typename TM>
-struct BPNew {  // p_new = z + beta p_old, per case
+template <typename TM>
+struct BPNew {  // p_new = z + beta p_old per case (FP64 Krylov, double case map)
   const TM* __restrict__ z;
-  const TK* __restrict__ p;
-  C4<TK> beta;
-  __device__ __forceinline__ C4<TK> operator()(int64_t i, int c0) const {
-    const C4<TK> zz = cvt4<TK>(ld4(z + i * kBatch + c0));
-    const C4<TK> pp = ld4(p + i * kBatch + c0);
-    C4<TK> o;
+  const double* __restrict__ p;
+  C4<double> beta;
+  __device__ __forceinline__ C4<double> operator()(int64_t i, int l) const {
+    const C4<double> zz = cvt4<double>(ldc<double>(z + i * kBatch, l));
+    const C4<double> pp = ldc<double>(p + i * kBatch, l);
+    C4<double> o;
 #pragma unroll
     for (int k = 0; k < 4; ++k) o.v[k] = zz.v[k] + beta.v[k] * pp.v[k];
     return o;
   }
 };
 
-template <int BR, int BC, Layout LY, typename T, typename XF>
-__device__ __forceinline__ void batch_block_row(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                                const T* __restrict__ av, int64_t stride, int64_t row, int c0,
-                                                const XF& xf, T (&acc)[BR][4]) {
+// ---------------------------------------------------------------------------------------
+// batched block-row product
+// ---------------------------------------------------------------------------------------
+// Vector load of W consecutive elements (W * sizeof(T) bytes, naturally aligned).
+template <typename T, int W>
+struct VLoad;
+template <>
+struct VLoad<float, 4> {
+  static __device__ __forceinline__ void load(const float* p, float (&o)[4]) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    o[0] = v.x;
+    o[1] = v.y;
+    o[2] = v.z;
+    o[3] = v.w;
+  }
+};
+template <>
+struct VLoad<float, 2> {
+  static __device__ __forceinline__ void load(const float* p, float (&o)[2]) {
+    const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+    o[0] = v.x;
+    o[1] = v.y;
+  }
+};
+template <>
+struct VLoad<float, 1> {
+  static __device__ __forceinline__ void load(const float* p, float (&o)[1]) { o[0] = __ldg(p); }
+};
+template <>
+struct VLoad<double, 2> {
+  static __device__ __forceinline__ void load(const double* p, double (&o)[2]) {
+    const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+    o[0] = v.x;
+    o[1] = v.y;
+  }
+};
+template <>
+struct VLoad<double, 1> {
+  static __device__ __forceinline__ void load(const double* p, double (&o)[1]) { o[0] = __ldg(p); }
+};
+
+// widest (<= 16 B) load that tiles a block of NB elements of T
+template <typename T, int NB>
+struct ChunkOf {
+  static constexpr int kBlockBytes = NB * (int)sizeof(T);
+  static constexpr int kBytes = (kBlockBytes % 16 == 0) ? 16 : (kBlockBytes % 8 == 0) ? 8 : (int)sizeof(T);
+  static constexpr int W = kBytes / (int)sizeof(T);  // elements per chunk
+  static constexpr int N = kBlockBytes / kBytes;     // chunks per block = chunks per lane per stage
+};
+
+// Batched block-row product: for every block q of the row and every (r, c) of the block,
+// fmacc(r, A(row, q)[r][c], xload(BC col_q + c, l)) -- fmacc accumulates the lane's four cases
+// (FmaAcc: acc[r][k] += a x[k]).
+//
+// The 8 lanes of a group walk their row in stages of 8 consecutive blocks.  A stage is loaded
+// coalesced -- component-major (kSoA): lane i holds block i; block-contiguous (kAoS): the 8
+// blocks are one contiguous span and lane i holds its 16/8/4-byte chunks i, i + 8, ... -- and
+// each block is then broadcast inside the group with shuffles.  The x values of TPG blocks
+// are gathered before their multiply-adds (unconditionally: blocks past the row end carry
+// zero values and gather node 0), so TPG x 3 vector loads per lane are in flight at once.
+// All 32 lanes of the warp must call (the 4 groups of a warp work on 4 rows at once);
+// `active` = false gives an empty row.
+template <int BR, int BC, Layout LY, int TPG, int S, typename T, typename XL, typename FA>
+__device__ __forceinline__ void batch_row_staged(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                 const T* __restrict__ av, int64_t stride, int64_t row, bool active,
+                                                 int l, const XL& xload, const FA& fmacc) {
+  constexpr int NB = BR * BC;
+  constexpr unsigned kFull = 0xffffffffu;
+  static_assert(8 % TPG == 0, "trip groups tile a stage");
+  using XV = decltype(xload(int64_t(0), 0));
+  const int gbase = threadIdx.x & 24;
+  int32_t q0 = 0, q1 = 0;
+  if (active) {
+    q0 = __ldg(rp + row);
+    q1 = __ldg(rp + row + 1);
+  }
+  // a team of S groups shares the row: group h of the team takes stages h, h + S, ...
+  const int h = ((threadIdx.x & 31) >> 3) % S;
+  const int nst = (q1 - q0 + 7) >> 3;
+  const int wst = __reduce_max_sync(kFull, nst > h ? (nst - h + S - 1) / S : 0);
+  for (int it = 0; it < wst; ++it) {
+    const int32_t qb = q0 + (h + it * S) * 8;
+    const int cnt = q1 - qb;  // blocks of this stage: min(8, cnt) (<= 0 once the row is done)
+    const int32_t q = qb + l;
+    const int32_t mcol = (l < cnt) ? __ldg(ci + q) : 0;
+    // this lane's share of the stage's block values
+    T mv[LY == kSoA ? NB : 1];
+    using CH = ChunkOf<T, NB>;
+    T mc[LY == kSoA ? 1 : CH::N][CH::W];
+    if constexpr (LY == kSoA) {
 #pragma unroll
-  for (int r = 0; r < BR; ++r)
+      for (int e = 0; e < NB; ++e) mv[e] = (l < cnt) ? __ldg(av + (int64_t)e * stride + q) : T(0);
+    } else {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) acc[r][k] = T(0);
-  const int32_t q0 = rp[row], q1 = rp[row + 1];
-#pragma unroll 2
-  for (int32_t q = q0; q < q1; ++q) {
-    const int64_t col = ci[q];
-    C4<T> xv[BC];
+      for (int j = 0; j < CH::N; ++j) {
+        const int cidx = l + 8 * j;           // chunk of the 8-block span
+        const int blk = (cidx * CH::W) / NB;  // chunks never straddle blocks
+        if (blk < cnt) {
+          VLoad<T, CH::W>::load(av + (int64_t)qb * NB + (int64_t)cidx * CH::W, mc[j]);
+        } else {
 #pragma unroll
-    for (int c = 0; c < BC; ++c) xv[c] = xf(col * BC + c, c0);
+          for (int w = 0; w < CH::W; ++w) mc[j][w] = T(0);
+        }
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < 8; g += TPG) {
+      XV xv[TPG][BC];
+#pragma unroll
+      for (int u = 0; u < TPG; ++u) {
+        const int64_t col = __shfl_sync(kFull, mcol, gbase | (g + u));
+#pragma unroll
+        for (int c = 0; c < BC; ++c) xv[u][c] = xload(col * BC + c, l);
+      }
+#pragma unroll
+      for (int u = 0; u < TPG; ++u) {
+        const int t = g + u;
+#pragma unroll
+        for (int r = 0; r < BR; ++r)
+#pragma unroll
+          for (int c = 0; c < BC; ++c) {
+            const int e = r * BC + c;
+            T a;
+            if constexpr (LY == kSoA) {
+              a = __shfl_sync(kFull, mv[e], gbase | t);
+            } else {
+              const int cid = (t * NB + e) / CH::W;
+              a = __shfl_sync(kFull, mc[cid >> 3][(t * NB + e) % CH::W], gbase | (cid & 7));
+            }
+            fmacc(r, a, xv[u][c]);
+          }
+      }
+    }
+  }
+  if constexpr (S > 1) fmacc.template team_reduce<S>();
+}
+
+// plain multiply-add accumulation of the lane's four cases
+template <int BR, typename T>
+struct FmaAcc {
+  T (&acc)[BR][4];
+  __device__ __forceinline__ FmaAcc(T (&a)[BR][4]) : acc(a) {
 #pragma unroll
     for (int r = 0; r < BR; ++r)
 #pragma unroll
-      for (int c = 0; c < BC; ++c) {
-        const T a = (LY == kSoA) ? av[(int64_t)(r * BC + c) * stride + q] : av[(int64_t)q * (BR * BC) + r * BC + c];
+      for (int k = 0; k < 4; ++k) acc[r][k] = T(0);
+  }
+  __device__ __forceinline__ void operator()(int r, T a, const C4<T>& x) const {
 #pragma unroll
-        for (int k = 0; k < 4; ++k) acc[r][k] = fma(a, xv[c].v[k], acc[r][k]);
+    for (int k = 0; k < 4; ++k) acc[r][k] = fma(a, x.v[k], acc[r][k]);
+  }
+  // sum over the S groups of a row team (lanes 8 and 16 apart), the same fixed order in
+  // every lane
+  template <int S>
+  __device__ __forceinline__ void team_reduce() const {
+#pragma unroll
+    for (int r = 0; r < BR; ++r)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if constexpr (S >= 2) acc[r][k] += __shfl_xor_sync(0xffffffffu, acc[r][k], 8);
+        if constexpr (S >= 4) acc[r][k] += __shfl_xor_sync(0xffffffffu, acc[r][k], 16);
       }
   }
-}
+};
 
 template <int BS>
 struct BLayout {
   static constexpr Layout value = (BS == 3) ? kSoA : kAoS;
 };
+// blocks whose x is gathered ahead of the multiply-adds (register budget)
+template <typename T>
+struct Tpg {
+  static constexpr int value = sizeof(T) == 4 ? 4 : 2;
+};
 
 // ---------------------------------------------------------------------------------------
-// batched V-cycle kernels (same arithmetic per case as the single-RHS smoother kernels)
+// batched V-cycle kernels (same arithmetic per case as the single-RHS smoother kernels);
+// vectors of type T use the case map of T
 // ---------------------------------------------------------------------------------------
-template <int BS, typename T>
+template <int BS, typename T, int S>
 __global__ void __launch_bounds__(kThreads) kb_pre_first(int64_t n_rows, const int32_t* __restrict__ rp,
                                                          const int32_t* __restrict__ ci, const T* __restrict__ av,
                                                          int64_t stride, const T* __restrict__ b,
@@ -194,15 +396,17 @@ __global__ void __launch_bounds__(kThreads) kb_pre_first(int64_t n_rows, const i
                                                          T* __restrict__ x, T* __restrict__ r, T* __restrict__ d,
                                                          T* __restrict__ res, const int* __restrict__ done) {
   if (*done) return;
-  BATCH_ROW_LOOP(n_rows) {
+  BATCH_TEAM_LOOP(n_rows, S) {
     T acc[BS][4];
-    batch_block_row<BS, BS, BLayout<BS>::value>(rp, ci, av, stride, row, c0, BD0<T>{b, dinv, inv_theta}, acc);
+    batch_row_staged<BS, BS, BLayout<BS>::value, Tpg<T>::value, S, T>(rp, ci, av, stride, row, row < n_rows, l,
+                                                                BD0<T, T>{b, dinv, inv_theta}, FmaAcc<BS, T>(acc));
+    if (row >= n_rows || !lead) continue;
 #pragma unroll
     for (int rr = 0; rr < BS; ++rr) {
       const int64_t i = row * BS + rr;
-      const int64_t o = i * kBatch + c0;
+      const int64_t o = i * kBatch;
       const T di = dinv[i];
-      const C4<T> bi = ld4(b + o);
+      const C4<T> bi = ldc<T>(b + o, l);
       C4<T> xo, ro, dd;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
@@ -219,19 +423,19 @@ __global__ void __launch_bounds__(kThreads) kb_pre_first(int64_t n_rows, const i
           dd.v[k] = d1;
         }
       }
-      st4(x + o, xo);
+      stc<T>(x + o, l, xo);
       if (deg == 1) {
-        st4(res + o, ro);
+        stc<T>(res + o, l, ro);
       } else {
-        st4(r + o, ro);
-        st4(d + o, dd);
+        stc<T>(r + o, l, ro);
+        stc<T>(d + o, l, dd);
       }
     }
   }
 }
 
 // r -= D^-1 A d_in; d_out = c1 d_in + c2 r; x += d_out; part (if set): b . x per case
-template <int BS, typename T>
+template <int BS, typename T, int S>
 __global__ void __launch_bounds__(kThreads) kb_cheb_step(int64_t n_rows, const int32_t* __restrict__ rp,
                                                          const int32_t* __restrict__ ci, const T* __restrict__ av,
                                                          int64_t stride, const T* __restrict__ dinv,
@@ -242,15 +446,17 @@ __global__ void __launch_bounds__(kThreads) kb_cheb_step(int64_t n_rows, const i
   if (*done) return;
   double dot[4] = {0.0, 0.0, 0.0, 0.0};
   {
-    BATCH_ROW_LOOP(n_rows) {
+    BATCH_TEAM_LOOP(n_rows, S) {
       T acc[BS][4];
-      batch_block_row<BS, BS, BLayout<BS>::value>(rp, ci, av, stride, row, c0, BLoad<T>{d_in}, acc);
+      batch_row_staged<BS, BS, BLayout<BS>::value, Tpg<T>::value, S, T>(rp, ci, av, stride, row, row < n_rows, l,
+                                                                  BLoad<T, T>{d_in}, FmaAcc<BS, T>(acc));
+      if (row >= n_rows || !lead) continue;
 #pragma unroll
       for (int rr = 0; rr < BS; ++rr) {
         const int64_t i = row * BS + rr;
-        const int64_t o = i * kBatch + c0;
+        const int64_t o = i * kBatch;
         const T di = dinv[i];
-        const C4<T> rv = ld4(r + o), dv = ld4(d_in + o), xv = ld4(x + o);
+        const C4<T> rv = ldc<T>(r + o, l), dv = ldc<T>(d_in + o, l), xv = ldc<T>(x + o, l);
         C4<T> ro, dn, xn;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -258,45 +464,47 @@ __global__ void __launch_bounds__(kThreads) kb_cheb_step(int64_t n_rows, const i
           dn.v[k] = c1 * dv.v[k] + c2 * ro.v[k];
           xn.v[k] = xv.v[k] + dn.v[k];
         }
-        st4(r + o, ro);
-        st4(d_out + o, dn);
-        st4(x + o, xn);
+        stc<T>(r + o, l, ro);
+        stc<T>(d_out + o, l, dn);
+        stc<T>(x + o, l, xn);
         if (part) {
-          const C4<T> bv = ld4(b + o);
+          const C4<T> bv = ldc<T>(b + o, l);
 #pragma unroll
           for (int k = 0; k < 4; ++k) dot[k] += (double)bv.v[k] * (double)xn.v[k];
         }
       }
     }
   }
-  if (part) write_case_parts(dot, part);
+  if (part) write_case_parts<T>(dot, part);
 }
 
 // res = b - A x
-template <int BS, typename T>
+template <int BS, typename T, int S>
 __global__ void __launch_bounds__(kThreads) kb_residual(int64_t n_rows, const int32_t* __restrict__ rp,
                                                         const int32_t* __restrict__ ci, const T* __restrict__ av,
                                                         int64_t stride, const T* __restrict__ b,
                                                         const T* __restrict__ x, T* __restrict__ res,
                                                         const int* __restrict__ done) {
   if (*done) return;
-  BATCH_ROW_LOOP(n_rows) {
+  BATCH_TEAM_LOOP(n_rows, S) {
     T acc[BS][4];
-    batch_block_row<BS, BS, BLayout<BS>::value>(rp, ci, av, stride, row, c0, BLoad<T>{x}, acc);
+    batch_row_staged<BS, BS, BLayout<BS>::value, Tpg<T>::value, S, T>(rp, ci, av, stride, row, row < n_rows, l,
+                                                                BLoad<T, T>{x}, FmaAcc<BS, T>(acc));
+    if (row >= n_rows || !lead) continue;
 #pragma unroll
     for (int rr = 0; rr < BS; ++rr) {
-      const int64_t o = (row * BS + rr) * kBatch + c0;
-      const C4<T> bv = ld4(b + o);
+      const int64_t o = (row * BS + rr) * kBatch;
+      const C4<T> bv = ldc<T>(b + o, l);
       C4<T> ro;
 #pragma unroll
       for (int k = 0; k < 4; ++k) ro.v[k] = bv.v[k] - acc[rr][k];
-      st4(res + o, ro);
+      stc<T>(res + o, l, ro);
     }
   }
 }
 
 // first post-smoothing step from x: r0 = D^-1 (b - A x), d0 = r0 / theta, x2 = x + d0
-template <int BS, typename T>
+template <int BS, typename T, int S>
 __global__ void __launch_bounds__(kThreads) kb_post_first(int64_t n_rows, const int32_t* __restrict__ rp,
                                                           const int32_t* __restrict__ ci, const T* __restrict__ av,
                                                           int64_t stride, const T* __restrict__ b,
@@ -307,15 +515,17 @@ __global__ void __launch_bounds__(kThreads) kb_post_first(int64_t n_rows, const 
   if (*done) return;
   double dot[4] = {0.0, 0.0, 0.0, 0.0};
   {
-    BATCH_ROW_LOOP(n_rows) {
+    BATCH_TEAM_LOOP(n_rows, S) {
       T acc[BS][4];
-      batch_block_row<BS, BS, BLayout<BS>::value>(rp, ci, av, stride, row, c0, BLoad<T>{x}, acc);
+      batch_row_staged<BS, BS, BLayout<BS>::value, Tpg<T>::value, S, T>(rp, ci, av, stride, row, row < n_rows, l,
+                                                                  BLoad<T, T>{x}, FmaAcc<BS, T>(acc));
+      if (row >= n_rows || !lead) continue;
 #pragma unroll
       for (int rr = 0; rr < BS; ++rr) {
         const int64_t i = row * BS + rr;
-        const int64_t o = i * kBatch + c0;
+        const int64_t o = i * kBatch;
         const T di = dinv[i];
-        const C4<T> bv = ld4(b + o), xv = ld4(x + o);
+        const C4<T> bv = ldc<T>(b + o, l), xv = ldc<T>(x + o, l);
         C4<T> ro, dd, xn;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -324,37 +534,38 @@ __global__ void __launch_bounds__(kThreads) kb_post_first(int64_t n_rows, const 
           xn.v[k] = xv.v[k] + dd.v[k];
           if (part) dot[k] += (double)bv.v[k] * (double)xn.v[k];
         }
-        st4(r + o, ro);
-        st4(d + o, dd);
-        st4(x2 + o, xn);
+        stc<T>(r + o, l, ro);
+        stc<T>(d + o, l, dd);
+        stc<T>(x2 + o, l, xn);
       }
     }
   }
-  if (part) write_case_parts(dot, part);
+  if (part) write_case_parts<T>(dot, part);
 }
 
 // y = A x or y += A x for the block-contiguous transfer operators (BR x BC blocks)
-template <int BR, int BC, typename T>
+template <int BR, int BC, typename T, int S>
 __global__ void __launch_bounds__(kThreads) kb_level_spmv(int64_t n_rows, const int32_t* __restrict__ rp,
                                                           const int32_t* __restrict__ ci, const T* __restrict__ av,
                                                           const T* __restrict__ x, T* __restrict__ y, int accumulate,
                                                           const int* __restrict__ done) {
   if (*done) return;
-  BATCH_ROW_LOOP(n_rows) {
+  BATCH_TEAM_LOOP(n_rows, S) {
     T acc[BR][4];
-    batch_block_row<BR, BC, kAoS>(rp, ci, av, 0, row, c0, BLoad<T>{x}, acc);
+    batch_row_staged<BR, BC, kAoS, Tpg<T>::value, S, T>(rp, ci, av, 0, row, row < n_rows, l, BLoad<T, T>{x}, FmaAcc<BR, T>(acc));
+    if (row >= n_rows || !lead) continue;
 #pragma unroll
     for (int rr = 0; rr < BR; ++rr) {
-      const int64_t o = (row * BR + rr) * kBatch + c0;
+      const int64_t o = (row * BR + rr) * kBatch;
       C4<T> v;
 #pragma unroll
       for (int k = 0; k < 4; ++k) v.v[k] = acc[rr][k];
       if (accumulate) {
-        const C4<T> yv = ld4(y + o);
+        const C4<T> yv = ldc<T>(y + o, l);
 #pragma unroll
         for (int k = 0; k < 4; ++k) v.v[k] += yv.v[k];
       }
-      st4(y + o, v);
+      stc<T>(y + o, l, v);
     }
   }
 }
@@ -377,7 +588,7 @@ __global__ void __launch_bounds__(kThreads) kb_coarse(int64_t n, const double* _
 }
 
 // ---------------------------------------------------------------------------------------
-// batched PCG kernels
+// batched PCG kernels (FP64 Krylov vectors: double case map)
 // ---------------------------------------------------------------------------------------
 
 // r = b, x = 0, rm = (TM) b (if rm), partC = b . b per case
@@ -387,17 +598,17 @@ __global__ void __launch_bounds__(kThreads) kb_init_vecs(int64_t n, const double
                                                          TM* __restrict__ rm, double* __restrict__ partC) {
   double dot[4] = {0.0, 0.0, 0.0, 0.0};
   {
-    BATCH_QUAD_LOOP(n) {
-      const C4<double> v = ld4(b + 4 * t);
-      st4(r + 4 * t, v);
-      st4(x + 4 * t, C4<double>{{0.0, 0.0, 0.0, 0.0}});
-      if (rm) st4(rm + 4 * t, cvt4<TM>(v));
+    BATCH_DOF_LOOP(n) {
+      const int64_t o = i * kBatch;
+      const C4<double> v = ldc<double>(b + o, l);
+      stc<double>(r + o, l, v);
+      stc<double>(x + o, l, C4<double>{{0.0, 0.0, 0.0, 0.0}});
+      if (rm) stc<double>(rm + o, l, cvt4<TM>(v));
 #pragma unroll
       for (int k = 0; k < 4; ++k) dot[k] += v.v[k] * v.v[k];
     }
-    (void)c0;
   }
-  write_case_parts(dot, partC);
+  write_case_parts<double>(dot, partC);
 }
 
 // per-case targets; cases with rtol_j >= 1 (already converged outside) or a zero right-hand
@@ -440,20 +651,20 @@ __global__ void __launch_bounds__(kThreads) kb_prec_vec(int64_t n, const T* __re
   if (*done) return;
   double dot[4] = {0.0, 0.0, 0.0, 0.0};
   {
-    BATCH_QUAD_LOOP(n) {
-      const C4<T> rv = ld4(r + 4 * t);
-      const T di = jacobi ? dinv[(4 * t) / kBatch] : T(1);
+    BATCH_DOF_LOOP(n) {
+      const int64_t o = i * kBatch;
+      const C4<T> rv = ldc<T>(r + o, l);
+      const T di = jacobi ? dinv[i] : T(1);
       C4<T> zv;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         zv.v[k] = jacobi ? di * rv.v[k] : rv.v[k];
         dot[k] += (double)rv.v[k] * (double)zv.v[k];
       }
-      st4(z + 4 * t, zv);
+      stc<T>(z + o, l, zv);
     }
-    (void)c0;
   }
-  write_case_parts(dot, partA);
+  write_case_parts<T>(dot, partA);
 }
 
 // rz_new = r . z (partA); beta = rz_new / rz (0 at the first iteration and for finished cases)
@@ -499,27 +710,28 @@ __global__ void __launch_bounds__(kThreads) kb_spmv_dot(int64_t n_rows, const in
   double dot[4] = {0.0, 0.0, 0.0, 0.0};
   {
     BATCH_ROW_LOOP(n_rows) {
-      const C4<double> beta = {{S->beta[c0], S->beta[c0 + 1], S->beta[c0 + 2], S->beta[c0 + 3]}};
-      const BPNew<double, TM> pf{z, p_old, beta};
+      const BPNew<TM> pf{z, p_old, case_scalars<double>(S->beta, l)};
       double acc[3][4];
-      batch_block_row<3, 3, kSoA>(rp, ci, av, stride, row, c0, pf, acc);
+      batch_row_staged<3, 3, kSoA, Tpg<double>::value, 1, double>(rp, ci, av, stride, row, row < n_rows, l, pf,
+                                                               FmaAcc<3, double>(acc));
+      if (row >= n_rows) continue;
 #pragma unroll
       for (int rr = 0; rr < 3; ++rr) {
         const int64_t i = row * 3 + rr;
-        const int64_t o = i * kBatch + c0;
-        const C4<double> pv = pf(i, c0);
+        const int64_t o = i * kBatch;
+        const C4<double> pv = pf(i, l);
         C4<double> qv;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           qv.v[k] = acc[rr][k];
           dot[k] += pv.v[k] * qv.v[k];
         }
-        st4(p_new + o, pv);
-        st4(q + o, qv);
+        stc<double>(p_new + o, l, pv);
+        stc<double>(q + o, l, qv);
       }
     }
   }
-  write_case_parts(dot, partB);
+  write_case_parts<double>(dot, partB);
 }
 
 // alpha = rz / (p . q) for the running cases; a non-positive curvature ends that case
@@ -550,25 +762,26 @@ __global__ void __launch_bounds__(kThreads) kb_update(int64_t n, double* __restr
   if (S->done) return;
   double dot[4] = {0.0, 0.0, 0.0, 0.0};
   {
-    BATCH_QUAD_LOOP(n) {
-      const double a0 = S->alpha[c0], a1 = S->alpha[c0 + 1], a2 = S->alpha[c0 + 2], a3 = S->alpha[c0 + 3];
-      const double a[4] = {a0, a1, a2, a3};
-      C4<double> xv = ld4(x + 4 * t), rv = ld4(r + 4 * t);
-      const C4<double> pv = ld4(p + 4 * t), qv = ld4(q + 4 * t);
+    const int l0 = threadIdx.x & 7;
+    const C4<double> a = case_scalars<double>(S->alpha, l0);
+    BATCH_DOF_LOOP(n) {
+      const int64_t o = i * kBatch;
+      C4<double> xv = ldc<double>(x + o, l), rv = ldc<double>(r + o, l);
+      const C4<double> pv = ldc<double>(p + o, l), qv = ldc<double>(q + o, l);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        if (a[k] != 0.0) {  // finished cases keep x and r exactly (their p may be anything)
-          xv.v[k] += a[k] * pv.v[k];
-          rv.v[k] -= a[k] * qv.v[k];
+        if (a.v[k] != 0.0) {  // finished cases keep x and r exactly (their p may be anything)
+          xv.v[k] += a.v[k] * pv.v[k];
+          rv.v[k] -= a.v[k] * qv.v[k];
         }
         dot[k] += rv.v[k] * rv.v[k];
       }
-      st4(x + 4 * t, xv);
-      st4(r + 4 * t, rv);
-      if (rm) st4(rm + 4 * t, cvt4<TM>(rv));
+      stc<double>(x + o, l, xv);
+      stc<double>(r + o, l, rv);
+      if (rm) stc<double>(rm + o, l, cvt4<TM>(rv));
     }
   }
-  write_case_parts(dot, partC);
+  write_case_parts<double>(dot, partC);
 }
 
 // convergence test of every running case; the batch ends when all cases are finished or
@@ -609,33 +822,104 @@ __global__ void kb_check(BlockScalars* S, const double* __restrict__ partC, int 
   }
 }
 
-// R = F - K U (FP64, component-major fine matrix); partC = R . R per case
+// ---------------------------------------------------------------------------------------
+// extra-precise refinement: U = U_hi + U_lo (double-double), R = F - K U with compensated
+// products and sums
+// ---------------------------------------------------------------------------------------
+// Error-free transformations: Knuth's TwoSum (a + b = s + e exactly) and TwoProduct by fused
+// multiply-add (a * b = p + e exactly), as in Ogita, Rump and Oishi, "Accurate sum and dot
+// product", SIAM J. Sci. Comput. 26 (2005).  The _rn intrinsics are never contracted or
+// reordered by the compiler.
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+  s = __dadd_rn(a, b);
+  const double bb = __dsub_rn(s, a);
+  e = __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
+}
+__device__ __forceinline__ void two_prod(double a, double b, double& p, double& e) {
+  p = __dmul_rn(a, b);
+  e = __fma_rn(a, b, -p);
+}
+
+struct DD4 {
+  C4<double> hi, lo;
+};
+template <typename M>
+struct DDLoad {
+  const double* __restrict__ hi;
+  const double* __restrict__ lo;
+  __device__ __forceinline__ DD4 operator()(int64_t i, int l) const {
+    return {ldc<M>(hi + i * kBatch, l), ldc<M>(lo + i * kBatch, l)};
+  }
+};
+// compensated accumulation (Dot2 of Ogita-Rump-Oishi): s + c carries about twice the FP64
+// precision of a plain sum of a (x_hi + x_lo)
+template <int BR>
+struct DdAcc {
+  double (&s)[BR][4];
+  double (&c)[BR][4];
+  __device__ __forceinline__ DdAcc(double (&s_)[BR][4], double (&c_)[BR][4]) : s(s_), c(c_) {
+#pragma unroll
+    for (int r = 0; r < BR; ++r)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) s[r][k] = c[r][k] = 0.0;
+  }
+  __device__ __forceinline__ void operator()(int r, double a, const DD4& x) const {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      double p, ep, t, es;
+      two_prod(a, x.hi.v[k], p, ep);
+      two_sum(s[r][k], p, t, es);
+      s[r][k] = t;
+      c[r][k] += (ep + es) + a * x.lo.v[k];
+    }
+  }
+};
+
+// R = F - K (U_hi + U_lo), rounded to FP64 from the compensated sum; partC = R . R per case
 __global__ void __launch_bounds__(kThreads) kb_outer_residual(int64_t n_rows, const int32_t* __restrict__ rp,
                                                               const int32_t* __restrict__ ci,
                                                               const double* __restrict__ av, int64_t stride,
                                                               const double* __restrict__ F,
-                                                              const double* __restrict__ U, double* __restrict__ R,
+                                                              const double* __restrict__ Uhi,
+                                                              const double* __restrict__ Ulo, double* __restrict__ R,
                                                               double* __restrict__ partC) {
   double dot[4] = {0.0, 0.0, 0.0, 0.0};
   {
     BATCH_ROW_LOOP(n_rows) {
-      double acc[3][4];
-      batch_block_row<3, 3, kSoA>(rp, ci, av, stride, row, c0, BLoad<double>{U}, acc);
+      double s[3][4], c[3][4];
+      batch_row_staged<3, 3, kSoA, 1, 1, double>(rp, ci, av, stride, row, row < n_rows, l,
+                                              DDLoad<double>{Uhi, Ulo}, DdAcc<3>(s, c));
+      if (row >= n_rows) continue;
 #pragma unroll
       for (int rr = 0; rr < 3; ++rr) {
-        const int64_t o = (row * 3 + rr) * kBatch + c0;
-        const C4<double> fv = ld4(F + o);
+        const int64_t o = (row * 3 + rr) * kBatch;
+        const C4<double> fv = ldc<double>(F + o, l);
         C4<double> rv;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-          rv.v[k] = fv.v[k] - acc[rr][k];
+          double t, e;
+          two_sum(fv.v[k], -s[rr][k], t, e);
+          rv.v[k] = t + (e - c[rr][k]);
           dot[k] += rv.v[k] * rv.v[k];
         }
-        st4(R + o, rv);
+        stc<double>(R + o, l, rv);
       }
     }
   }
-  write_case_parts(dot, partC);
+  write_case_parts<double>(dot, partC);
+}
+
+// (U_hi, U_lo) += X, renormalised so that U_hi = fl(U_hi + U_lo)
+__global__ void kb_accumulate(int64_t n, double* __restrict__ Uhi, double* __restrict__ Ulo,
+                              const double* __restrict__ X) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n * kBatch;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double s, e, h, g;
+    two_sum(Uhi[i], X[i], s, e);
+    two_sum(s, __dadd_rn(Ulo[i], e), h, g);
+    Uhi[i] = h;
+    Ulo[i] = g;
+  }
 }
 
 // partC = x . x per case
@@ -643,27 +927,19 @@ __global__ void __launch_bounds__(kThreads) kb_dot_self(int64_t n, const double*
                                                         double* __restrict__ partC) {
   double dot[4] = {0.0, 0.0, 0.0, 0.0};
   {
-    BATCH_QUAD_LOOP(n) {
-      const C4<double> v = ld4(x + 4 * t);
+    BATCH_DOF_LOOP(n) {
+      const C4<double> v = ldc<double>(x + i * kBatch, l);
 #pragma unroll
       for (int k = 0; k < 4; ++k) dot[k] += v.v[k] * v.v[k];
     }
-    (void)c0;
   }
-  write_case_parts(dot, partC);
+  write_case_parts<double>(dot, partC);
 }
 
 // S->rr[j] = sum of partC (one CTA)
 __global__ void kb_reduce_rr(BlockScalars* S, const double* __restrict__ partC, int nparts) {
   const double rr = reduce_case_parts(partC, nparts);
   if (threadIdx.x < kBatch) S->rr[threadIdx.x] = rr;
-}
-
-// U += X
-__global__ void kb_accumulate(int64_t n, double* __restrict__ U, const double* __restrict__ X) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n * kBatch;
-       i += (int64_t)gridDim.x * blockDim.x)
-    U[i] += X[i];
 }
 
 // pack columns [j0, j0 + m) of a row-major n x ld matrix into the n x kBatch batch (zero
@@ -738,12 +1014,20 @@ struct BPrec<double> {
   static double* rm(BlockWork&) { return nullptr; }  // the V-cycle reads the FP64 r directly
 };
 
+// long rows (>= 4 stages of 8 blocks on average) are shared by the 4 groups of a warp
 template <int BR, int BC, typename T>
 void batch_level_spmv(const DevBsr& M, const T* vals, const T* x, T* y, int accumulate, const int* done,
                       cudaStream_t st) {
-  auto k = kb_level_spmv<BR, BC, T>;
-  k<<<resident_grid(k, kThreads, rows_work(M.n_rows)), kThreads, 0, st>>>(M.n_rows, M.rp.p, M.ci.p, vals, x, y,
-                                                                          accumulate, done);
+  const bool team = M.n_rows > 0 && M.nnzb >= 32 * M.n_rows;
+  if (team) {
+    auto k = kb_level_spmv<BR, BC, T, 4>;
+    k<<<resident_grid(k, kThreads, rows_work(M.n_rows * 4)), kThreads, 0, st>>>(M.n_rows, M.rp.p, M.ci.p, vals, x,
+                                                                                y, accumulate, done);
+  } else {
+    auto k = kb_level_spmv<BR, BC, T, 1>;
+    k<<<resident_grid(k, kThreads, rows_work(M.n_rows)), kThreads, 0, st>>>(M.n_rows, M.rp.p, M.ci.p, vals, x, y,
+                                                                            accumulate, done);
+  }
 }
 
 // one batched V-cycle at level lvl: out = V(b); part (if set) receives b . out per case
@@ -764,28 +1048,29 @@ int batch_vcycle(Solid* s, AmgHierarchy& H, BlockWork& W, int lvl, const T* b, T
   const int deg = H.degree;
   const T it = (T)L.inv_theta;
   const int64_t sd = (lvl == 0) ? s->nnzb : 0;
-  const int work = rows_work(nr);
   auto run = [&](auto bs_tag) -> int {
     constexpr int BS = decltype(bs_tag)::value;
+    constexpr int S = (BS == 3) ? 1 : 4;  // coarse 6x6 levels: rows of ~50-250 blocks, one warp each
+    const int work = rows_work(nr * S);
     auto rg = [&](auto kern) { return resident_grid(kern, kThreads, work); };
     const int32_t* rp = lvl == 0 ? s->row_ptr.p : L.A.rp.p;
     const int32_t* ci = lvl == 0 ? s->col_idx.p : L.A.ci.p;
     const T* av = lvl == 0 ? BPrec<T>::A0(s) : BPrec<T>::Av(L);
     const T c1 = deg >= 2 ? (T)L.c1[0] : T(0), c2 = deg >= 2 ? (T)L.c2[0] : T(0);
-    kb_pre_first<BS, T><<<rg(kb_pre_first<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, deg, c1, c2,
+    kb_pre_first<BS, T, S><<<rg(kb_pre_first<BS, T, S>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, deg, c1, c2,
                                                                       V.x.p, V.r.p, V.d.p, V.res.p, done);
     W.launches++;
     T* din = V.d.p;
     T* dout = V.d2.p;
     for (int k = 2; k < deg; ++k) {
-      kb_cheb_step<BS, T><<<rg(kb_cheb_step<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout, V.r.p,
+      kb_cheb_step<BS, T, S><<<rg(kb_cheb_step<BS, T, S>), kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout, V.r.p,
                                                                         V.x.p, (T)L.c1[k - 1], (T)L.c2[k - 1], b,
                                                                         nullptr, done);
       W.launches++;
       std::swap(din, dout);
     }
     if (deg >= 2) {
-      kb_residual<BS, T><<<rg(kb_residual<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, V.x.p, V.res.p, done);
+      kb_residual<BS, T, S><<<rg(kb_residual<BS, T, S>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, V.x.p, V.res.p, done);
       W.launches++;
     }
     const bool last = lvl + 1 >= nlev;
@@ -797,18 +1082,18 @@ int batch_vcycle(Solid* s, AmgHierarchy& H, BlockWork& W, int lvl, const T* b, T
     batch_level_spmv<BS, 6, T>(L.P, BPrec<T>::Pv(L), xc, V.x.p, 1, done, st);
     W.launches++;
     double* part_last = (deg == 1) ? part : nullptr;
-    const int gpf = rg(kb_post_first<BS, T>);
+    const int gpf = rg(kb_post_first<BS, T, S>);
     if (part_last) W.npA = gpf;
-    kb_post_first<BS, T><<<gpf, kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, V.x.p, out, V.r.p, V.d.p,
+    kb_post_first<BS, T, S><<<gpf, kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, V.x.p, out, V.r.p, V.d.p,
                                                    part_last, done);
     W.launches++;
     din = V.d.p;
     dout = V.d2.p;
     for (int k = 1; k < deg; ++k) {
       double* pk = (k == deg - 1) ? part : nullptr;
-      const int gcs = rg(kb_cheb_step<BS, T>);
+      const int gcs = rg(kb_cheb_step<BS, T, S>);
       if (pk) W.npA = gcs;
-      kb_cheb_step<BS, T><<<gcs, kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout, V.r.p, out,
+      kb_cheb_step<BS, T, S><<<gcs, kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout, V.r.p, out,
                                                     (T)L.c1[k - 1], (T)L.c2[k - 1], b, pk, done);
       W.launches++;
       std::swap(din, dout);
@@ -926,6 +1211,7 @@ int ensure_block_work(Solid* s, int vmode, int precond) {
     W.n = n;
     WN_CHECK(W.F.alloc(nb));
     WN_CHECK(W.U.alloc(nb));
+    WN_CHECK(W.Ulo.alloc(nb));
     WN_CHECK(W.R.alloc(nb));
     WN_CHECK(W.x.alloc(nb));
     WN_CHECK(W.r.alloc(nb));
@@ -1002,8 +1288,11 @@ struct BatchResult {
   double case_rel[kBatch] = {};
 };
 
-// FP64 refinement over the batch in W.F (m live cases): U = 0, R = F; while some case has
+// Refinement over the batch in W.F (m live cases): U = 0, R = F; while some case has
 // ||R_j|| > rtol ||F_j||: batched PCG on R with per-case inner targets, U += X, R = F - K U.
+// U is kept as a double-double pair and R is evaluated with compensated products and sums,
+// so the test resolves residuals below the FP64 rounding level of K U (which for load cases
+// with large displacements lies near 1e-8 of ||F||); U_hi is returned.
 template <typename TM>
 int batch_outer(Solid* s, BlockWork& W, int vmode, int m, const wn_solve_params& prm, int chunk, cudaStream_t st,
                 BatchResult& res) {
@@ -1019,6 +1308,7 @@ int batch_outer(Solid* s, BlockWork& W, int vmode, int m, const wn_solve_params&
     rr[j] = hS.rr[j];
   }
   WN_CUDA(cudaMemsetAsync(W.U.p, 0, vb, st));
+  WN_CUDA(cudaMemsetAsync(W.Ulo.p, 0, vb, st));
   WN_CUDA(cudaMemcpyAsync(W.R.p, W.F.p, vb, cudaMemcpyDeviceToDevice, st));
   const int max_outer = prm.max_outer > 0 ? prm.max_outer : 10;
   bool first = true;
@@ -1026,7 +1316,7 @@ int batch_outer(Solid* s, BlockWork& W, int vmode, int m, const wn_solve_params&
     if (!first) {
       W.npC = resident_grid(kb_outer_residual, kThreads, rows_work(s->n_nodes));
       kb_outer_residual<<<W.npC, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, s->nnzb,
-                                                    W.F.p, W.U.p, W.R.p, W.partC.p);
+                                                    W.F.p, W.U.p, W.Ulo.p, W.R.p, W.partC.p);
       kb_reduce_rr<<<1, kThreads, 0, st>>>(S1, W.partC.p, W.npC);
       W.launches += 2;
       WN_CUDA(cudaGetLastError());
@@ -1063,7 +1353,7 @@ int batch_outer(Solid* s, BlockWork& W, int vmode, int m, const wn_solve_params&
       res.case_iters[j] += hS.col_iters[j];
       if (hS.col_status[j] == WN_EBREAKDOWN) res.case_status[j] = WN_EBREAKDOWN;
     }
-    kb_accumulate<<<grid_for(n * kBatch, 1, kThreads, 8), kThreads, 0, st>>>(n, W.U.p, W.x.p);
+    kb_accumulate<<<grid_for(n * kBatch, 1, kThreads, 8), kThreads, 0, st>>>(n, W.U.p, W.Ulo.p, W.x.p);
     W.launches++;
     WN_CUDA(cudaGetLastError());
   }
