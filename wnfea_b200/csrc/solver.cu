@@ -361,8 +361,10 @@ struct XPNew2 {  // p_j = z_j + beta p_old_j, z in the preconditioner's precisio
 // iteration k: rz = sum(partA); beta = rz / rz_prev (0 at k = 0); p_new = z + beta p_old;
 // q = A p_new; partB = p_new . q.  Parity par = k & 1 selects the p buffers and rz slot.
 // TK: Krylov vectors / matrix precision; TM: preconditioner output precision.
+// The lane's own p_new entry is formed before the row product so that its loads overlap the
+// matrix stream; the FP64 variant then needs up to 48 registers (5 resident CTAs per SM).
 template <int BS, typename TK, typename TM>
-__global__ void __launch_bounds__(kThreads, (BS == 3) ? kMinBlocks : 1) k_spmv_dot(int64_t n_rows, const int32_t* __restrict__ rp,
+__global__ void __launch_bounds__(kThreads, (BS == 3) ? (sizeof(TK) == 4 ? kMinBlocks : 5) : 1) k_spmv_dot(int64_t n_rows, const int32_t* __restrict__ rp,
                                                        const int32_t* __restrict__ ci, const TK* __restrict__ av, int64_t stride,
                                                        const TM* __restrict__ z, const TK* __restrict__ p_old,
                                                        TK* __restrict__ p_new, TK* __restrict__ q,
@@ -376,12 +378,13 @@ __global__ void __launch_bounds__(kThreads, (BS == 3) ? kMinBlocks : 1) k_spmv_d
   double dot = 0.0;
   GROUP_ROW_LOOP(n_rows, GroupOf<BS>::value) {
     const bool active = row < n_rows;
+    const bool own = active && lane < BS;
+    const int64_t i = row * BS + lane;
+    const TK pi = own ? (TK)z[i] + beta * p_old[i] : TK(0);
     TK acc[BS];
     group_block_row<BS, BS, GroupOf<BS>::value, LayoutOf<BS>::value, TK, TK>(rp, ci, av, stride, row, active,
         XPNew2<TK, TM>{z, p_old, beta}, acc, lane);
-    if (active && lane < BS) {
-      const int64_t i = row * BS + lane;
-      const TK pi = (TK)z[i] + beta * p_old[i];
+    if (own) {
       const TK qi = pick<BS>(acc, lane);
       p_new[i] = pi;
       q[i] = qi;
