@@ -93,10 +93,14 @@ def run_only(args):
         u = torch.empty_like(F)
         prec = 1 if args.only == "solve-mixed" else 0
 
+        info = {}
+
         def op():
             prm = _lib.SolveParams(1e-8, 2000, 2, prec, 0.0, 10, 8, 1)
             stt = _lib.SolveStats()
             _lib.call("wn_solve_device", s.handle, F.data_ptr(), u.data_ptr(), prm, stt, st)
+            info.update(iterations=stt.iterations, outer=stt.outer_iterations, rel_res=stt.rel_res,
+                        device_ms=stt.solve_seconds * 1e3)
     else:
         prec = 1 if args.only == "spmv32" else 0
         dt = torch.float32 if prec else torch.float64
@@ -114,6 +118,8 @@ def run_only(args):
     torch.cuda.synchronize()
     out = {"only": args.only, "ms_per_op": (time.perf_counter() - t0) * 1e3 / args.steps,
            "elements": meta["n_elements"], "nnz_blocks": s.nnzb}
+    if args.only in ("solve-mixed", "solve-fp64"):
+        out.update(info)
     if args.only == "solve-multi":
         out.update({"cases": args.cases, "iterations": info["iterations"], "outer": info["outer_iterations"],
                     "status": info["status"], "max_rel_res": info["rel_res"],

@@ -170,7 +170,10 @@ typedef struct wn_solve_stats {
   int outer_iterations;  /* refinement steps (0 for FP64)                            */
   int status;            /* 0 converged, WN_ENOCONV, WN_EBREAKDOWN                   */
   int n_levels;          /* AMG levels including the coarsest (0 without AMG)        */
-  double rel_res;        /* final true ||F - K u|| / ||F|| (FP64 matrix)             */
+  double rel_res;        /* final true ||F - K u|| / ||F|| (FP64 matrix) of the refined
+                            solution, kept as a double-double pair; the FP64 u returned
+                            is its rounding, whose own residual is at most about
+                            max(rel_res, eps64 || |K| |u| || / ||F||)                */
   double solve_seconds;  /* device time of the solve (CUDA events)                   */
   double setup_seconds;  /* wall time of the last AMG setup                          */
   int64_t kernel_launches; /* kernels issued by the solve (graph replays counted per kernel) */

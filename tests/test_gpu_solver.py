@@ -164,3 +164,34 @@ def test_fp32_iterative_refinement_mode_on_small_mesh(golden):
     u, st = solve_c3d10_system(K, F, method="pcg", rtol=1e-8, preconditioner="amg", precision="mixed_fp32_ir")
     assert st["status"] == 0 and st["rel_res"] < 1e-8 and st["outer_iters"] >= 2
     assert np.linalg.norm(u - g["u_direct"]) / np.linalg.norm(g["u_direct"]) < 1e-6
+
+
+def _residual_longdouble(K, u, F):
+    """(||F - K u|| / ||F||, eps64 || |K| |u| || / ||F||) with the products and sums in extended
+    precision (x86 80-bit): the residual of the FP64 vector u, resolved below the FP64 rounding
+    level of K u, and that rounding level (no FP64 vector has a residual much below it)."""
+    Kc = K.tocsr()
+    uu = u.astype(np.longdouble)[Kc.indices]
+    prod = Kc.data.astype(np.longdouble) * uu
+    Ku = np.add.reduceat(prod, Kc.indptr[:-1])
+    aKu = np.add.reduceat(np.abs(prod), Kc.indptr[:-1])
+    r = F.astype(np.longdouble) - Ku
+    fn = np.sqrt((F.astype(np.longdouble) ** 2).sum())
+    return float(np.sqrt((r * r).sum()) / fn), float(np.finfo(np.float64).eps * np.sqrt((aKu * aKu).sum()) / fn)
+
+
+@pytest.mark.parametrize("precision,rtol", [("fp64", 1e-12), ("mixed_fp32", 1e-10)])
+def test_tight_tolerance_on_lateral_load(precision, rtol):
+    """A weak-axis (lateral) tip load: large displacements put the FP64 rounding level of K u
+    near the requested residual.  The refined (double-double) solution reaches rtol; the FP64
+    vector returned is its rounding, whose residual is at rtol or at the FP64 rounding level."""
+    m = _ibeam(40, seed=1)
+    K, F, _ = assemble_c3d10_sparse_3dof(m)
+    Ko, Fo = _oracle_K(m)
+    tip = np.flatnonzero(m.mesh_nodes[:, 0] >= m.mesh_nodes[:, 0].max() - 1e-12)
+    Fy = np.zeros_like(F)
+    Fy[3 * tip + 1] = 50e3 / len(tip)
+    u, st = solve_c3d10_system(K, Fy, method="pcg", rtol=rtol, precision=precision, max_iter=4000)
+    assert st["status"] == 0 and st["rel_res"] <= rtol
+    res, floor = _residual_longdouble(Ko, u, Fy)
+    assert res <= 2 * max(rtol, floor)

@@ -118,7 +118,7 @@ struct SolverWork {
   int npA = 0, npB = 0, npC = 0;
   DArray<double> partA, partB, partC;
   DArray<PcgScalars> scal;   // [0] = FP64 / inner solve, [1] = outer refinement
-  DArray<double> u64, r64;  // outer refinement vectors
+  DArray<double> u64, ulo, r64;  // outer refinement: u = u64 + ulo (double-double), r = F - K u
   DArray<float> r32;
   DArray<double> dinv64;      // Jacobi (point) of the fine matrix
   DArray<float> dinv32;

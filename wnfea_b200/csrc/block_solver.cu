@@ -22,6 +22,7 @@
 #include "amg.h"
 #include "block.h"
 #include "common.cuh"
+#include "eft.cuh"
 #include "solid.h"
 #include "spmv.cuh"
 #include "solver.h"
@@ -826,20 +827,7 @@ __global__ void kb_check(BlockScalars* S, const double* __restrict__ partC, int 
 // extra-precise refinement: U = U_hi + U_lo (double-double), R = F - K U with compensated
 // products and sums
 // ---------------------------------------------------------------------------------------
-// Error-free transformations: Knuth's TwoSum (a + b = s + e exactly) and TwoProduct by fused
-// multiply-add (a * b = p + e exactly), as in Ogita, Rump and Oishi, "Accurate sum and dot
-// product", SIAM J. Sci. Comput. 26 (2005).  The _rn intrinsics are never contracted or
-// reordered by the compiler.
-__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
-  s = __dadd_rn(a, b);
-  const double bb = __dsub_rn(s, a);
-  e = __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
-}
-__device__ __forceinline__ void two_prod(double a, double b, double& p, double& e) {
-  p = __dmul_rn(a, b);
-  e = __fma_rn(a, b, -p);
-}
-
+// (two_sum / two_prod: error-free transformations, eft.cuh)
 struct DD4 {
   C4<double> hi, lo;
 };

@@ -24,6 +24,7 @@
 
 #include "amg.h"
 #include "common.cuh"
+#include "eft.cuh"
 #include "kernels.h"
 #include "solid.h"
 #include "spmv.cuh"
@@ -469,35 +470,80 @@ __global__ void __launch_bounds__(kThreads) k_dot_self(int64_t n, const T* __res
 // mixed-precision refinement kernels (FP64)
 // ---------------------------------------------------------------------------------------
 
-// r64 = F - K64 u64, r32 = (float) r64, partC = r64 . r64
-__global__ void __launch_bounds__(kThreads, kMinBlocks) k_outer_residual(int64_t n_rows, const int32_t* __restrict__ rp,
-                                                             const int32_t* __restrict__ ci,
-                                                             const double* __restrict__ av, int64_t stride, const double* __restrict__ F,
-                                                             const double* __restrict__ u, double* __restrict__ r64,
-                                                             float* __restrict__ r32, double* __restrict__ partC) {
+// r64 = F - K64 (u + ulo) from compensated products and sums (Dot2), rounded to FP64 at the
+// end; r32 = (float) r64; partC = r64 . r64.  16 lanes per block row, each with a (sum, error)
+// pair over its blocks, combined by a butterfly of TwoSums (the same order in every lane).
+__global__ void __launch_bounds__(kThreads) k_outer_residual_dd(int64_t n_rows, const int32_t* __restrict__ rp,
+                                                                const int32_t* __restrict__ ci,
+                                                                const double* __restrict__ av, int64_t stride,
+                                                                const double* __restrict__ F,
+                                                                const double* __restrict__ u,
+                                                                const double* __restrict__ ulo,
+                                                                double* __restrict__ r64, float* __restrict__ r32,
+                                                                double* __restrict__ partC) {
   __shared__ double sh[kThreads / 32];
-  double s = 0.0;
+  double rr = 0.0;
   GROUP_ROW_LOOP(n_rows, 16) {
     const bool active = row < n_rows;
-    double acc[3];
-    group_block_row<3, 3, 16, kSoA, double, double>(rp, ci, av, stride, row, active, XLoad<double, double>{u}, acc,
-                                                    lane);
+    double s[3] = {0.0, 0.0, 0.0}, c[3] = {0.0, 0.0, 0.0};
+    if (active) {
+      const int32_t q1 = __ldg(rp + row + 1);
+      for (int32_t q = __ldg(rp + row) + lane; q < q1; q += 16) {
+        const int64_t col = __ldg(ci + q);
+        double uh[3], ul[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          uh[k] = u[col * 3 + k];
+          ul[k] = ulo[col * 3 + k];
+        }
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            const double a = __ldg(av + (int64_t)(r * 3 + k) * stride + q);
+            double p, ep, t, es;
+            two_prod(a, uh[k], p, ep);
+            two_sum(s[r], p, t, es);
+            s[r] = t;
+            c[r] += (ep + es) + a * ul[k];
+          }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) {
+        const double s2 = __shfl_xor_sync(0xffffffffu, s[r], o);
+        const double c2 = __shfl_xor_sync(0xffffffffu, c[r], o);
+        double t, e;
+        two_sum(s[r], s2, t, e);
+        s[r] = t;
+        c[r] = (c[r] + c2) + e;
+      }
     if (active && lane < 3) {
       const int64_t i = row * 3 + lane;
-      const double ri = F[i] - pick<3>(acc, lane);
+      const double sv = pick<3>(s, lane), cv = pick<3>(c, lane);
+      double t, e;
+      two_sum(F[i], -sv, t, e);
+      const double ri = t + (e - cv);
       r64[i] = ri;
       if (r32) r32[i] = (float)ri;
-      s += ri * ri;
+      rr += ri * ri;
     }
   }
-  write_part(s, partC, sh);
+  write_part(rr, partC, sh);
 }
 
-// u64 += (double) dx
+// (u, ulo) += dx as a double-double pair, renormalised so that u = fl(u + ulo)
 template <typename T>
-__global__ void k_accumulate(int64_t n, double* __restrict__ u, const T* __restrict__ dx) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    u[i] += (double)dx[i];
+__global__ void k_accumulate(int64_t n, double* __restrict__ u, double* __restrict__ ulo, const T* __restrict__ dx) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double s, e, h, g;
+    two_sum(u[i], (double)dx[i], s, e);
+    two_sum(s, __dadd_rn(ulo[i], e), h, g);
+    u[i] = h;
+    ulo[i] = g;
+  }
 }
 
 __global__ void k_fill_dinv(int64_t n_rows, int64_t nnzb, const int32_t* __restrict__ diag_block,
@@ -812,6 +858,7 @@ static int ensure_work(Solid* s) {
     WN_CHECK(W.p64.alloc(n));
     WN_CHECK(W.p32.alloc(n));
     WN_CHECK(W.u64.alloc(n));
+    WN_CHECK(W.ulo.alloc(n));
     WN_CHECK(W.r64.alloc(n));
     WN_CHECK(W.r32.alloc(n));
     WN_CHECK(W.dinv64.alloc(n));
@@ -887,11 +934,11 @@ int solver_setup(Solid* s, const wn_amg_params& prm) {
 // ---------------------------------------------------------------------------------------
 // solve
 // ---------------------------------------------------------------------------------------
-static int true_residual(Solid* s, SolverWork& W, const double* F, const double* u, float* r32, cudaStream_t st,
-                         double* rr) {
-  W.npC = resident_grid(k_outer_residual, kThreads, (s->n_nodes * 32 + kThreads - 1) / kThreads);
-  k_outer_residual<<<W.npC, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, s->nnzb, F, u,
-                                                            W.r64.p, r32, W.partC.p);
+// r64 = F - K (u64 + ulo) with the compensated kernel; *rr = ||r64||^2
+static int true_residual(Solid* s, SolverWork& W, const double* F, float* r32, cudaStream_t st, double* rr) {
+  W.npC = resident_grid(k_outer_residual_dd, kThreads, (s->n_nodes * 32 + kThreads - 1) / kThreads);
+  k_outer_residual_dd<<<W.npC, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, s->nnzb, F,
+                                                  W.u64.p, W.ulo.p, W.r64.p, r32, W.partC.p);
   k_reduce_rr<<<1, kThreads, 0, st>>>(W.scal.p + 1, W.partC.p, W.npC);
   W.launches += 2;
   WN_CUDA(cudaGetLastError());
@@ -902,9 +949,12 @@ static int true_residual(Solid* s, SolverWork& W, const double* F, const double*
   return 0;
 }
 
-// Outer loop common to all modes: u = 0; r = F - K u (FP64); while ||r|| > rtol ||F||: solve
-// K d = r approximately with the inner PCG, u += d, recompute the FP64 residual.
-//   mode 0 (fp64):  inner PCG FP64 (matrix, vectors, V-cycle), target 0.5 rtol ||F|| / ||r||
+// Outer loop common to all modes: u = 0; r = F - K u; while ||r|| > rtol ||F||: solve K d = r
+// approximately with the inner PCG, u += d, recompute the residual.  u is kept as a
+// double-double pair and r is evaluated with compensated products and sums, so the test
+// resolves residuals below the FP64 rounding level of K u (which for load cases with large
+// displacements can lie near 1e-8 ||F||); the returned u is the pair rounded to FP64.
+//   mode 0 (fp64):  inner PCG FP64 (matrix, vectors, V-cycle), target 0.25 rtol ||F|| / ||r||
 //   mode 1 (mixed): inner PCG FP64 with an FP32 AMG V-cycle (FP32 values, vectors and
 //                   accumulation; FP64 coarsest inverse), same target
 //   mode 2 (fp32 IR): inner PCG entirely FP32 (FP32 K SpMV) to max(inner_rtol, target);
@@ -917,11 +967,12 @@ static int outer_loop(Solid* s, SolverWork& W, int mode, const double* F, double
   const int max_outer = prm.max_outer > 0 ? prm.max_outer : 10;
   PcgScalars hS{};
   WN_CUDA(cudaMemsetAsync(W.u64.p, 0, n * sizeof(double), st));
+  WN_CUDA(cudaMemsetAsync(W.ulo.p, 0, n * sizeof(double), st));
   WN_CUDA(cudaMemcpyAsync(W.r64.p, F, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
   *rr = fnorm * fnorm;
   bool first = true;
   while (true) {
-    if (!first) WN_CHECK(true_residual(s, W, F, W.u64.p, mode == 2 ? W.r32.p : nullptr, st, rr));
+    if (!first) WN_CHECK(true_residual(s, W, F, mode == 2 ? W.r32.p : nullptr, st, rr));
     const double rn = std::sqrt(*rr);
     if (!std::isfinite(*rr)) {
       *status = WN_EBREAKDOWN;
@@ -932,12 +983,15 @@ static int outer_loop(Solid* s, SolverWork& W, int mode, const double* F, double
       *status = WN_ENOCONV;
       break;
     }
-    double target = std::min(0.5, 0.5 * prm.rtol * fnorm / rn);
+    // inner target a quarter of the remaining factor: the inner PCG's recursive residual drifts
+    // from the true one by FP64 rounding (about 5e-9 ||F|| on the 1M-DOF I-beam), so a target
+    // of rtol / 4 lets the first pass meet rtol on the true residual without a second pass
+    double target = std::min(0.5, 0.25 * prm.rtol * fnorm / rn);
     if (mode == 2) {
       const double inner = prm.inner_rtol > 0.0 ? prm.inner_rtol : 1e-4;
       target = std::max(target, inner);
       if (first) {  // r32 = (float) F
-        WN_CHECK(true_residual(s, W, F, W.u64.p, W.r32.p, st, rr));
+        WN_CHECK(true_residual(s, W, F, W.r32.p, st, rr));
       }
     }
     first = false;
@@ -955,7 +1009,7 @@ static int outer_loop(Solid* s, SolverWork& W, int mode, const double* F, double
       break;
     }
     PcgBufs<TK, TM> B = pcg_bufs<TK, TM>(s, W);
-    k_accumulate<TK><<<vec_grid(n), kThreads, 0, st>>>(n, W.u64.p, B.x);
+    k_accumulate<TK><<<vec_grid(n), kThreads, 0, st>>>(n, W.u64.p, W.ulo.p, B.x);
     W.launches++;
     WN_CUDA(cudaGetLastError());
   }
