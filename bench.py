@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--cpu-iters", type=int, default=12, help="scipy cg iterations in the CPU sample")
     ap.add_argument("--skip-jacobi", action="store_true", help="do not measure the Jacobi iteration count")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-multi", action="store_true", help="do not time the batched load cases")
+    ap.add_argument("--skip-adjoint", action="store_true", help="do not run the adjoint workload")
+    ap.add_argument("--fd-elements", type=int, default=50, help="elements of the finite-difference check")
     ap.add_argument("--cases", type=int, default=32, help="load cases of the batched (multi-RHS) solve")
     ap.add_argument("--only", choices=["solve-mixed", "solve-fp64", "solve-multi", "spmv32", "spmv64"], default=None,
                     help="profiling mode: run only this operation (warmup + steps times) and print its time")
@@ -260,6 +263,116 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def batched_cases(args, m, s, stream, ms_single):
+    """Load cases solved together: tip forces of magnitude U[10, 100] kN along directions
+    uniform on the sphere (seeded), one multi-RHS solve of the batch (FP64 PCG, FP32 V-cycle,
+    per-case true residual 1e-8), device-resident F and U."""
+    import torch
+
+    from wnfea_b200.mesh import tip_load_cases
+
+    Fm = torch.from_numpy(tip_load_cases(m.mesh_nodes, n_cases=args.cases, seed=0)).cuda()
+    Um = torch.empty_like(Fm)
+    sptr = stream.cuda_stream
+    s.solve_multi_device(Fm, Um, rtol=1e-8, precision=1, stream=sptr)  # warm-up (workspace, graph)
+    reps = max(1, min(args.steps, 3))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        info = s.solve_multi_device(Fm, Um, rtol=1e-8, precision=1, stream=sptr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    ndof = 3 * s.n_nodes
+    return {"cases": args.cases, "ms_per_batch": ms, "ms_per_case": ms / args.cases,
+            "case_dof_per_s": args.cases * ndof / (ms * 1e-3),
+            "speedup_vs_single_case_solves": args.cases * ms_single / ms,
+            "batched_iterations": info["iterations"], "outer_passes": info["outer_iterations"],
+            "status": info["status"], "max_case_rel_res": info["rel_res"],
+            "case_iterations_min_max": [int(info["case_iterations"].min()), int(info["case_iterations"].max())],
+            "workload": "same I-beam, tip forces U[10, 100] kN, direction uniform on the sphere (seed 0)"}
+
+
+def adjoint_workload(args, stream):
+    """Compliance adjoint on the 2 x 1 x 0.5 m block (60 x 30 x 15 hexes, 162,000 C3D10,
+    per-element E log-uniform in [1, 210] GPa, seed 0; bottom clamped, 10 kN/m^2 top pressure):
+    mixed-precision forward solve, dC/dE and dC/dF through torch.autograd, and a central
+    finite-difference check on seeded elements (h = 1e-3 E_e, FP64 solves to 1e-12)."""
+    import torch
+
+    from wnfea_b200.autograd import ComplianceProblem
+    from wnfea_b200.mesh import generate_c3d10_pressure_block
+    from wnfea_b200.model import solid_element_props, solid_load_vector
+
+    mb, meta = generate_c3d10_pressure_block(seed=0)
+    props = solid_element_props(mb)
+    prob = ComplianceProblem.from_model(mb, precision="mixed_fp32", rtol=1e-8, reuse_hierarchy=True)
+    E = torch.from_numpy(props[:, 0].copy()).cuda().requires_grad_(True)
+    F = torch.from_numpy(solid_load_vector(mb)).cuda().requires_grad_(True)
+    t0 = time.perf_counter()
+    C = prob.compliance(E, F)  # first forward builds the hierarchy
+    C.backward()
+    torch.cuda.synchronize()
+    first_s = time.perf_counter() - t0
+    setup_s = prob.last_stats["setup_seconds"]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for _ in range(reps):
+            fn()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]) / reps
+
+    Ed, Fd = E.detach(), F.detach()
+    solve_ms = timed(lambda: prob.solve(Ed, Fd), 3)
+    it_mixed = prob.last_stats["iterations"]
+    u, Fb = prob.solve(Ed, Fd)
+    grad_ms = timed(lambda: prob.gradient(u), 20)
+    g_mixed = prob.gradient(u)[0].cpu().numpy()
+
+    def fwd_bwd():
+        E.grad = None
+        F.grad = None
+        prob.compliance(E, F).backward()
+
+    autograd_ms = timed(fwd_bwd, 3)
+    # finite differences: FP64 solves to a true residual of 1e-12 (same hierarchy)
+    prob.precision, prob.rtol = "fp64", 1e-12
+    u64, Fb64 = prob.solve(Ed, Fd)
+    g64 = prob.gradient(u64)[0].cpu().numpy()
+    rng = np.random.default_rng(0)
+    els = rng.choice(len(props), size=args.fd_elements, replace=False)
+    errs = []
+    t0 = time.perf_counter()
+    for e in els:
+        h = 1e-3 * float(props[e, 0])
+        c = []
+        for sg in (1.0, -1.0):
+            Ep = Ed.clone()
+            Ep[e] += sg * h
+            up, Fbp = prob.solve(Ep, Fd)
+            c.append(float(torch.dot(Fbp, up)))
+        fd = (c[0] - c[1]) / (2 * h)
+        errs.append(abs(fd - g64[e]) / abs(g64[e]))
+    fd_s = time.perf_counter() - t0
+    prob.precision, prob.rtol = "mixed_fp32", 1e-8
+    ndof = 3 * len(mb.mesh_nodes)
+    return {"workload": f"C3D10 block 60x30x15 hexes, {meta['n_elements']} el / {ndof} DOFs, E log-uniform "
+                        "[1, 210] GPa (seed 0), bottom clamped, 10 kN/m^2 top pressure",
+            "grad_kernel_ms": grad_ms, "autograd_forward_backward_ms": autograd_ms,
+            "forward_solve_ms": solve_ms, "forward_iterations": it_mixed, "amg_setup_s": setup_s,
+            "first_forward_backward_s": first_s,
+            "fd_check": {"elements": int(args.fd_elements), "h": "1e-3 E_e", "solves": "FP64 to rel.res 1e-12",
+                         "max_rel_err": float(max(errs)), "median_rel_err": float(np.median(errs)),
+                         "seconds": fd_s},
+            "mixed_vs_fp64_gradient_max_rel_diff": float(np.max(np.abs(g_mixed - g64)) / np.max(np.abs(g64)))}
+
+
 def run_ours(args):
     import torch
 
@@ -368,6 +481,9 @@ def run_ours(args):
     torch.cuda.synchronize()
     adjoint_ms = ev[0].elapsed_time(ev[1]) / 10
 
+    multi = None if args.skip_multi else batched_cases(args, m, s, stream, ms_mixed)
+    adjoint = None if args.skip_adjoint else adjoint_workload(args, stream)
+
     # roofline: fine-level BSR3 SpMV, FP32 and FP64, event-timed on this stream
     nb, n_nodes = s.nnzb, s.n_nodes
     x64 = torch.randn(3 * n_nodes, dtype=torch.float64, device="cuda")
@@ -442,7 +558,10 @@ def run_ours(args):
         "assembly_ms": assembly_ms,
         "assembly_wall_s_first_call": t_asm_wall,
         "amg_setup_s": setup_s,
-        "adjoint_grad_ms": adjoint_ms,
+        "adjoint_grad_ms": adjoint["grad_kernel_ms"] if adjoint else None,
+        "adjoint_grad_ms_ibeam_field": adjoint_ms,
+        "adjoint": adjoint,
+        "multi_rhs": multi,
         "jacobi_pcg_iterations": jacobi_iters,
         "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak,
                      "traffic": ncu_traffic("bsr3_spmv_f32_ibeam200k.txt"), "peak_kind": peak_kind,
