@@ -247,7 +247,9 @@ int wn_c3d10_element_stiffness_noalloc(int64_t n_el, const double* d_nodes, cons
 /* Internal forces F_int = sum_e f_e(u) with f_e = sum_g w|J| B^T C B u_e (c3d10.py:252-283),
  * atomic-free (node gather in element order).  Same argument list and U/F_int stride of 6
  * as the reference's compute_c3d10_internal_forces_native (kernels.cpp:244-252); host
- * buffers; F_int is accumulated into (the reference's += scatter). */
+ * buffers; F_int is accumulated into (the reference's += scatter).  The node incidence is
+ * built on the GPU each call; the device buffers are a per-device workspace kept between
+ * calls (grown when a larger mesh arrives, held until exit), and calls are serialised. */
 int wn_c3d10_internal_forces(const double* nodes, const int32_t* solid_elements, const double* props, const double* U,
                              double* F_int, int n_solids, int n_nodes);
 /* Handle variant on device pointers: f_int (3 n_nodes, overwritten) from u (3 n_nodes). */

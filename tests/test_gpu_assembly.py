@@ -163,6 +163,37 @@ def test_internal_forces_reference_signature_stride6():
     assert np.array_equal(got[:, 3:], np.ones((n, 3)))
 
 
+def test_internal_forces_reference_signature_workspace_reuse():
+    """The host-buffer call keeps its device buffers between calls: alternating meshes of
+    different sizes give the device-resident kernel's bits every time; a bad node index is
+    rejected."""
+    meshes = [_c1(), generate_c3d10_ibeam_structured(n_slices=6, length=4.0 * 6 / 315, seed=2)[0]]
+    ref = []
+    for m in meshes:
+        props = np.ascontiguousarray(solid_element_props(m))
+        sysm = SolidSystem(m.mesh_nodes, m.solid_elements)
+        sysm.assemble(props, apply_bcs=False)
+        n = len(m.mesh_nodes)
+        u = np.random.default_rng(n).standard_normal(3 * n) * 1e-4
+        ref.append((m, props, u, sysm.internal_forces(u)))
+    for m, props, u, f_dev in ref + ref[::-1]:
+        n = len(m.mesh_nodes)
+        U6 = np.zeros(6 * n)
+        U6.reshape(n, 6)[:, :3] = u.reshape(n, 3)
+        F6 = np.zeros(6 * n)
+        _lib.call("wn_c3d10_internal_forces", _lib.ptr(np.ascontiguousarray(m.mesh_nodes)),
+                  _lib.ptr(np.ascontiguousarray(m.solid_elements, dtype=np.int32)), _lib.ptr(props), _lib.ptr(U6),
+                  _lib.ptr(F6), len(m.solid_elements), n)
+        assert np.array_equal(F6.reshape(n, 6)[:, :3].ravel(), f_dev)
+    m, props, u, _ = ref[0]
+    bad = np.ascontiguousarray(m.solid_elements, dtype=np.int32).copy()
+    bad[3, 4] = len(m.mesh_nodes)
+    n = len(m.mesh_nodes)
+    with pytest.raises(_lib.WnError):
+        _lib.call("wn_c3d10_internal_forces", _lib.ptr(np.ascontiguousarray(m.mesh_nodes)), _lib.ptr(bad),
+                  _lib.ptr(props), _lib.ptr(np.zeros(6 * n)), _lib.ptr(np.zeros(6 * n)), len(bad), n)
+
+
 def test_internal_forces_and_adjoint_match_oracle():
     m, _ = generate_c3d10_ibeam_structured(n_slices=6, length=4.0 * 6 / 315, seed=8)
     props = solid_element_props(m)

@@ -324,6 +324,129 @@ int launch_ke_upper(int64_t n_el, const double* nodes, const int32_t* conn, cons
   return 0;
 }
 
+// ---------------------------------------------------------------------------------------
+// node incidence on the device (for the stateless internal-force call)
+// ---------------------------------------------------------------------------------------
+__global__ void incidence_count_kernel(int64_t n_entries, int64_t nn, const int32_t* __restrict__ conn,
+                                       int32_t* __restrict__ counts, int* __restrict__ bad) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n_entries;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t v = conn[k];
+    if (v < 0 || v >= nn) {
+      *bad = 1;
+      continue;
+    }
+    atomicAdd(&counts[v], 1);  // integer counts: order-independent
+  }
+}
+
+// inclusive scan of one value per thread over a 1024-thread CTA
+__device__ __forceinline__ int64_t block_scan_1024(int64_t v, int64_t* sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  if (lane == 31) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    int64_t t = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t u = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += u;
+    }
+    sh[lane] = t;
+  }
+  __syncthreads();
+  const int64_t r = v + (w > 0 ? sh[w - 1] : 0);
+  __syncthreads();
+  return r;
+}
+
+// per 1024-entry chunk: out[i] = exclusive prefix inside the chunk, tot[chunk] = chunk sum
+__global__ void __launch_bounds__(1024) scan_chunks_kernel(int64_t n, const int32_t* __restrict__ in,
+                                                          int64_t* __restrict__ out, int64_t* __restrict__ tot) {
+  __shared__ int64_t sh[32];
+  const int64_t i = blockIdx.x * 1024 + threadIdx.x;
+  const int64_t v = i < n ? in[i] : 0;
+  const int64_t inc = block_scan_1024(v, sh);
+  if (i < n) out[i] = inc - v;
+  if (threadIdx.x == 1023) tot[blockIdx.x] = inc;
+}
+
+// one CTA: exclusive scan of the chunk sums in place (any count, in passes of 1024), total to *total
+__global__ void __launch_bounds__(1024) scan_totals_kernel(int64_t n_chunks, int64_t* __restrict__ tot,
+                                                          int64_t* __restrict__ total) {
+  __shared__ int64_t sh[32];
+  __shared__ int64_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int64_t base = 0; base < n_chunks; base += 1024) {
+    const int64_t i = base + threadIdx.x;
+    const int64_t v = i < n_chunks ? tot[i] : 0;
+    const int64_t inc = block_scan_1024(v, sh);
+    const int64_t c = carry;
+    if (i < n_chunks) tot[i] = c + inc - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry = c + inc;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void scan_add_kernel(int64_t n, const int64_t* __restrict__ tot, int64_t* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] += tot[i >> 10];
+}
+
+__global__ void incidence_fill_kernel(int64_t n_entries, int64_t nn, const int32_t* __restrict__ conn,
+                                      const int64_t* __restrict__ inc_ptr, int32_t* __restrict__ cursor,
+                                      int32_t* __restrict__ inc) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n_entries;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t v = conn[k];
+    if (v < 0 || v >= nn) continue;
+    const int32_t p = atomicAdd(&cursor[v], 1);
+    inc[inc_ptr[v] + p] = (int32_t)k;
+  }
+}
+
+// each node's entries in ascending e * 10 + a (insertion sort; ~10-50 entries per node), so
+// that the node gather sums in a fixed order whatever order the fill wrote them in
+__global__ void incidence_sort_kernel(int64_t nn, const int64_t* __restrict__ inc_ptr, int32_t* __restrict__ inc) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nn; v += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = inc_ptr[v], e = inc_ptr[v + 1];
+    for (int64_t i = s + 1; i < e; ++i) {
+      const int32_t key = inc[i];
+      int64_t j = i - 1;
+      while (j >= s && inc[j] > key) {
+        inc[j + 1] = inc[j];
+        --j;
+      }
+      inc[j + 1] = key;
+    }
+  }
+}
+
+int launch_build_incidence(int64_t nn, int64_t ne, const int32_t* conn, int32_t* counts, int64_t* inc_ptr,
+                           int32_t* inc, int64_t* scan, int* flags, cudaStream_t st) {
+  const int64_t n_entries = ne * 10;
+  const int64_t n_chunks = (nn + 1023) / 1024;
+  WN_CUDA(cudaMemsetAsync(counts, 0, nn * sizeof(int32_t), st));
+  WN_CUDA(cudaMemsetAsync(flags, 0, 2 * sizeof(int), st));
+  incidence_count_kernel<<<grid_for(n_entries, 1, 256, 8), 256, 0, st>>>(n_entries, nn, conn, counts, flags);
+  scan_chunks_kernel<<<(int)n_chunks, 1024, 0, st>>>(nn, counts, inc_ptr, scan);
+  scan_totals_kernel<<<1, 1024, 0, st>>>(n_chunks, scan, inc_ptr + nn);
+  scan_add_kernel<<<grid_for(nn, 1, 256, 8), 256, 0, st>>>(nn, scan, inc_ptr);
+  WN_CUDA(cudaMemsetAsync(counts, 0, nn * sizeof(int32_t), st));
+  incidence_fill_kernel<<<grid_for(n_entries, 1, 256, 8), 256, 0, st>>>(n_entries, nn, conn, inc_ptr, counts, inc);
+  incidence_sort_kernel<<<grid_for(nn, 1, 256, 8), 256, 0, st>>>(nn, inc_ptr, inc);
+  WN_CUDA(cudaGetLastError());
+  return 0;
+}
+
 int launch_gather_assemble(int64_t nnzb, const int32_t* gptr, const int32_t* gsrc, const double* ke,
                            const int32_t* block_row, const int32_t* col_idx, const uint8_t* fixed, double* k64,
                            float* k32, cudaStream_t st) {

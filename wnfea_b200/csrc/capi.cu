@@ -3,6 +3,7 @@
 #include <cstdarg>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 
@@ -62,6 +63,49 @@ static int read_flag(Solid* s, cudaStream_t st, int* value) {
 }  // namespace wn
 
 using namespace wn;
+
+namespace {
+
+// Device buffers of the stateless host-buffer internal-force call, kept per device and grown
+// on demand (never shrunk) so that repeated calls neither allocate nor free.
+struct FintWorkspace {
+  DArray<double> nodes, props, u, f, fe;
+  DArray<int32_t> conn, counts, inc;
+  DArray<int64_t> inc_ptr, scan;
+  DArray<int> flags;
+  template <typename T>
+  static int at_least(DArray<T>& a, int64_t n) {
+    return a.n >= n ? 0 : a.alloc(n);
+  }
+  int grow(int64_t nn, int64_t ne) {
+    WN_CHECK(at_least(nodes, nn * 3));
+    WN_CHECK(at_least(u, nn * 6));
+    WN_CHECK(at_least(f, nn * 6));
+    WN_CHECK(at_least(props, ne * 2));
+    WN_CHECK(at_least(fe, ne * 30));
+    WN_CHECK(at_least(conn, ne * 10));
+    WN_CHECK(at_least(counts, nn));
+    WN_CHECK(at_least(inc, ne * 10));
+    WN_CHECK(at_least(scan, (nn + 1023) / 1024 + 1));
+    WN_CHECK(at_least(inc_ptr, nn + 1));
+    WN_CHECK(at_least(flags, 2));
+    return 0;
+  }
+};
+
+std::mutex& fint_workspace_mutex() {
+  static std::mutex mu;
+  return mu;
+}
+
+FintWorkspace& fint_workspace(int dev) {
+  static std::map<int, std::unique_ptr<FintWorkspace>> ws;
+  auto& p = ws[dev];
+  if (!p) p.reset(new FintWorkspace());
+  return *p;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -338,38 +382,29 @@ int wn_c3d10_internal_forces(const double* nodes, const int32_t* solid_elements,
              "wn_c3d10_internal_forces: bad argument");
   if (n_solids == 0) return 0;
   WN_REQUIRE(solid_elements && props, WN_EINVAL, "wn_c3d10_internal_forces: null argument");
-  Bsr3Pattern pat;
-  // only the node incidence is needed; build it directly
-  std::vector<int64_t> inc_ptr(n_nodes + 1, 0);
-  for (int64_t k = 0; k < (int64_t)n_solids * 10; ++k) {
-    WN_REQUIRE(solid_elements[k] >= 0 && solid_elements[k] < n_nodes, WN_EMESH,
-               "wn_c3d10_internal_forces: node index out of range");
-    inc_ptr[solid_elements[k] + 1]++;
-  }
-  for (int i = 0; i < n_nodes; ++i) inc_ptr[i + 1] += inc_ptr[i];
-  std::vector<int32_t> inc((int64_t)n_solids * 10);
-  {
-    std::vector<int64_t> pos(inc_ptr.begin(), inc_ptr.end() - 1);
-    for (int64_t e = 0; e < n_solids; ++e)
-      for (int a = 0; a < 10; ++a) inc[pos[solid_elements[e * 10 + a]]++] = (int32_t)(e * 10 + a);
-  }
-  DArray<double> dn, dp, du, dfe, df;
-  DArray<int32_t> dc, dinc;
-  DArray<int64_t> dptr;
-  DArray<int> flags;
-  WN_CHECK(dn.upload(nodes, (int64_t)n_nodes * 3));
-  WN_CHECK(dc.upload(solid_elements, (int64_t)n_solids * 10));
-  WN_CHECK(dp.upload(props, (int64_t)n_solids * 2));
-  WN_CHECK(du.upload(U, (int64_t)n_nodes * 6));
-  WN_CHECK(df.upload(F_int, (int64_t)n_nodes * 6));
-  WN_CHECK(dptr.upload(inc_ptr));
-  WN_CHECK(dinc.upload(inc));
-  WN_CHECK(dfe.alloc((int64_t)n_solids * 30));
-  WN_CHECK(flags.alloc(1));
-  WN_CHECK(flags.zero());
-  WN_CHECK(launch_element_force(n_solids, dn.p, dc.p, dp.p, du.p, 6, dfe.p, nullptr, nullptr, flags.p, 0));
-  WN_CHECK(launch_node_gather(n_nodes, dptr.p, dinc.p, dfe.p, 6, 1, df.p, 0));
-  WN_CUDA(cudaMemcpy(F_int, df.p, df.bytes(), cudaMemcpyDeviceToHost));
+  int dev = 0;
+  WN_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(fint_workspace_mutex());
+  FintWorkspace& w = fint_workspace(dev);
+  const int64_t ne = n_solids, nn = n_nodes;
+  WN_CHECK(w.grow(nn, ne));
+  cudaStream_t st = 0;
+  WN_CUDA(cudaMemcpyAsync(w.nodes.p, nodes, nn * 3 * sizeof(double), cudaMemcpyHostToDevice, st));
+  WN_CUDA(cudaMemcpyAsync(w.conn.p, solid_elements, ne * 10 * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  WN_CUDA(cudaMemcpyAsync(w.props.p, props, ne * 2 * sizeof(double), cudaMemcpyHostToDevice, st));
+  WN_CUDA(cudaMemcpyAsync(w.u.p, U, nn * 6 * sizeof(double), cudaMemcpyHostToDevice, st));
+  WN_CUDA(cudaMemcpyAsync(w.f.p, F_int, nn * 6 * sizeof(double), cudaMemcpyHostToDevice, st));
+  // node -> (element, local node) incidence on the device, in ascending e * 10 + a per node
+  WN_CHECK(launch_build_incidence(nn, ne, w.conn.p, w.counts.p, w.inc_ptr.p, w.inc.p, w.scan.p, w.flags.p, st));
+  int bad = 0;
+  WN_CUDA(cudaMemcpyAsync(&bad, w.flags.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  WN_CUDA(cudaStreamSynchronize(st));
+  WN_REQUIRE(bad == 0, WN_EMESH, "wn_c3d10_internal_forces: node index out of range");
+  WN_CHECK(launch_element_force(ne, w.nodes.p, w.conn.p, w.props.p, w.u.p, 6, w.fe.p, nullptr, nullptr,
+                                w.flags.p + 1, st));
+  WN_CHECK(launch_node_gather(nn, w.inc_ptr.p, w.inc.p, w.fe.p, 6, 1, w.f.p, st));
+  WN_CUDA(cudaMemcpyAsync(F_int, w.f.p, nn * 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  WN_CUDA(cudaStreamSynchronize(st));
   return 0;
 }
 

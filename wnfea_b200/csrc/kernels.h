@@ -18,6 +18,11 @@ int launch_element_force(int64_t n_el, const double* nodes, const int32_t* conn,
                          int* flags, cudaStream_t st);
 int launch_node_gather(int64_t n_nodes, const int64_t* inc_ptr, const int32_t* inc_ea, const double* fe, int stride,
                        int accumulate, double* out, cudaStream_t st);
+// Node -> (element, local node) incidence of a C3D10 connectivity on the device: inc_ptr (nn + 1)
+// and inc (10 ne entries e * 10 + a, ascending within each node).  counts: nn ints, scan:
+// ceil(nn / 1024) + 1 int64 scratch; flags[0] is set when a node index is out of range.
+int launch_build_incidence(int64_t nn, int64_t ne, const int32_t* conn, int32_t* counts, int64_t* inc_ptr,
+                           int32_t* inc, int64_t* scan, int* flags, cudaStream_t st);
 int launch_stress(int64_t n_el, int64_t n_nodes, const double* nodes, const int32_t* conn, const double* props,
                   const double* u, const int64_t* inc_ptr, const int32_t* inc_ea, double* cell_sig, double* cell_vm,
                   double* nodal_vm, cudaStream_t st);
