@@ -19,6 +19,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -306,33 +308,47 @@ void rows_to_bsr(int br, int bc, int64_t n_rows, int64_t n_cols, std::vector<std
   });
 }
 
-// C = A * B for block-sparse A (ar x ac blocks) and B (ac x bc2 blocks)
-void spgemm(const View& A, const View& B, HostBsr& C) {
+// C = A * B for block-sparse A (AR x AK blocks) and B (AK x BC blocks).  The block shapes
+// are compile-time so that the block products unroll and vectorise: the coarse operators of
+// 3D meshes reach hundreds of 6x6 blocks per row, and these products are most of the setup.
+template <int AR, int AK, int BC>
+void spgemm_blocks(const View& A, const View& B, HostBsr& C) {
   std::vector<std::vector<int32_t>> rc(A.n_rows);
   std::vector<std::vector<double>> rv(A.n_rows);
-  const int ar = A.br, ak = A.bc, bcn = B.bc;
   par_rows(A.n_rows, [&](int64_t a, int64_t b, int) {
     RowAcc acc;
-    acc.init(B.n_cols, ar * bcn);
+    acc.init(B.n_cols, AR * BC);
     for (int64_t i = a; i < b; ++i) {
       for (int32_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
         const int32_t j = A.ci[k];
-        const double* ab = A.v + (size_t)k * ar * ak;
+        const double* ab = A.v + (size_t)k * AR * AK;
         for (int32_t q = B.rp[j]; q < B.rp[j + 1]; ++q) {
-          const double* bb = B.v + (size_t)q * ak * bcn;
+          const double* bb = B.v + (size_t)q * AK * BC;
           double* c = acc.slot(B.ci[q]);
-          for (int r = 0; r < ar; ++r)
-            for (int s = 0; s < ak; ++s) {
-              const double av = ab[r * ak + s];
-              if (av == 0.0) continue;
-              for (int t = 0; t < bcn; ++t) c[r * bcn + t] += av * bb[s * bcn + t];
+          for (int r = 0; r < AR; ++r)
+            for (int s = 0; s < AK; ++s) {
+              const double av = ab[r * AK + s];
+              for (int t = 0; t < BC; ++t) c[r * BC + t] += av * bb[s * BC + t];
             }
         }
       }
       acc.flush(rc[i], rv[i]);
     }
   });
-  rows_to_bsr(ar, bcn, A.n_rows, B.n_cols, rc, rv, C);
+  rows_to_bsr(AR, BC, A.n_rows, B.n_cols, rc, rv, C);
+}
+
+// the shapes of the Galerkin products: A0 P0 (3x3 . 3x6), R0 (A0 P0) (6x3 . 3x6), coarse (6x6)
+void spgemm(const View& A, const View& B, HostBsr& C) {
+  if (A.br == 3 && A.bc == 3 && B.bc == 6) return spgemm_blocks<3, 3, 6>(A, B, C);
+  if (A.br == 6 && A.bc == 3 && B.bc == 6) return spgemm_blocks<6, 3, 6>(A, B, C);
+  if (A.br == 6 && A.bc == 6 && B.bc == 6) return spgemm_blocks<6, 6, 6>(A, B, C);
+  if (A.br == 3 && A.bc == 3 && B.bc == 3) return spgemm_blocks<3, 3, 3>(A, B, C);
+  if (A.br == 6 && A.bc == 6 && B.bc == 3) return spgemm_blocks<6, 6, 3>(A, B, C);
+  if (A.br == 3 && A.bc == 6 && B.bc == 6) return spgemm_blocks<3, 6, 6>(A, B, C);
+  // no other shape occurs in the hierarchy
+  std::fprintf(stderr, "amg_build: unexpected block product %dx%d . %dx%d\n", A.br, A.bc, B.br, B.bc);
+  std::abort();
 }
 
 // transpose of a block-sparse matrix (blocks transposed too); rows of T in source-row order
