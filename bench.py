@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--skip-adjoint", action="store_true", help="do not run the adjoint workload")
     ap.add_argument("--fd-elements", type=int, default=50, help="elements of the finite-difference check")
     ap.add_argument("--cases", type=int, default=32, help="load cases of the batched (multi-RHS) solve")
+    ap.add_argument("--order", choices=["native", "scrambled", "rcm"], default="native",
+                    help="profiling mode: node numbering -- the generator's, a seeded random one, or RCM of that")
     ap.add_argument("--only", choices=["solve-mixed", "solve-fp64", "solve-multi", "spmv32", "spmv64"], default=None,
                     help="profiling mode: run only this operation (warmup + steps times) and print its time")
     return ap.parse_args()
@@ -76,6 +78,8 @@ def run_only(args):
     from wnfea_b200.solid_solver import assemble_c3d10_sparse_3dof
 
     m, meta = build_model(args.slices)
+    if args.order != "native":
+        m = renumber(m, args.order)
     K, F_np, _ = assemble_c3d10_sparse_3dof(m)
     s = K.system
     st = torch.cuda.current_stream().cuda_stream
@@ -119,7 +123,7 @@ def run_only(args):
     for _ in range(args.steps):
         op()
     torch.cuda.synchronize()
-    out = {"only": args.only, "ms_per_op": (time.perf_counter() - t0) * 1e3 / args.steps,
+    out = {"only": args.only, "order": args.order, "ms_per_op": (time.perf_counter() - t0) * 1e3 / args.steps,
            "elements": meta["n_elements"], "nnz_blocks": s.nnzb}
     if args.only in ("solve-mixed", "solve-fp64"):
         out.update(info)
@@ -129,6 +133,24 @@ def run_only(args):
                     "device_ms": info["solve_seconds"] * 1e3,
                     "case_iterations": [int(v) for v in info["case_iterations"]]})
     print(json.dumps(out))
+
+
+def renumber(m, order):
+    """The I-beam with a seeded random node numbering (an arbitrary mesher's), or RCM of it."""
+    n = len(m.mesh_nodes)
+    perm = np.random.default_rng(0).permutation(n)
+    inv = np.empty(n, dtype=np.int64)
+    inv[perm] = np.arange(n)
+    m.mesh_nodes = m.mesh_nodes[perm].copy()
+    m.solid_elements = inv[m.solid_elements].astype(np.int32)
+    for item in list(m.supports) + list(m.loads):
+        if not item.is_geometry_node:
+            item.node_id = int(inv[item.node_id])
+    if order == "rcm":
+        from wnfea_b200.rcm import apply_rcm_to_model
+
+        m = apply_rcm_to_model(m)[0]
+    return m
 
 
 def build_model(slices):

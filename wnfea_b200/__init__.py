@@ -25,6 +25,14 @@ from .beam import (
     prepare_batch_data,
     solve_nonlinear_jfnk,
 )
+from .rcm import (
+    apply_rcm_to_model,
+    compute_matrix_bandwidth,
+    compute_node_adjacency_matrix,
+    compute_rcm_order,
+    permute_solution_to_original,
+)
+from .vtu import VTUExporter, export_vtu
 from .mixed_precision import FULL_FP64, MIXED_FP32, TRI_PRECISION, PrecisionConfig
 from .solid_solver import (
     assemble_c3d10_sparse_3dof,
@@ -42,4 +50,6 @@ __all__ = [
     "PrecisionConfig", "MIXED_FP32", "FULL_FP64", "TRI_PRECISION",
     "compute_internal_forces_fast", "prepare_batch_data", "solve_nonlinear_jfnk", "NonLinearConvergenceError",
     "BeamFrame", "ComplianceProblem", "Compliance",
+    "apply_rcm_to_model", "compute_matrix_bandwidth", "compute_node_adjacency_matrix", "compute_rcm_order",
+    "permute_solution_to_original", "VTUExporter", "export_vtu",
 ]
