@@ -186,6 +186,21 @@ int wn_solve_device(void* h, const double* d_F, double* d_u, const wn_solve_para
 /* Host buffers F, u (copies in and out). */
 int wn_solve(void* h, const double* F, double* u, const wn_solve_params* params, wn_solve_stats* stats);
 
+/* Linear 6-DOF-per-node systems (beam frames; the reference's GPU AMG-PCG of
+ * BlockBeamAMGPreconditioner.solve_pcg -> hip_solve_pcg_amg, fast_kernels.py:598-663 and
+ * hip_kernels.cpp:1746-2546): a solver handle with 6x6 blocks (row-major, block-contiguous)
+ * that wn_amg_setup, wn_solve / wn_solve_device, wn_solid_info / _get_pattern and
+ * wn_solid_destroy accept; the C3D10-only entry points return WN_ESTATE for it.  The AMG's
+ * near-null space is the 6 rigid-body modes of 6-DOF nodes (translations; rotations w moving a
+ * node by w x X and turning it by w), zero on fixed DOFs.  Columns sorted and unique per row,
+ * a diagonal block in every row; fixed_mask (6 n_nodes, optional) marks Dirichlet DOFs whose
+ * rows/columns the caller has already made identity. */
+int wn_bsr6_system_create(int64_t n_nodes, const int32_t* row_ptr, const int32_t* col_idx, const double* values,
+                          const double* coords, const uint8_t* fixed_mask, void** out_handle);
+/* The same from a beam handle's last assembled tangent (wn_beam_evaluate with
+ * assemble_tangent = 1; apply_bcs = 1 for a constrained frame), values copied on the device. */
+int wn_beam_linear_system(void* beam, void** out_handle);
+
 /* Multi-right-hand-side solve (no reference counterpart: the reference solves load cases one
  * solve_c3d10_pcg call at a time, solid_solver.py:197-308).  F, U: row-major n x n_rhs
  * (n = 3 n_nodes, load case j in column j).  Cases are solved in batches of 32 sharing every

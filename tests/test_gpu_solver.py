@@ -195,3 +195,22 @@ def test_tight_tolerance_on_lateral_load(precision, rtol):
     assert st["status"] == 0 and st["rel_res"] <= rtol
     res, floor = _residual_longdouble(Ko, u, Fy)
     assert res <= 2 * max(rtol, floor)
+
+
+def test_tiny_mesh_hierarchy_without_levels():
+    """Fewer DOFs than the coarse-solve size: the 'V-cycle' is the dense coarse solve alone."""
+    from wnfea_b200.mesh import tip_load_cases
+
+    m, _ = generate_c3d10_kuhn_block(length=0.2, width=0.1, height=0.1, nx=2, ny=2, nz=2)
+    K, F, _ = assemble_c3d10_sparse_3dof(m)
+    Ko, Fo = _oracle_K(m)
+    ur = spsolve(Ko.tocsc(), Fo)
+    for precision in ("fp64", "mixed_fp32"):
+        u, st = solve_c3d10_system(K, F, method="pcg", rtol=1e-10, precision=precision)
+        assert st["status"] == 0 and st["levels"] == 1
+        assert np.linalg.norm(u - ur) <= 1e-8 * np.linalg.norm(ur)
+    Fm = tip_load_cases(m.mesh_nodes, n_cases=3, seed=0)
+    U, stm = K.system.solve_multi(Fm, rtol=1e-10, precision=1)
+    assert stm["status"] == 0
+    Ur = spsolve(Ko.tocsc(), Fm)
+    assert np.linalg.norm(U - Ur) <= 1e-8 * np.linalg.norm(Ur)

@@ -114,6 +114,8 @@ SIGNATURES: dict[str, tuple] = {
     "wn_amg_host_coarse": (_I, [_P, _PI64, _P, _P]),
     "wn_solve_device": (_I, [_P, _P, _P, C.POINTER(SolveParams), C.POINTER(SolveStats), _U]),
     "wn_solve": (_I, [_P, _P, _P, C.POINTER(SolveParams), C.POINTER(SolveStats)]),
+    "wn_bsr6_system_create": (_I, [_I64, _P, _P, _P, _P, _P, C.POINTER(_P)]),
+    "wn_beam_linear_system": (_I, [_P, C.POINTER(_P)]),
     "wn_solve_multi_device": (_I, [_P, _I, _P, _P, C.POINTER(SolveParams), C.POINTER(SolveStats), _P, _P, _U]),
     "wn_solve_multi": (_I, [_P, _I, _P, _P, C.POINTER(SolveParams), C.POINTER(SolveStats), _P, _P]),
     "wn_beam_internal_forces": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I]),

@@ -159,6 +159,85 @@ class BeamFrame:
         return x, it.value, rr.value, rc
 
 
+class FrameSystem:
+    """A linear 6-DOF-per-node system on the GPU (``wn_beam_linear_system``): smoothed-
+    aggregation AMG over the 6 rigid-body modes of beam nodes and PCG, in FP64 or with an FP32
+    V-cycle -- the B200 counterpart of BlockBeamAMGPreconditioner.solve_pcg ->
+    hip_solve_pcg_amg (fast_kernels.py:598-663)."""
+
+    def __init__(self, frame: BeamFrame):
+        h = C.c_void_p()
+        call("wn_beam_linear_system", frame._h, C.byref(h))
+        self._h = h
+        self.n = frame.n
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().wn_solid_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def amg_setup(self, params=None) -> float:
+        from .amg import AMGParams
+
+        prm = (params or AMGParams()).to_c()
+        t0 = time.perf_counter()
+        call("wn_amg_setup", self._h, C.byref(prm))
+        return time.perf_counter() - t0
+
+    def solve(self, F: np.ndarray, rtol: float = 1e-8, max_iter: int = 2000, precision: str = "mixed_fp32",
+              chunk: int = 8):
+        """U with K U = F (F zero on fixed DOFs); returns (U, stats dict)."""
+        prec = {"fp64": 0, "mixed_fp32": 1}[precision]
+        F = np.ascontiguousarray(F, dtype=np.float64)
+        U = np.empty_like(F)
+        prm = _lib.SolveParams(rtol, max_iter, 2, prec, 0.0, 10, chunk, 1)
+        st = _lib.SolveStats()
+        call("wn_solve", self._h, ptr(F), ptr(U), C.byref(prm), C.byref(st))
+        return U, {f: getattr(st, f) for f, _ in _lib.SolveStats._fields_}
+
+    def solve_device(self, F, U, rtol: float = 1e-8, max_iter: int = 2000, precision: str = "mixed_fp32",
+                     stream: int = 0):
+        prm = _lib.SolveParams(rtol, max_iter, 2, {"fp64": 0, "mixed_fp32": 1}[precision], 0.0, 10, 8, 1)
+        st = _lib.SolveStats()
+        call("wn_solve_device", self._h, _lib.dptr(F), _lib.dptr(U), C.byref(prm), C.byref(st), stream)
+        return {f: getattr(st, f) for f, _ in _lib.SolveStats._fields_}
+
+
+def frame_linear_system(model: FEAModel) -> tuple[BeamFrame, FrameSystem, np.ndarray]:
+    """(frame, system, F): the frame's stiffness at U = 0 with its fixed DOFs made identity,
+    as a GPU AMG-PCG system, and the load vector with zeros on the fixed DOFs.  Only fixed
+    (zero) supports: a prescribed non-zero value raises."""
+    dofs, vals = get_boundary_constraints(model)
+    if np.any(vals != 0.0):
+        raise ValueError("frame_linear_system: prescribed non-zero displacements are not supported")
+    frame = BeamFrame(model)
+    mask = np.zeros(frame.n, dtype=np.uint8)
+    mask[dofs] = 1
+    frame.set_fixed(mask)
+    frame.assemble_tangent(np.zeros(frame.n), apply_bcs=True)
+    F = build_external_force_vector(model)
+    F[dofs] = 0.0
+    return frame, FrameSystem(frame), F
+
+
+def solve_frame_linear(model: FEAModel, rtol: float = 1e-8, precision: str = "mixed_fp32", amg_params=None,
+                       max_iter: int = 2000):
+    """Linear static solve of a beam frame on the GPU -> (U (n_nodes * 6,), stats)."""
+    frame, system, F = frame_linear_system(model)
+    setup_s = system.amg_setup(amg_params)
+    U, st = system.solve(F, rtol=rtol, max_iter=max_iter, precision=precision)
+    st["setup_seconds"] = setup_s
+    system.close()
+    frame.close()
+    return U, st
+
+
 def _mesh_node(model: FEAModel, node_id: int, is_geometry_node: bool):
     if is_geometry_node:
         return model.geometry_to_mesh_node_map.get(node_id)

@@ -401,26 +401,28 @@ void symmetrize(HostBsr& A) {
 
 }  // namespace
 
-int amg_build(const wn_amg_params& prm, int64_t n0, const int32_t* rp0, const int32_t* ci0, const double* v0,
-              const double* coords, const uint8_t* fixed, HostHierarchy& out) {
+int amg_build(const wn_amg_params& prm, int64_t n0, int bs0, const int32_t* rp0, const int32_t* ci0,
+              const double* v0, const double* coords, const uint8_t* fixed, HostHierarchy& out) {
   out = HostHierarchy();
   out.params = prm;
-  WN_REQUIRE(n0 > 0 && rp0 && ci0 && v0 && coords, WN_EINVAL, "amg_build: bad argument");
-  // near-null space on level 0: the 6 rigid-body modes, zero on fixed DOFs
-  std::vector<double> B((size_t)n0 * 3 * 6, 0.0);
+  WN_REQUIRE(n0 > 0 && rp0 && ci0 && v0 && coords && (bs0 == 3 || bs0 == 6), WN_EINVAL, "amg_build: bad argument");
+  // near-null space on level 0: the 6 rigid-body modes, zero on fixed DOFs.  Rows ux, uy, uz
+  // (and for 6-DOF nodes rx, ry, rz); columns tx, ty, tz, rx, ry, rz (the layout of
+  // amg_preconditioner.py:30-69): a rotation w moves a node by w x X and turns it by w.
+  std::vector<double> B((size_t)n0 * bs0 * 6, 0.0);
   for (int64_t i = 0; i < n0; ++i) {
     const double X = coords[i * 3], Y = coords[i * 3 + 1], Z = coords[i * 3 + 2];
-    double* b = &B[(size_t)i * 18];
-    // rows ux, uy, uz; columns tx, ty, tz, rx, ry, rz (amg_preconditioner.py:30-69 layout)
-    const double m[3][6] = {{1, 0, 0, 0, Z, -Y}, {0, 1, 0, -Z, 0, X}, {0, 0, 1, Y, -X, 0}};
-    for (int r = 0; r < 3; ++r) {
-      const bool fx = fixed && fixed[i * 3 + r];
+    double* b = &B[(size_t)i * bs0 * 6];
+    const double m[6][6] = {{1, 0, 0, 0, Z, -Y}, {0, 1, 0, -Z, 0, X}, {0, 0, 1, Y, -X, 0},
+                            {0, 0, 0, 1, 0, 0},  {0, 0, 0, 0, 1, 0},  {0, 0, 0, 0, 0, 1}};
+    for (int r = 0; r < bs0; ++r) {
+      const bool fx = fixed && fixed[i * bs0 + r];
       for (int c = 0; c < 6; ++c) b[r * 6 + c] = fx ? 0.0 : m[r][c];
     }
   }
-  View A{3, 3, n0, n0, rp0, ci0, v0};
+  View A{bs0, bs0, n0, n0, rp0, ci0, v0};
   HostBsr Aown;
-  int bs = 3;
+  int bs = bs0;
   int64_t n = n0;
   for (int lvl = 0;; ++lvl) {
     const int64_t ndof = n * bs;

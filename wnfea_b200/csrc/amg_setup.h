@@ -38,8 +38,8 @@ struct HostHierarchy {
 
 // Build the hierarchy from the fine BSR3 matrix (FP64), node coordinates (n x 3) and the
 // Dirichlet mask (3n, may be null).  Returns WN_OK or a WN_E* code (message set).
-int amg_build(const wn_amg_params& prm, int64_t n_nodes, const int32_t* rp, const int32_t* ci, const double* vals,
-              const double* coords, const uint8_t* fixed, HostHierarchy& out);
+int amg_build(const wn_amg_params& prm, int64_t n0, int bs0, const int32_t* rp0, const int32_t* ci0,
+              const double* v0, const double* coords, const uint8_t* fixed, HostHierarchy& out);
 
 wn_amg_params amg_default_params();
 

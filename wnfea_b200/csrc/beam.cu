@@ -586,6 +586,21 @@ int wn_beam_get_tangent(void* h, double* values) {
   return 0;
 }
 
+int wn_beam_linear_system(void* h, void** out) {
+  WN_REQUIRE(h && out, WN_EINVAL, "wn_beam_linear_system: null argument");
+  Beam* b = as_beam(h);
+  WN_REQUIRE(b->assembled, WN_ESTATE, "wn_beam_linear_system: assemble the tangent first");
+  WN_CUDA(cudaSetDevice(b->device));
+  std::vector<double> coords(b->n_nodes * 3);
+  std::vector<uint8_t> fixed(b->n_nodes * 6);
+  WN_CUDA(cudaMemcpy(coords.data(), b->nodes.p, coords.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  WN_CUDA(cudaMemcpy(fixed.data(), b->fixed.p, fixed.size(), cudaMemcpyDeviceToHost));
+  bool any = false;
+  for (uint8_t f : fixed) any = any || f;
+  return make_bsr6_system(b->n_nodes, b->h_rp.data(), b->h_ci.data(), b->K.p, true, coords.data(),
+                          any ? fixed.data() : nullptr, out);
+}
+
 int wn_beam_solve_device(void* h, const double* d_b, double* d_x, int method, double rtol, int max_iter, int* iters,
                          double* rel_res, uintptr_t stream) {
   WN_REQUIRE(h && d_b && d_x && rtol > 0 && max_iter > 0 && method >= 0 && method <= 2, WN_EINVAL,

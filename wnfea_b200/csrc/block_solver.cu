@@ -910,6 +910,22 @@ __global__ void kb_accumulate(int64_t n, double* __restrict__ Uhi, double* __res
   }
 }
 
+// part = a . b per case (the r . z of a hierarchy that is only its coarsest level)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) kb_dot_pair(int64_t n, const T* __restrict__ a, const T* __restrict__ b,
+                                                        double* __restrict__ part, const int* __restrict__ done) {
+  if (*done) return;
+  double dot[4] = {0.0, 0.0, 0.0, 0.0};
+  {
+    BATCH_DOF_LOOP(n) {
+      const C4<T> av = ldc<T>(a + i * kBatch, l), bv = ldc<T>(b + i * kBatch, l);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) dot[k] += (double)av.v[k] * (double)bv.v[k];
+    }
+  }
+  write_case_parts<T>(dot, part);
+}
+
 // partC = x . x per case
 __global__ void __launch_bounds__(kThreads) kb_dot_self(int64_t n, const double* __restrict__ x,
                                                         double* __restrict__ partC) {
@@ -1027,6 +1043,13 @@ int batch_vcycle(Solid* s, AmgHierarchy& H, BlockWork& W, int lvl, const T* b, T
     kb_coarse<T><<<resident_grid(kb_coarse<T>, kThreads, (H.n_coarse * 32 + kThreads - 1) / kThreads), kThreads, 0,
                    st>>>(H.n_coarse, H.coarse_inv.p, b, out, done);
     W.launches++;
+    if (part) {  // a hierarchy without levels: the PCG's r . z comes from here
+      const int g = resident_grid(kb_dot_pair<T>, kThreads, quads_work(H.n_coarse));
+      W.npA = g;
+      kb_dot_pair<T><<<g, kThreads, 0, st>>>(H.n_coarse, b, out, part, done);
+      W.launches++;
+    }
+    WN_CUDA(cudaGetLastError());
     return 0;
   }
   DevLevel& L = H.levels[lvl];
@@ -1360,6 +1383,7 @@ int batch_outer(Solid* s, BlockWork& W, int vmode, int m, const wn_solve_params&
 int solver_solve_multi(Solid* s, int n_rhs, const double* F, double* U, const wn_solve_params& prm,
                        wn_solve_stats* stats, int* case_iters, double* case_rel, cudaStream_t st) {
   WN_REQUIRE(s->assembled, WN_ESTATE, "multi-RHS solve: matrix not assembled");
+  WN_REQUIRE(s->bs == 3, WN_ESTATE, "multi-RHS solve: not a C3D10 system");
   WN_REQUIRE(n_rhs >= 0, WN_EINVAL, "multi-RHS solve: n_rhs >= 0 required");
   WN_REQUIRE(prm.precond >= 0 && prm.precond <= 2, WN_EINVAL, "multi-RHS solve: precond in {0, 1, 2}");
   WN_REQUIRE(prm.precision == 0 || prm.precision == 1, WN_EINVAL,

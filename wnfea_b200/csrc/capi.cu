@@ -60,6 +60,61 @@ static int read_flag(Solid* s, cudaStream_t st, int* value) {
   return 0;
 }
 
+__global__ void to_float_kernel(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+int make_bsr6_system(int64_t n, const int32_t* rp, const int32_t* ci, const double* values, bool values_on_device,
+                     const double* coords, const uint8_t* fixed, void** out) {
+  *out = nullptr;
+  WN_REQUIRE(n < (int64_t)INT32_MAX / 6 && rp[0] == 0, WN_EINVAL, "6x6 system: bad row pointer");
+  const int64_t nnzb = rp[n];
+  std::vector<int32_t> diag(n, -1);
+  for (int64_t i = 0; i < n; ++i) {
+    WN_REQUIRE(rp[i + 1] >= rp[i], WN_EINVAL, "6x6 system: row pointer not monotone");
+    for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
+      WN_REQUIRE(ci[k] >= 0 && ci[k] < n, WN_EINVAL, "6x6 system: column index out of range");
+      WN_REQUIRE(k == rp[i] || ci[k] > ci[k - 1], WN_EINVAL, "6x6 system: columns not sorted / unique in row %lld",
+                 (long long)i);
+      if (ci[k] == i) diag[i] = k;
+    }
+    WN_REQUIRE(diag[i] >= 0, WN_EINVAL, "6x6 system: row %lld has no diagonal block", (long long)i);
+  }
+  int dev = 0;
+  WN_CUDA(cudaGetDevice(&dev));
+  std::unique_ptr<Solid> s(new Solid());
+  s->device = dev;
+  s->bs = 6;
+  s->n_nodes = n;
+  s->n_el = 0;
+  s->nnzb = nnzb;
+  s->h_row_ptr.assign(rp, rp + n + 1);
+  s->h_col_idx.assign(ci, ci + nnzb);
+  s->h_diag_block = diag;
+  s->h_nodes.assign(coords, coords + n * 3);
+  s->h_fixed.assign(n * 6, 0);
+  if (fixed)
+    for (int64_t i = 0; i < n * 6; ++i) s->h_fixed[i] = fixed[i] ? 1 : 0;
+  WN_CHECK(s->row_ptr.upload(s->h_row_ptr));
+  WN_CHECK(s->col_idx.upload(s->h_col_idx));
+  WN_CHECK(s->diag_block.upload(s->h_diag_block));
+  WN_CHECK(s->fixed.upload(s->h_fixed));
+  WN_CHECK(s->flags.alloc(16));
+  WN_CHECK(s->flags.zero());
+  WN_CHECK(s->k64.alloc(nnzb * 36));
+  WN_CHECK(s->k32.alloc(nnzb * 36));
+  WN_CUDA(cudaMemcpy(s->k64.p, values, nnzb * 36 * sizeof(double),
+                     values_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice));
+  to_float_kernel<<<grid_for(nnzb * 36, 1, 256, 8), 256>>>(nnzb * 36, s->k64.p, s->k32.p);
+  WN_CUDA(cudaGetLastError());
+  WN_CUDA(cudaDeviceSynchronize());
+  s->assembled = true;
+  s->bcs_applied = fixed != nullptr;
+  *out = s.release();
+  return 0;
+}
+
 }  // namespace wn
 
 using namespace wn;
@@ -187,6 +242,13 @@ int wn_bsr3_pattern_host(int64_t n_nodes, int64_t n_el, const int32_t* conn, int
   return 0;
 }
 
+int wn_bsr6_system_create(int64_t n_nodes, const int32_t* row_ptr, const int32_t* col_idx, const double* values,
+                          const double* coords, const uint8_t* fixed_mask, void** out_handle) {
+  WN_REQUIRE(out_handle && row_ptr && col_idx && values && coords && n_nodes > 0, WN_EINVAL,
+             "wn_bsr6_system_create: bad argument");
+  return make_bsr6_system(n_nodes, row_ptr, col_idx, values, false, coords, fixed_mask, out_handle);
+}
+
 int wn_solid_destroy(void* h) {
   if (!h) return 0;
   Solid* s = as_solid(h);
@@ -215,6 +277,7 @@ int wn_solid_get_pattern(void* h, int32_t* row_ptr, int32_t* col_idx) {
 int wn_solid_get_map(void* h, int32_t* emap) {
   WN_REQUIRE(h && emap, WN_EINVAL, "wn_solid_get_map: null argument");
   Solid* s = as_solid(h);
+  WN_REQUIRE(s->bs == 3, WN_ESTATE, "wn_solid_get_map: not a C3D10 system");
   WN_CHECK(select_device(s));
   WN_CUDA(cudaMemcpy(emap, s->emap.p, s->emap.bytes(), cudaMemcpyDeviceToHost));
   return 0;
@@ -223,6 +286,7 @@ int wn_solid_get_map(void* h, int32_t* emap) {
 int wn_solid_set_fixed(void* h, const uint8_t* fixed_mask) {
   WN_REQUIRE(h, WN_EINVAL, "wn_solid_set_fixed: null handle");
   Solid* s = as_solid(h);
+  WN_REQUIRE(s->bs == 3, WN_ESTATE, "wn_solid_set_fixed: not a C3D10 system");
   WN_CHECK(select_device(s));
   if (fixed_mask) {
     for (int64_t i = 0; i < s->n_nodes * 3; ++i) s->h_fixed[i] = fixed_mask[i] ? 1 : 0;
@@ -236,6 +300,7 @@ int wn_solid_set_fixed(void* h, const uint8_t* fixed_mask) {
 int wn_assemble_c3d10_device(void* h, const double* d_props, int apply_bcs, uintptr_t stream) {
   WN_REQUIRE(h && (d_props || as_solid(h)->n_el == 0), WN_EINVAL, "wn_assemble_c3d10: null argument");
   Solid* s = as_solid(h);
+  WN_REQUIRE(s->bs == 3, WN_ESTATE, "wn_assemble_c3d10_device: not a C3D10 system");
   WN_CHECK(select_device(s));
   cudaStream_t st = (cudaStream_t)stream;
   WN_CHECK(s->props.alloc(s->n_el * 2));
@@ -267,6 +332,7 @@ int wn_assemble_c3d10(void* h, const double* props, int apply_bcs) {
 int wn_solid_get_values(void* h, double* values) {
   WN_REQUIRE(h && values, WN_EINVAL, "wn_solid_get_values: null argument");
   Solid* s = as_solid(h);
+  WN_REQUIRE(s->bs == 3, WN_ESTATE, "wn_solid_get_values: not a C3D10 system");
   WN_REQUIRE(s->assembled, WN_ESTATE, "wn_solid_get_values: not assembled");
   WN_CHECK(select_device(s));
   // device values are component-major (9 arrays of nnzb); return row-major blocks
@@ -292,6 +358,7 @@ int wn_solid_device_arrays(void* h, const double** k64, const float** k32, const
 int wn_spmv_solid_device(void* h, int precision, const void* x, void* y, uintptr_t stream) {
   WN_REQUIRE(h && x && y, WN_EINVAL, "wn_spmv_solid_device: null argument");
   Solid* s = as_solid(h);
+  WN_REQUIRE(s->bs == 3, WN_ESTATE, "wn_spmv_solid_device: not a C3D10 system");
   WN_REQUIRE(s->assembled, WN_ESTATE, "wn_spmv_solid_device: not assembled");
   WN_CHECK(select_device(s));
   if (precision == 0)
@@ -411,6 +478,7 @@ int wn_c3d10_internal_forces(const double* nodes, const int32_t* solid_elements,
 int wn_fint_c3d10_device(void* h, const double* d_u, double* d_fint, uintptr_t stream) {
   WN_REQUIRE(h && d_u && d_fint, WN_EINVAL, "wn_fint_c3d10_device: null argument");
   Solid* s = as_solid(h);
+  WN_REQUIRE(s->bs == 3, WN_ESTATE, "wn_fint_c3d10_device: not a C3D10 system");
   WN_REQUIRE(s->props.n == s->n_el * 2, WN_ESTATE, "wn_fint_c3d10_device: no material properties (assemble first)");
   WN_CHECK(select_device(s));
   cudaStream_t st = (cudaStream_t)stream;
@@ -437,6 +505,7 @@ int wn_stress_c3d10_device(void* h, const double* d_u, double* d_cell_sig, doubl
                            uintptr_t stream) {
   WN_REQUIRE(h && d_u && d_cell_sig && d_cell_vm && d_nodal_vm, WN_EINVAL, "wn_stress_c3d10_device: null argument");
   Solid* s = as_solid(h);
+  WN_REQUIRE(s->bs == 3, WN_ESTATE, "wn_stress_c3d10_device: not a C3D10 system");
   WN_REQUIRE(s->props.n == s->n_el * 2, WN_ESTATE, "wn_stress_c3d10_device: no material properties");
   WN_CHECK(select_device(s));
   return launch_stress(s->n_el, s->n_nodes, s->nodes.p, s->conn.p, s->props.p, d_u, s->inc_ptr.p, s->inc_ea.p,
@@ -462,6 +531,7 @@ int wn_stress_c3d10(void* h, const double* u, double* cell_sig, double* cell_vm,
 int wn_adjoint_compliance_device(void* h, const double* d_u, double* d_grad_E, double* d_grad_F, uintptr_t stream) {
   WN_REQUIRE(h && d_u, WN_EINVAL, "wn_adjoint_compliance_device: null argument");
   Solid* s = as_solid(h);
+  WN_REQUIRE(s->bs == 3, WN_ESTATE, "wn_adjoint_compliance_device: not a C3D10 system");
   WN_REQUIRE(s->props.n == s->n_el * 2, WN_ESTATE, "wn_adjoint_compliance_device: no material properties");
   WN_CHECK(select_device(s));
   cudaStream_t st = (cudaStream_t)stream;

@@ -115,7 +115,7 @@ int wn_amg_setup_host(int64_t n_nodes, const int32_t* row_ptr, const int32_t* co
   WN_REQUIRE(out && row_ptr && col_idx && values && coords && n_nodes > 0, WN_EINVAL,
              "wn_amg_setup_host: bad argument");
   auto* hh = new HostAmgHandle();
-  int rc = amg_build(params ? *params : amg_default_params(), n_nodes, row_ptr, col_idx, values, coords, fixed_mask,
+  int rc = amg_build(params ? *params : amg_default_params(), n_nodes, 3, row_ptr, col_idx, values, coords, fixed_mask,
                      hh->h);
   if (rc != 0) {
     delete hh;
@@ -174,7 +174,7 @@ int wn_solve(void* h, const double* F, double* u, const wn_solve_params* params,
   WN_REQUIRE(h && F && u && params, WN_EINVAL, "wn_solve: null argument");
   Solid* s = reinterpret_cast<Solid*>(h);
   WN_CUDA(cudaSetDevice(s->device));
-  const int64_t n = s->n_nodes * 3;
+  const int64_t n = s->n_nodes * s->bs;
   DArray<double> dF, du;
   WN_CHECK(dF.upload(F, n));
   WN_CHECK(du.alloc(n));

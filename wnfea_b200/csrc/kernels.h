@@ -38,4 +38,9 @@ int launch_solid_spmv_f64(int64_t n_rows, const int32_t* rp, const int32_t* ci, 
 int launch_solid_spmv_f32(int64_t n_rows, const int32_t* rp, const int32_t* ci, const float* v, int64_t nnzb,
                           const float* x, float* y, cudaStream_t st);
 
+// A linear 6-DOF-per-node system (block-contiguous row-major 6x6 values; host pattern arrays,
+// values on the host or the device) as a solver handle with bs = 6 (capi.cu).
+int make_bsr6_system(int64_t n, const int32_t* rp, const int32_t* ci, const double* values, bool values_on_device,
+                     const double* coords, const uint8_t* fixed, void** out);
+
 }  // namespace wn

@@ -19,6 +19,10 @@ struct BlockWork;     // block.h
 struct Solid {
   int device = 0;
   int64_t n_nodes = 0, n_el = 0, nnzb = 0;
+  // DOFs per node: 3 for the C3D10 system (component-major 3x3 values), 6 for a linear
+  // beam-frame system made by wn_bsr6_system_create / wn_beam_linear_system (block-contiguous
+  // 6x6 values); only the AMG and the single-RHS solve accept bs = 6
+  int bs = 3;
   // host copies kept for the CSR/BSR export and the AMG setup
   std::vector<int32_t> h_row_ptr, h_col_idx, h_diag_block;
   std::vector<double> h_nodes;

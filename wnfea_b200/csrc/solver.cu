@@ -456,6 +456,18 @@ __global__ void k_reduce_rr(PcgScalars* S, const double* __restrict__ partC, int
   if (threadIdx.x == 0) S->rr = rr;
 }
 
+// partials of a . b
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_dot_pair(int64_t n, const T* __restrict__ a, const T* __restrict__ b,
+                                                       double* __restrict__ part, const PcgScalars* __restrict__ S) {
+  __shared__ double sh[kThreads / 32];
+  if (S->done) return;
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    s += (double)a[i] * (double)b[i];
+  write_part(s, part, sh);
+}
+
 // partials of x . x
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_dot_self(int64_t n, const T* __restrict__ x, double* __restrict__ part) {
@@ -471,8 +483,10 @@ __global__ void __launch_bounds__(kThreads) k_dot_self(int64_t n, const T* __res
 // ---------------------------------------------------------------------------------------
 
 // r64 = F - K64 (u + ulo) from compensated products and sums (Dot2), rounded to FP64 at the
-// end; r32 = (float) r64; partC = r64 . r64.  16 lanes per block row, each with a (sum, error)
-// pair over its blocks, combined by a butterfly of TwoSums (the same order in every lane).
+// end; r32 = (float) r64; partC = r64 . r64.  A group of lanes per block row (16 for 3x3
+// component-major blocks, 32 for 6x6 block-contiguous ones), each with a (sum, error) pair over
+// its blocks, combined by a butterfly of TwoSums (the same order in every lane).
+template <int BS>
 __global__ void __launch_bounds__(kThreads) k_outer_residual_dd(int64_t n_rows, const int32_t* __restrict__ rp,
                                                                 const int32_t* __restrict__ ci,
                                                                 const double* __restrict__ av, int64_t stride,
@@ -481,26 +495,30 @@ __global__ void __launch_bounds__(kThreads) k_outer_residual_dd(int64_t n_rows, 
                                                                 const double* __restrict__ ulo,
                                                                 double* __restrict__ r64, float* __restrict__ r32,
                                                                 double* __restrict__ partC) {
+  constexpr int G = GroupOf<BS>::value;
   __shared__ double sh[kThreads / 32];
   double rr = 0.0;
-  GROUP_ROW_LOOP(n_rows, 16) {
+  GROUP_ROW_LOOP(n_rows, G) {
     const bool active = row < n_rows;
-    double s[3] = {0.0, 0.0, 0.0}, c[3] = {0.0, 0.0, 0.0};
+    double s[BS], c[BS];
+#pragma unroll
+    for (int r = 0; r < BS; ++r) s[r] = c[r] = 0.0;
     if (active) {
       const int32_t q1 = __ldg(rp + row + 1);
-      for (int32_t q = __ldg(rp + row) + lane; q < q1; q += 16) {
+      for (int32_t q = __ldg(rp + row) + lane; q < q1; q += G) {
         const int64_t col = __ldg(ci + q);
-        double uh[3], ul[3];
+        double uh[BS], ul[BS];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          uh[k] = u[col * 3 + k];
-          ul[k] = ulo[col * 3 + k];
+        for (int k = 0; k < BS; ++k) {
+          uh[k] = u[col * BS + k];
+          ul[k] = ulo[col * BS + k];
         }
 #pragma unroll
-        for (int r = 0; r < 3; ++r)
+        for (int r = 0; r < BS; ++r)
 #pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            const double a = __ldg(av + (int64_t)(r * 3 + k) * stride + q);
+          for (int k = 0; k < BS; ++k) {
+            const double a = (LayoutOf<BS>::value == kSoA) ? __ldg(av + (int64_t)(r * BS + k) * stride + q)
+                                                            : __ldg(av + (int64_t)q * BS * BS + r * BS + k);
             double p, ep, t, es;
             two_prod(a, uh[k], p, ep);
             two_sum(s[r], p, t, es);
@@ -510,9 +528,9 @@ __global__ void __launch_bounds__(kThreads) k_outer_residual_dd(int64_t n_rows, 
       }
     }
 #pragma unroll
-    for (int r = 0; r < 3; ++r)
+    for (int r = 0; r < BS; ++r)
 #pragma unroll
-      for (int o = 8; o > 0; o >>= 1) {
+      for (int o = G / 2; o > 0; o >>= 1) {
         const double s2 = __shfl_xor_sync(0xffffffffu, s[r], o);
         const double c2 = __shfl_xor_sync(0xffffffffu, c[r], o);
         double t, e;
@@ -520,9 +538,9 @@ __global__ void __launch_bounds__(kThreads) k_outer_residual_dd(int64_t n_rows, 
         s[r] = t;
         c[r] = (c[r] + c2) + e;
       }
-    if (active && lane < 3) {
-      const int64_t i = row * 3 + lane;
-      const double sv = pick<3>(s, lane), cv = pick<3>(c, lane);
+    if (active && lane < BS) {
+      const int64_t i = row * BS + lane;
+      const double sv = pick<BS>(s, lane), cv = pick<BS>(c, lane);
       double t, e;
       two_sum(F[i], -sv, t, e);
       const double ri = t + (e - cv);
@@ -546,14 +564,16 @@ __global__ void k_accumulate(int64_t n, double* __restrict__ u, double* __restri
   }
 }
 
-__global__ void k_fill_dinv(int64_t n_rows, int64_t nnzb, const int32_t* __restrict__ diag_block,
+// 1 / diag of the fine matrix: 3x3 component-major (stride nnzb) or 6x6 block-contiguous
+__global__ void k_fill_dinv(int64_t n_rows, int bs, int64_t nnzb, const int32_t* __restrict__ diag_block,
                             const double* __restrict__ k64,
                             double* __restrict__ d64, float* __restrict__ d32) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_rows * 3;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_rows * bs;
        t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t row = t / 3;
-    const int c = (int)(t - row * 3);
-    const double dv = k64[(int64_t)(c * 4) * nnzb + diag_block[row]];  // component-major values
+    const int64_t row = t / bs;
+    const int c = (int)(t - row * bs);
+    const double dv = (bs == 3) ? k64[(int64_t)(c * 4) * nnzb + diag_block[row]]
+                                : k64[(int64_t)diag_block[row] * 36 + c * 7];
     const double inv = (fabs(dv) > 1e-12) ? 1.0 / dv : 1.0;  // solid_solver.py:230
     d64[t] = inv;
     d32[t] = (float)inv;
@@ -618,6 +638,13 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
     k_coarse<T><<<resident_grid(k_coarse<T>, kThreads, (H.n_coarse * 32 + kThreads - 1) / kThreads), kThreads, 0,
                   st>>>(H.n_coarse, H.coarse_inv.p, b, out, S);
     W.launches++;
+    if (part) {  // a hierarchy without levels: the PCG's r . z comes from here
+      const int g = resident_grid(k_dot_pair<T>, kThreads, (H.n_coarse + kThreads - 1) / kThreads);
+      W.npA = g;
+      k_dot_pair<T><<<g, kThreads, 0, st>>>(H.n_coarse, b, out, part, S);
+      W.launches++;
+    }
+    WN_CUDA(cudaGetLastError());
     return 0;
   }
   DevLevel& L = H.levels[lvl];
@@ -746,11 +773,15 @@ static int pcg_iteration(Solid* s, SolverWork& W, int precond, int k, PcgScalars
   const int par = k & 1;
   TK* p_new = par ? B.p1 : B.p0;
   TK* p_old = par ? B.p0 : B.p1;
-  const int gsd = resident_grid(k_spmv_dot<3, TK, TM>, kThreads, (s->n_nodes * 32 + kThreads - 1) / kThreads);
   const int gup = resident_grid(k_update<TK, TM>, kThreads, (W.n + kThreads - 1) / kThreads);
-  k_spmv_dot<3, TK, TM><<<gsd, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, B.A, s->nnzb, B.z,
-                                                                 p_old, p_new, B.q, W.partA.p, W.partB.p,
-                                                                 W.npA, k == 0, par, S);
+  auto spmv_dot = [&](auto bs_tag) {
+    constexpr int BS = decltype(bs_tag)::value;
+    const int g = resident_grid(k_spmv_dot<BS, TK, TM>, kThreads, (s->n_nodes * 32 + kThreads - 1) / kThreads);
+    k_spmv_dot<BS, TK, TM><<<g, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, B.A, s->nnzb, B.z, p_old,
+                                                   p_new, B.q, W.partA.p, W.partB.p, W.npA, k == 0, par, S);
+    return g;
+  };
+  const int gsd = s->bs == 3 ? spmv_dot(std::integral_constant<int, 3>{}) : spmv_dot(std::integral_constant<int, 6>{});
   W.npB = gsd;
   k_update<TK, TM><<<gup, kThreads, 0, st>>>(W.n, B.x, B.r, B.rm, p_new, B.q, W.partB.p, W.partC.p, W.npB, par, S);
   W.npC = gup;
@@ -852,7 +883,7 @@ static void cheb_coefficients(const wn_amg_params& prm, DevLevel& L) {
 static int ensure_work(Solid* s) {
   if (!s->work) s->work.reset(new SolverWork());
   SolverWork& W = *s->work;
-  const int64_t n = s->n_nodes * 3;
+  const int64_t n = s->n_nodes * s->bs;
   if (W.n != n) {
     W.n = n;
     WN_CHECK(W.p64.alloc(n));
@@ -882,14 +913,19 @@ int solver_setup(Solid* s, const wn_amg_params& prm) {
   WN_REQUIRE(prm.smoother_degree >= 1 && prm.smoother_degree <= 8, WN_EINVAL, "AMG setup: smoother_degree in [1, 8]");
   WN_REQUIRE(prm.max_levels >= 1 && prm.max_levels <= 16, WN_EINVAL, "AMG setup: max_levels in [1, 16]");
   const auto t0 = std::chrono::steady_clock::now();
-  std::vector<double> soa(s->nnzb * 9), vals(s->nnzb * 9);
+  const int nb = s->bs * s->bs;
+  std::vector<double> soa(s->nnzb * nb), vals(s->nnzb * nb);
   WN_CUDA(cudaMemcpy(soa.data(), s->k64.p, soa.size() * sizeof(double), cudaMemcpyDeviceToHost));
-  for (int64_t b = 0; b < s->nnzb; ++b)  // component-major on the device -> row-major blocks
-    for (int k = 0; k < 9; ++k) vals[b * 9 + k] = soa[k * s->nnzb + b];
+  if (s->bs == 3) {
+    for (int64_t b = 0; b < s->nnzb; ++b)  // component-major on the device -> row-major blocks
+      for (int k = 0; k < 9; ++k) vals[b * 9 + k] = soa[k * s->nnzb + b];
+  } else {
+    vals.swap(soa);  // 6x6 blocks are stored row-major already
+  }
   std::vector<double>().swap(soa);
   std::unique_ptr<AmgHierarchy> H(new AmgHierarchy());
   const uint8_t* fixed = s->bcs_applied ? s->h_fixed.data() : nullptr;
-  WN_CHECK(amg_build(prm, s->n_nodes, s->h_row_ptr.data(), s->h_col_idx.data(), vals.data(), s->h_nodes.data(),
+  WN_CHECK(amg_build(prm, s->n_nodes, s->bs, s->h_row_ptr.data(), s->h_col_idx.data(), vals.data(), s->h_nodes.data(),
                      fixed, H->host));
   H->degree = prm.smoother_degree;
   static uint64_t next_id = 0;
@@ -936,9 +972,15 @@ int solver_setup(Solid* s, const wn_amg_params& prm) {
 // ---------------------------------------------------------------------------------------
 // r64 = F - K (u64 + ulo) with the compensated kernel; *rr = ||r64||^2
 static int true_residual(Solid* s, SolverWork& W, const double* F, float* r32, cudaStream_t st, double* rr) {
-  W.npC = resident_grid(k_outer_residual_dd, kThreads, (s->n_nodes * 32 + kThreads - 1) / kThreads);
-  k_outer_residual_dd<<<W.npC, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, s->nnzb, F,
-                                                  W.u64.p, W.ulo.p, W.r64.p, r32, W.partC.p);
+  auto launch = [&](auto kern) {
+    W.npC = resident_grid(kern, kThreads, (s->n_nodes * 32 + kThreads - 1) / kThreads);
+    kern<<<W.npC, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, s->nnzb, F, W.u64.p, W.ulo.p,
+                                     W.r64.p, r32, W.partC.p);
+  };
+  if (s->bs == 3)
+    launch(k_outer_residual_dd<3>);
+  else
+    launch(k_outer_residual_dd<6>);
   k_reduce_rr<<<1, kThreads, 0, st>>>(W.scal.p + 1, W.partC.p, W.npC);
   W.launches += 2;
   WN_CUDA(cudaGetLastError());
@@ -1034,7 +1076,7 @@ int solver_solve(Solid* s, const double* F, double* u, const wn_solve_params& pr
   const int64_t n = W.n;
   const int chunk = prm.chunk > 0 ? prm.chunk : 8;
   PcgScalars hS{};
-  k_fill_dinv<<<vec_grid(n), kThreads, 0, st>>>(s->n_nodes, s->nnzb, s->diag_block.p, s->k64.p, W.dinv64.p,
+  k_fill_dinv<<<vec_grid(n), kThreads, 0, st>>>(s->n_nodes, s->bs, s->nnzb, s->diag_block.p, s->k64.p, W.dinv64.p,
                                                  W.dinv32.p);
   W.launches++;
   WN_CUDA(cudaEventRecord(W.ev0, st));
@@ -1083,7 +1125,7 @@ int amg_vcycle(Solid* s, int precision, const void* r, void* z, cudaStream_t st)
   WN_REQUIRE(s->amg, WN_ESTATE, "vcycle: no AMG hierarchy (call wn_amg_setup)");
   WN_CHECK(ensure_work(s));
   SolverWork& W = *s->work;
-  k_fill_dinv<<<vec_grid(W.n), kThreads, 0, st>>>(s->n_nodes, s->nnzb, s->diag_block.p, s->k64.p, W.dinv64.p,
+  k_fill_dinv<<<vec_grid(W.n), kThreads, 0, st>>>(s->n_nodes, s->bs, s->nnzb, s->diag_block.p, s->k64.p, W.dinv64.p,
                                                   W.dinv32.p);
   WN_CUDA(cudaMemsetAsync(W.scal.p, 0, sizeof(PcgScalars), st));  // done = 0
   if (precision == 0)
