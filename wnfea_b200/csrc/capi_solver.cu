@@ -175,11 +175,16 @@ int wn_solve(void* h, const double* F, double* u, const wn_solve_params* params,
   Solid* s = reinterpret_cast<Solid*>(h);
   WN_CUDA(cudaSetDevice(s->device));
   const int64_t n = s->n_nodes * s->bs;
-  DArray<double> dF, du;
-  WN_CHECK(dF.upload(F, n));
-  WN_CHECK(du.alloc(n));
-  WN_CHECK(solver_solve(s, dF.p, du.p, *params, stats, 0));
-  WN_CUDA(cudaMemcpy(u, du.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+  // staged through page-locked memory: a device copy from / into pageable memory (a freshly
+  // allocated result array in particular) runs at a fraction of the link's speed
+  WN_CHECK(s->io_f.alloc(n));
+  WN_CHECK(s->io_u.alloc(n));
+  WN_CHECK(s->io_pin.at_least(2 * n));
+  std::memcpy(s->io_pin.p, F, n * sizeof(double));
+  WN_CUDA(cudaMemcpy(s->io_f.p, s->io_pin.p, n * sizeof(double), cudaMemcpyHostToDevice));
+  WN_CHECK(solver_solve(s, s->io_f.p, s->io_u.p, *params, stats, 0));
+  WN_CUDA(cudaMemcpy(s->io_pin.p + n, s->io_u.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+  std::memcpy(u, s->io_pin.p + n, n * sizeof(double));
   return 0;
 }
 

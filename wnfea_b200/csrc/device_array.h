@@ -59,4 +59,26 @@ struct DArray {
   size_t bytes() const { return sizeof(T) * (size_t)n; }
 };
 
+// Page-locked host buffer (cudaMallocHost), grown on demand, for full-speed staging copies.
+template <typename T>
+struct PinnedArray {
+  T* p = nullptr;
+  int64_t n = 0;
+  PinnedArray() = default;
+  PinnedArray(const PinnedArray&) = delete;
+  PinnedArray& operator=(const PinnedArray&) = delete;
+  ~PinnedArray() {
+    if (p) cudaFreeHost(p);
+  }
+  int at_least(int64_t count) {
+    if (p && n >= count) return 0;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+    WN_CUDA(cudaMallocHost((void**)&p, sizeof(T) * (size_t)count));
+    n = count;
+    return 0;
+  }
+};
+
 }  // namespace wn

@@ -48,6 +48,10 @@ struct Solid {
   std::unique_ptr<AmgHierarchy> amg;
   std::unique_ptr<SolverWork> work;
   std::unique_ptr<BlockWork> bwork;
+  // host-buffer solve: device copies of F / u and a page-locked staging buffer (2 n), kept
+  // between calls so that a call neither allocates nor copies from pageable memory
+  DArray<double> io_f, io_u;
+  PinnedArray<double> io_pin;
   ~Solid();
 };
 
