@@ -69,6 +69,19 @@ struct BlockLoad<double, 18> {
     BlockLoadVec<18>::load_d(p, v);
   }
 };
+// 3x6 / 6x3 FP32 blocks (prolongation / restriction of the fine level): 72 bytes, 8-byte aligned
+template <>
+struct BlockLoad<float, 18> {
+  __device__ __forceinline__ static void load(const float* __restrict__ p, float (&v)[18]) {
+    const float2* q = reinterpret_cast<const float2*>(p);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const float2 t = __ldg(q + k);
+      v[2 * k] = t.x;
+      v[2 * k + 1] = t.y;
+    }
+  }
+};
 template <>
 struct BlockLoad<float, 36> {
   __device__ __forceinline__ static void load(const float* __restrict__ p, float (&v)[36]) {
