@@ -35,6 +35,9 @@ extern "C" {
 #define WN_ENOTSPD (-6)
 #define WN_EALLOC (-7)
 #define WN_ETOOBIG (-8)
+/* a bounded device-side wait (the streamed fine-matrix pipeline) ran out of time: the kernel
+ * returned early and the results of the call are not valid */
+#define WN_ETIMEOUT (-9)
 
 /* ---------------------------------------------------------------------------------------
  * Library
@@ -93,6 +96,18 @@ int wn_solid_device_arrays(void* h, const double** k64, const float** k32, const
 /* y = K x for the assembled matrix: precision 0 = FP64 values/accumulation, 1 = FP32
  * values/accumulation (x, y are float then).  Device pointers. */
 int wn_spmv_solid_device(void* h, int precision, const void* x, void* y, uintptr_t stream);
+/* Status word of the streamed fine-matrix products of wn_spmv_solid_device: WN_OK, or
+ * WN_ETIMEOUT when a bounded pipeline wait of a call since the last reset ran out of time (the
+ * y of that call is not valid).  Synchronises the device; reset != 0 clears the word. */
+int wn_solid_stream_status(void* h, int reset, int* status);
+/* The row tiles the streamed fine-matrix kernels cut a 3x3 block-row pattern into (host only):
+ * tiles[4 t .. 4 t + 3] = (first row, end row, first block, end block) of tile t, whole rows
+ * in order, at most WN_STREAM_TILE_BLOCKS blocks and WN_STREAM_TILE_ROWS rows per tile.
+ * *n_tiles = 0 when a row alone exceeds the block capacity (those matrices use the register
+ * row kernels).  tiles may be null to query the count. */
+#define WN_STREAM_TILE_BLOCKS 512
+#define WN_STREAM_TILE_ROWS 120
+int wn_stream_tiles_host(int64_t n_rows, const int32_t* row_ptr, int32_t* tiles, int64_t capacity, int64_t* n_tiles);
 
 /* ---------------------------------------------------------------------------------------
  * Smoothed-aggregation AMG + PCG solver (no reference counterpart for C3D10: the reference's

@@ -28,6 +28,28 @@ void set_error(const char* fmt, ...) {
 }
 const char* last_error() { return g_last_error.c_str(); }
 
+// CTAs per SM of a kernel with `smem` bytes of dynamic shared memory, after raising the
+// kernel's dynamic shared memory limit to `smem` (once per device); 0 if the kernel cannot
+// be launched with that much
+int stream_ctas_per_sm(const void* kernel, int threads, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, int> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  std::lock_guard<std::mutex> lock(mu);
+  auto key = std::make_pair(dev, kernel);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int n = 0;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess || n < 0) {
+    cudaGetLastError();
+    n = 0;
+  }
+  cache[key] = n;
+  return n;
+}
+
 int occupancy_per_sm(const void* kernel, int threads) {
   static std::mutex mu;
   static std::map<std::pair<const void*, int>, int> cache;
@@ -209,6 +231,21 @@ int wn_solid_create(int64_t n_nodes, int64_t n_el, const double* nodes, const in
   st = st ? st : s->fixed.alloc(n_nodes * 3);
   st = st ? st : s->fixed.zero();
   if (st == 0) {
+    std::vector<StreamTile> plan;
+    std::vector<PackTile> d32, d64;
+    if (build_stream_tiles(pat.row_ptr.data(), n_nodes, plan) && !plan.empty()) {
+      const int64_t b32 = build_pack_tiles<float>(plan, d32), b64 = build_pack_tiles<double>(plan, d64);
+      if (b32 > 0 && b64 > 0 && plan.size() < (size_t)INT32_MAX) {
+        st = st ? st : s->stream_plan.upload(plan);
+        st = st ? st : s->pack_desc32.upload(d32);
+        st = st ? st : s->pack_desc64.upload(d64);
+        s->pack_size32 = b32;
+        s->pack_size64 = b64;
+        s->n_stream_tiles = (int)plan.size();
+      }
+    }
+  }
+  if (st == 0) {
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
       set_error("wn_solid_create: %s", cudaGetErrorString(e));
@@ -312,6 +349,14 @@ int wn_assemble_c3d10_device(void* h, const double* d_props, int apply_bcs, uint
   WN_CHECK(launch_ke_upper(s->n_el, s->nodes.p, s->conn.p, s->props.p, s->ke.p, s->flags.p, st));
   WN_CHECK(launch_gather_assemble(s->nnzb, s->gptr.p, s->gsrc.p, s->ke.p, s->block_row.p, s->col_idx.p,
                                   apply_bcs ? s->fixed.p : nullptr, s->k64.p, s->k32.p, st));
+  s->packed = false;
+  if (s->n_stream_tiles > 0) {  // tile-major copies for the streamed fine-level kernels
+    WN_CHECK(s->pack32.alloc(s->pack_size32));
+    WN_CHECK(s->pack64.alloc(s->pack_size64));
+    WN_CHECK(launch_pack_tiles(s->n_stream_tiles, s->stream_plan.p, s->pack_desc32.p, s->pack_desc64.p, s->row_ptr.p,
+                               s->col_idx.p, s->k32.p, s->k64.p, s->nnzb, s->pack32.p, s->pack64.p, st));
+    s->packed = true;
+  }
   int flag = 0;
   WN_CHECK(read_flag(s, st, &flag));
   WN_REQUIRE(flag == 0, WN_EMESH, "wn_assemble_c3d10: non-positive Jacobian determinant in a C3D10 element");
@@ -355,12 +400,46 @@ int wn_solid_device_arrays(void* h, const double** k64, const float** k32, const
   return 0;
 }
 
+int wn_stream_tiles_host(int64_t n_rows, const int32_t* row_ptr, int32_t* tiles, int64_t capacity, int64_t* n_tiles) {
+  WN_REQUIRE(row_ptr && n_tiles && n_rows >= 0, WN_EINVAL, "wn_stream_tiles_host: bad argument");
+  std::vector<StreamTile> t;
+  if (!build_stream_tiles(row_ptr, n_rows, t)) {
+    *n_tiles = 0;
+    return 0;
+  }
+  *n_tiles = (int64_t)t.size();
+  if (tiles) {
+    WN_REQUIRE(capacity >= (int64_t)t.size(), WN_EINVAL, "wn_stream_tiles_host: capacity %lld < %lld tiles",
+               (long long)capacity, (long long)t.size());
+    memcpy(tiles, t.data(), t.size() * sizeof(StreamTile));
+  }
+  return 0;
+}
+
+int wn_solid_stream_status(void* h, int reset, int* status) {
+  WN_REQUIRE(h && status, WN_EINVAL, "wn_solid_stream_status: null argument");
+  Solid* s = as_solid(h);
+  WN_CHECK(select_device(s));
+  WN_CUDA(cudaDeviceSynchronize());
+  WN_CUDA(cudaMemcpy(status, s->flags.p + kStreamStatusWord, sizeof(int), cudaMemcpyDeviceToHost));
+  if (reset) WN_CUDA(cudaMemset(s->flags.p + kStreamStatusWord, 0, sizeof(int)));
+  return 0;
+}
+
 int wn_spmv_solid_device(void* h, int precision, const void* x, void* y, uintptr_t stream) {
   WN_REQUIRE(h && x && y, WN_EINVAL, "wn_spmv_solid_device: null argument");
   Solid* s = as_solid(h);
   WN_REQUIRE(s->bs == 3, WN_ESTATE, "wn_spmv_solid_device: not a C3D10 system");
   WN_REQUIRE(s->assembled, WN_ESTATE, "wn_spmv_solid_device: not assembled");
   WN_CHECK(select_device(s));
+  if (precision == 0 || precision == 1) {
+    if (s->packed) {
+      const int rc = launch_solid_spmv_stream(precision, precision == 0 ? s->pack_desc64.p : s->pack_desc32.p,
+                                              s->n_stream_tiles, precision == 0 ? s->pack64.p : s->pack32.p, x, y,
+                                              s->flags.p + kStreamStatusWord, (cudaStream_t)stream);
+      if (rc != 0) return rc < 0 ? rc : 0;
+    }
+  }
   if (precision == 0)
     return launch_solid_spmv_f64(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, s->nnzb, (const double*)x,
                                  (double*)y, (cudaStream_t)stream);

@@ -80,6 +80,7 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 // Grid of at most one full wave: blocks resident on all SMs at once for `kernel` with
 // `threads` threads per CTA (occupancy queried once per kernel), capped by the work.
 int occupancy_per_sm(const void* kernel, int threads);  // cached per (kernel, threads), capi.cu
+int stream_ctas_per_sm(const void* kernel, int threads, size_t smem);  // capi.cu
 
 template <typename K>
 inline int resident_grid(K kernel, int threads, int64_t work_ctas) {

@@ -1,4 +1,6 @@
-// Owning device allocation (cudaMalloc / cudaFree) with size bookkeeping.
+// Owning device allocation (cudaMalloc / cudaFree) with size bookkeeping.  Every allocation
+// carries kTailSlack bytes beyond its n elements, so a 16-byte-granular bulk copy of a range
+// that ends at the last element (rounded up to 16 bytes) stays inside the allocation.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -10,6 +12,8 @@
 #include "common.cuh"
 
 namespace wn {
+
+constexpr size_t kTailSlack = 16;
 
 template <typename T>
 struct DArray {
@@ -42,7 +46,7 @@ struct DArray {
     if (count == n && p) return 0;
     release();
     if (count <= 0) return 0;
-    WN_CUDA(cudaMalloc((void**)&p, sizeof(T) * (size_t)count));
+    WN_CUDA(cudaMalloc((void**)&p, sizeof(T) * (size_t)count + kTailSlack));
     n = count;
     return 0;
   }

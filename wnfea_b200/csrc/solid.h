@@ -9,12 +9,15 @@
 
 #include "device_array.h"
 #include "pattern.h"
+#include "stream.cuh"
 
 namespace wn {
 
 struct AmgHierarchy;  // amg.h
 struct SolverWork;    // solver.cu
 struct BlockWork;     // block.h
+
+constexpr int kStreamStatusWord = 8;
 
 struct Solid {
   int device = 0;
@@ -42,7 +45,16 @@ struct Solid {
   DArray<float> k32;        // nnzb x 9
   DArray<double> ke;        // scratch: n_el x 55 x 9 element blocks
   DArray<double> fe;        // scratch: n_el x 30 element forces
-  DArray<int> flags;        // device status words
+  DArray<int> flags;        // device status words ([kStreamStatusWord]: streamed SpMV)
+  // row tiles of the fine matrix for the streamed kernels (stream.cuh) and the tile-major
+  // packs of the FP32 / FP64 values they read (refreshed by every assembly); no tiles when a
+  // row exceeds the tile capacity, and the register row kernels are used instead
+  DArray<StreamTile> stream_plan;
+  int n_stream_tiles = 0;
+  DArray<PackTile> pack_desc32, pack_desc64;
+  int64_t pack_size32 = 0, pack_size64 = 0;
+  DArray<unsigned char> pack32, pack64;
+  bool packed = false;
   bool assembled = false;
   bool bcs_applied = false;
   std::unique_ptr<AmgHierarchy> amg;

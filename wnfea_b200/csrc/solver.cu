@@ -581,6 +581,195 @@ __global__ void k_fill_dinv(int64_t n_rows, int bs, int64_t nnzb, const int32_t*
 }
 
 // ---------------------------------------------------------------------------------------
+// streamed fine-level kernels: the arithmetic of k_pre_first / k_cheb_step / k_residual /
+// k_post_first / k_spmv_dot on the 3x3 fine matrix, with the matrix streamed through shared
+// memory by bulk async copies (stream.cuh).  Each epilogue loads the row's own operands
+// before the row product (load) and writes its results after it (store).
+// ---------------------------------------------------------------------------------------
+template <typename T>
+struct EpiPreFirst {
+  const T* __restrict__ b;
+  const T* __restrict__ dinv;
+  T inv_theta;
+  int deg;
+  T c1, c2;
+  T* __restrict__ x;
+  T* __restrict__ r;
+  T* __restrict__ d;
+  T* __restrict__ res;
+  struct Pre {
+    T bi, di;
+  };
+  __device__ __forceinline__ Pre load(int64_t i) const { return {b[i], dinv[i]}; }
+  __device__ __forceinline__ double store(int64_t i, const Pre& p, T t) const {
+    const T d0 = p.di * p.bi * inv_theta;
+    if (deg == 1) {
+      x[i] = d0;
+      res[i] = p.bi - t;
+    } else {
+      const T r1 = p.di * p.bi - p.di * t;
+      const T d1 = c1 * d0 + c2 * r1;
+      x[i] = d0 + d1;
+      r[i] = r1;
+      d[i] = d1;
+    }
+    return 0.0;
+  }
+};
+
+template <typename T>
+struct EpiCheb {
+  const T* __restrict__ dinv;
+  const T* __restrict__ d_in;
+  T* __restrict__ d_out;
+  T* __restrict__ r;
+  T* __restrict__ x;
+  T c1, c2;
+  const T* __restrict__ b;
+  int want_dot;
+  struct Pre {
+    T di, dd, ri, xi;
+  };
+  __device__ __forceinline__ Pre load(int64_t i) const { return {dinv[i], d_in[i], r[i], x[i]}; }
+  __device__ __forceinline__ double store(int64_t i, const Pre& p, T t) const {
+    const T ri = p.ri - p.di * t;
+    const T dn = c1 * p.dd + c2 * ri;
+    const T xn = p.xi + dn;
+    r[i] = ri;
+    d_out[i] = dn;
+    x[i] = xn;
+    return want_dot ? (double)b[i] * (double)xn : 0.0;
+  }
+};
+
+template <typename T>
+struct EpiResidual {
+  const T* __restrict__ b;
+  T* __restrict__ res;
+  struct Pre {
+    T bi;
+  };
+  __device__ __forceinline__ Pre load(int64_t i) const { return {b[i]}; }
+  __device__ __forceinline__ double store(int64_t i, const Pre& p, T t) const {
+    res[i] = p.bi - t;
+    return 0.0;
+  }
+};
+
+template <typename T>
+struct EpiPostFirst {
+  const T* __restrict__ b;
+  const T* __restrict__ dinv;
+  T inv_theta;
+  const T* __restrict__ x;
+  T* __restrict__ x2;
+  T* __restrict__ r;
+  T* __restrict__ d;
+  int want_dot;
+  struct Pre {
+    T di, bi, xi;
+  };
+  __device__ __forceinline__ Pre load(int64_t i) const { return {dinv[i], b[i], x[i]}; }
+  __device__ __forceinline__ double store(int64_t i, const Pre& p, T t) const {
+    const T r0 = p.di * (p.bi - t);
+    const T d0 = r0 * inv_theta;
+    const T xn = p.xi + d0;
+    r[i] = r0;
+    d[i] = d0;
+    x2[i] = xn;
+    return want_dot ? (double)p.bi * (double)xn : 0.0;
+  }
+};
+
+template <typename TK, typename TM>
+struct EpiSpmvDot {
+  const TM* __restrict__ z;
+  const TK* __restrict__ p_old;
+  TK beta;
+  TK* __restrict__ p_new;
+  TK* __restrict__ q;
+  struct Pre {
+    TK pi;
+  };
+  __device__ __forceinline__ Pre load(int64_t i) const { return {(TK)z[i] + beta * p_old[i]}; }
+  __device__ __forceinline__ double store(int64_t i, const Pre& p, TK t) const {
+    p_new[i] = p.pi;
+    q[i] = t;
+    return (double)p.pi * (double)t;
+  }
+};
+
+// the fine matrix as the streamed kernels see it: the tile-major pack of one precision
+struct FineStream {
+  const PackTile* tiles;
+  int n_tiles;
+  const unsigned char* pack;
+};
+
+template <typename T, typename XF, typename EPI>
+__global__ void __launch_bounds__(kStreamThreads, StreamDefault<T>::kCtasPerSm) k_stream_rows(FineStream m, XF xf, EPI epi,
+                                                                   double* __restrict__ part,
+                                                                   PcgScalars* __restrict__ S) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ double sh[kStreamThreads / 32];
+  if (S->done) return;
+  const double dot = stream_rows<T, typename StreamDefault<T>::type>(m.tiles, m.n_tiles, m.pack, xf, epi, smem,
+                                                                     &S->status, &S->done);
+  if (part) write_part(dot, part, sh);
+}
+
+// k_spmv_dot with the matrix streamed: beta from the partials of r . z, p_new = z + beta p_old,
+// q = A p_new, partials of p_new . q
+template <typename TK, typename TM>
+__global__ void __launch_bounds__(kStreamThreads, StreamDefault<TK>::kCtasPerSm) k_stream_spmv_dot(FineStream m, const TM* __restrict__ z,
+                                                                       const TK* __restrict__ p_old,
+                                                                       TK* __restrict__ p_new, TK* __restrict__ q,
+                                                                       const double* __restrict__ partA,
+                                                                       double* __restrict__ partB, int nparts,
+                                                                       int first, int par, PcgScalars* __restrict__ S) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ double sh[kStreamThreads / 32];
+  if (S->done) return;
+  const double rz = reduce_parts(partA, nparts, sh);
+  const double rz_prev = S->rz[par ^ 1];
+  const TK beta = first ? TK(0) : (TK)(rz / rz_prev);
+  const double dot = stream_rows<TK, typename StreamDefault<TK>::type>(m.tiles, m.n_tiles, m.pack, XPNew2<TK, TM>{z, p_old, beta},
+                                     EpiSpmvDot<TK, TM>{z, p_old, beta, p_new, q}, smem, &S->status, &S->done);
+  write_part(dot, partB, sh);
+  if (blockIdx.x == 0 && threadIdx.x == 0) S->rz[par] = rz;
+}
+
+// grid of a streamed kernel (one persistent wave), 0 if it cannot run on this device
+template <typename T, typename K>
+static int stream_grid(K kern, int n_tiles) {
+  const int per_sm = stream_ctas_per_sm(reinterpret_cast<const void*>(kern), kStreamThreads, stream_smem_bytes<T>());
+  if (per_sm < 1) return 0;
+  return std::max(1, std::min(n_tiles, kNumSMs * per_sm));
+}
+
+template <typename T>
+static FineStream fine_stream(Solid* s) {
+  if constexpr (sizeof(T) == 4)
+    return {s->pack_desc32.p, s->n_stream_tiles, s->pack32.p};
+  else
+    return {s->pack_desc64.p, s->n_stream_tiles, s->pack64.p};
+}
+
+// launch a streamed row kernel; false (nothing launched) when the fine matrix has no tile plan
+// or the kernel cannot be configured
+template <typename T, typename XF, typename EPI>
+static bool launch_stream_rows(Solid* s, XF xf, EPI epi, double* part, PcgScalars* S, cudaStream_t st,
+                               int* grid_out) {
+  if (s->bs != 3 || !s->packed) return false;
+  auto kern = k_stream_rows<T, XF, EPI>;
+  const int g = stream_grid<T>(kern, s->n_stream_tiles);
+  if (g == 0) return false;
+  kern<<<g, kStreamThreads, stream_smem_bytes<T>(), st>>>(fine_stream<T>(s), xf, epi, part, S);
+  if (grid_out) *grid_out = g;
+  return true;
+}
+
+// ---------------------------------------------------------------------------------------
 // host orchestration
 // ---------------------------------------------------------------------------------------
 static inline int rows_grid(int64_t n_rows) { return grid_for(n_rows, 32, kThreads, 8); }
@@ -632,7 +821,7 @@ static void level_A(Solid* s, DevLevel& L, int lvl, const int32_t*& rp, const in
 // part (if not null) receives the partials of b . out.
 template <typename T>
 static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b, T* out, double* part,
-                  const PcgScalars* S, cudaStream_t st) {
+                  PcgScalars* S, cudaStream_t st) {
   const int nlev = (int)H.levels.size();
   if (lvl == nlev) {  // coarsest
     k_coarse<T><<<resident_grid(k_coarse<T>, kThreads, (H.n_coarse * 32 + kThreads - 1) / kThreads), kThreads, 0,
@@ -665,21 +854,32 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
     const T* av;
     level_A<BS, T>(s, L, lvl, rp, ci, av);
     // pre-smoothing (+ residual)
+    // the fine 3x3 level streams its matrix through shared memory (stream.cuh) when it has a
+    // tile plan; coarse levels use the register row kernels
+    const bool stream = BS == 3 && lvl == 0;
     const T c1 = deg >= 2 ? (T)L.c1[0] : T(0), c2 = deg >= 2 ? (T)L.c2[0] : T(0);
-    k_pre_first<BS, T><<<rg(k_pre_first<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, deg, c1, c2,
-                                                                    V.x.p, V.r.p, V.d.p, V.res.p, S);
+    if (!(stream && launch_stream_rows<T>(s, XD0<T>{b, dinv, it},
+                                          EpiPreFirst<T>{b, dinv, it, deg, c1, c2, V.x.p, V.r.p, V.d.p, V.res.p},
+                                          nullptr, S, st, nullptr)))
+      k_pre_first<BS, T><<<rg(k_pre_first<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, deg, c1, c2,
+                                                                      V.x.p, V.r.p, V.d.p, V.res.p, S);
     W.launches++;
     T* din = V.d.p;
     T* dout = V.d2.p;
     for (int k = 2; k < deg; ++k) {
-      k_cheb_step<BS, T><<<rg(k_cheb_step<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout, V.r.p,
-                                                                      V.x.p, (T)L.c1[k - 1], (T)L.c2[k - 1], b,
-                                                                      nullptr, S);
+      const T ck1 = (T)L.c1[k - 1], ck2 = (T)L.c2[k - 1];
+      if (!(stream && launch_stream_rows<T>(s, XLoad<T, T>{din},
+                                            EpiCheb<T>{dinv, din, dout, V.r.p, V.x.p, ck1, ck2, b, 0}, nullptr, S,
+                                            st, nullptr)))
+        k_cheb_step<BS, T><<<rg(k_cheb_step<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout, V.r.p,
+                                                                        V.x.p, ck1, ck2, b, nullptr, S);
       W.launches++;
       std::swap(din, dout);
     }
     if (deg >= 2) {
-      k_residual<BS, T><<<rg(k_residual<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, V.x.p, V.res.p, S);
+      if (!(stream && launch_stream_rows<T>(s, XLoad<T, T>{V.x.p}, EpiResidual<T>{b, V.res.p}, nullptr, S, st,
+                                            nullptr)))
+        k_residual<BS, T><<<rg(k_residual<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, V.x.p, V.res.p, S);
       W.launches++;
     }
     // restriction b_c = R res
@@ -694,19 +894,30 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
     W.launches++;
     // post-smoothing: result in `out`
     double* part_last = (deg == 1) ? part : nullptr;
-    const int gpf = rg(k_post_first<BS, T>);
+    int gpf = 0;
+    if (!(stream && launch_stream_rows<T>(s, XLoad<T, T>{V.x.p},
+                                          EpiPostFirst<T>{b, dinv, it, V.x.p, out, V.r.p, V.d.p, part_last != nullptr},
+                                          part_last, S, st, &gpf))) {
+      gpf = rg(k_post_first<BS, T>);
+      k_post_first<BS, T><<<gpf, kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, V.x.p, out, V.r.p, V.d.p,
+                                                     part_last, S);
+    }
     if (part_last) W.npA = gpf;
-    k_post_first<BS, T><<<gpf, kThreads, 0, st>>>(
-        nr, rp, ci, av, sd, b, dinv, it, V.x.p, out, V.r.p, V.d.p, part_last, S);
     W.launches++;
     din = V.d.p;
     dout = V.d2.p;
     for (int k = 1; k < deg; ++k) {
       double* pk = (k == deg - 1) ? part : nullptr;
-      const int gcs = rg(k_cheb_step<BS, T>);
+      const T ck1 = (T)L.c1[k - 1], ck2 = (T)L.c2[k - 1];
+      int gcs = 0;
+      if (!(stream && launch_stream_rows<T>(s, XLoad<T, T>{din},
+                                            EpiCheb<T>{dinv, din, dout, V.r.p, out, ck1, ck2, b, pk != nullptr}, pk, S,
+                                            st, &gcs))) {
+        gcs = rg(k_cheb_step<BS, T>);
+        k_cheb_step<BS, T><<<gcs, kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout, V.r.p, out, ck1, ck2, b, pk,
+                                                     S);
+      }
       if (pk) W.npA = gcs;
-      k_cheb_step<BS, T><<<gcs, kThreads, 0, st>>>(
-          nr, rp, ci, av, sd, dinv, din, dout, V.r.p, out, (T)L.c1[k - 1], (T)L.c2[k - 1], b, pk, S);
       W.launches++;
       std::swap(din, dout);
     }
@@ -724,7 +935,7 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
 
 // z = M r with partials of r . z into partA
 template <typename T>
-static int apply_prec(Solid* s, SolverWork& W, int precond, const T* r, T* z, const PcgScalars* S, cudaStream_t st) {
+static int apply_prec(Solid* s, SolverWork& W, int precond, const T* r, T* z, PcgScalars* S, cudaStream_t st) {
   if (precond == 2) return vcycle<T>(s, *s->amg, W, 0, r, z, W.partA.p, S, st);
   const int gp = resident_grid(k_prec_vec<T>, kThreads, (W.n + kThreads - 1) / kThreads);
   W.npA = gp;
@@ -776,6 +987,15 @@ static int pcg_iteration(Solid* s, SolverWork& W, int precond, int k, PcgScalars
   const int gup = resident_grid(k_update<TK, TM>, kThreads, (W.n + kThreads - 1) / kThreads);
   auto spmv_dot = [&](auto bs_tag) {
     constexpr int BS = decltype(bs_tag)::value;
+    if (BS == 3 && s->packed) {  // the fine matrix streamed through shared memory
+      auto kern = k_stream_spmv_dot<TK, TM>;
+      const int g = stream_grid<TK>(kern, s->n_stream_tiles);
+      if (g > 0) {
+        kern<<<g, kStreamThreads, stream_smem_bytes<TK>(), st>>>(fine_stream<TK>(s), B.z, p_old, p_new, B.q,
+                                                                 W.partA.p, W.partB.p, W.npA, k == 0, par, S);
+        return g;
+      }
+    }
     const int g = resident_grid(k_spmv_dot<BS, TK, TM>, kThreads, (s->n_nodes * 32 + kThreads - 1) / kThreads);
     k_spmv_dot<BS, TK, TM><<<g, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, B.A, s->nnzb, B.z, p_old,
                                                    p_new, B.q, W.partA.p, W.partB.p, W.npA, k == 0, par, S);
@@ -1046,8 +1266,8 @@ static int outer_loop(Solid* s, SolverWork& W, int mode, const double* F, double
                                 prm.use_graph, W.scal.p, st, &hS)));
     *total_iters += hS.iters;
     ++*outer;
-    if (hS.status == WN_EBREAKDOWN) {
-      *status = WN_EBREAKDOWN;
+    if (hS.status == WN_EBREAKDOWN || hS.status == WN_ETIMEOUT) {
+      *status = hS.status;
       break;
     }
     PcgBufs<TK, TM> B = pcg_bufs<TK, TM>(s, W);

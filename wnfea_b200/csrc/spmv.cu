@@ -5,6 +5,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "spmv.cuh"
+#include "stream.cuh"
 
 namespace wn {
 
@@ -42,6 +43,58 @@ static int launch(int64_t n_rows, const int32_t* rp, const int32_t* ci, const T*
   if (n_rows == 0) return 0;
   const int grid = resident_grid(bsr_spmv_kernel<BR, BC, G, L, T>, 256, (n_rows * G + 255) / 256);
   bsr_spmv_kernel<BR, BC, G, L, T><<<grid, 256, 0, st>>>(n_rows, rp, ci, v, stride, x, y, a, b);
+  WN_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// y = A x on the fine 3x3 matrix streamed through shared memory (stream.cuh)
+template <typename T>
+struct EpiY {
+  T* __restrict__ y;
+  struct Pre {};
+  __device__ __forceinline__ Pre load(int64_t) const { return {}; }
+  __device__ __forceinline__ double store(int64_t i, const Pre&, T t) const {
+    y[i] = t;
+    return 0.0;
+  }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kStreamThreads, StreamDefault<T>::kCtasPerSm) k_stream_spmv(const PackTile* __restrict__ tiles, int n_tiles,
+                                                                   const unsigned char* __restrict__ pack,
+                                                                   const T* __restrict__ x, T* __restrict__ y,
+                                                                   int* __restrict__ status) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  stream_rows<T, typename StreamDefault<T>::type>(tiles, n_tiles, pack, XLoad<T, T>{x}, EpiY<T>{y}, smem, status,
+                                                  nullptr);
+}
+
+template <typename T>
+static int launch_stream(const PackTile* tiles, int n_tiles, const unsigned char* pack, const T* x, T* y, int* status,
+                         cudaStream_t st) {
+  if (!tiles || !pack || n_tiles == 0) return 0;
+  auto kern = k_stream_spmv<T>;
+  const int per_sm = stream_ctas_per_sm(reinterpret_cast<const void*>(kern), kStreamThreads, stream_smem_bytes<T>());
+  if (per_sm < 1) return 0;
+  const int grid = std::max(1, std::min(n_tiles, kNumSMs * per_sm));
+  kern<<<grid, kStreamThreads, stream_smem_bytes<T>(), st>>>(tiles, n_tiles, pack, x, y, status);
+  WN_CUDA(cudaGetLastError());
+  return 1;
+}
+
+int launch_solid_spmv_stream(int precision, const PackTile* tiles, int n_tiles, const unsigned char* pack,
+                             const void* x, void* y, int* status, cudaStream_t st) {
+  if (precision == 0) return launch_stream<double>(tiles, n_tiles, pack, (const double*)x, (double*)y, status, st);
+  return launch_stream<float>(tiles, n_tiles, pack, (const float*)x, (float*)y, status, st);
+}
+
+int launch_pack_tiles(int n_tiles, const StreamTile* plan, const PackTile* d32, const PackTile* d64, const int32_t* rp,
+                      const int32_t* ci, const float* k32, const double* k64, int64_t nnzb, unsigned char* pack32,
+                      unsigned char* pack64, cudaStream_t st) {
+  if (n_tiles == 0) return 0;
+  const int grid = std::min(n_tiles, kNumSMs * 8);
+  k_pack_tiles<float><<<grid, 256, 0, st>>>(n_tiles, plan, d32, rp, ci, k32, nnzb, pack32);
+  k_pack_tiles<double><<<grid, 256, 0, st>>>(n_tiles, plan, d64, rp, ci, k64, nnzb, pack64);
   WN_CUDA(cudaGetLastError());
   return 0;
 }

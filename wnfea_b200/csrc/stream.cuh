@@ -1,0 +1,426 @@
+// Streamed row engine for the fine-level matrix on sm_100a: 3x3 blocks, 32-bit row pointers and
+// column indices, FP32 or FP64 values.
+//
+// The fine matrix is the one array every fine-level kernel of the solve reads in full (40 B per
+// block in FP32, 76 B in FP64, against 12-24 B of x gathers that L2 serves), so its kernels are
+// HBM-bound, and a warp-per-row kernel that chains row_ptr -> values -> x gathers leaves HBM
+// idle while it waits.  Here the matrix is cut into tiles of whole rows (at most kStreamCap
+// blocks and kStreamRowCap rows) and streamed through shared memory:
+//   * after each assembly the values are packed tile-major ("pack"): tile t is one 128-byte
+//     aligned segment holding its 9 value components (component-major, cntp = cnt rounded up
+//     to 4 per component), its column indices and its local row starts (uint16), so the whole
+//     tile moves with ONE bulk async copy (cp.async.bulk, the TMA's 1-D form) -- a bulk copy
+//     costs the issuing thread a fixed ~70-90 ns on B200 whatever its size, so a tile of 11
+//     separate copies (9 components of the component-major matrix, columns, row pointers)
+//     held one producer to ~1 tile per microsecond;
+//   * one producer thread per CTA issues the copies into a ring of stage buffers, with an L2
+//     evict-first hint so the streamed matrix does not push the vectors out of L2, and
+//     signals completion through an mbarrier per stage (expect_tx bytes); the producer warp
+//     holds the next 32 tile descriptors, one per lane, so no copy waits on a descriptor load;
+//   * consumer warps wait on the stage, compute their rows from shared memory (G lanes per
+//     block row, lane l taking the row's blocks l, l + G, ... -- the assignment and summation
+//     order of the register kernels in spmv.cuh -- with U blocks' gathers in flight per lane),
+//     and release the stage through a second mbarrier;
+//   * CTAs are persistent and take fixed runs of tiles, so the per-CTA dot partials come out in
+//     a fixed order (deterministic two-stage dots).
+// Every wait is bounded in time: a wait that runs out sets the caller's status word to
+// WN_ETIMEOUT and its done flag, the CTA stops issuing, waits (bounded) for its copies in
+// flight and returns.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "wnfea_cuda.h"
+
+namespace wn {
+
+// a tile of the fine matrix: block rows [r0, r1) holding blocks [b0, b1) (the plan)
+struct StreamTile {
+  int32_t r0, r1, b0, b1;
+};
+// the device descriptor of a packed tile: rows [r0, r1), segment at byte 128 seg of the pack,
+// cntp blocks per value component (the tile's block count rounded up to 4)
+struct PackTile {
+  int32_t r0, r1, seg, cntp;
+};
+
+constexpr int kStreamCap = WN_STREAM_TILE_BLOCKS;   // blocks per tile at most (a multiple of 4)
+constexpr int kStreamRowCap = WN_STREAM_TILE_ROWS;  // rows per tile at most
+static_assert(kStreamCap % 4 == 0, "tile capacity: a multiple of 4 blocks");
+// shared memory ahead of the stage buffers: full / empty mbarriers (<= 8 stages), the abort
+// flag at byte 256, the stage descriptors at byte 384
+constexpr int kStreamHeader = 512;
+
+// Byte layout of a packed tile segment (also its stage buffer image):
+//   [0, 9 cntp sizeof(T))      values, component k of local block b at k * cntp + b
+//   [col_off, + 4 cntp)        column indices (padding: 0)
+//   [row_off, + 2 (nr + 1))    local row starts (uint16), rounded up to 16 bytes
+// and the whole segment rounded up to 128 bytes.
+__host__ __device__ constexpr int pack_cntp(int cnt) { return (cnt + 3) & ~3; }
+template <typename T>
+__host__ __device__ constexpr uint32_t pack_col_off(int cntp) {
+  return 9u * (uint32_t)cntp * (uint32_t)sizeof(T);
+}
+template <typename T>
+__host__ __device__ constexpr uint32_t pack_row_off(int cntp) {
+  return pack_col_off<T>(cntp) + 4u * (uint32_t)cntp;
+}
+template <typename T>
+__host__ __device__ constexpr uint32_t pack_bytes(int cntp, int nr) {
+  return (pack_row_off<T>(cntp) + ((2u * (uint32_t)(nr + 1) + 15u) & ~15u) + 127u) & ~127u;
+}
+
+// Shape of a streamed kernel: tile capacity (blocks, rows), consumer warps, lanes per block
+// row, stage buffers, blocks a lane has in flight per row and rows a lane group computes
+// together (their gathers all issued before the first multiply-add).
+template <int CAP, int ROWS, int WARPS, int G, int STAGES, int UNROLL, int RPG = 1>
+struct StreamCfg {
+  static constexpr int kCap = CAP, kRowCap = ROWS, kWarps = WARPS, kG = G, kStages = STAGES, kUnroll = UNROLL;
+  static constexpr int kRpg = RPG;
+  static constexpr int kThreads = (WARPS + 1) * 32;
+  static_assert(CAP % 4 == 0 && ROWS < 65535 && CAP < 65536 && 32 % G == 0 && STAGES >= 2 && STAGES <= 8,
+                "stream shape");
+  template <typename T>
+  static constexpr uint32_t stage_bytes() {
+    return pack_bytes<T>(CAP, ROWS);
+  }
+};
+
+// the shapes the library launches (tiles of the handle's plan: kStreamCap / kStreamRowCap)
+template <typename T>
+struct StreamDefault;
+// (measured on the 1M-DOF I-beam, 17,125 tiles: FP32 SpMV 64 us with 8 consumer warps, 3
+// stages of 20.7 KB and 3 CTAs per SM, against 72-90 us for 12-16 warps at 2 CTAs or 4-8 stages
+// at 1 CTA; FP64 104 us with 8 warps, 2 stages of 39 KB and 2 CTAs per SM)
+template <>
+struct StreamDefault<float> {
+  using type = StreamCfg<kStreamCap, kStreamRowCap, 8, 16, 3, 2>;
+  static constexpr int kCtasPerSm = 3;
+};
+template <>
+struct StreamDefault<double> {
+  using type = StreamCfg<kStreamCap, kStreamRowCap, 8, 16, 2, 2>;
+  static constexpr int kCtasPerSm = 2;
+};
+constexpr int kStreamThreads = 9 * 32;  // threads of the default shapes
+static_assert(StreamDefault<float>::type::kThreads == kStreamThreads &&
+                  StreamDefault<double>::type::kThreads == kStreamThreads,
+              "default shapes share one block size");
+
+template <typename T, typename Cfg = typename StreamDefault<T>::type>
+constexpr size_t stream_smem_bytes() {
+  return kStreamHeader + (size_t)Cfg::kStages * Cfg::template stage_bytes<T>();
+}
+
+// Tiles of whole rows, greedy in row order, at most `cap` blocks and `row_cap` rows each.
+// False if a row alone exceeds `cap` blocks (the engine then cannot take the matrix).
+inline bool build_stream_tiles(const int32_t* rp, int64_t n_rows, std::vector<StreamTile>& out,
+                               int cap = kStreamCap, int row_cap = kStreamRowCap) {
+  out.clear();
+  int64_t r = 0;
+  while (r < n_rows) {
+    const int64_t r0 = r;
+    if (rp[r + 1] - rp[r] > cap) return false;
+    while (r < n_rows && r - r0 < row_cap && rp[r + 1] - rp[r0] <= cap) ++r;
+    out.push_back({(int32_t)r0, (int32_t)r, rp[r0], rp[r]});
+  }
+  return true;
+}
+
+// Segment descriptors of the pack for value type T; returns the pack size in bytes (-1 when
+// it would not be addressable with 32-bit 128-byte segment indices).
+template <typename T>
+inline int64_t build_pack_tiles(const std::vector<StreamTile>& plan, std::vector<PackTile>& out) {
+  out.resize(plan.size());
+  int64_t seg = 0;  // in 128-byte units
+  for (size_t t = 0; t < plan.size(); ++t) {
+    const StreamTile& p = plan[t];
+    const int cntp = pack_cntp(p.b1 - p.b0);
+    if (seg > INT32_MAX) return -1;
+    out[t] = {p.r0, p.r1, (int32_t)seg, cntp};
+    seg += pack_bytes<T>(cntp, p.r1 - p.r0) / 128;
+  }
+  return seg * 128;
+}
+
+#if defined(__CUDACC__)
+
+// Pack the component-major matrix (component k of block b at v[k * stride + b]) tile-major:
+// one CTA per tile, grid-stride; padding is written as zeros.
+template <typename T>
+__global__ void __launch_bounds__(256) k_pack_tiles(int n_tiles, const StreamTile* __restrict__ plan,
+                                                    const PackTile* __restrict__ desc, const int32_t* __restrict__ rp,
+                                                    const int32_t* __restrict__ ci, const T* __restrict__ v,
+                                                    int64_t stride, unsigned char* __restrict__ pack) {
+  for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    const StreamTile p = plan[t];
+    const PackTile d = desc[t];
+    const int cnt = p.b1 - p.b0, cntp = d.cntp, nr = p.r1 - p.r0;
+    unsigned char* seg = pack + (size_t)d.seg * 128;
+    T* sv = reinterpret_cast<T*>(seg);
+    for (int k = 0; k < 9; ++k)
+      for (int b = threadIdx.x; b < cntp; b += blockDim.x)
+        sv[k * cntp + b] = b < cnt ? v[(int64_t)k * stride + p.b0 + b] : T(0);
+    int32_t* sc = reinterpret_cast<int32_t*>(seg + pack_col_off<T>(cntp));
+    for (int b = threadIdx.x; b < cntp; b += blockDim.x) sc[b] = b < cnt ? ci[p.b0 + b] : 0;
+    uint16_t* sr = reinterpret_cast<uint16_t*>(seg + pack_row_off<T>(cntp));
+    const int slots = (int)(pack_bytes<T>(cntp, nr) - pack_row_off<T>(cntp)) / 2;
+    for (int i = threadIdx.x; i < slots; i += blockDim.x) sr[i] = (uint16_t)(i <= nr ? rp[p.r0 + i] - p.b0 : 0);
+  }
+}
+
+constexpr unsigned long long kStreamWaitLimitNs = 4000000000ull;  // 4 s
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+
+// bulk async copy global -> this CTA's shared memory, completion counted on `bar` (bytes and
+// both addresses multiples of 16)
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar, uint64_t pol) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(pol)
+      : "memory");
+}
+
+// one thread: wait for the phase of `parity` to complete; false after the time limit or when
+// `abort_flag` is raised (abort_flag may be null)
+__device__ __forceinline__ bool wait_thread(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (uint32_t n = 1;; ++n) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((n & 63) == 0) {
+      if (abort_flag && *abort_flag) return false;
+      if (global_ns() - t0 > kStreamWaitLimitNs) return false;
+    }
+  }
+}
+
+// a full warp: every lane polls, the warp leaves together (all lanes saw the phase complete,
+// or one lane saw the limit / the abort flag)
+__device__ __forceinline__ bool wait_warp(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  if (__all_sync(0xffffffffu, mbar_try_wait(bar, parity))) return true;
+  const unsigned long long t0 = global_ns();
+  for (uint32_t n = 1;; ++n) {
+    if (__all_sync(0xffffffffu, mbar_try_wait(bar, parity))) return true;
+    if ((n & 63) == 0) {
+      const bool stop = *abort_flag != 0 || global_ns() - t0 > kStreamWaitLimitNs;
+      if (__any_sync(0xffffffffu, stop)) return false;
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T pick3(const T (&a)[3], int l) {
+  return l == 0 ? a[0] : (l == 1 ? a[1] : a[2]);
+}
+
+// The engine.  Every thread of a CTA of Cfg::kThreads threads calls it once (dynamic shared
+// memory of stream_smem_bytes<T, Cfg>()); the pack was built from a plan with Cfg's
+// capacities.  Per row DOF i = 3 row + c of the CTA's tiles the owning lane calls
+// pre = epi.load(i) before the row product and dot += epi.store(i, pre, (A x)_i) after it,
+// with x_j = xf(j).  Returns the thread's dot sum (0 for the producer warp).
+template <typename T, typename Cfg, typename XF, typename EPI>
+__device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles, int n_tiles,
+                                              const unsigned char* __restrict__ pack, const XF& xf, const EPI& epi,
+                                              unsigned char* smem, int* status, int* done) {
+  constexpr int STAGES = Cfg::kStages;
+  constexpr uint32_t SB = Cfg::template stage_bytes<T>();
+  constexpr int G = Cfg::kG;
+  constexpr int U = Cfg::kUnroll;
+  constexpr int R = Cfg::kRpg;
+  constexpr int GPW = 32 / G;  // row groups per warp
+  constexpr int NCW = Cfg::kWarps;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* empty = full + STAGES;
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + 256);
+  int4* descs = reinterpret_cast<int4*>(smem + 384);
+  unsigned char* stages = smem + kStreamHeader;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // this CTA's tiles: a contiguous run [tb, te)
+  const int tb = (int)((int64_t)blockIdx.x * n_tiles / gridDim.x);
+  const int te = (int)((int64_t)(blockIdx.x + 1) * n_tiles / gridDim.x);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, NCW);
+    }
+    *abort_flag = 0;
+    mbar_init_fence();
+  }
+  __syncthreads();
+  double dot = 0.0;
+  auto fail = [&]() {
+    *abort_flag = 1;
+    *status = WN_ETIMEOUT;
+    if (done) *(volatile int*)done = 1;
+  };
+
+  if (warp == NCW) {  // producer warp: lane 0 issues, the warp holds the tile descriptors
+    const uint64_t pol = l2_evict_first_policy();
+    auto load_chunk = [&](int c) {  // descriptors of tiles tb + 32 c + lane
+      const int t = tb + 32 * c + lane;
+      return t < te ? *reinterpret_cast<const int4*>(tiles + t) : make_int4(0, 0, 0, 0);
+    };
+    int4 cur = load_chunk(0), nxt = load_chunk(1);
+    int j = 0;  // tiles issued
+    bool ok = true;
+    for (int t = tb; t < te; ++t, ++j) {
+      const int q = j & 31;
+      int4 d;
+      d.x = __shfl_sync(0xffffffffu, cur.x, q);
+      d.y = __shfl_sync(0xffffffffu, cur.y, q);
+      d.z = __shfl_sync(0xffffffffu, cur.z, q);
+      d.w = __shfl_sync(0xffffffffu, cur.w, q);
+      if (q == 31) {
+        cur = nxt;
+        nxt = load_chunk((j >> 5) + 2);
+      }
+      if (lane == 0) {
+        const int s = j % STAGES;
+        if (j >= STAGES && !wait_thread(empty + s, (uint32_t)((j / STAGES - 1) & 1), abort_flag)) {
+          ok = false;
+        } else {
+          descs[s] = d;
+          const uint32_t bytes = pack_bytes<T>(d.w, d.y - d.x);
+          mbar_arrive_expect_tx(full + s, bytes);
+          bulk_load(stages + (size_t)s * SB, pack + (size_t)d.z * 128, bytes, full + s, pol);
+        }
+      }
+      if (!__shfl_sync(0xffffffffu, ok, 0)) break;
+    }
+    if (lane == 0 && !ok) {
+      fail();
+      // let the copies already issued land before the CTA can exit
+      for (int s = 0; s < STAGES && s < j; ++s) wait_thread(full + s, (uint32_t)(((j - 1 - s) / STAGES) & 1), nullptr);
+    }
+    __syncwarp();
+    return 0.0;
+  }
+
+  // consumer warps
+  const int gl = lane % G, grp = lane / G;
+  int j = 0;
+  for (int t = tb; t < te; ++t, ++j) {
+    const int s = j % STAGES;
+    if (!wait_warp(full + s, (uint32_t)((j / STAGES) & 1), abort_flag)) {
+      if (lane == 0) fail();
+      break;
+    }
+    const unsigned char* st = stages + (size_t)s * SB;
+    const int4 d = descs[s];
+    const int r0 = d.x, nr = d.y - d.x, cntp = d.w;
+    const T* sv = reinterpret_cast<const T*>(st);
+    const int32_t* scol = reinterpret_cast<const int32_t*>(st + pack_col_off<T>(cntp));
+    const uint16_t* srp = reinterpret_cast<const uint16_t*>(st + pack_row_off<T>(cntp));
+    // warps take the tile's rows round-robin in passes of GPW * R rows (group g of a pass owns
+    // rows base + q GPW + g, q < R), starting from a warp that rotates per tile
+    const int wslot = (warp + j) % NCW;
+    for (int base = wslot * GPW * R; base < nr; base += NCW * GPW * R) {
+      int rs[R], re[R];
+      typename EPI::Pre pre[R];
+      T acc[R][3];
+      int len = 0;
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int lr = base + q * GPW + grp;
+        const bool active = lr < nr;
+        rs[q] = active ? srp[lr] : 0;
+        re[q] = active ? srp[lr + 1] : 0;
+        len = max(len, re[q] - rs[q]);
+        pre[q] = typename EPI::Pre{};
+        if (active && gl < 3) pre[q] = epi.load((int64_t)(r0 + lr) * 3 + gl);
+        acc[q][0] = acc[q][1] = acc[q][2] = T(0);
+      }
+      // U blocks of each of the R rows in flight per lane: their gathers are issued before the
+      // first multiply-add; each row's sum still runs over the lane's blocks in order
+      // (b, b + G, b + 2G, ...)
+      for (int o = gl; o < len; o += G * U) {
+        int col[R][U];
+        T xv[R][U][3];
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+#pragma unroll
+          for (int u = 0; u < U; ++u) col[q][u] = (rs[q] + o + u * G < re[q]) ? scol[rs[q] + o + u * G] : 0;
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) xv[q][u][c] = xf((int64_t)col[q][u] * 3 + c);
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int b = rs[q] + o + u * G;
+            if (b < re[q]) {
+              T v[9];
+#pragma unroll
+              for (int k = 0; k < 9; ++k) v[k] = sv[k * cntp + b];
+#pragma unroll
+              for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) acc[q][r] = fma(v[r * 3 + c], xv[q][u][c], acc[q][r]);
+            }
+          }
+      }
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          T v = acc[q][r];
+#pragma unroll
+          for (int o2 = G / 2; o2 > 0; o2 >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o2);
+          acc[q][r] = v;
+        }
+        const int lr = base + q * GPW + grp;
+        if (lr < nr && gl < 3) dot += epi.store((int64_t)(r0 + lr) * 3 + gl, pre[q], pick3(acc[q], gl));
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(empty + s);
+  }
+  return dot;
+}
+
+#endif  // __CUDACC__
+
+}  // namespace wn
