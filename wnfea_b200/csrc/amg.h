@@ -9,6 +9,7 @@
 
 #include "amg_setup.h"
 #include "device_array.h"
+#include "stream_mat.h"
 
 namespace wn {
 
@@ -37,6 +38,10 @@ struct LevelVecs {
   }
 };
 
+// level matrices at least this large (FP32 bytes) are streamed from tile-major packs; smaller
+// ones stay resident in L2 between passes and keep the register row kernels
+constexpr int64_t kStreamMinBytes = 32ll << 20;
+
 struct DevLevel {
   int bs = 3;
   int64_t n_nodes = 0;
@@ -52,6 +57,9 @@ struct DevLevel {
   double inv_theta = 0.0;
   std::vector<double> c1, c2;  // Chebyshev step coefficients k = 1..deg-1
   DevBsr P, R;
+  // the same matrices prepared for the streamed kernels (level matrices of at least
+  // kStreamMinBytes in FP32; n_tiles == 0 otherwise)
+  StreamMat As, Ps, Rs;
   LevelVecs<double> v64;
   LevelVecs<float> v32;
 };

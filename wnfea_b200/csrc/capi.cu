@@ -130,6 +130,8 @@ int make_bsr6_system(int64_t n, const int32_t* rp, const int32_t* ci, const doub
                      values_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice));
   to_float_kernel<<<grid_for(nnzb * 36, 1, 256, 8), 256>>>(nnzb * 36, s->k64.p, s->k32.p);
   WN_CUDA(cudaGetLastError());
+  WN_CHECK(s->fine.make_plan(rp, n, 6, 6));
+  WN_CHECK(s->fine.pack(s->row_ptr.p, s->col_idx.p, s->k32.p, s->k64.p, 0, 0));
   WN_CUDA(cudaDeviceSynchronize());
   s->assembled = true;
   s->bcs_applied = fixed != nullptr;
@@ -230,21 +232,7 @@ int wn_solid_create(int64_t n_nodes, int64_t n_el, const double* nodes, const in
   st = st ? st : s->flags.zero();
   st = st ? st : s->fixed.alloc(n_nodes * 3);
   st = st ? st : s->fixed.zero();
-  if (st == 0) {
-    std::vector<StreamTile> plan;
-    std::vector<PackTile> d32, d64;
-    if (build_stream_tiles(pat.row_ptr.data(), n_nodes, plan) && !plan.empty()) {
-      const int64_t b32 = build_pack_tiles<float>(plan, d32), b64 = build_pack_tiles<double>(plan, d64);
-      if (b32 > 0 && b64 > 0 && plan.size() < (size_t)INT32_MAX) {
-        st = st ? st : s->stream_plan.upload(plan);
-        st = st ? st : s->pack_desc32.upload(d32);
-        st = st ? st : s->pack_desc64.upload(d64);
-        s->pack_size32 = b32;
-        s->pack_size64 = b64;
-        s->n_stream_tiles = (int)plan.size();
-      }
-    }
-  }
+  st = st ? st : s->fine.make_plan(pat.row_ptr.data(), n_nodes, 3, 3);
   if (st == 0) {
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
@@ -349,14 +337,8 @@ int wn_assemble_c3d10_device(void* h, const double* d_props, int apply_bcs, uint
   WN_CHECK(launch_ke_upper(s->n_el, s->nodes.p, s->conn.p, s->props.p, s->ke.p, s->flags.p, st));
   WN_CHECK(launch_gather_assemble(s->nnzb, s->gptr.p, s->gsrc.p, s->ke.p, s->block_row.p, s->col_idx.p,
                                   apply_bcs ? s->fixed.p : nullptr, s->k64.p, s->k32.p, st));
-  s->packed = false;
-  if (s->n_stream_tiles > 0) {  // tile-major copies for the streamed fine-level kernels
-    WN_CHECK(s->pack32.alloc(s->pack_size32));
-    WN_CHECK(s->pack64.alloc(s->pack_size64));
-    WN_CHECK(launch_pack_tiles(s->n_stream_tiles, s->stream_plan.p, s->pack_desc32.p, s->pack_desc64.p, s->row_ptr.p,
-                               s->col_idx.p, s->k32.p, s->k64.p, s->nnzb, s->pack32.p, s->pack64.p, st));
-    s->packed = true;
-  }
+  // tile-major copies for the streamed fine-level kernels
+  WN_CHECK(s->fine.pack(s->row_ptr.p, s->col_idx.p, s->k32.p, s->k64.p, s->nnzb, st));
   int flag = 0;
   WN_CHECK(read_flag(s, st, &flag));
   WN_REQUIRE(flag == 0, WN_EMESH, "wn_assemble_c3d10: non-positive Jacobian determinant in a C3D10 element");
@@ -433,9 +415,9 @@ int wn_spmv_solid_device(void* h, int precision, const void* x, void* y, uintptr
   WN_REQUIRE(s->assembled, WN_ESTATE, "wn_spmv_solid_device: not assembled");
   WN_CHECK(select_device(s));
   if (precision == 0 || precision == 1) {
-    if (s->packed) {
-      const int rc = launch_solid_spmv_stream(precision, precision == 0 ? s->pack_desc64.p : s->pack_desc32.p,
-                                              s->n_stream_tiles, precision == 0 ? s->pack64.p : s->pack32.p, x, y,
+    if (s->fine.packed) {
+      const int rc = launch_solid_spmv_stream(precision, precision == 0 ? s->fine.d64.p : s->fine.d32.p,
+                                              s->fine.n_tiles, precision == 0 ? s->fine.p64.p : s->fine.p32.p, x, y,
                                               s->flags.p + kStreamStatusWord, (cudaStream_t)stream);
       if (rc != 0) return rc < 0 ? rc : 0;
     }

@@ -41,13 +41,8 @@ int launch_solid_spmv_f32(int64_t n_rows, const int32_t* rp, const int32_t* ci, 
 // (stream.cuh); returns 1 when launched, 0 when the kernel cannot run here, < 0 on error; a
 // pipeline wait that runs out of time writes WN_ETIMEOUT to *status
 struct PackTile;
-struct StreamTile;
 int launch_solid_spmv_stream(int precision, const PackTile* tiles, int n_tiles, const unsigned char* pack,
                              const void* x, void* y, int* status, cudaStream_t st);
-// pack the component-major FP32 and FP64 values tile-major (spmv.cu)
-int launch_pack_tiles(int n_tiles, const StreamTile* plan, const PackTile* d32, const PackTile* d64, const int32_t* rp,
-                      const int32_t* ci, const float* k32, const double* k64, int64_t nnzb, unsigned char* pack32,
-                      unsigned char* pack64, cudaStream_t st);
 
 // A linear 6-DOF-per-node system (block-contiguous row-major 6x6 values; host pattern arrays,
 // values on the host or the device) as a solver handle with bs = 6 (capi.cu).

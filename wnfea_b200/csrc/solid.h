@@ -9,7 +9,7 @@
 
 #include "device_array.h"
 #include "pattern.h"
-#include "stream.cuh"
+#include "stream_mat.h"
 
 namespace wn {
 
@@ -46,15 +46,9 @@ struct Solid {
   DArray<double> ke;        // scratch: n_el x 55 x 9 element blocks
   DArray<double> fe;        // scratch: n_el x 30 element forces
   DArray<int> flags;        // device status words ([kStreamStatusWord]: streamed SpMV)
-  // row tiles of the fine matrix for the streamed kernels (stream.cuh) and the tile-major
-  // packs of the FP32 / FP64 values they read (refreshed by every assembly); no tiles when a
-  // row exceeds the tile capacity, and the register row kernels are used instead
-  DArray<StreamTile> stream_plan;
-  int n_stream_tiles = 0;
-  DArray<PackTile> pack_desc32, pack_desc64;
-  int64_t pack_size32 = 0, pack_size64 = 0;
-  DArray<unsigned char> pack32, pack64;
-  bool packed = false;
+  // the fine matrix prepared for the streamed kernels (stream.cuh): tile plan made with the
+  // pattern, FP32 / FP64 tile-major packs refreshed by every assembly
+  StreamMat fine;
   bool assembled = false;
   bool bcs_applied = false;
   std::unique_ptr<AmgHierarchy> amg;

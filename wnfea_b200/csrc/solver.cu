@@ -231,8 +231,8 @@ __global__ void __launch_bounds__(kThreads) k_level_spmv(int64_t n_rows, const i
 
 // launch k_level_spmv with a group size matched to the mean row length
 template <int BR, int BC, typename T>
-static void level_spmv(const DevBsr& M, const T* vals, const T* x, T* y, int accumulate, const PcgScalars* S,
-                       cudaStream_t st) {
+static void level_spmv_rows(const DevBsr& M, const T* vals, const T* x, T* y, int accumulate, const PcgScalars* S,
+                            cudaStream_t st) {
   const double avg = M.n_rows ? (double)M.nnzb / (double)M.n_rows : 0.0;
   if (avg >= 24.0) {
     auto k = k_level_spmv<BR, BC, 32, T>;
@@ -699,74 +699,96 @@ struct EpiSpmvDot {
   }
 };
 
-// the fine matrix as the streamed kernels see it: the tile-major pack of one precision
-struct FineStream {
+template <typename T>
+struct EpiLevel {  // y = A x (accumulate = 0) or y += A x (the transfer operators)
+  T* __restrict__ y;
+  int accumulate;
+  struct Pre {
+    T yi;
+  };
+  __device__ __forceinline__ Pre load(int64_t i) const { return {accumulate ? y[i] : T(0)}; }
+  __device__ __forceinline__ double store(int64_t i, const Pre& p, T t) const {
+    y[i] = accumulate ? p.yi + t : t;
+    return 0.0;
+  }
+};
+
+// a matrix as the streamed kernels see it: the tile-major pack of one precision
+struct StreamView {
   const PackTile* tiles;
   int n_tiles;
   const unsigned char* pack;
 };
 
-template <typename T, typename XF, typename EPI>
-__global__ void __launch_bounds__(kStreamThreads, StreamDefault<T>::kCtasPerSm) k_stream_rows(FineStream m, XF xf, EPI epi,
-                                                                   double* __restrict__ part,
-                                                                   PcgScalars* __restrict__ S) {
+template <typename T>
+static StreamView stream_view(const StreamMat& m) {
+  if constexpr (sizeof(T) == 4)
+    return {m.d32.p, m.n_tiles, m.p32.p};
+  else
+    return {m.d64.p, m.n_tiles, m.p64.p};
+}
+
+template <typename T, int BR, int BC, typename XF, typename EPI>
+__global__ void __launch_bounds__(kStreamThreads, (StreamDefault<T, BR, BC>::kCtasPerSm))
+    k_stream_rows(StreamView m, XF xf, EPI epi, double* __restrict__ part, PcgScalars* __restrict__ S) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ double sh[kStreamThreads / 32];
   if (S->done) return;
-  const double dot = stream_rows<T, typename StreamDefault<T>::type>(m.tiles, m.n_tiles, m.pack, xf, epi, smem,
-                                                                     &S->status, &S->done);
+  const double dot = stream_rows<T, BR, BC, typename StreamDefault<T, BR, BC>::type>(
+      m.tiles, m.n_tiles, m.pack, xf, epi, smem, &S->status, &S->done);
   if (part) write_part(dot, part, sh);
 }
 
 // k_spmv_dot with the matrix streamed: beta from the partials of r . z, p_new = z + beta p_old,
 // q = A p_new, partials of p_new . q
-template <typename TK, typename TM>
-__global__ void __launch_bounds__(kStreamThreads, StreamDefault<TK>::kCtasPerSm) k_stream_spmv_dot(FineStream m, const TM* __restrict__ z,
-                                                                       const TK* __restrict__ p_old,
-                                                                       TK* __restrict__ p_new, TK* __restrict__ q,
-                                                                       const double* __restrict__ partA,
-                                                                       double* __restrict__ partB, int nparts,
-                                                                       int first, int par, PcgScalars* __restrict__ S) {
+template <int BS, typename TK, typename TM>
+__global__ void __launch_bounds__(kStreamThreads, (StreamDefault<TK, BS, BS>::kCtasPerSm))
+    k_stream_spmv_dot(StreamView m, const TM* __restrict__ z, const TK* __restrict__ p_old, TK* __restrict__ p_new,
+                      TK* __restrict__ q, const double* __restrict__ partA, double* __restrict__ partB, int nparts,
+                      int first, int par, PcgScalars* __restrict__ S) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ double sh[kStreamThreads / 32];
   if (S->done) return;
   const double rz = reduce_parts(partA, nparts, sh);
   const double rz_prev = S->rz[par ^ 1];
   const TK beta = first ? TK(0) : (TK)(rz / rz_prev);
-  const double dot = stream_rows<TK, typename StreamDefault<TK>::type>(m.tiles, m.n_tiles, m.pack, XPNew2<TK, TM>{z, p_old, beta},
-                                     EpiSpmvDot<TK, TM>{z, p_old, beta, p_new, q}, smem, &S->status, &S->done);
+  const double dot = stream_rows<TK, BS, BS, typename StreamDefault<TK, BS, BS>::type>(
+      m.tiles, m.n_tiles, m.pack, XPNew2<TK, TM>{z, p_old, beta}, EpiSpmvDot<TK, TM>{z, p_old, beta, p_new, q}, smem,
+      &S->status, &S->done);
   write_part(dot, partB, sh);
   if (blockIdx.x == 0 && threadIdx.x == 0) S->rz[par] = rz;
 }
 
 // grid of a streamed kernel (one persistent wave), 0 if it cannot run on this device
-template <typename T, typename K>
+template <typename T, int BR, int BC, typename K>
 static int stream_grid(K kern, int n_tiles) {
-  const int per_sm = stream_ctas_per_sm(reinterpret_cast<const void*>(kern), kStreamThreads, stream_smem_bytes<T>());
+  const int per_sm =
+      stream_ctas_per_sm(reinterpret_cast<const void*>(kern), kStreamThreads, stream_smem_bytes<T, BR, BC>());
   if (per_sm < 1) return 0;
   return std::max(1, std::min(n_tiles, kNumSMs * per_sm));
 }
 
-template <typename T>
-static FineStream fine_stream(Solid* s) {
-  if constexpr (sizeof(T) == 4)
-    return {s->pack_desc32.p, s->n_stream_tiles, s->pack32.p};
-  else
-    return {s->pack_desc64.p, s->n_stream_tiles, s->pack64.p};
-}
-
-// launch a streamed row kernel; false (nothing launched) when the fine matrix has no tile plan
-// or the kernel cannot be configured
-template <typename T, typename XF, typename EPI>
-static bool launch_stream_rows(Solid* s, XF xf, EPI epi, double* part, PcgScalars* S, cudaStream_t st,
+// launch a streamed row kernel on matrix m (BR x BC blocks); false (nothing launched) when m
+// has no current pack of that shape or the kernel cannot be configured
+template <typename T, int BR, int BC, typename XF, typename EPI>
+static bool launch_stream_rows(const StreamMat& m, XF xf, EPI epi, double* part, PcgScalars* S, cudaStream_t st,
                                int* grid_out) {
-  if (s->bs != 3 || !s->packed) return false;
-  auto kern = k_stream_rows<T, XF, EPI>;
-  const int g = stream_grid<T>(kern, s->n_stream_tiles);
+  if (!m.packed || m.br != BR || m.bc != BC) return false;
+  auto kern = k_stream_rows<T, BR, BC, XF, EPI>;
+  const int g = stream_grid<T, BR, BC>(kern, m.n_tiles);
   if (g == 0) return false;
-  kern<<<g, kStreamThreads, stream_smem_bytes<T>(), st>>>(fine_stream<T>(s), xf, epi, part, S);
+  kern<<<g, kStreamThreads, stream_smem_bytes<T, BR, BC>(), st>>>(stream_view<T>(m), xf, epi, part, S);
   if (grid_out) *grid_out = g;
   return true;
+}
+
+// y = M x or y += M x for a transfer operator: streamed from its pack when it has one, else the
+// register row kernel
+template <int BR, int BC, typename T>
+static void level_spmv(const DevBsr& M, const StreamMat& Ms, const T* vals, const T* x, T* y, int accumulate,
+                       PcgScalars* S, cudaStream_t st) {
+  if (launch_stream_rows<T, BR, BC>(Ms, XLoad<T, T>{x}, EpiLevel<T>{y, accumulate}, nullptr, S, st, nullptr)) return;
+  level_spmv_rows<BR, BC, T>(M, vals, x, y, accumulate, S, st);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -853,12 +875,13 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
     const int32_t* ci;
     const T* av;
     level_A<BS, T>(s, L, lvl, rp, ci, av);
-    // pre-smoothing (+ residual)
-    // the fine 3x3 level streams its matrix through shared memory (stream.cuh) when it has a
-    // tile plan; coarse levels use the register row kernels
-    const bool stream = BS == 3 && lvl == 0;
+    // pre-smoothing (+ residual).  A level whose matrix has a current tile-major pack (the fine
+    // level; coarse levels too large for L2) streams it through shared memory (stream.cuh);
+    // the others use the register row kernels
+    const StreamMat& Am = (lvl == 0) ? s->fine : L.As;
+    const bool stream = Am.packed;
     const T c1 = deg >= 2 ? (T)L.c1[0] : T(0), c2 = deg >= 2 ? (T)L.c2[0] : T(0);
-    if (!(stream && launch_stream_rows<T>(s, XD0<T>{b, dinv, it},
+    if (!(stream && launch_stream_rows<T, BS, BS>(Am, XD0<T>{b, dinv, it},
                                           EpiPreFirst<T>{b, dinv, it, deg, c1, c2, V.x.p, V.r.p, V.d.p, V.res.p},
                                           nullptr, S, st, nullptr)))
       k_pre_first<BS, T><<<rg(k_pre_first<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, deg, c1, c2,
@@ -868,7 +891,7 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
     T* dout = V.d2.p;
     for (int k = 2; k < deg; ++k) {
       const T ck1 = (T)L.c1[k - 1], ck2 = (T)L.c2[k - 1];
-      if (!(stream && launch_stream_rows<T>(s, XLoad<T, T>{din},
+      if (!(stream && launch_stream_rows<T, BS, BS>(Am, XLoad<T, T>{din},
                                             EpiCheb<T>{dinv, din, dout, V.r.p, V.x.p, ck1, ck2, b, 0}, nullptr, S,
                                             st, nullptr)))
         k_cheb_step<BS, T><<<rg(k_cheb_step<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout, V.r.p,
@@ -877,7 +900,7 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
       std::swap(din, dout);
     }
     if (deg >= 2) {
-      if (!(stream && launch_stream_rows<T>(s, XLoad<T, T>{V.x.p}, EpiResidual<T>{b, V.res.p}, nullptr, S, st,
+      if (!(stream && launch_stream_rows<T, BS, BS>(Am, XLoad<T, T>{V.x.p}, EpiResidual<T>{b, V.res.p}, nullptr, S, st,
                                             nullptr)))
         k_residual<BS, T><<<rg(k_residual<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, V.x.p, V.res.p, S);
       W.launches++;
@@ -886,16 +909,16 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
     DevLevel* Ln = lvl + 1 < nlev ? &H.levels[lvl + 1] : nullptr;
     T* bc = Ln ? Prec<T>::vecs(*Ln).b.p : Prec<T>::cb(H);
     T* xc = Ln ? Prec<T>::vecs(*Ln).x2.p : Prec<T>::cx(H);
-    level_spmv<6, BS, T>(L.R, Prec<T>::Rv(L), V.res.p, bc, 0, S, st);
+    level_spmv<6, BS, T>(L.R, L.Rs, Prec<T>::Rv(L), V.res.p, bc, 0, S, st);
     W.launches++;
     WN_CHECK(vcycle<T>(s, H, W, lvl + 1, bc, xc, nullptr, S, st));
     // prolongation x += P x_c
-    level_spmv<BS, 6, T>(L.P, Prec<T>::Pv(L), xc, V.x.p, 1, S, st);
+    level_spmv<BS, 6, T>(L.P, L.Ps, Prec<T>::Pv(L), xc, V.x.p, 1, S, st);
     W.launches++;
     // post-smoothing: result in `out`
     double* part_last = (deg == 1) ? part : nullptr;
     int gpf = 0;
-    if (!(stream && launch_stream_rows<T>(s, XLoad<T, T>{V.x.p},
+    if (!(stream && launch_stream_rows<T, BS, BS>(Am, XLoad<T, T>{V.x.p},
                                           EpiPostFirst<T>{b, dinv, it, V.x.p, out, V.r.p, V.d.p, part_last != nullptr},
                                           part_last, S, st, &gpf))) {
       gpf = rg(k_post_first<BS, T>);
@@ -910,7 +933,7 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
       double* pk = (k == deg - 1) ? part : nullptr;
       const T ck1 = (T)L.c1[k - 1], ck2 = (T)L.c2[k - 1];
       int gcs = 0;
-      if (!(stream && launch_stream_rows<T>(s, XLoad<T, T>{din},
+      if (!(stream && launch_stream_rows<T, BS, BS>(Am, XLoad<T, T>{din},
                                             EpiCheb<T>{dinv, din, dout, V.r.p, out, ck1, ck2, b, pk != nullptr}, pk, S,
                                             st, &gcs))) {
         gcs = rg(k_cheb_step<BS, T>);
@@ -987,12 +1010,12 @@ static int pcg_iteration(Solid* s, SolverWork& W, int precond, int k, PcgScalars
   const int gup = resident_grid(k_update<TK, TM>, kThreads, (W.n + kThreads - 1) / kThreads);
   auto spmv_dot = [&](auto bs_tag) {
     constexpr int BS = decltype(bs_tag)::value;
-    if (BS == 3 && s->packed) {  // the fine matrix streamed through shared memory
-      auto kern = k_stream_spmv_dot<TK, TM>;
-      const int g = stream_grid<TK>(kern, s->n_stream_tiles);
+    if (s->fine.packed && s->fine.br == BS) {  // the fine matrix streamed through shared memory
+      auto kern = k_stream_spmv_dot<BS, TK, TM>;
+      const int g = stream_grid<TK, BS, BS>(kern, s->fine.n_tiles);
       if (g > 0) {
-        kern<<<g, kStreamThreads, stream_smem_bytes<TK>(), st>>>(fine_stream<TK>(s), B.z, p_old, p_new, B.q,
-                                                                 W.partA.p, W.partB.p, W.npA, k == 0, par, S);
+        kern<<<g, kStreamThreads, stream_smem_bytes<TK, BS, BS>(), st>>>(
+            stream_view<TK>(s->fine), B.z, p_old, p_new, B.q, W.partA.p, W.partB.p, W.npA, k == 0, par, S);
         return g;
       }
     }
@@ -1169,6 +1192,15 @@ int solver_setup(Solid* s, const wn_amg_params& prm) {
     cheb_coefficients(prm, L);
     WN_CHECK(L.P.upload(h.P));
     WN_CHECK(L.R.upload(h.R));
+    // matrices too large to stay in L2 between passes are streamed from tile-major packs
+    auto stream_if_large = [&](StreamMat& m, const HostBsr& hb, const DevBsr& db) -> int {
+      if (hb.nnzb() * hb.br * hb.bc * (int64_t)sizeof(float) < kStreamMinBytes) return 0;
+      WN_CHECK(m.make_plan(hb.rp.data(), hb.n_rows, hb.br, hb.bc));
+      return m.pack(db.rp.p, db.ci.p, db.v32.p, db.v64.p, 0, 0);
+    };
+    if (l > 0) WN_CHECK(stream_if_large(L.As, h.A, L.A));
+    WN_CHECK(stream_if_large(L.Ps, h.P, L.P));
+    WN_CHECK(stream_if_large(L.Rs, h.R, L.R));
     WN_CHECK(L.v64.alloc(h.n_nodes * h.bs));
     WN_CHECK(L.v32.alloc(h.n_nodes * h.bs));
   }

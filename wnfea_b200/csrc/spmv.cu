@@ -60,13 +60,13 @@ struct EpiY {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(kStreamThreads, StreamDefault<T>::kCtasPerSm) k_stream_spmv(const PackTile* __restrict__ tiles, int n_tiles,
+__global__ void __launch_bounds__(kStreamThreads, (StreamDefault<T, 3, 3>::kCtasPerSm)) k_stream_spmv(const PackTile* __restrict__ tiles, int n_tiles,
                                                                    const unsigned char* __restrict__ pack,
                                                                    const T* __restrict__ x, T* __restrict__ y,
                                                                    int* __restrict__ status) {
   extern __shared__ __align__(128) unsigned char smem[];
-  stream_rows<T, typename StreamDefault<T>::type>(tiles, n_tiles, pack, XLoad<T, T>{x}, EpiY<T>{y}, smem, status,
-                                                  nullptr);
+  stream_rows<T, 3, 3, typename StreamDefault<T, 3, 3>::type>(tiles, n_tiles, pack, XLoad<T, T>{x}, EpiY<T>{y},
+                                                               smem, status, nullptr);
 }
 
 template <typename T>
@@ -74,10 +74,11 @@ static int launch_stream(const PackTile* tiles, int n_tiles, const unsigned char
                          cudaStream_t st) {
   if (!tiles || !pack || n_tiles == 0) return 0;
   auto kern = k_stream_spmv<T>;
-  const int per_sm = stream_ctas_per_sm(reinterpret_cast<const void*>(kern), kStreamThreads, stream_smem_bytes<T>());
+  const int per_sm =
+      stream_ctas_per_sm(reinterpret_cast<const void*>(kern), kStreamThreads, stream_smem_bytes<T, 3, 3>());
   if (per_sm < 1) return 0;
   const int grid = std::max(1, std::min(n_tiles, kNumSMs * per_sm));
-  kern<<<grid, kStreamThreads, stream_smem_bytes<T>(), st>>>(tiles, n_tiles, pack, x, y, status);
+  kern<<<grid, kStreamThreads, stream_smem_bytes<T, 3, 3>(), st>>>(tiles, n_tiles, pack, x, y, status);
   WN_CUDA(cudaGetLastError());
   return 1;
 }
@@ -86,17 +87,6 @@ int launch_solid_spmv_stream(int precision, const PackTile* tiles, int n_tiles, 
                              const void* x, void* y, int* status, cudaStream_t st) {
   if (precision == 0) return launch_stream<double>(tiles, n_tiles, pack, (const double*)x, (double*)y, status, st);
   return launch_stream<float>(tiles, n_tiles, pack, (const float*)x, (float*)y, status, st);
-}
-
-int launch_pack_tiles(int n_tiles, const StreamTile* plan, const PackTile* d32, const PackTile* d64, const int32_t* rp,
-                      const int32_t* ci, const float* k32, const double* k64, int64_t nnzb, unsigned char* pack32,
-                      unsigned char* pack64, cudaStream_t st) {
-  if (n_tiles == 0) return 0;
-  const int grid = std::min(n_tiles, kNumSMs * 8);
-  k_pack_tiles<float><<<grid, 256, 0, st>>>(n_tiles, plan, d32, rp, ci, k32, nnzb, pack32);
-  k_pack_tiles<double><<<grid, 256, 0, st>>>(n_tiles, plan, d64, rp, ci, k64, nnzb, pack64);
-  WN_CUDA(cudaGetLastError());
-  return 0;
 }
 
 int launch_solid_spmv_f64(int64_t n_rows, const int32_t* rp, const int32_t* ci, const double* v, int64_t nnzb,

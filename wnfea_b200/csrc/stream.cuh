@@ -1,5 +1,6 @@
-// Streamed row engine for the fine-level matrix on sm_100a: 3x3 blocks, 32-bit row pointers and
-// column indices, FP32 or FP64 values.
+// Streamed row engine for block-sparse matrices on sm_100a: BR x BC blocks (3x3 for the fine
+// level, 6x6 for AMG level 1, 3x6 / 6x3 for its prolongator / restrictor), 32-bit row pointers
+// and column indices, FP32 or FP64 values.
 //
 // The fine matrix is the one array every fine-level kernel of the solve reads in full (40 B per
 // block in FP32, 76 B in FP64, against 12-24 B of x gathers that L2 serves), so its kernels are
@@ -7,8 +8,8 @@
 // idle while it waits.  Here the matrix is cut into tiles of whole rows (at most kStreamCap
 // blocks and kStreamRowCap rows) and streamed through shared memory:
 //   * after each assembly the values are packed tile-major ("pack"): tile t is one 128-byte
-//     aligned segment holding its 9 value components (component-major, cntp = cnt rounded up
-//     to 4 per component), its column indices and its local row starts (uint16), so the whole
+//     aligned segment holding its BR * BC value components (component-major, cntp = cnt rounded
+//     up to 4 per component), its column indices and its local row starts (uint16), so the whole
 //     tile moves with ONE bulk async copy (cp.async.bulk, the TMA's 1-D form) -- a bulk copy
 //     costs the issuing thread a fixed ~70-90 ns on B200 whatever its size, so a tile of 11
 //     separate copies (9 components of the component-major matrix, columns, row pointers)
@@ -54,23 +55,24 @@ static_assert(kStreamCap % 4 == 0, "tile capacity: a multiple of 4 blocks");
 // flag at byte 256, the stage descriptors at byte 384
 constexpr int kStreamHeader = 512;
 
-// Byte layout of a packed tile segment (also its stage buffer image):
-//   [0, 9 cntp sizeof(T))      values, component k of local block b at k * cntp + b
+// Byte layout of a packed tile segment of NV = BR * BC values per block (also its stage buffer
+// image):
+//   [0, NV cntp sizeof(T))     values, component k of local block b at k * cntp + b
 //   [col_off, + 4 cntp)        column indices (padding: 0)
 //   [row_off, + 2 (nr + 1))    local row starts (uint16), rounded up to 16 bytes
 // and the whole segment rounded up to 128 bytes.
 __host__ __device__ constexpr int pack_cntp(int cnt) { return (cnt + 3) & ~3; }
-template <typename T>
+template <typename T, int NV>
 __host__ __device__ constexpr uint32_t pack_col_off(int cntp) {
-  return 9u * (uint32_t)cntp * (uint32_t)sizeof(T);
+  return (uint32_t)NV * (uint32_t)cntp * (uint32_t)sizeof(T);
 }
-template <typename T>
+template <typename T, int NV>
 __host__ __device__ constexpr uint32_t pack_row_off(int cntp) {
-  return pack_col_off<T>(cntp) + 4u * (uint32_t)cntp;
+  return pack_col_off<T, NV>(cntp) + 4u * (uint32_t)cntp;
 }
-template <typename T>
+template <typename T, int NV>
 __host__ __device__ constexpr uint32_t pack_bytes(int cntp, int nr) {
-  return (pack_row_off<T>(cntp) + ((2u * (uint32_t)(nr + 1) + 15u) & ~15u) + 127u) & ~127u;
+  return (pack_row_off<T, NV>(cntp) + ((2u * (uint32_t)(nr + 1) + 15u) & ~15u) + 127u) & ~127u;
 }
 
 // Shape of a streamed kernel: tile capacity (blocks, rows), consumer warps, lanes per block
@@ -83,36 +85,50 @@ struct StreamCfg {
   static constexpr int kThreads = (WARPS + 1) * 32;
   static_assert(CAP % 4 == 0 && ROWS < 65535 && CAP < 65536 && 32 % G == 0 && STAGES >= 2 && STAGES <= 8,
                 "stream shape");
-  template <typename T>
+  template <typename T, int NV>
   static constexpr uint32_t stage_bytes() {
-    return pack_bytes<T>(CAP, ROWS);
+    return pack_bytes<T, NV>(CAP, ROWS);
   }
 };
 
-// the shapes the library launches (tiles of the handle's plan: kStreamCap / kStreamRowCap)
-template <typename T>
+// The shapes the library launches, per value type and block shape (all 8 consumer warps + 1
+// producer warp: kStreamThreads threads).  3x3 (fine level; measured on the 1M-DOF I-beam,
+// 17,125 tiles: FP32 SpMV 64 us with 8 consumer warps, 3 stages of 20.7 KB and 3 CTAs per SM,
+// against 72-90 us for 12-16 warps at 2 CTAs or 4-8 stages at 1 CTA; FP64 104 us with 2 stages
+// of 39 KB and 2 CTAs per SM).  6x6 (AMG level 1, rows of ~54 blocks) and 6x3 (restriction,
+// rows of ~105 blocks): a warp per row; 3x6 (prolongation, rows of ~5.5 blocks): 8 lanes per row.
+constexpr int kStreamThreads = 9 * 32;
+template <typename T, int BR, int BC>
 struct StreamDefault;
-// (measured on the 1M-DOF I-beam, 17,125 tiles: FP32 SpMV 64 us with 8 consumer warps, 3
-// stages of 20.7 KB and 3 CTAs per SM, against 72-90 us for 12-16 warps at 2 CTAs or 4-8 stages
-// at 1 CTA; FP64 104 us with 8 warps, 2 stages of 39 KB and 2 CTAs per SM)
 template <>
-struct StreamDefault<float> {
+struct StreamDefault<float, 3, 3> {
   using type = StreamCfg<kStreamCap, kStreamRowCap, 8, 16, 3, 2>;
   static constexpr int kCtasPerSm = 3;
 };
 template <>
-struct StreamDefault<double> {
+struct StreamDefault<double, 3, 3> {
   using type = StreamCfg<kStreamCap, kStreamRowCap, 8, 16, 2, 2>;
   static constexpr int kCtasPerSm = 2;
 };
-constexpr int kStreamThreads = 9 * 32;  // threads of the default shapes
-static_assert(StreamDefault<float>::type::kThreads == kStreamThreads &&
-                  StreamDefault<double>::type::kThreads == kStreamThreads,
-              "default shapes share one block size");
+template <typename T>
+struct StreamDefault<T, 6, 6> {
+  using type = StreamCfg<256, kStreamRowCap, 8, 32, 2, 1>;
+  static constexpr int kCtasPerSm = sizeof(T) == 4 ? 2 : 1;
+};
+template <typename T>
+struct StreamDefault<T, 6, 3> {
+  using type = StreamCfg<512, kStreamRowCap, 8, 32, 2, 2>;
+  static constexpr int kCtasPerSm = sizeof(T) == 4 ? 2 : 1;
+};
+template <typename T>
+struct StreamDefault<T, 3, 6> {
+  using type = StreamCfg<512, kStreamRowCap, 8, 8, 2, 1>;
+  static constexpr int kCtasPerSm = sizeof(T) == 4 ? 2 : 1;
+};
 
-template <typename T, typename Cfg = typename StreamDefault<T>::type>
+template <typename T, int BR, int BC, typename Cfg = typename StreamDefault<T, BR, BC>::type>
 constexpr size_t stream_smem_bytes() {
-  return kStreamHeader + (size_t)Cfg::kStages * Cfg::template stage_bytes<T>();
+  return kStreamHeader + (size_t)Cfg::kStages * Cfg::template stage_bytes<T, BR * BC>();
 }
 
 // Tiles of whole rows, greedy in row order, at most `cap` blocks and `row_cap` rows each.
@@ -132,7 +148,7 @@ inline bool build_stream_tiles(const int32_t* rp, int64_t n_rows, std::vector<St
 
 // Segment descriptors of the pack for value type T; returns the pack size in bytes (-1 when
 // it would not be addressable with 32-bit 128-byte segment indices).
-template <typename T>
+template <typename T, int NV>
 inline int64_t build_pack_tiles(const std::vector<StreamTile>& plan, std::vector<PackTile>& out) {
   out.resize(plan.size());
   int64_t seg = 0;  // in 128-byte units
@@ -141,16 +157,17 @@ inline int64_t build_pack_tiles(const std::vector<StreamTile>& plan, std::vector
     const int cntp = pack_cntp(p.b1 - p.b0);
     if (seg > INT32_MAX) return -1;
     out[t] = {p.r0, p.r1, (int32_t)seg, cntp};
-    seg += pack_bytes<T>(cntp, p.r1 - p.r0) / 128;
+    seg += pack_bytes<T, NV>(cntp, p.r1 - p.r0) / 128;
   }
   return seg * 128;
 }
 
 #if defined(__CUDACC__)
 
-// Pack the component-major matrix (component k of block b at v[k * stride + b]) tile-major:
-// one CTA per tile, grid-stride; padding is written as zeros.
-template <typename T>
+// Pack a matrix of NV values per block tile-major: source component k of block b at
+// v[k * stride + b] (component-major, stride > 0) or v[b * NV + k] (block-contiguous,
+// stride == 0).  One CTA per tile, grid-stride; padding is written as zeros.
+template <typename T, int NV>
 __global__ void __launch_bounds__(256) k_pack_tiles(int n_tiles, const StreamTile* __restrict__ plan,
                                                     const PackTile* __restrict__ desc, const int32_t* __restrict__ rp,
                                                     const int32_t* __restrict__ ci, const T* __restrict__ v,
@@ -161,13 +178,20 @@ __global__ void __launch_bounds__(256) k_pack_tiles(int n_tiles, const StreamTil
     const int cnt = p.b1 - p.b0, cntp = d.cntp, nr = p.r1 - p.r0;
     unsigned char* seg = pack + (size_t)d.seg * 128;
     T* sv = reinterpret_cast<T*>(seg);
-    for (int k = 0; k < 9; ++k)
-      for (int b = threadIdx.x; b < cntp; b += blockDim.x)
-        sv[k * cntp + b] = b < cnt ? v[(int64_t)k * stride + p.b0 + b] : T(0);
-    int32_t* sc = reinterpret_cast<int32_t*>(seg + pack_col_off<T>(cntp));
+    if (stride > 0) {
+      for (int k = 0; k < NV; ++k)
+        for (int b = threadIdx.x; b < cntp; b += blockDim.x)
+          sv[k * cntp + b] = b < cnt ? v[(int64_t)k * stride + p.b0 + b] : T(0);
+    } else {
+      for (int q = threadIdx.x; q < NV * cntp; q += blockDim.x) {  // read coalesced, write strided
+        const int b = q / NV, k = q - b * NV;
+        sv[k * cntp + b] = b < cnt ? v[((int64_t)p.b0 + b) * NV + k] : T(0);
+      }
+    }
+    int32_t* sc = reinterpret_cast<int32_t*>(seg + pack_col_off<T, NV>(cntp));
     for (int b = threadIdx.x; b < cntp; b += blockDim.x) sc[b] = b < cnt ? ci[p.b0 + b] : 0;
-    uint16_t* sr = reinterpret_cast<uint16_t*>(seg + pack_row_off<T>(cntp));
-    const int slots = (int)(pack_bytes<T>(cntp, nr) - pack_row_off<T>(cntp)) / 2;
+    uint16_t* sr = reinterpret_cast<uint16_t*>(seg + pack_row_off<T, NV>(cntp));
+    const int slots = (int)(pack_bytes<T, NV>(cntp, nr) - pack_row_off<T, NV>(cntp)) / 2;
     for (int i = threadIdx.x; i < slots; i += blockDim.x) sr[i] = (uint16_t)(i <= nr ? rp[p.r0 + i] - p.b0 : 0);
   }
 }
@@ -248,27 +272,33 @@ __device__ __forceinline__ bool wait_warp(uint64_t* bar, uint32_t parity, volati
   }
 }
 
-template <typename T>
-__device__ __forceinline__ T pick3(const T (&a)[3], int l) {
-  return l == 0 ? a[0] : (l == 1 ? a[1] : a[2]);
+template <int N, typename T>
+__device__ __forceinline__ T pick_lane(const T (&a)[N], int l) {
+  T v = a[0];
+#pragma unroll
+  for (int k = 1; k < N; ++k)
+    if (l == k) v = a[k];
+  return v;
 }
 
 // The engine.  Every thread of a CTA of Cfg::kThreads threads calls it once (dynamic shared
-// memory of stream_smem_bytes<T, Cfg>()); the pack was built from a plan with Cfg's
-// capacities.  Per row DOF i = 3 row + c of the CTA's tiles the owning lane calls
-// pre = epi.load(i) before the row product and dot += epi.store(i, pre, (A x)_i) after it,
-// with x_j = xf(j).  Returns the thread's dot sum (0 for the producer warp).
-template <typename T, typename Cfg, typename XF, typename EPI>
+// memory of stream_smem_bytes<T, BR, BC, Cfg>()); the pack was built from a plan with Cfg's
+// capacities.  Per row DOF i = BR row + c of the CTA's tiles the owning lane (c < BR <= G)
+// calls pre = epi.load(i) before the row product and dot += epi.store(i, pre, (A x)_i) after
+// it, with x_j = xf(j) (j = BC col + c).  Returns the thread's dot sum (0 for the producer).
+template <typename T, int BR, int BC, typename Cfg, typename XF, typename EPI>
 __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles, int n_tiles,
                                               const unsigned char* __restrict__ pack, const XF& xf, const EPI& epi,
                                               unsigned char* smem, int* status, int* done) {
+  constexpr int NV = BR * BC;
   constexpr int STAGES = Cfg::kStages;
-  constexpr uint32_t SB = Cfg::template stage_bytes<T>();
+  constexpr uint32_t SB = Cfg::template stage_bytes<T, NV>();
   constexpr int G = Cfg::kG;
   constexpr int U = Cfg::kUnroll;
   constexpr int R = Cfg::kRpg;
   constexpr int GPW = 32 / G;  // row groups per warp
   constexpr int NCW = Cfg::kWarps;
+  static_assert(BR <= G, "a lane per row DOF");
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + STAGES;
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + 256);
@@ -320,7 +350,7 @@ __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles
           ok = false;
         } else {
           descs[s] = d;
-          const uint32_t bytes = pack_bytes<T>(d.w, d.y - d.x);
+          const uint32_t bytes = pack_bytes<T, NV>(d.w, d.y - d.x);
           mbar_arrive_expect_tx(full + s, bytes);
           bulk_load(stages + (size_t)s * SB, pack + (size_t)d.z * 128, bytes, full + s, pol);
         }
@@ -349,15 +379,15 @@ __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles
     const int4 d = descs[s];
     const int r0 = d.x, nr = d.y - d.x, cntp = d.w;
     const T* sv = reinterpret_cast<const T*>(st);
-    const int32_t* scol = reinterpret_cast<const int32_t*>(st + pack_col_off<T>(cntp));
-    const uint16_t* srp = reinterpret_cast<const uint16_t*>(st + pack_row_off<T>(cntp));
+    const int32_t* scol = reinterpret_cast<const int32_t*>(st + pack_col_off<T, NV>(cntp));
+    const uint16_t* srp = reinterpret_cast<const uint16_t*>(st + pack_row_off<T, NV>(cntp));
     // warps take the tile's rows round-robin in passes of GPW * R rows (group g of a pass owns
     // rows base + q GPW + g, q < R), starting from a warp that rotates per tile
     const int wslot = (warp + j) % NCW;
     for (int base = wslot * GPW * R; base < nr; base += NCW * GPW * R) {
       int rs[R], re[R];
       typename EPI::Pre pre[R];
-      T acc[R][3];
+      T acc[R][BR];
       int len = 0;
 #pragma unroll
       for (int q = 0; q < R; ++q) {
@@ -367,15 +397,16 @@ __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles
         re[q] = active ? srp[lr + 1] : 0;
         len = max(len, re[q] - rs[q]);
         pre[q] = typename EPI::Pre{};
-        if (active && gl < 3) pre[q] = epi.load((int64_t)(r0 + lr) * 3 + gl);
-        acc[q][0] = acc[q][1] = acc[q][2] = T(0);
+        if (active && gl < BR) pre[q] = epi.load((int64_t)(r0 + lr) * BR + gl);
+#pragma unroll
+        for (int r = 0; r < BR; ++r) acc[q][r] = T(0);
       }
       // U blocks of each of the R rows in flight per lane: their gathers are issued before the
       // first multiply-add; each row's sum still runs over the lane's blocks in order
       // (b, b + G, b + 2G, ...)
       for (int o = gl; o < len; o += G * U) {
         int col[R][U];
-        T xv[R][U][3];
+        T xv[R][U][BC];
 #pragma unroll
         for (int q = 0; q < R; ++q)
 #pragma unroll
@@ -385,34 +416,31 @@ __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles
 #pragma unroll
           for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) xv[q][u][c] = xf((int64_t)col[q][u] * 3 + c);
+            for (int c = 0; c < BC; ++c) xv[q][u][c] = xf((int64_t)col[q][u] * BC + c);
 #pragma unroll
         for (int q = 0; q < R; ++q)
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             const int b = rs[q] + o + u * G;
             if (b < re[q]) {
-              T v[9];
 #pragma unroll
-              for (int k = 0; k < 9; ++k) v[k] = sv[k * cntp + b];
+              for (int r = 0; r < BR; ++r)
 #pragma unroll
-              for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) acc[q][r] = fma(v[r * 3 + c], xv[q][u][c], acc[q][r]);
+                for (int c = 0; c < BC; ++c) acc[q][r] = fma(sv[(r * BC + c) * cntp + b], xv[q][u][c], acc[q][r]);
             }
           }
       }
 #pragma unroll
       for (int q = 0; q < R; ++q) {
 #pragma unroll
-        for (int r = 0; r < 3; ++r) {
+        for (int r = 0; r < BR; ++r) {
           T v = acc[q][r];
 #pragma unroll
           for (int o2 = G / 2; o2 > 0; o2 >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o2);
           acc[q][r] = v;
         }
         const int lr = base + q * GPW + grp;
-        if (lr < nr && gl < 3) dot += epi.store((int64_t)(r0 + lr) * 3 + gl, pre[q], pick3(acc[q], gl));
+        if (lr < nr && gl < BR) dot += epi.store((int64_t)(r0 + lr) * BR + gl, pre[q], pick_lane<BR>(acc[q], gl));
       }
     }
     __syncwarp();

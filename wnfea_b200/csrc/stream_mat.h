@@ -1,0 +1,34 @@
+// A block-sparse matrix prepared for the streamed kernels (stream.cuh): its tile plan, the
+// segment descriptors of its FP32 and FP64 tile-major packs, and the packs themselves.  The
+// plan depends on the pattern only (made once); the packs are refreshed whenever the values
+// change.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_array.h"
+#include "stream.cuh"
+
+namespace wn {
+
+struct StreamMat {
+  int br = 0, bc = 0;
+  int n_tiles = 0;  // 0: not streamed (a row exceeds the tile capacity, or no plan made)
+  DArray<StreamTile> plan;
+  DArray<PackTile> d32, d64;
+  DArray<unsigned char> p32, p64;
+  int64_t size32 = 0, size64 = 0;
+  bool packed = false;  // the packs hold the current values
+  // Tile plan and descriptors of a br x bc matrix from its host row pointer (shapes 3x3, 6x6,
+  // 3x6, 6x3; others are left unstreamed).  Packs are allocated by pack().
+  int make_plan(const int32_t* h_rp, int64_t n_rows, int br, int bc);
+  // Pack the device values (component-major with the given stride, or block-contiguous when
+  // stride == 0) into both packs; a no-op without a plan.
+  int pack(const int32_t* rp, const int32_t* ci, const float* v32, const double* v64, int64_t stride,
+           cudaStream_t st);
+  // drop the plan and packs (the matrix is then run by the register kernels)
+  void clear();
+};
+
+}  // namespace wn
