@@ -628,9 +628,12 @@ struct EpiCheb {
   const T* __restrict__ b;
   int want_dot;
   struct Pre {
-    T di, dd, ri, xi;
+    T di, dd, ri, xi, bi;
   };
-  __device__ __forceinline__ Pre load(int64_t i) const { return {dinv[i], d_in[i], r[i], x[i]}; }
+  // b_i (for the dot) is loaded with the other operands, before the row product
+  __device__ __forceinline__ Pre load(int64_t i) const {
+    return {dinv[i], d_in[i], r[i], x[i], want_dot ? b[i] : T(0)};
+  }
   __device__ __forceinline__ double store(int64_t i, const Pre& p, T t) const {
     const T ri = p.ri - p.di * t;
     const T dn = c1 * p.dd + c2 * ri;
@@ -638,7 +641,7 @@ struct EpiCheb {
     r[i] = ri;
     d_out[i] = dn;
     x[i] = xn;
-    return want_dot ? (double)b[i] * (double)xn : 0.0;
+    return want_dot ? (double)p.bi * (double)xn : 0.0;
   }
 };
 

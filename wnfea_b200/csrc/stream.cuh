@@ -96,7 +96,8 @@ struct StreamCfg {
 // 17,125 tiles: FP32 SpMV 64 us with 8 consumer warps, 3 stages of 20.7 KB and 3 CTAs per SM,
 // against 72-90 us for 12-16 warps at 2 CTAs or 4-8 stages at 1 CTA; FP64 104 us with 2 stages
 // of 39 KB and 2 CTAs per SM).  6x6 (AMG level 1, rows of ~54 blocks) and 6x3 (restriction,
-// rows of ~105 blocks): a warp per row; 3x6 (prolongation, rows of ~5.5 blocks): 8 lanes per row.
+// rows of ~105 blocks): a warp per row; 3x6 (prolongation, rows of ~5.5 blocks): 4 lanes per
+// row, two blocks in flight per lane.
 constexpr int kStreamThreads = 9 * 32;
 template <typename T, int BR, int BC>
 struct StreamDefault;
@@ -122,7 +123,7 @@ struct StreamDefault<T, 6, 3> {
 };
 template <typename T>
 struct StreamDefault<T, 3, 6> {
-  using type = StreamCfg<512, kStreamRowCap, 8, 8, 2, 1>;
+  using type = StreamCfg<512, kStreamRowCap, 8, 4, 2, 2>;
   static constexpr int kCtasPerSm = sizeof(T) == 4 ? 2 : 1;
 };
 
