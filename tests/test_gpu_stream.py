@@ -117,3 +117,25 @@ def test_streamed_solve_modes_agree():
     np.testing.assert_allclose(u32, u64, rtol=0, atol=1e-8 * np.abs(u64).max())
     u64b, _ = s.solve(F, rtol=1e-10, precision=0)
     assert np.array_equal(u64, u64b)  # deterministic dots and products
+
+
+def test_streamed_spmv_unaligned_vectors():
+    """x and y one element past an aligned address: the paired gathers of a 3-DOF block fall
+    back to scalar loads and the product is unchanged."""
+    import torch
+
+    m = _trimmed_block(2)
+    s = SolidSystem(m.mesh_nodes, m.solid_elements)
+    s.assemble(solid_element_props(m), apply_bcs=False)
+    n = 3 * s.n_nodes
+    x = np.random.default_rng(3).standard_normal(n)
+    for dt, prec in ((torch.float64, 0), (torch.float32, 1)):
+        base = torch.zeros(n + 1, dtype=dt, device="cuda")
+        base[1:] = torch.from_numpy(x).to(dt)
+        xa = base[1:].clone()
+        ya, yu = torch.empty_like(xa), torch.zeros(n + 1, dtype=dt, device="cuda")
+        _lib.call("wn_spmv_solid_device", s.handle, prec, xa.data_ptr(), ya.data_ptr(), 0)
+        _lib.call("wn_spmv_solid_device", s.handle, prec, base[1:].data_ptr(), yu[1:].data_ptr(), 0)
+        torch.cuda.synchronize()
+        assert torch.equal(ya, yu[1:])
+    assert _status(s) == 0
