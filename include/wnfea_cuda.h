@@ -124,6 +124,9 @@ typedef struct wn_amg_params {
   double prolong_omega;    /* P = (I - prolong_omega / rho * D^-1 A) P_tent             (4/3)  */
   int smooth_prolongator;  /* 1 = smoothed aggregation, 0 = plain (tentative) aggregation      */
   int power_iters;         /* power iterations for rho(D^-1 A)                          (15)   */
+  double stream_min_mb;    /* level matrices / transfer operators of at least this many MB
+                              in FP32 are streamed from tile-major packs, smaller ones stay
+                              L2-resident on the register row kernels; < 0: none     (4)    */
 } wn_amg_params;
 
 /* Defaults above. */

@@ -139,3 +139,27 @@ def test_streamed_spmv_unaligned_vectors():
         torch.cuda.synchronize()
         assert torch.equal(ya, yu[1:])
     assert _status(s) == 0
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_streamed_coarse_levels_match_register_kernels(precision):
+    """Every AMG level matrix and transfer operator streamed from its pack (stream_min_mb = 0)
+    against none streamed (stream_min_mb = -1): same iterations, same solution to rounding (the
+    6x6 level products sum in the register kernels' order; the 3x6 prolongation uses 4 lanes
+    per row instead of 8, which reorders its sums)."""
+    from wnfea_b200.amg import AMGParams
+    from wnfea_b200.model import solid_fixed_dofs, solid_load_vector
+
+    m, _ = generate_c3d10_ibeam_structured(n_slices=24, length=0.3, seed=5)
+    s = SolidSystem(m.mesh_nodes, m.solid_elements)
+    s.set_fixed(solid_fixed_dofs(m))
+    s.assemble(solid_element_props(m), apply_bcs=True)
+    F = solid_load_vector(m)
+    out = []
+    for mb in (-1.0, 0.0):
+        s.amg_setup(AMGParams(stream_min_mb=mb))
+        u, st = s.solve(F, rtol=1e-9, precision=precision)
+        assert st["status"] == 0 and st["rel_res"] <= 1e-9
+        out.append((u, st["iterations"]))
+    assert out[0][1] == out[1][1]
+    np.testing.assert_allclose(out[1][0], out[0][0], rtol=0, atol=1e-9 * np.abs(out[0][0]).max())

@@ -34,6 +34,7 @@ class AmgParams(C.Structure):
         ("prolong_omega", C.c_double),
         ("smooth_prolongator", C.c_int),
         ("power_iters", C.c_int),
+        ("stream_min_mb", C.c_double),
     ]
 
 

@@ -31,6 +31,7 @@ class AMGParams:
     prolong_omega: float = 4.0 / 3.0
     smooth_prolongator: int = 1
     power_iters: int = 15
+    stream_min_mb: float = 4.0
 
     def to_c(self) -> _lib.AmgParams:
         return _lib.AmgParams(**{f.name: getattr(self, f.name) for f in fields(self)})

@@ -38,10 +38,6 @@ struct LevelVecs {
   }
 };
 
-// level matrices at least this large (FP32 bytes) are streamed from tile-major packs; smaller
-// ones stay resident in L2 between passes and keep the register row kernels
-constexpr int64_t kStreamMinBytes = 32ll << 20;
-
 struct DevLevel {
   int bs = 3;
   int64_t n_nodes = 0;
@@ -57,8 +53,8 @@ struct DevLevel {
   double inv_theta = 0.0;
   std::vector<double> c1, c2;  // Chebyshev step coefficients k = 1..deg-1
   DevBsr P, R;
-  // the same matrices prepared for the streamed kernels (level matrices of at least
-  // kStreamMinBytes in FP32; n_tiles == 0 otherwise)
+  // the same matrices prepared for the streamed kernels (those of at least
+  // wn_amg_params.stream_min_mb in FP32; n_tiles == 0 otherwise)
   StreamMat As, Ps, Rs;
   LevelVecs<double> v64;
   LevelVecs<float> v32;

@@ -42,6 +42,7 @@ wn_amg_params amg_default_params() {
   p.prolong_omega = 4.0 / 3.0;
   p.smooth_prolongator = 1;
   p.power_iters = 15;
+  p.stream_min_mb = 4.0;
   return p;
 }
 

@@ -1195,9 +1195,13 @@ int solver_setup(Solid* s, const wn_amg_params& prm) {
     cheb_coefficients(prm, L);
     WN_CHECK(L.P.upload(h.P));
     WN_CHECK(L.R.upload(h.R));
-    // matrices too large to stay in L2 between passes are streamed from tile-major packs
+    // matrices of at least stream_min_mb MB (FP32) are streamed from tile-major packs (on the
+    // 1M-DOF I-beam: level 1 and the transfers of levels 0-1, 24-142 MB; streaming level 2 and
+    // the level-1 transfers too, at 4 MB rather than 32 MB, took 0.8 ms off a 47 ms solve)
     auto stream_if_large = [&](StreamMat& m, const HostBsr& hb, const DevBsr& db) -> int {
-      if (hb.nnzb() * hb.br * hb.bc * (int64_t)sizeof(float) < kStreamMinBytes) return 0;
+      if (prm.stream_min_mb < 0.0 ||
+          (double)(hb.nnzb() * hb.br * hb.bc * (int64_t)sizeof(float)) < prm.stream_min_mb * 1048576.0)
+        return 0;
       WN_CHECK(m.make_plan(hb.rp.data(), hb.n_rows, hb.br, hb.bc));
       return m.pack(db.rp.p, db.ci.p, db.v32.p, db.v64.p, 0, 0);
     };
