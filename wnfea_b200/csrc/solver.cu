@@ -127,6 +127,7 @@ __global__ void __launch_bounds__(kThreads, (BS == 3) ? kMinBlocks : 1) k_pre_fi
                                                         T inv_theta, int deg, T c1, T c2, T* __restrict__ x,
                                                         T* __restrict__ r, T* __restrict__ d, T* __restrict__ res,
                                                         const PcgScalars* __restrict__ S) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   if (S->done) return;
   GROUP_ROW_LOOP(n_rows, GroupOf<BS>::value) {
     const bool active = row < n_rows;
@@ -161,6 +162,7 @@ __global__ void __launch_bounds__(kThreads, (BS == 3) ? kMinBlocks : 1) k_cheb_s
                                                         T* __restrict__ d_out, T* __restrict__ r, T* __restrict__ x,
                                                         T c1, T c2, const T* __restrict__ b, double* __restrict__ part,
                                                         const PcgScalars* __restrict__ S) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   __shared__ double sh[kThreads / 32];
   if (S->done) return;
   double dot = 0.0;
@@ -189,6 +191,7 @@ __global__ void __launch_bounds__(kThreads, (BS == 3) ? kMinBlocks : 1) k_residu
                                                        const int32_t* __restrict__ ci, const T* __restrict__ av, int64_t stride,
                                                        const T* __restrict__ b, const T* __restrict__ x,
                                                        T* __restrict__ res, const PcgScalars* __restrict__ S) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   if (S->done) return;
   GROUP_ROW_LOOP(n_rows, GroupOf<BS>::value) {
     const bool active = row < n_rows;
@@ -210,6 +213,7 @@ __global__ void __launch_bounds__(kThreads) k_level_spmv(int64_t n_rows, const i
                                                          const int32_t* __restrict__ ci, const T* __restrict__ av,
                                                          const T* __restrict__ x, T* __restrict__ y, int accumulate,
                                                          const PcgScalars* __restrict__ S) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   if (S->done) return;
   constexpr int RPW = 32 / G;
   const int lane = threadIdx.x & 31;
@@ -258,6 +262,7 @@ __global__ void __launch_bounds__(kThreads, (BS == 3) ? kMinBlocks : 1) k_post_f
                                                          T inv_theta, const T* __restrict__ x, T* __restrict__ x2,
                                                          T* __restrict__ r, T* __restrict__ d, double* __restrict__ part,
                                                          const PcgScalars* __restrict__ S) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   __shared__ double sh[kThreads / 32];
   if (S->done) return;
   double dot = 0.0;
@@ -285,6 +290,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) k_coarse(int64_t n, const double* __restrict__ inv,
                                                      const T* __restrict__ b, T* __restrict__ x,
                                                      const PcgScalars* __restrict__ S) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   if (S->done) return;
   WARP_ROW_LOOP(n) {
     double s = 0.0;
@@ -304,6 +310,7 @@ template <typename TK, typename TM>
 __global__ void __launch_bounds__(kThreads) k_init_vecs(int64_t n, const TK* __restrict__ b, TK* __restrict__ x,
                                                         TK* __restrict__ r, TM* __restrict__ rm,
                                                         double* __restrict__ partC) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   __shared__ double sh[kThreads / 32];
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -318,6 +325,7 @@ __global__ void __launch_bounds__(kThreads) k_init_vecs(int64_t n, const TK* __r
 
 __global__ void k_init_scalars(PcgScalars* S, const double* __restrict__ partC, int nparts, double rtol,
                                int max_iter) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   __shared__ double sh[kThreads / 32];
   const double bb = reduce_parts(partC, nparts, sh);
   if (threadIdx.x == 0) {
@@ -339,6 +347,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) k_prec_vec(int64_t n, const T* __restrict__ r, const T* __restrict__ dinv,
                                                        int jacobi, T* __restrict__ z, double* __restrict__ partA,
                                                        const PcgScalars* __restrict__ S) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   __shared__ double sh[kThreads / 32];
   if (S->done) return;
   double s = 0.0;
@@ -371,6 +380,7 @@ __global__ void __launch_bounds__(kThreads, (BS == 3) ? (sizeof(TK) == 4 ? kMinB
                                                        TK* __restrict__ p_new, TK* __restrict__ q,
                                                        const double* __restrict__ partA, double* __restrict__ partB,
                                                        int nparts, int first, int par, PcgScalars* __restrict__ S) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   __shared__ double sh[kThreads / 32];
   if (S->done) return;
   const double rz = reduce_parts(partA, nparts, sh);
@@ -403,6 +413,7 @@ __global__ void __launch_bounds__(kThreads) k_update(int64_t n, TK* __restrict__
                                                      const TK* __restrict__ q, const double* __restrict__ partB,
                                                      double* __restrict__ partC, int nparts, int par,
                                                      PcgScalars* __restrict__ S) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   __shared__ double sh[kThreads / 32];
   if (S->done) return;
   const double gamma = reduce_parts(partB, nparts, sh);
@@ -430,6 +441,7 @@ __global__ void __launch_bounds__(kThreads) k_update(int64_t n, TK* __restrict__
 // convergence test after an iteration (one CTA); the iteration count lives on the device so
 // that a captured chunk of iterations can be replayed any number of times
 __global__ void k_check(PcgScalars* S, const double* __restrict__ partC, int nparts) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   __shared__ double sh[kThreads / 32];
   if (S->done) return;
   const double rr = reduce_parts(partC, nparts, sh);
@@ -451,6 +463,7 @@ __global__ void k_check(PcgScalars* S, const double* __restrict__ partC, int npa
 
 // S->rr = sum(partC) (one CTA)
 __global__ void k_reduce_rr(PcgScalars* S, const double* __restrict__ partC, int nparts) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   __shared__ double sh[kThreads / 32];
   const double rr = reduce_parts(partC, nparts, sh);
   if (threadIdx.x == 0) S->rr = rr;
@@ -460,6 +473,7 @@ __global__ void k_reduce_rr(PcgScalars* S, const double* __restrict__ partC, int
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_dot_pair(int64_t n, const T* __restrict__ a, const T* __restrict__ b,
                                                        double* __restrict__ part, const PcgScalars* __restrict__ S) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   __shared__ double sh[kThreads / 32];
   if (S->done) return;
   double s = 0.0;
@@ -471,6 +485,7 @@ __global__ void __launch_bounds__(kThreads) k_dot_pair(int64_t n, const T* __res
 // partials of x . x
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_dot_self(int64_t n, const T* __restrict__ x, double* __restrict__ part) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   __shared__ double sh[kThreads / 32];
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -495,6 +510,7 @@ __global__ void __launch_bounds__(kThreads) k_outer_residual_dd(int64_t n_rows, 
                                                                 const double* __restrict__ ulo,
                                                                 double* __restrict__ r64, float* __restrict__ r32,
                                                                 double* __restrict__ partC) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   constexpr int G = GroupOf<BS>::value;
   __shared__ double sh[kThreads / 32];
   double rr = 0.0;
@@ -555,6 +571,7 @@ __global__ void __launch_bounds__(kThreads) k_outer_residual_dd(int64_t n_rows, 
 // (u, ulo) += dx as a double-double pair, renormalised so that u = fl(u + ulo)
 template <typename T>
 __global__ void k_accumulate(int64_t n, double* __restrict__ u, double* __restrict__ ulo, const T* __restrict__ dx) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double s, e, h, g;
     two_sum(u[i], (double)dx[i], s, e);
@@ -568,6 +585,7 @@ __global__ void k_accumulate(int64_t n, double* __restrict__ u, double* __restri
 __global__ void k_fill_dinv(int64_t n_rows, int bs, int64_t nnzb, const int32_t* __restrict__ diag_block,
                             const double* __restrict__ k64,
                             double* __restrict__ d64, float* __restrict__ d32) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_rows * bs;
        t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t row = t / bs;
@@ -731,16 +749,61 @@ static StreamView stream_view(const StreamMat& m) {
     return {m.d64.p, m.n_tiles, m.p64.p};
 }
 
+// Launched with programmatic stream serialisation (launch_pdl): the first tiles of the matrix
+// are in flight before the predecessor has finished.
 template <typename T, int BR, int BC, typename XF, typename EPI>
 __global__ void __launch_bounds__(kStreamThreads, (StreamDefault<T, BR, BC>::kCtasPerSm))
     k_stream_rows(StreamView m, XF xf, EPI epi, double* __restrict__ part, PcgScalars* __restrict__ S) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ double sh[kStreamThreads / 32];
-  if (S->done) return;
+  pdl_trigger();
+  bool skipped = false;
   const double dot = stream_rows<T, BR, BC, typename StreamDefault<T, BR, BC>::type>(
-      m.tiles, m.n_tiles, m.pack, xf, epi, smem, &S->status, &S->done);
-  if (part) write_part(dot, part, sh);
+      m.tiles, m.n_tiles, m.pack, xf, epi, smem, &S->status, &S->done, &skipped);
+  if (part && !skipped) write_part(dot, part, sh);
 }
+
+// p_new = z + beta p_old with beta read from shared memory (set after the programmatic wait)
+template <typename TK, typename TM>
+struct XPNewS {
+  const TM* __restrict__ z;
+  const TK* __restrict__ p;
+  const double* beta;
+  __device__ __forceinline__ TK operator()(int64_t j) const { return (TK)z[j] + (TK)*beta * p[j]; }
+};
+template <typename TK, typename TM>
+struct EpiSpmvDotS {
+  const TM* __restrict__ z;
+  const TK* __restrict__ p_old;
+  const double* beta;
+  TK* __restrict__ p_new;
+  TK* __restrict__ q;
+  struct Pre {
+    TK pi;
+  };
+  __device__ __forceinline__ Pre load(int64_t i) const { return {(TK)z[i] + (TK)*beta * p_old[i]}; }
+  __device__ __forceinline__ double store(int64_t i, const Pre& p, TK t) const {
+    p_new[i] = p.pi;
+    q[i] = t;
+    return (double)p.pi * (double)t;
+  }
+};
+// rz = sum(partA) and beta = rz / rz_prev (0 on the first iteration), into shared memory
+struct BetaHook {
+  const double* partA;
+  int nparts, first, par;
+  const PcgScalars* S;
+  double* sh;
+  double* rz_beta;  // shared: [0] rz, [1] beta
+  __device__ __forceinline__ void operator()() const {
+    const double rz = reduce_parts(partA, nparts, sh);
+    if (threadIdx.x == 0) {
+      rz_beta[0] = rz;
+      rz_beta[1] = first ? 0.0 : rz / S->rz[par ^ 1];
+    }
+    __syncthreads();
+  }
+};
 
 // k_spmv_dot with the matrix streamed: beta from the partials of r . z, p_new = z + beta p_old,
 // q = A p_new, partials of p_new . q
@@ -751,15 +814,35 @@ __global__ void __launch_bounds__(kStreamThreads, (StreamDefault<TK, BS, BS>::kC
                       int first, int par, PcgScalars* __restrict__ S) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ double sh[kStreamThreads / 32];
-  if (S->done) return;
-  const double rz = reduce_parts(partA, nparts, sh);
-  const double rz_prev = S->rz[par ^ 1];
-  const TK beta = first ? TK(0) : (TK)(rz / rz_prev);
+  __shared__ double rz_beta[2];
+  pdl_trigger();
+  bool skipped = false;
   const double dot = stream_rows<TK, BS, BS, typename StreamDefault<TK, BS, BS>::type>(
-      m.tiles, m.n_tiles, m.pack, XPNew2<TK, TM>{z, p_old, beta}, EpiSpmvDot<TK, TM>{z, p_old, beta, p_new, q}, smem,
-      &S->status, &S->done);
+      m.tiles, m.n_tiles, m.pack, XPNewS<TK, TM>{z, p_old, rz_beta + 1},
+      EpiSpmvDotS<TK, TM>{z, p_old, rz_beta + 1, p_new, q}, smem, &S->status, &S->done, &skipped,
+      BetaHook{partA, nparts, first, par, S, sh, rz_beta});
+  if (skipped) return;
   write_part(dot, partB, sh);
-  if (blockIdx.x == 0 && threadIdx.x == 0) S->rz[par] = rz;
+  if (blockIdx.x == 0 && threadIdx.x == 0) S->rz[par] = rz_beta[0];
+}
+
+// launch with programmatic stream serialisation: the kernel may begin (and start streaming its
+// matrix) while its predecessor on the stream finishes; it waits (griddepcontrol) before
+// reading anything the predecessor wrote
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_pdl(void (*kern)(KArgs...), int grid, int threads, size_t smem, cudaStream_t st,
+                              Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
 // grid of a streamed kernel (one persistent wave), 0 if it cannot run on this device
@@ -780,7 +863,11 @@ static bool launch_stream_rows(const StreamMat& m, XF xf, EPI epi, double* part,
   auto kern = k_stream_rows<T, BR, BC, XF, EPI>;
   const int g = stream_grid<T, BR, BC>(kern, m.n_tiles);
   if (g == 0) return false;
-  kern<<<g, kStreamThreads, stream_smem_bytes<T, BR, BC>(), st>>>(stream_view<T>(m), xf, epi, part, S);
+  if (launch_pdl(kern, g, kStreamThreads, stream_smem_bytes<T, BR, BC>(), st, stream_view<T>(m), xf, epi, part, S) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
   if (grid_out) *grid_out = g;
   return true;
 }
@@ -1017,9 +1104,12 @@ static int pcg_iteration(Solid* s, SolverWork& W, int precond, int k, PcgScalars
       auto kern = k_stream_spmv_dot<BS, TK, TM>;
       const int g = stream_grid<TK, BS, BS>(kern, s->fine.n_tiles);
       if (g > 0) {
-        kern<<<g, kStreamThreads, stream_smem_bytes<TK, BS, BS>(), st>>>(
-            stream_view<TK>(s->fine), B.z, p_old, p_new, B.q, W.partA.p, W.partB.p, W.npA, k == 0, par, S);
-        return g;
+        const cudaError_t e =
+            launch_pdl(kern, g, kStreamThreads, stream_smem_bytes<TK, BS, BS>(), st, stream_view<TK>(s->fine),
+                       (const TM*)B.z, (const TK*)p_old, p_new, B.q, (const double*)W.partA.p, W.partB.p, W.npA,
+                       (int)(k == 0), par, S);
+        if (e == cudaSuccess) return g;
+        cudaGetLastError();
       }
     }
     const int g = resident_grid(k_spmv_dot<BS, TK, TM>, kThreads, (s->n_nodes * 32 + kThreads - 1) / kThreads);

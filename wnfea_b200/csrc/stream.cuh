@@ -52,7 +52,7 @@ constexpr int kStreamCap = WN_STREAM_TILE_BLOCKS;   // blocks per tile at most (
 constexpr int kStreamRowCap = WN_STREAM_TILE_ROWS;  // rows per tile at most
 static_assert(kStreamCap % 4 == 0, "tile capacity: a multiple of 4 blocks");
 // shared memory ahead of the stage buffers: full / empty mbarriers (<= 8 stages), the abort
-// flag at byte 256, the stage descriptors at byte 384
+// flag at byte 256 and the skip flag at 260, the stage descriptors at byte 384
 constexpr int kStreamHeader = 512;
 
 // Byte layout of a packed tile segment of NV = BR * BC values per block (also its stage buffer
@@ -273,6 +273,18 @@ __device__ __forceinline__ bool wait_warp(uint64_t* bar, uint32_t parity, volati
   }
 }
 
+// Programmatic dependent launch (griddepcontrol): a kernel launched with programmatic stream
+// serialisation may start while its predecessor is still running; pdl_wait() blocks until the
+// predecessor has completed and its memory is visible (an immediate return for an ordinary
+// launch); pdl_trigger() lets this kernel's dependents be scheduled.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// called by every thread of the CTA once the predecessor's results are visible
+struct NoHook {
+  __device__ __forceinline__ void operator()() const {}
+};
+
 template <int N, typename T>
 __device__ __forceinline__ T pick_lane(const T (&a)[N], int l) {
   T v = a[0];
@@ -287,10 +299,15 @@ __device__ __forceinline__ T pick_lane(const T (&a)[N], int l) {
 // capacities.  Per row DOF i = BR row + c of the CTA's tiles the owning lane (c < BR <= G)
 // calls pre = epi.load(i) before the row product and dot += epi.store(i, pre, (A x)_i) after
 // it, with x_j = xf(j) (j = BC col + c).  Returns the thread's dot sum (0 for the producer).
-template <typename T, int BR, int BC, typename Cfg, typename XF, typename EPI>
+// The first stages' copies (the matrix only) are issued before pdl_wait(), so under a
+// programmatic dependent launch they overlap the predecessor's tail; then every thread runs
+// hook(), and when *done is set (read after the wait) the CTA lets those copies land and
+// returns with *skipped = true.
+template <typename T, int BR, int BC, typename Cfg, typename XF, typename EPI, typename HOOK = NoHook>
 __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles, int n_tiles,
                                               const unsigned char* __restrict__ pack, const XF& xf, const EPI& epi,
-                                              unsigned char* smem, int* status, int* done) {
+                                              unsigned char* smem, int* status, int* done, bool* skipped = nullptr,
+                                              const HOOK& hook = HOOK{}) {
   constexpr int NV = BR * BC;
   constexpr int STAGES = Cfg::kStages;
   constexpr uint32_t SB = Cfg::template stage_bytes<T, NV>();
@@ -303,6 +320,7 @@ __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + STAGES;
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + 256);
+  volatile int* skip_flag = reinterpret_cast<volatile int*>(smem + 260);
   int4* descs = reinterpret_cast<int4*>(smem + 384);
   unsigned char* stages = smem + kStreamHeader;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -325,16 +343,19 @@ __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles
     if (done) *(volatile int*)done = 1;
   };
 
-  if (warp == NCW) {  // producer warp: lane 0 issues, the warp holds the tile descriptors
-    const uint64_t pol = l2_evict_first_policy();
-    auto load_chunk = [&](int c) {  // descriptors of tiles tb + 32 c + lane
-      const int t = tb + 32 * c + lane;
-      return t < te ? *reinterpret_cast<const int4*>(tiles + t) : make_int4(0, 0, 0, 0);
-    };
-    int4 cur = load_chunk(0), nxt = load_chunk(1);
-    int j = 0;  // tiles issued
-    bool ok = true;
-    for (int t = tb; t < te; ++t, ++j) {
+  // producer warp: lane 0 issues, the warp holds the tile descriptors of tiles tb + 32 c + lane
+  // in chunks (the next chunk loaded while the current one is issued)
+  const int n_my = te - tb;
+  uint64_t pol = 0;
+  int4 cur = make_int4(0, 0, 0, 0), nxt = make_int4(0, 0, 0, 0);
+  int j = 0;  // tiles issued
+  bool ok = true;
+  auto load_chunk = [&](int c) {
+    const int t = tb + 32 * c + lane;
+    return t < te ? *reinterpret_cast<const int4*>(tiles + t) : make_int4(0, 0, 0, 0);
+  };
+  auto issue = [&](int j_end) {  // the whole producer warp: issue tiles j .. j_end - 1
+    for (; j < j_end; ++j) {
       const int q = j & 31;
       int4 d;
       d.x = __shfl_sync(0xffffffffu, cur.x, q);
@@ -358,6 +379,28 @@ __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles
       }
       if (!__shfl_sync(0xffffffffu, ok, 0)) break;
     }
+  };
+  const int pre = n_my < STAGES ? n_my : STAGES;
+  if (warp == NCW) {
+    pol = l2_evict_first_policy();
+    cur = load_chunk(0);
+    nxt = load_chunk(1);
+    issue(pre);  // free stages: no waits
+  }
+  pdl_wait();
+  if (threadIdx.x == 0) *skip_flag = (done && *(volatile int*)done) ? 1 : 0;
+  __syncthreads();
+  hook();
+  const bool skip = *skip_flag != 0;
+  if (skipped) *skipped = skip;
+  if (skip) {  // let the copies already issued land before the CTA can exit
+    if (warp == NCW && lane == 0)
+      for (int s = 0; s < pre; ++s) wait_thread(full + s, 0u, nullptr);
+    return 0.0;
+  }
+
+  if (warp == NCW) {
+    issue(n_my);
     if (lane == 0 && !ok) {
       fail();
       // let the copies already issued land before the CTA can exit
@@ -369,8 +412,7 @@ __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles
 
   // consumer warps
   const int gl = lane % G, grp = lane / G;
-  int j = 0;
-  for (int t = tb; t < te; ++t, ++j) {
+  for (j = 0; j < n_my; ++j) {
     const int s = j % STAGES;
     if (!wait_warp(full + s, (uint32_t)((j / STAGES) & 1), abort_flag)) {
       if (lane == 0) fail();
