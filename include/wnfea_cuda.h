@@ -117,7 +117,7 @@ int wn_stream_tiles_host(int64_t n_rows, const int32_t* row_ptr, int32_t* tiles,
 typedef struct wn_amg_params {
   double strength_theta;   /* strong if |A_ij|_F >= theta sqrt(|A_ii|_F |A_jj|_F)      (0.08) */
   int max_levels;          /* including the coarsest                                   (10)   */
-  int coarse_size;         /* stop coarsening at <= this many scalar DOFs               (1000) */
+  int coarse_size;         /* stop coarsening at <= this many scalar DOFs               (1500) */
   int smoother_degree;     /* Chebyshev degree per pre-/post-smoothing                  (2)    */
   double cheb_lower;       /* lambda_min = cheb_lower * lambda_max                      (1/30) */
   double cheb_safety;      /* lambda_max = cheb_safety * rho(D^-1 A) estimate          (1.1)  */

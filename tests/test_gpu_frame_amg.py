@@ -8,6 +8,7 @@ import pytest
 from scipy.sparse.linalg import spsolve
 
 from wnfea_b200 import _lib
+from wnfea_b200.amg import AMGParams
 from wnfea_b200.beam import frame_linear_system, solve_frame_linear
 from wnfea_b200.frames import generate_frame_grid, generate_space_frame
 
@@ -20,7 +21,8 @@ def test_space_frame_matches_direct_solve(precision, rtol, tol):
     frame, system, F = frame_linear_system(m)
     K = frame.tangent_bsr().tocsr()
     assert abs(K - K.T).max() <= 1e-9 * abs(K).max()  # the stiffness at U = 0 is symmetric
-    system.amg_setup()
+    # 1,260 DOFs: a coarse size below the default keeps a multi-level hierarchy in the test
+    system.amg_setup(AMGParams(coarse_size=300))
     U, st = system.solve(F, rtol=rtol, precision=precision)
     assert st["status"] == 0 and st["rel_res"] <= rtol and st["n_levels"] >= 2
     Ur = spsolve(K.tocsc(), F)

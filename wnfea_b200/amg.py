@@ -24,7 +24,7 @@ from ._lib import call, ptr
 class AMGParams:
     strength_theta: float = 0.08
     max_levels: int = 10
-    coarse_size: int = 1000
+    coarse_size: int = 1500
     smoother_degree: int = 2
     cheb_lower: float = 1.0 / 30.0
     cheb_safety: float = 1.1

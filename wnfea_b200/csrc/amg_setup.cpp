@@ -35,7 +35,7 @@ wn_amg_params amg_default_params() {
   wn_amg_params p;
   p.strength_theta = 0.08;
   p.max_levels = 10;
-  p.coarse_size = 1000;
+  p.coarse_size = 1500;
   p.smoother_degree = 2;
   p.cheb_lower = 1.0 / 30.0;
   p.cheb_safety = 1.1;
@@ -71,6 +71,38 @@ void par_rows(int64_t n, const std::function<void(int64_t, int64_t, int)>& fn) {
     if (a >= b) break;
     th.emplace_back(fn, a, b, t);
   }
+  for (auto& x : th) x.join();
+}
+
+// sum_k a[k] b[k] over n terms in a fixed order (four interleaved partial sums, then
+// ((s0 + s1) + (s2 + s3)) + tail): vectorisable, and the same result for any thread count
+inline double dot_fixed(const double* a, const double* b, int64_t n) {
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  int64_t k = 0;
+  for (; k + 4 <= n; k += 4) {
+    s0 += a[k] * b[k];
+    s1 += a[k + 1] * b[k + 1];
+    s2 += a[k + 2] * b[k + 2];
+    s3 += a[k + 3] * b[k + 3];
+  }
+  double s = (s0 + s1) + (s2 + s3);
+  for (; k < n; ++k) s += a[k] * b[k];
+  return s;
+}
+
+// fn(i) for i < n on the host threads, thread t taking i = t, t + nth, ... (for work that
+// shrinks or grows with i)
+void par_interleaved(int64_t n, const std::function<void(int64_t)>& fn) {
+  const int nth = host_threads();
+  if (nth <= 1 || n < 64) {
+    for (int64_t i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int t = 0; t < nth && t < n; ++t)
+    th.emplace_back([&, t]() {
+      for (int64_t i = t; i < n; i += nth) fn(i);
+    });
   for (auto& x : th) x.join();
 }
 
@@ -535,44 +567,44 @@ int amg_build(const wn_amg_params& prm, int64_t n0, int bs0, const int32_t* rp0,
     for (int64_t j = 0; j < nc && !any; ++j) any = D[(size_t)i * nc + j] != 0.0;
     if (!any) D[(size_t)i * nc + i] = 1.0;
   }
+  // Cholesky A = L L^T (left-looking; row-major L, the dot products run over contiguous rows)
   std::vector<double> Lf(D);
   for (int64_t j = 0; j < nc; ++j) {
-    double s = Lf[(size_t)j * nc + j];
-    for (int64_t k = 0; k < j; ++k) s -= Lf[(size_t)j * nc + k] * Lf[(size_t)j * nc + k];
+    const double* lj = &Lf[(size_t)j * nc];
+    const double s = Lf[(size_t)j * nc + j] - dot_fixed(lj, lj, j);
     WN_REQUIRE(s > 0.0 && std::isfinite(s), WN_ENOTSPD, "amg_build: coarsest matrix not SPD (pivot %lld)",
                (long long)j);
     const double ljj = std::sqrt(s);
     Lf[(size_t)j * nc + j] = ljj;
-    par_rows(nc - j - 1, [&](int64_t a, int64_t b, int) {
-      for (int64_t t = a; t < b; ++t) {
-        const int64_t i = j + 1 + t;
-        double v = Lf[(size_t)i * nc + j];
-        for (int64_t k = 0; k < j; ++k) v -= Lf[(size_t)i * nc + k] * Lf[(size_t)j * nc + k];
-        Lf[(size_t)i * nc + j] = v / ljj;
-      }
-    });
+    for (int64_t i = j + 1; i < nc; ++i) {
+      double* li = &Lf[(size_t)i * nc];
+      li[j] = (li[j] - dot_fixed(li, lj, j)) / ljj;
+    }
   }
-  // W = L^-1 (lower triangular), column by column
-  std::vector<double> W((size_t)nc * nc, 0.0);
-  par_rows(nc, [&](int64_t a, int64_t b, int) {
-    for (int64_t c = a; c < b; ++c) {
-      W[(size_t)c * nc + c] = 1.0 / Lf[(size_t)c * nc + c];
-      for (int64_t i = c + 1; i < nc; ++i) {
-        double s = 0.0;
-        for (int64_t k = c; k < i; ++k) s += Lf[(size_t)i * nc + k] * W[(size_t)k * nc + c];
-        W[(size_t)i * nc + c] = -s / Lf[(size_t)i * nc + i];
-      }
+  // Wt = (L^-1)^T, upper triangular, row c = column c of L^-1 (forward substitution on e_c);
+  // rows are independent and split over the host threads (interleaved: the work per row falls
+  // with c)
+  std::vector<double> Wt((size_t)nc * nc, 0.0);
+  par_interleaved(nc, [&](int64_t c) {
+    double* wc = &Wt[(size_t)c * nc];
+    wc[c] = 1.0 / Lf[(size_t)c * nc + c];
+    for (int64_t i = c + 1; i < nc; ++i) {
+      const double* li = &Lf[(size_t)i * nc];
+      wc[i] = -dot_fixed(li + c, wc + c, i - c) / li[i];
     }
   });
+  // A^-1 = L^-T L^-1: (A^-1)_ij = sum_{k >= max(i, j)} Wt_ik Wt_jk, the upper half computed and
+  // mirrored
   out.coarse_inv.assign((size_t)nc * nc, 0.0);
-  par_rows(nc, [&](int64_t a, int64_t b, int) {
-    for (int64_t i = a; i < b; ++i)
-      for (int64_t j = 0; j < nc; ++j) {
-        double s = 0.0;
-        for (int64_t k = std::max(i, j); k < nc; ++k) s += W[(size_t)k * nc + i] * W[(size_t)k * nc + j];
-        out.coarse_inv[(size_t)i * nc + j] = s;
-      }
+  par_interleaved(nc, [&](int64_t i) {
+    const double* wi = &Wt[(size_t)i * nc];
+    for (int64_t j = i; j < nc; ++j) {
+      const double* wj = &Wt[(size_t)j * nc];
+      out.coarse_inv[(size_t)i * nc + j] = dot_fixed(wi + j, wj + j, nc - j);
+    }
   });
+  for (int64_t i = 0; i < nc; ++i)
+    for (int64_t j = 0; j < i; ++j) out.coarse_inv[(size_t)i * nc + j] = out.coarse_inv[(size_t)j * nc + i];
   // the last coarse matrix (BSR) is kept for tests through coarse_A only
   return WN_OK;
 }
