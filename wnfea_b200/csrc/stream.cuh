@@ -1,6 +1,6 @@
 // Streamed row engine for block-sparse matrices on sm_100a: BR x BC blocks (3x3 for the fine
-// level, 6x6 for AMG level 1, 3x6 / 6x3 for its prolongator / restrictor), 32-bit row pointers
-// and column indices, FP32 or FP64 values.
+// level, 6x6 for the AMG levels too large to stay in L2, 3x6 / 6x3 for the fine level's
+// prolongator / restrictor), 32-bit row pointers and column indices, FP32 or FP64 values.
 //
 // The fine matrix is the one array every fine-level kernel of the solve reads in full (40 B per
 // block in FP32, 76 B in FP64, against 12-24 B of x gathers that L2 serves), so its kernels are
@@ -23,7 +23,10 @@
 //     order of the register kernels in spmv.cuh -- with U blocks' gathers in flight per lane),
 //     and release the stage through a second mbarrier;
 //   * CTAs are persistent and take fixed runs of tiles, so the per-CTA dot partials come out in
-//     a fixed order (deterministic two-stage dots).
+//     a fixed order (deterministic two-stage dots);
+//   * the first stages' copies are issued before griddepcontrol.wait: under a programmatic
+//     dependent launch a kernel's CTAs start streaming their matrix while the previous kernel
+//     on the stream finishes, and read vectors, partials and flags only after the wait.
 // Every wait is bounded in time: a wait that runs out sets the caller's status word to
 // WN_ETIMEOUT and its done flag, the CTA stops issuing, waits (bounded) for its copies in
 // flight and returns.
