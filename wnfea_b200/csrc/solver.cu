@@ -285,19 +285,38 @@ __global__ void __launch_bounds__(kThreads, (BS == 3) ? kMinBlocks : 1) k_post_f
   if (part) write_part(dot, part, sh);
 }
 
-// coarsest level: x = A_c^-1 b with the dense FP64 inverse (one warp per row)
+// coarsest level: x = A_c^-1 b with the dense FP64 inverse.  Four warps per row (two rows per
+// CTA), each lane with four independent partial sums over columns 128 apart, combined in a fixed
+// order, so a 1,500-column row takes three dependent load rounds instead of ~47.
+constexpr int kCoarseWarpsPerRow = 4;
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_coarse(int64_t n, const double* __restrict__ inv,
                                                      const T* __restrict__ b, T* __restrict__ x,
                                                      const PcgScalars* __restrict__ S) {
-  pdl_trigger();  // dependents launched programmatically may start their prologue
+  __shared__ double part[kThreads / 32];
   if (S->done) return;
-  WARP_ROW_LOOP(n) {
-    double s = 0.0;
-    const double* rowp = inv + row * n;
-    for (int64_t j = lane; j < n; j += 32) s += rowp[j] * (double)b[j];
-    s = warp_sum(s);
-    if (lane == 0) x[row] = (T)s;
+  constexpr int RPC = (kThreads / 32) / kCoarseWarpsPerRow;  // rows per CTA
+  constexpr int STEP = 32 * kCoarseWarpsPerRow;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, q = w % kCoarseWarpsPerRow;
+  for (int64_t row0 = (int64_t)blockIdx.x * RPC; row0 < n; row0 += (int64_t)gridDim.x * RPC) {
+    const int64_t row = row0 + w / kCoarseWarpsPerRow;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    if (row < n) {
+      const double* rowp = inv + row * n;
+      int64_t j = q * 32 + lane;
+      for (; j + 3 * STEP < n; j += 4 * STEP) {
+        s0 += __ldg(rowp + j) * (double)b[j];
+        s1 += __ldg(rowp + j + STEP) * (double)b[j + STEP];
+        s2 += __ldg(rowp + j + 2 * STEP) * (double)b[j + 2 * STEP];
+        s3 += __ldg(rowp + j + 3 * STEP) * (double)b[j + 3 * STEP];
+      }
+      for (; j < n; j += STEP) s0 += __ldg(rowp + j) * (double)b[j];
+    }
+    const double s = warp_sum((s0 + s1) + (s2 + s3));
+    if (lane == 0) part[w] = s;
+    __syncthreads();
+    if (q == 0 && lane == 0 && row < n) x[row] = (T)((part[w] + part[w + 1]) + (part[w + 2] + part[w + 3]));
+    __syncthreads();
   }
 }
 
@@ -936,7 +955,8 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
                   PcgScalars* S, cudaStream_t st) {
   const int nlev = (int)H.levels.size();
   if (lvl == nlev) {  // coarsest
-    k_coarse<T><<<resident_grid(k_coarse<T>, kThreads, (H.n_coarse * 32 + kThreads - 1) / kThreads), kThreads, 0,
+    constexpr int rows_per_cta = (kThreads / 32) / kCoarseWarpsPerRow;
+    k_coarse<T><<<resident_grid(k_coarse<T>, kThreads, (H.n_coarse + rows_per_cta - 1) / rows_per_cta), kThreads, 0,
                   st>>>(H.n_coarse, H.coarse_inv.p, b, out, S);
     W.launches++;
     if (part) {  // a hierarchy without levels: the PCG's r . z comes from here
