@@ -96,6 +96,10 @@ int wn_solid_device_arrays(void* h, const double** k64, const float** k32, const
 /* y = K x for the assembled matrix: precision 0 = FP64 values/accumulation, 1 = FP32
  * values/accumulation (x, y are float then).  Device pointers. */
 int wn_spmv_solid_device(void* h, int precision, const void* x, void* y, uintptr_t stream);
+/* Streamed fine-level kernels on (enable != 0, the default) or off.  Off drops the tile plan and
+ * the FP32 / FP64 tile-major packs (about 1 GB per million DOFs) and runs the fine level on the
+ * register row kernels; on rebuilds them (and packs the current values).  Synchronises. */
+int wn_solid_set_stream(void* h, int enable);
 /* Status word of the streamed fine-matrix products of wn_spmv_solid_device: WN_OK, or
  * WN_ETIMEOUT when a bounded pipeline wait of a call since the last reset ran out of time (the
  * y of that call is not valid).  Synchronises the device; reset != 0 clears the word. */

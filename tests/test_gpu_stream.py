@@ -163,3 +163,36 @@ def test_streamed_coarse_levels_match_register_kernels(precision):
         out.append((u, st["iterations"]))
     assert out[0][1] == out[1][1]
     np.testing.assert_allclose(out[1][0], out[0][0], rtol=0, atol=1e-9 * np.abs(out[0][0]).max())
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_register_fine_level_matches_streamed(precision):
+    """Streaming switched off (the register row kernels, the path of meshes whose rows exceed
+    the tile capacity) against the streamed fine level: same iterations, same solution to
+    rounding; the SpMV of the register path against the oracle; streaming back on restores
+    the streamed results bit for bit."""
+    import torch
+    from wnfea_b200.model import solid_fixed_dofs, solid_load_vector
+
+    m, _ = generate_c3d10_ibeam_structured(n_slices=24, length=0.3, seed=6)
+    s = SolidSystem(m.mesh_nodes, m.solid_elements)
+    s.set_fixed(solid_fixed_dofs(m))
+    s.assemble(solid_element_props(m), apply_bcs=True)
+    F = solid_load_vector(m)
+    s.amg_setup()
+    u_on, st_on = s.solve(F, rtol=1e-9, precision=precision)
+    s.set_streaming(False)
+    u_off, st_off = s.solve(F, rtol=1e-9, precision=precision)
+    assert st_off["status"] == 0 and st_off["rel_res"] <= 1e-9
+    assert abs(st_off["iterations"] - st_on["iterations"]) <= 1
+    np.testing.assert_allclose(u_off, u_on, rtol=0, atol=1e-9 * np.abs(u_on).max())
+    rp, ci = s.pattern()
+    Kc = sp.bsr_matrix((s.values(), ci, rp), shape=(3 * s.n_nodes,) * 2).tocsr()
+    x = np.random.default_rng(1).standard_normal(3 * s.n_nodes)
+    dx = torch.from_numpy(x).cuda()
+    dy = torch.empty_like(dx)
+    _lib.call("wn_spmv_solid_device", s.handle, 0, dx.data_ptr(), dy.data_ptr(), 0)
+    assert np.all(np.abs(dy.cpu().numpy() - Kc @ x) <= 256 * np.finfo(np.float64).eps * (np.abs(Kc) @ np.abs(x)))
+    s.set_streaming(True)
+    u_again, st_again = s.solve(F, rtol=1e-9, precision=precision)
+    assert st_again["iterations"] == st_on["iterations"] and np.array_equal(u_again, u_on)

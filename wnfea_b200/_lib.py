@@ -89,6 +89,7 @@ SIGNATURES: dict[str, tuple] = {
     "wn_solid_get_values": (_I, [_P, _P]),
     "wn_solid_device_arrays": (_I, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
     "wn_spmv_solid_device": (_I, [_P, _I, _P, _P, _U]),
+    "wn_solid_set_stream": (_I, [_P, _I]),
     "wn_solid_stream_status": (_I, [_P, _I, _PI]),
     "wn_stream_tiles_host": (_I, [_I64, _P, _P, _I64, C.POINTER(_I64)]),
     "wn_spmv_bsr_f64_device": (_I, [_I, _I, _I64, _P, _P, _P, _P, _P, _D, _D, _U]),

@@ -338,7 +338,7 @@ int wn_assemble_c3d10_device(void* h, const double* d_props, int apply_bcs, uint
   WN_CHECK(launch_gather_assemble(s->nnzb, s->gptr.p, s->gsrc.p, s->ke.p, s->block_row.p, s->col_idx.p,
                                   apply_bcs ? s->fixed.p : nullptr, s->k64.p, s->k32.p, st));
   // tile-major copies for the streamed fine-level kernels
-  WN_CHECK(s->fine.pack(s->row_ptr.p, s->col_idx.p, s->k32.p, s->k64.p, s->nnzb, st));
+  if (s->stream_fine) WN_CHECK(s->fine.pack(s->row_ptr.p, s->col_idx.p, s->k32.p, s->k64.p, s->nnzb, st));
   int flag = 0;
   WN_CHECK(read_flag(s, st, &flag));
   WN_REQUIRE(flag == 0, WN_EMESH, "wn_assemble_c3d10: non-positive Jacobian determinant in a C3D10 element");
@@ -394,6 +394,29 @@ int wn_stream_tiles_host(int64_t n_rows, const int32_t* row_ptr, int32_t* tiles,
     WN_REQUIRE(capacity >= (int64_t)t.size(), WN_EINVAL, "wn_stream_tiles_host: capacity %lld < %lld tiles",
                (long long)capacity, (long long)t.size());
     memcpy(tiles, t.data(), t.size() * sizeof(StreamTile));
+  }
+  return 0;
+}
+
+int wn_solid_set_stream(void* h, int enable) {
+  WN_REQUIRE(h, WN_EINVAL, "wn_solid_set_stream: null handle");
+  Solid* s = as_solid(h);
+  WN_REQUIRE(s->bs == 3, WN_ESTATE, "wn_solid_set_stream: not a C3D10 system");
+  WN_CHECK(select_device(s));
+  WN_CUDA(cudaDeviceSynchronize());
+  s->stream_fine = enable != 0;
+  // captured PCG chunks hold the launches (and pack pointers) of the current path: drop them
+  if (s->work)
+    for (auto& a : s->work->graphs)
+      for (auto& g : a) g.reset();
+  if (!s->stream_fine) {
+    s->fine.clear();
+    return 0;
+  }
+  if (s->fine.n_tiles == 0) WN_CHECK(s->fine.make_plan(s->h_row_ptr.data(), s->n_nodes, 3, 3));
+  if (s->assembled && !s->fine.packed) {
+    WN_CHECK(s->fine.pack(s->row_ptr.p, s->col_idx.p, s->k32.p, s->k64.p, s->nnzb, 0));
+    WN_CUDA(cudaDeviceSynchronize());
   }
   return 0;
 }

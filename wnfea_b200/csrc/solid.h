@@ -49,6 +49,7 @@ struct Solid {
   // the fine matrix prepared for the streamed kernels (stream.cuh): tile plan made with the
   // pattern, FP32 / FP64 tile-major packs refreshed by every assembly
   StreamMat fine;
+  bool stream_fine = true;  // wn_solid_set_stream: plan and packs kept (else the register kernels)
   bool assembled = false;
   bool bcs_applied = false;
   std::unique_ptr<AmgHierarchy> amg;

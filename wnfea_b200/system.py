@@ -69,6 +69,11 @@ class SolidSystem:
         call("wn_solid_get_map", self._h, ptr(m))
         return m
 
+    def set_streaming(self, enable: bool) -> None:
+        """Streamed fine-level kernels (tile-major packs, the default) on or off; off frees the
+        packs (about 1 GB per million DOFs) and runs the fine level on the register row kernels."""
+        call("wn_solid_set_stream", self._h, int(bool(enable)))
+
     # -- assembly ---------------------------------------------------------------------------
     def set_fixed(self, fixed_dofs) -> None:
         mask = np.zeros(3 * self.n_nodes, dtype=np.uint8)
