@@ -18,6 +18,8 @@ from wnfea_b200.model import solid_element_props, solid_fixed_dofs, solid_load_v
 def _system(which):
     if which == "c1":
         m, _ = generate_c3d10_kuhn_block()
+    elif which == "block":
+        m, _ = generate_c3d10_kuhn_block(nx=12, ny=5, nz=7)
     else:
         m, _ = generate_c3d10_ibeam_structured(n_slices=12, length=4.0 * 12 / 315, seed=3)
     K, F, fixed = solid.assemble(m.mesh_nodes, m.solid_elements, solid_element_props(m), solid_load_vector(m),
@@ -90,3 +92,44 @@ def test_setup_is_deterministic():
     for a, b in zip(H1.levels, H2.levels):
         assert np.array_equal(a.P.data, b.P.data) and a.rho == b.rho
     assert np.array_equal(H1.coarse_inv, H2.coarse_inv)
+
+
+_DUMP = r"""
+import sys, numpy as np, scipy.sparse as sp
+sys.path.insert(0, sys.argv[2])
+from tests.test_amg_host import _system
+from wnfea_b200.amg import AMGParams, setup_host
+m, K, F, mask = _system("block")
+H = setup_host(sp.bsr_matrix(K, blocksize=(3, 3)), m.mesh_nodes, mask, AMGParams(coarse_size=700))
+out = {"coarse_A": H.coarse_A, "coarse_inv": H.coarse_inv}
+for l, L in enumerate(H.levels):
+    out[f"P{l}"] = L.P.data
+    out[f"dinv{l}"] = L.dinv
+    out[f"rho{l}"] = np.array([L.rho])
+    if L.A is not None:
+        out[f"A{l}"] = L.A.data
+np.savez(sys.argv[1], **out)
+"""
+
+
+def test_setup_is_identical_for_any_thread_count(tmp_path):
+    """The host setup (aggregation, smoothed prolongator, Galerkin products, dense coarsest
+    Cholesky and inverse) in two processes with 1 and 5 host threads: every exported array is
+    bit-identical.  The mesh is large enough (4,125 nodes, coarsest > 64 DOFs) for the row and
+    interleaved parallel loops to split."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parent.parent
+    res = []
+    for nth in ("1", "5"):
+        f = tmp_path / f"h{nth}.npz"
+        env = dict(os.environ, WN_HOST_THREADS=nth)
+        subprocess.run([sys.executable, "-c", _DUMP, str(f), str(root)], check=True, env=env, cwd=root, timeout=600)
+        res.append(np.load(f))
+    a, b = res
+    assert sorted(a.files) == sorted(b.files) and a["coarse_inv"].shape[0] > 64
+    for k in a.files:
+        assert np.array_equal(a[k], b[k]), k

@@ -12,6 +12,7 @@
 #include "pattern.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <thread>
 #include <vector>
 
@@ -32,7 +33,14 @@ static void parallel_for(int64_t n, int nthreads, const std::function<void(int64
   for (auto& x : th) x.join();
 }
 
+// host threads for the setup loops: WN_HOST_THREADS when set (read once per process), else the
+// hardware concurrency, at most 32.  Every result is the same for any thread count.
 int host_threads() {
+  static const int forced = [] {
+    const char* e = std::getenv("WN_HOST_THREADS");
+    return e ? std::atoi(e) : 0;
+  }();
+  if (forced > 0) return forced < 64 ? forced : 64;
   unsigned h = std::thread::hardware_concurrency();
   if (h == 0) h = 1;
   if (h > 32) h = 32;
