@@ -109,3 +109,13 @@ def test_ragged_rows():
 def test_row_over_capacity_gives_no_plan():
     rp = np.array([0, 10, 10 + CAP + 1, 10 + CAP + 5], dtype=np.int32)
     assert len(tiles_of(rp)) == 0
+
+
+def test_tiles_host_rejects_small_capacity():
+    rp = np.arange(0, 5 * 600 + 1, 5, dtype=np.int32)  # 600 rows of 5 blocks -> several tiles
+    cnt = C.c_int64()
+    _lib.call("wn_stream_tiles_host", 600, _lib.ptr(rp), None, 0, C.byref(cnt))
+    assert cnt.value >= 5
+    buf = np.zeros((1, 4), dtype=np.int32)
+    with pytest.raises(_lib.WnError):
+        _lib.call("wn_stream_tiles_host", 600, _lib.ptr(rp), _lib.ptr(buf), 1, C.byref(cnt))
