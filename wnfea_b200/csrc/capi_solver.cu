@@ -1,8 +1,5 @@
 // extern "C" boundary of the AMG setup and the PCG / mixed-precision solver.
-#include <algorithm>
 #include <cstring>
-#include <thread>
-#include <vector>
 
 #include "amg.h"
 #include "common.cuh"
@@ -173,25 +170,6 @@ int wn_solve_device(void* h, const double* d_F, double* d_u, const wn_solve_para
   return solver_solve(s, d_F, d_u, *params, stats, (cudaStream_t)stream);
 }
 
-// host copy split over the host threads: one thread moves ~10 GB/s, so staging a 1M-DOF FP64
-// vector through the page-locked buffer would cost ~0.8 ms each way on one core
-static void parallel_memcpy(void* dst, const void* src, size_t bytes) {
-  const int nth = std::min(wn::host_threads(), 8);
-  if (nth <= 1 || bytes < (size_t(2) << 20)) {
-    std::memcpy(dst, src, bytes);
-    return;
-  }
-  const size_t chunk = ((bytes + nth - 1) / nth + 63) & ~size_t(63);
-  std::vector<std::thread> th;
-  for (int t = 0; t < nth; ++t) {
-    const size_t a = (size_t)t * chunk;
-    if (a >= bytes) break;
-    const size_t b = std::min(bytes, a + chunk);
-    th.emplace_back([=]() { std::memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, b - a); });
-  }
-  for (auto& x : th) x.join();
-}
-
 int wn_solve(void* h, const double* F, double* u, const wn_solve_params* params, wn_solve_stats* stats) {
   WN_REQUIRE(h && F && u && params, WN_EINVAL, "wn_solve: null argument");
   Solid* s = reinterpret_cast<Solid*>(h);
@@ -202,11 +180,11 @@ int wn_solve(void* h, const double* F, double* u, const wn_solve_params* params,
   WN_CHECK(s->io_f.alloc(n));
   WN_CHECK(s->io_u.alloc(n));
   WN_CHECK(s->io_pin.at_least(2 * n));
-  parallel_memcpy(s->io_pin.p, F, n * sizeof(double));
+  std::memcpy(s->io_pin.p, F, n * sizeof(double));
   WN_CUDA(cudaMemcpy(s->io_f.p, s->io_pin.p, n * sizeof(double), cudaMemcpyHostToDevice));
   WN_CHECK(solver_solve(s, s->io_f.p, s->io_u.p, *params, stats, 0));
   WN_CUDA(cudaMemcpy(s->io_pin.p + n, s->io_u.p, n * sizeof(double), cudaMemcpyDeviceToHost));
-  parallel_memcpy(u, s->io_pin.p + n, n * sizeof(double));
+  std::memcpy(u, s->io_pin.p + n, n * sizeof(double));
   return 0;
 }
 
