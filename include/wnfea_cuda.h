@@ -104,6 +104,13 @@ int wn_solid_set_stream(void* h, int enable);
  * WN_ETIMEOUT when a bounded pipeline wait of a call since the last reset ran out of time (the
  * y of that call is not valid).  Synchronises the device; reset != 0 clears the word. */
 int wn_solid_stream_status(void* h, int reset, int* status);
+/* Failure-detection hook of the streamed fine-matrix kernels (for tests; no reference
+ * counterpart).  wait_limit_ns bounds each pipeline wait (0 restores the default of 4 s).
+ * withhold_tile >= 0 makes the producer skip that tile's copy, so the consumers' wait for it
+ * runs out: the call reports WN_ETIMEOUT (wn_solid_stream_status for wn_spmv_solid_device,
+ * stats.status for the solves) and every kernel still waits, bounded, for the copies it did
+ * issue before it exits; -1 turns it off.  Synchronises; drops the handle's captured graphs. */
+int wn_solid_stream_test_hook(void* h, int64_t wait_limit_ns, int withhold_tile);
 /* The row tiles the streamed fine-matrix kernels cut a 3x3 block-row pattern into (host only):
  * tiles[4 t .. 4 t + 3] = (first row, end row, first block, end block) of tile t, whole rows
  * in order, at most WN_STREAM_TILE_BLOCKS blocks and WN_STREAM_TILE_ROWS rows per tile.
@@ -178,9 +185,15 @@ int wn_amg_host_coarse(void* hier, int64_t* n_coarse, double* Ac, double* Ac_inv
 typedef struct wn_solve_params {
   double rtol;        /* stop when ||F - K u|| <= rtol ||F||                          */
   int max_iter;       /* total PCG iterations (inner iterations for mixed)            */
-  int precond;        /* 0 none, 1 point Jacobi (solid_solver.py:228-236), 2 AMG      */
-  int precision;      /* 0 FP64 throughout; 1 FP32 inner PCG + AMG inside FP64
-                         iterative refinement (solid_solver.py:271-300)                */
+  int precond;        /* 0 none, 1 point Jacobi (solid_solver.py:228-236), 2 AMG,
+                         3 block Jacobi: pseudo-inverses of the diagonal node blocks
+                         (solid_solver.py:237-258)                                    */
+  int precision;      /* 0 FP64 throughout;
+                         1 FP64 PCG (FP64 SpMV, vectors, dots) with the preconditioner in
+                           FP32 (AMG: FP32 V-cycle values, vectors and accumulation, FP64
+                           coarsest inverse), inside the FP64 true-residual loop;
+                         2 FP32 PCG (FP32 SpMV and preconditioner, FP64 dots) inside FP64
+                           iterative refinement (the scheme of solid_solver.py:271-300) */
   double inner_rtol;  /* mixed: inner relative tolerance (<= 0: max(1e-4, rtol))      */
   int max_outer;      /* mixed: refinement steps (<= 0: 10)                           */
   int chunk;          /* iterations per CUDA-graph replay / host convergence check    */
@@ -272,13 +285,15 @@ int wn_c3d10_element_stiffness(int64_t n_el, const double* coords, const double*
  * every GPU loading the library holds until exit (about 8.1 MB).  It calls no cudaMalloc,
  * cudaFree or allocating library routine.
  *   - n_el > WN_NOALLOC_MAX_ELEMENTS returns WN_ETOOBIG (split the batch);
- *   - the first call on a device looks up the scratch address and loads the element
- *     kernel's constant tables: make that first call before any stream capture;
+ *   - a conn entry outside [0, n_nodes) returns WN_EINVAL: the kernel checks every index
+ *     before it reads coordinates, and that element's Ke is zero;
+ *   - the first call on a device looks up the scratch address (cudaGetSymbolAddress, with
+ *     that device current): make that first call before any stream capture;
  *   - all calls share the scratch, so calls that overlap on the GPU (other streams, other
  *     threads) race: serialise them;
  *   - the call synchronises `stream` to report WN_EMESH for det J <= 0. */
 #define WN_NOALLOC_MAX_ELEMENTS 2048
-int wn_c3d10_element_stiffness_noalloc(int64_t n_el, const double* d_nodes, const int32_t* d_conn,
+int wn_c3d10_element_stiffness_noalloc(int64_t n_el, int64_t n_nodes, const double* d_nodes, const int32_t* d_conn,
                                        const double* d_props, double* d_Ke, uintptr_t stream);
 
 /* Internal forces F_int = sum_e f_e(u) with f_e = sum_g w|J| B^T C B u_e (c3d10.py:252-283),

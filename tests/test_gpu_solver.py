@@ -108,13 +108,45 @@ def test_jacobi_pcg_matches_reference_iterations():
     assert np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref) < 1e-6
 
 
+def test_block_jacobi_pcg_matches_reference_iterations():
+    """3x3 block-Jacobi PCG (pseudo-inverse of every node block, solid_solver.py:237-258)."""
+    m, _ = generate_c3d10_kuhn_block()
+    K, F, _ = assemble_c3d10_sparse_3dof(m)
+    Ko, Fo = _oracle_K(m)
+    _, its_ref, _, _ = solid.pcg(Ko, Fo, rtol=0.5e-8, max_iter=5000, preconditioner="block_jacobi")
+    _, its_pt, _, _ = solid.pcg(Ko, Fo, rtol=0.5e-8, max_iter=5000, preconditioner="jacobi")
+    assert its_ref != its_pt  # the two preconditioners are told apart by their counts
+    _, st1 = K.system.solve(F, rtol=1e-8, max_iter=5000, precond=3, max_outer=1)
+    assert st1["outer_iterations"] == 1
+    its = st1["iterations"]
+    assert abs(its - its_ref) <= 0.06 * its_ref + 3, (its, its_ref)
+    u_ref = spsolve(Ko.tocsc(), Fo)
+    for precision, tol in (("fp64", 1e-6), ("mixed_fp32", 1e-6)):
+        u, its_all, rel, _ = solve_c3d10_pcg(K, F, rtol=1e-8, max_iter=5000, preconditioner="block_jacobi",
+                                             precision=precision)
+        assert rel <= 1e-8, (precision, rel)
+        assert np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref) < tol, precision
+
+
+def test_reference_default_preconditioner_is_jacobi():
+    """solve_c3d10_pcg / solve_c3d10_system keep the reference's defaults (point Jacobi, rtol
+    1e-6, 2000 iterations, FP64): the default call runs the Jacobi recurrence."""
+    m, _ = generate_c3d10_kuhn_block()
+    K, F, _ = assemble_c3d10_sparse_3dof(m)
+    _, its_default, rel_default, _ = solve_c3d10_pcg(K, F)
+    _, its_jac, rel_jac, _ = solve_c3d10_pcg(K, F, preconditioner="jacobi")
+    assert its_default == its_jac and rel_default == rel_jac
+    _, st = solve_c3d10_system(K, F, method="pcg")
+    assert st["method"] == "pcg_jacobi_fp64" and st["iterations"] == its_jac
+
+
 def test_ibeam_fp64_and_mixed_agree():
     m = _ibeam(24, seed=7)
     K, F, _ = assemble_c3d10_sparse_3dof(m)
     Ko, Fo = _oracle_K(m)
     u_ref = spsolve(Ko.tocsc(), Fo)
-    u64, st64 = solve_c3d10_system(K, F, method="pcg", rtol=1e-10, precision="fp64")
-    u32, st32 = solve_c3d10_system(K, F, method="pcg", rtol=1e-8, precision="mixed_fp32")
+    u64, st64 = solve_c3d10_system(K, F, method="pcg", rtol=1e-10, preconditioner="amg", precision="fp64")
+    u32, st32 = solve_c3d10_system(K, F, method="pcg", rtol=1e-8, preconditioner="amg", precision="mixed_fp32")
     assert st64["status"] == 0 and st32["status"] == 0
     assert np.linalg.norm(u64 - u_ref) / np.linalg.norm(u_ref) < 1e-8
     assert np.linalg.norm(u32 - u_ref) / np.linalg.norm(u_ref) < 1e-6
@@ -151,8 +183,8 @@ def test_zero_rhs_and_iteration_limit_and_nan():
 def test_solve_is_deterministic():
     m = _ibeam(8, seed=4)
     K, F, _ = assemble_c3d10_sparse_3dof(m)
-    u1, _ = solve_c3d10_system(K, F, method="pcg", rtol=1e-9, precision="mixed_fp32")
-    u2, _ = solve_c3d10_system(K, F, method="pcg", rtol=1e-9, precision="mixed_fp32")
+    u1, _ = solve_c3d10_system(K, F, method="pcg", rtol=1e-9, preconditioner="amg", precision="mixed_fp32")
+    u2, _ = solve_c3d10_system(K, F, method="pcg", rtol=1e-9, preconditioner="amg", precision="mixed_fp32")
     assert np.array_equal(u1, u2)
 
 
@@ -191,7 +223,7 @@ def test_tight_tolerance_on_lateral_load(precision, rtol):
     tip = np.flatnonzero(m.mesh_nodes[:, 0] >= m.mesh_nodes[:, 0].max() - 1e-12)
     Fy = np.zeros_like(F)
     Fy[3 * tip + 1] = 50e3 / len(tip)
-    u, st = solve_c3d10_system(K, Fy, method="pcg", rtol=rtol, precision=precision, max_iter=4000)
+    u, st = solve_c3d10_system(K, Fy, method="pcg", rtol=rtol, preconditioner="amg", precision=precision, max_iter=4000)
     assert st["status"] == 0 and st["rel_res"] <= rtol
     res, floor = _residual_longdouble(Ko, u, Fy)
     assert res <= 2 * max(rtol, floor)
@@ -206,7 +238,7 @@ def test_tiny_mesh_hierarchy_without_levels():
     Ko, Fo = _oracle_K(m)
     ur = spsolve(Ko.tocsc(), Fo)
     for precision in ("fp64", "mixed_fp32"):
-        u, st = solve_c3d10_system(K, F, method="pcg", rtol=1e-10, precision=precision)
+        u, st = solve_c3d10_system(K, F, method="pcg", rtol=1e-10, preconditioner="amg", precision=precision)
         assert st["status"] == 0 and st["levels"] == 1
         assert np.linalg.norm(u - ur) <= 1e-8 * np.linalg.norm(ur)
     Fm = tip_load_cases(m.mesh_nodes, n_cases=3, seed=0)

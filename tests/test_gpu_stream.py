@@ -196,3 +196,49 @@ def test_register_fine_level_matches_streamed(precision):
     s.set_streaming(True)
     u_again, st_again = s.solve(F, rtol=1e-9, precision=precision)
     assert st_again["iterations"] == st_on["iterations"] and np.array_equal(u_again, u_on)
+
+
+def test_stream_wait_runs_out_and_the_handle_recovers():
+    """Failure detection of the streamed pipeline, with no fault: the test hook makes the
+    producer withhold one tile's copy (nothing arms that stage), so the consumers' bounded wait
+    for it must run out after the short limit.  The product and the solve must report
+    WN_ETIMEOUT; every CTA waits for the copies it did issue before it exits, so the context stays
+    usable, and once the hook is off the next product and solve on the same handle are
+    bit-identical to clean ones."""
+    import torch
+
+    m = generate_c3d10_ibeam_structured(n_slices=20, length=4.0 * 20 / 315, seed=5)[0]
+    s = SolidSystem(m.mesh_nodes, m.solid_elements)
+    s.assemble(solid_element_props(m), apply_bcs=False)
+    rp, _ = s.pattern()
+    nt = C.c_int64(0)
+    _lib.call("wn_stream_tiles_host", s.n_nodes, _lib.ptr(rp), None, 0, C.byref(nt))
+    assert nt.value > 8
+    x = torch.from_numpy(np.random.default_rng(3).standard_normal(3 * s.n_nodes)).cuda()
+    y_ref, y = torch.empty_like(x), torch.empty_like(x)
+    _lib.call("wn_spmv_solid_device", s.handle, 0, x.data_ptr(), y_ref.data_ptr(), 0)
+    assert _status(s) == 0
+    for tile in (0, nt.value // 2, nt.value - 1):
+        _lib.call("wn_solid_stream_test_hook", s.handle, 200_000, tile)  # 0.2 ms stage waits
+        for prec, xv, yv in ((0, x, y), (1, x.float(), torch.empty_like(x, dtype=torch.float32))):
+            _lib.call("wn_spmv_solid_device", s.handle, prec, xv.data_ptr(), yv.data_ptr(), 0)
+            assert _status(s) == -9, (tile, prec)  # WN_ETIMEOUT, status word reset by _status
+    _lib.call("wn_solid_stream_test_hook", s.handle, 0, -1)
+    _lib.call("wn_spmv_solid_device", s.handle, 0, x.data_ptr(), y.data_ptr(), 0)
+    assert _status(s) == 0
+    assert torch.equal(y, y_ref)
+
+    # the solver: its fine-level kernels (V-cycle and PCG product) stream the same matrix
+    from wnfea_b200.solid_solver import assemble_c3d10_sparse_3dof
+
+    K, F, _ = assemble_c3d10_sparse_3dof(m)  # root clamped, tip shear
+    sfix = K.system
+    for precision in (0, 1):
+        u_clean, st_clean = sfix.solve(F, rtol=1e-8, precision=precision)
+        assert st_clean["status"] == 0
+        _lib.call("wn_solid_stream_test_hook", sfix.handle, 200_000, nt.value // 3)
+        _, st_bad = sfix.solve(F, rtol=1e-8, precision=precision)
+        assert st_bad["status"] == -9, st_bad
+        _lib.call("wn_solid_stream_test_hook", sfix.handle, 0, -1)
+        u_again, st_again = sfix.solve(F, rtol=1e-8, precision=precision)
+        assert st_again["status"] == 0 and np.array_equal(u_again, u_clean)

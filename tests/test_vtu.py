@@ -60,7 +60,7 @@ def test_solid_export_matches_oracle_stresses(tmp_path):
 
     m, _ = generate_c3d10_kuhn_block()
     K, F, _ = assemble_c3d10_sparse_3dof(m)
-    u, _ = solve_c3d10_system(K, F, method="pcg", rtol=1e-10, precision="fp64")
+    u, _ = solve_c3d10_system(K, F, method="pcg", rtol=1e-10, preconditioner="amg", precision="fp64")
     m.displacements = u
     path = export_vtu(m, tmp_path / "c1.vtu")
     piece, a = _arrays(path)

@@ -91,12 +91,13 @@ SIGNATURES: dict[str, tuple] = {
     "wn_spmv_solid_device": (_I, [_P, _I, _P, _P, _U]),
     "wn_solid_set_stream": (_I, [_P, _I]),
     "wn_solid_stream_status": (_I, [_P, _I, _PI]),
+    "wn_solid_stream_test_hook": (_I, [_P, _I64, _I]),
     "wn_stream_tiles_host": (_I, [_I64, _P, _P, _I64, C.POINTER(_I64)]),
     "wn_spmv_bsr_f64_device": (_I, [_I, _I, _I64, _P, _P, _P, _P, _P, _D, _D, _U]),
     "wn_spmv_bsr_f32_device": (_I, [_I, _I, _I64, _P, _P, _P, _P, _P, _F, _F, _U]),
     "wn_spmv_bsr_f64": (_I, [_I, _I, _I64, _I64, _I64, _P, _P, _P, _P, _P, _D, _D]),
     "wn_c3d10_element_stiffness": (_I, [_I64, _P, _P, _P]),
-    "wn_c3d10_element_stiffness_noalloc": (_I, [_I64, _P, _P, _P, _P, _U]),
+    "wn_c3d10_element_stiffness_noalloc": (_I, [_I64, _I64, _P, _P, _P, _P, _U]),
     "wn_c3d10_internal_forces": (_I, [_P, _P, _P, _P, _P, _I, _I]),
     "wn_fint_c3d10_device": (_I, [_P, _P, _P, _U]),
     "wn_fint_c3d10": (_I, [_P, _P, _P]),

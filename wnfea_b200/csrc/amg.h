@@ -126,10 +126,13 @@ struct SolverWork {
   DArray<float> r32;
   DArray<double> dinv64;      // Jacobi (point) of the fine matrix
   DArray<float> dinv32;
+  DArray<double> binv64;      // block-Jacobi: pseudo-inverses of the diagonal blocks (row-major per node)
+  DArray<float> binv32;
   PcgVecs<double> p64;
   PcgVecs<float> p32;
-  // captured chunk graphs: [mode 0 fp64 / 1 mixed / 2 fp32][preconditioner 0 none / 1 jacobi / 2 amg]
-  GraphCache graphs[3][3];
+  // captured chunk graphs: [mode 0 fp64 / 1 mixed / 2 fp32]
+  //                        [preconditioner 0 none / 1 jacobi / 2 amg / 3 block jacobi]
+  GraphCache graphs[3][4];
   int64_t launches = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaStream_t own = nullptr;  // used when the caller passes the legacy default stream

@@ -17,28 +17,10 @@
 
 namespace wn {
 
-// (a, b) of upper-triangle index t (inverse of tri_index)
-__constant__ unsigned char c_tri_a[55];
-__constant__ unsigned char c_tri_b[55];
-
-static int ensure_tri_tables() {
-  static thread_local int done_dev = -1;
-  int dev = 0;
-  WN_CUDA(cudaGetDevice(&dev));
-  if (done_dev == dev) return 0;
-  unsigned char ta[55], tb[55];
-  int t = 0;
-  for (int a = 0; a < 10; ++a)
-    for (int b = a; b < 10; ++b) {
-      ta[t] = (unsigned char)a;
-      tb[t] = (unsigned char)b;
-      ++t;
-    }
-  WN_CUDA(cudaMemcpyToSymbol(c_tri_a, ta, sizeof(ta)));
-  WN_CUDA(cudaMemcpyToSymbol(c_tri_b, tb, sizeof(tb)));
-  done_dev = dev;
-  return 0;
-}
+// (a, b) of upper-triangle index t (inverse of tri_index: t runs over a = 0..9, b = a..9),
+// statically initialised, so no set-up call uploads them
+__constant__ unsigned char c_tri_a[55] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 1, 1, 1, 2, 2, 2, 2, 2, 2, 2, 2, 3, 3, 3, 3, 3, 3, 3, 4, 4, 4, 4, 4, 4, 5, 5, 5, 5, 5, 6, 6, 6, 6, 7, 7, 7, 8, 8, 9};
+__constant__ unsigned char c_tri_b[55] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 1, 2, 3, 4, 5, 6, 7, 8, 9, 2, 3, 4, 5, 6, 7, 8, 9, 3, 4, 5, 6, 7, 8, 9, 4, 5, 6, 7, 8, 9, 5, 6, 7, 8, 9, 6, 7, 8, 9, 7, 8, 9, 8, 9, 9};
 
 constexpr int KE_TILE = 16;      // elements per CTA
 constexpr int KE_THREADS = 256;  // threads per CTA
@@ -58,8 +40,10 @@ __device__ __forceinline__ void load_coords(const double* __restrict__ nodes, co
 // Ke upper triangle of elements [0, n_el): out[(e * 55 + t) * 9 + 3 i + j].
 // Phase 1: one thread per (element, Gauss point) computes dN/dx and w|J| into shared
 // memory.  Phase 2: all threads produce the 495 block entries of the tile's elements,
-// written contiguously.  An element with det J <= 0 raises bit 0 of *flags.
-__global__ void __launch_bounds__(KE_THREADS) ke_upper_kernel(int64_t n_el, const double* __restrict__ nodes,
+// written contiguously.  An element with det J <= 0 raises bit 0 of *flags; an element with a
+// node index outside [0, n_nodes) raises bit 1, reads no coordinates and gets a zero Ke.
+__global__ void __launch_bounds__(KE_THREADS) ke_upper_kernel(int64_t n_el, int64_t n_nodes,
+                                                              const double* __restrict__ nodes,
                                                               const int32_t* __restrict__ conn,
                                                               const double* __restrict__ props,
                                                               double* __restrict__ out, int* __restrict__ flags) {
@@ -72,11 +56,26 @@ __global__ void __launch_bounds__(KE_THREADS) ke_upper_kernel(int64_t n_el, cons
     if (threadIdx.x < KE_TILE * 4) {
       const int le = threadIdx.x >> 2, g = threadIdx.x & 3;
       if (le < ne) {
-        double X[10][3];
-        load_coords(nodes, conn, e0 + le, X);
+        bool in_range = true;
+#pragma unroll
+        for (int a = 0; a < 10; ++a) {
+          const int32_t v = conn[(e0 + le) * 10 + a];
+          in_range = in_range && v >= 0 && (int64_t)v < n_nodes;
+        }
         double dndx[3][10];
-        const double det = gp_cartesian(g, X, dndx);
-        if (!(det > 0.0)) flags[0] = 1;
+        double det = 0.0;
+        if (in_range) {
+          double X[10][3];
+          load_coords(nodes, conn, e0 + le, X);
+          det = gp_cartesian(g, X, dndx);
+          if (!(det > 0.0)) atomicOr(flags, 1);
+        } else {
+          atomicOr(flags, 2);
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int a = 0; a < 10; ++a) dndx[i][a] = 0.0;
+        }
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -313,13 +312,12 @@ __global__ void nodal_average_kernel(int64_t n_nodes, const int64_t* __restrict_
 // ---------------------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------------------
-int launch_ke_upper(int64_t n_el, const double* nodes, const int32_t* conn, const double* props, double* out,
-                    int* flags, cudaStream_t st) {
-  WN_CHECK(ensure_tri_tables());
+int launch_ke_upper(int64_t n_el, int64_t n_nodes, const double* nodes, const int32_t* conn, const double* props,
+                    double* out, int* flags, cudaStream_t st) {
   if (n_el == 0) return 0;
   const int64_t tiles = (n_el + KE_TILE - 1) / KE_TILE;
   const int grid = (int)std::min<int64_t>(tiles, (int64_t)kNumSMs * 8);
-  ke_upper_kernel<<<grid, KE_THREADS, 0, st>>>(n_el, nodes, conn, props, out, flags);
+  ke_upper_kernel<<<grid, KE_THREADS, 0, st>>>(n_el, n_nodes, nodes, conn, props, out, flags);
   WN_CUDA(cudaGetLastError());
   return 0;
 }

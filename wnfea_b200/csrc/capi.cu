@@ -334,7 +334,7 @@ int wn_assemble_c3d10_device(void* h, const double* d_props, int apply_bcs, uint
   WN_CHECK(s->k64.alloc(s->nnzb * 9));
   WN_CHECK(s->k32.alloc(s->nnzb * 9));
   WN_CUDA(cudaMemsetAsync(s->flags.p, 0, sizeof(int), st));
-  WN_CHECK(launch_ke_upper(s->n_el, s->nodes.p, s->conn.p, s->props.p, s->ke.p, s->flags.p, st));
+  WN_CHECK(launch_ke_upper(s->n_el, s->n_nodes, s->nodes.p, s->conn.p, s->props.p, s->ke.p, s->flags.p, st));
   WN_CHECK(launch_gather_assemble(s->nnzb, s->gptr.p, s->gsrc.p, s->ke.p, s->block_row.p, s->col_idx.p,
                                   apply_bcs ? s->fixed.p : nullptr, s->k64.p, s->k32.p, st));
   // tile-major copies for the streamed fine-level kernels
@@ -431,6 +431,21 @@ int wn_solid_stream_status(void* h, int reset, int* status) {
   return 0;
 }
 
+int wn_solid_stream_test_hook(void* h, int64_t wait_limit_ns, int withhold_tile) {
+  WN_REQUIRE(h, WN_EINVAL, "wn_solid_stream_test_hook: null handle");
+  Solid* s = as_solid(h);
+  WN_REQUIRE(wait_limit_ns >= 0, WN_EINVAL, "wn_solid_stream_test_hook: negative wait limit");
+  WN_CHECK(select_device(s));
+  WN_CUDA(cudaDeviceSynchronize());
+  s->fine.ctl.wait_ns = wait_limit_ns > 0 ? (unsigned long long)wait_limit_ns : kStreamWaitLimitNs;
+  s->fine.ctl.withhold = withhold_tile >= 0 ? withhold_tile : -1;
+  // captured PCG chunks carry the old control values as kernel parameters: drop them
+  if (s->work)
+    for (auto& a : s->work->graphs)
+      for (auto& g : a) g.reset();
+  return 0;
+}
+
 int wn_spmv_solid_device(void* h, int precision, const void* x, void* y, uintptr_t stream) {
   WN_REQUIRE(h && x && y, WN_EINVAL, "wn_spmv_solid_device: null argument");
   Solid* s = as_solid(h);
@@ -441,7 +456,8 @@ int wn_spmv_solid_device(void* h, int precision, const void* x, void* y, uintptr
     if (s->fine.packed) {
       const int rc = launch_solid_spmv_stream(precision, precision == 0 ? s->fine.d64.p : s->fine.d32.p,
                                               s->fine.n_tiles, precision == 0 ? s->fine.p64.p : s->fine.p32.p, x, y,
-                                              s->flags.p + kStreamStatusWord, (cudaStream_t)stream);
+                                              s->flags.p + kStreamStatusWord, s->fine.ctl.wait_ns,
+                                              s->fine.ctl.withhold, (cudaStream_t)stream);
       if (rc != 0) return rc < 0 ? rc : 0;
     }
   }
@@ -506,7 +522,7 @@ int wn_c3d10_element_stiffness(int64_t n_el, const double* coords, const double*
   WN_CHECK(dke.alloc(n_el * 55 * 9));
   WN_CHECK(flags.alloc(1));
   WN_CHECK(flags.zero());
-  WN_CHECK(launch_ke_upper(n_el, dn.p, dc.p, dp.p, dke.p, flags.p, 0));
+  WN_CHECK(launch_ke_upper(n_el, n_el * 10, dn.p, dc.p, dp.p, dke.p, flags.p, 0));
   std::vector<double> up(n_el * 55 * 9);
   int flag = 0;
   WN_CUDA(cudaMemcpy(up.data(), dke.p, dke.bytes(), cudaMemcpyDeviceToHost));

@@ -8,8 +8,9 @@
 namespace wn {
 
 // c3d10.cu
-int launch_ke_upper(int64_t n_el, const double* nodes, const int32_t* conn, const double* props, double* out,
-                    int* flags, cudaStream_t st);
+// flags: bit 0 = det J <= 0, bit 1 = node index outside [0, n_nodes) (that element: zero Ke)
+int launch_ke_upper(int64_t n_el, int64_t n_nodes, const double* nodes, const int32_t* conn, const double* props,
+                    double* out, int* flags, cudaStream_t st);
 int launch_gather_assemble(int64_t nnzb, const int32_t* gptr, const int32_t* gsrc, const double* ke,
                            const int32_t* block_row, const int32_t* col_idx, const uint8_t* fixed, double* k64,
                            float* k32, cudaStream_t st);
@@ -39,10 +40,12 @@ int launch_solid_spmv_f32(int64_t n_rows, const int32_t* rp, const int32_t* ci, 
                           const float* x, float* y, cudaStream_t st);
 // the same product with the matrix streamed through shared memory from its tile-major pack
 // (stream.cuh); returns 1 when launched, 0 when the kernel cannot run here, < 0 on error; a
-// pipeline wait that runs out of time writes WN_ETIMEOUT to *status
+// pipeline wait that runs out of time (wait_ns; withhold >= 0: the failure-test hook of
+// stream.cuh) writes WN_ETIMEOUT to *status
 struct PackTile;
 int launch_solid_spmv_stream(int precision, const PackTile* tiles, int n_tiles, const unsigned char* pack,
-                             const void* x, void* y, int* status, cudaStream_t st);
+                             const void* x, void* y, int* status, unsigned long long wait_ns, int withhold,
+                             cudaStream_t st);
 
 // A linear 6-DOF-per-node system (block-contiguous row-major 6x6 values; host pattern arrays,
 // values on the host or the device) as a solver handle with bs = 6 (capi.cu).

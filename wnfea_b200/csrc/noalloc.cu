@@ -25,7 +25,9 @@ constexpr int64_t kScratchDoubles = kHeaderDoubles + kNoAllocMaxElements * 55 * 
 // Shared by every call on a device and kept until the process exits (about 8.1 MB).
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
-// Device address of g_noalloc_scratch per device ordinal, looked up once per device.
+// Device address of g_noalloc_scratch per device ordinal, looked up once per device (the first
+// call on each device, with that device current).  The element kernel's constant tables are
+// statically initialised, so this lookup is the only set-up.
 static std::mutex g_mutex;
 static void* g_scratch_addr[64] = {nullptr};
 
@@ -73,9 +75,10 @@ __global__ void expand_upper_kernel(int64_t n_el, const double* __restrict__ upp
 
 using namespace wn;
 
-extern "C" int wn_c3d10_element_stiffness_noalloc(int64_t n_el, const double* d_nodes, const int32_t* d_conn,
-                                                   const double* d_props, double* d_Ke, uintptr_t stream) {
-  WN_REQUIRE(n_el >= 0, WN_EINVAL, "wn_c3d10_element_stiffness_noalloc: negative element count");
+extern "C" int wn_c3d10_element_stiffness_noalloc(int64_t n_el, int64_t n_nodes, const double* d_nodes,
+                                                   const int32_t* d_conn, const double* d_props, double* d_Ke,
+                                                   uintptr_t stream) {
+  WN_REQUIRE(n_el >= 0 && n_nodes >= 0, WN_EINVAL, "wn_c3d10_element_stiffness_noalloc: negative size");
   WN_REQUIRE(n_el <= kNoAllocMaxElements, WN_ETOOBIG,
              "wn_c3d10_element_stiffness_noalloc: %lld elements exceed the fixed scratch capacity of %lld; "
              "split the batch or use wn_c3d10_element_stiffness",
@@ -85,15 +88,19 @@ extern "C" int wn_c3d10_element_stiffness_noalloc(int64_t n_el, const double* d_
   cudaStream_t st = (cudaStream_t)stream;
   double* scratch = nullptr;
   WN_CHECK(scratch_address(&scratch));
-  int* status = reinterpret_cast<int*>(scratch);  // header: det J <= 0 flag, cleared per call
+  int* status = reinterpret_cast<int*>(scratch);  // header: error bits, cleared per call
   double* upper = scratch + kHeaderDoubles;
   WN_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
-  WN_CHECK(launch_ke_upper(n_el, d_nodes, d_conn, d_props, upper, status, st));
+  // the element kernel checks every node index against n_nodes before it reads coordinates
+  WN_CHECK(launch_ke_upper(n_el, n_nodes, d_nodes, d_conn, d_props, upper, status, st));
   expand_upper_kernel<<<grid_for(n_el * 900, 1, 256, 8), 256, 0, st>>>(n_el, upper, d_Ke);
   WN_CUDA(cudaGetLastError());
   int flag = 0;
   WN_CUDA(cudaMemcpyAsync(&flag, status, sizeof(int), cudaMemcpyDeviceToHost, st));
   WN_CUDA(cudaStreamSynchronize(st));
+  WN_REQUIRE(!(flag & 2), WN_EINVAL,
+             "wn_c3d10_element_stiffness_noalloc: a connectivity entry lies outside [0, n_nodes = %lld)",
+             (long long)n_nodes);
   WN_REQUIRE(flag == 0, WN_EMESH, "wn_c3d10_element_stiffness_noalloc: non-positive Jacobian determinant");
   return 0;
 }

@@ -15,8 +15,11 @@
 //   * the iterations are captured once into a CUDA graph (a chunk of iterations whose
 //     kernels return early once the device-side convergence flag is set); the host reads
 //     the flag once per chunk instead of once per iteration (hip_kernels.cpp:2465-2476);
-//   * mixed precision: FP32 matrix / V-cycle / vectors with FP32 accumulation inside an
-//     FP64 refinement loop whose residual r = F - K u uses the FP64 matrix.
+//   * precision modes: FP64 throughout; "mixed" = FP64 PCG (FP64 SpMV, vectors, dots) with
+//     an FP32 preconditioner (the V-cycle's values, vectors and accumulation in FP32, FP64
+//     coarsest inverse); "fp32 IR" = FP32 PCG (FP32 SpMV) inside FP64 iterative refinement.
+//     Every mode runs inside an FP64 refinement loop whose residual r = F - K u uses the FP64
+//     matrix with compensated arithmetic.
 #include <chrono>
 #include <type_traits>
 #include <cmath>
@@ -375,6 +378,109 @@ __global__ void __launch_bounds__(kThreads) k_prec_vec(int64_t n, const T* __res
     const T zi = jacobi ? dinv[i] * ri : ri;
     z[i] = zi;
     s += (double)ri * (double)zi;
+  }
+  write_part(s, partA, sh);
+}
+
+// Block-Jacobi preconditioner (solid_solver.py:237-258): the pseudo-inverse of every BS x BS
+// diagonal block, as the reference's numpy.linalg.pinv of the 3x3 node blocks.  The diagonal
+// blocks of the assembled stiffness are symmetric (each entry and its transpose sum the same
+// element contributions in the same order), so pinv = V diag(1 / lambda) V^T from a cyclic
+// Jacobi eigen-decomposition (Golub & Van Loan, Matrix Computations, sec. 8.5), eigenvalues with
+// |lambda| <= 1e-15 max |lambda| taken as zero (numpy's default cutoff relative to the largest
+// singular value).  One thread per node in FP64; the FP32 copy serves the mixed modes.  Output
+// row-major per node: b[(node * BS + i) * BS + j].
+template <int BS>
+__global__ void k_fill_block_pinv(int64_t n_nodes, int64_t nnzb, const int32_t* __restrict__ diag_block,
+                                  const double* __restrict__ k64, double* __restrict__ b64,
+                                  float* __restrict__ b32) {
+  for (int64_t node = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; node < n_nodes;
+       node += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t db = diag_block[node];
+    double a[BS][BS], v[BS][BS];
+#pragma unroll
+    for (int i = 0; i < BS; ++i)
+#pragma unroll
+      for (int j = 0; j < BS; ++j) {
+        a[i][j] = (BS == 3) ? k64[(int64_t)(3 * i + j) * nnzb + db] : k64[db * BS * BS + i * BS + j];
+        v[i][j] = (i == j) ? 1.0 : 0.0;
+      }
+    // fixed sweep count: the cyclic method converges quadratically; 12 sweeps reach the FP64
+    // level for blocks of this size, rotations with a zero off-diagonal entry are skipped
+    for (int sweep = 0; sweep < 12; ++sweep) {
+#pragma unroll
+      for (int p = 0; p < BS - 1; ++p)
+#pragma unroll
+        for (int q = p + 1; q < BS; ++q) {
+          const double apq = a[p][q];
+          if (apq == 0.0) continue;
+          const double theta = (a[q][q] - a[p][p]) / (2.0 * apq);
+          const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+          const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+#pragma unroll
+          for (int k = 0; k < BS; ++k) {  // A <- A J (columns p, q)
+            const double akp = a[k][p], akq = a[k][q];
+            a[k][p] = c * akp - s * akq;
+            a[k][q] = s * akp + c * akq;
+          }
+#pragma unroll
+          for (int k = 0; k < BS; ++k) {  // A <- J^T A (rows p, q)
+            const double apk = a[p][k], aqk = a[q][k];
+            a[p][k] = c * apk - s * aqk;
+            a[q][k] = s * apk + c * aqk;
+          }
+          a[p][q] = a[q][p] = 0.0;
+#pragma unroll
+          for (int k = 0; k < BS; ++k) {  // V <- V J
+            const double vkp = v[k][p], vkq = v[k][q];
+            v[k][p] = c * vkp - s * vkq;
+            v[k][q] = s * vkp + c * vkq;
+          }
+        }
+    }
+    double lmax = 0.0;
+#pragma unroll
+    for (int i = 0; i < BS; ++i) lmax = fmax(lmax, fabs(a[i][i]));
+    double inv[BS];
+#pragma unroll
+    for (int i = 0; i < BS; ++i) inv[i] = (fabs(a[i][i]) > 1e-15 * lmax) ? 1.0 / a[i][i] : 0.0;
+#pragma unroll
+    for (int i = 0; i < BS; ++i)
+#pragma unroll
+      for (int j = 0; j < BS; ++j) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < BS; ++k) s += v[i][k] * inv[k] * v[j][k];
+        b64[(node * BS + i) * BS + j] = s;
+        b32[(node * BS + i) * BS + j] = (float)s;
+      }
+  }
+}
+
+// z = B^-1 r per node with the block pseudo-inverses; partA = r . z
+template <int BS, typename T>
+__global__ void __launch_bounds__(kThreads) k_prec_block(int64_t n_nodes, const T* __restrict__ r,
+                                                         const T* __restrict__ binv, T* __restrict__ z,
+                                                         double* __restrict__ partA,
+                                                         const PcgScalars* __restrict__ S) {
+  pdl_trigger();  // dependents launched programmatically may start their prologue
+  __shared__ double sh[kThreads / 32];
+  if (S->done) return;
+  double s = 0.0;
+  for (int64_t node = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; node < n_nodes;
+       node += (int64_t)gridDim.x * blockDim.x) {
+    T rv[BS];
+#pragma unroll
+    for (int j = 0; j < BS; ++j) rv[j] = r[node * BS + j];
+    const T* b = binv + node * BS * BS;
+#pragma unroll
+    for (int i = 0; i < BS; ++i) {
+      T zi = T(0);
+#pragma unroll
+      for (int j = 0; j < BS; ++j) zi += b[i * BS + j] * rv[j];
+      z[node * BS + i] = zi;
+      s += (double)rv[i] * (double)zi;
+    }
   }
   write_part(s, partA, sh);
 }
@@ -758,14 +864,15 @@ struct StreamView {
   const PackTile* tiles;
   int n_tiles;
   const unsigned char* pack;
+  StreamCtl ctl;
 };
 
 template <typename T>
 static StreamView stream_view(const StreamMat& m) {
   if constexpr (sizeof(T) == 4)
-    return {m.d32.p, m.n_tiles, m.p32.p};
+    return {m.d32.p, m.n_tiles, m.p32.p, m.ctl};
   else
-    return {m.d64.p, m.n_tiles, m.p64.p};
+    return {m.d64.p, m.n_tiles, m.p64.p, m.ctl};
 }
 
 // Launched with programmatic stream serialisation (launch_pdl): the first tiles of the matrix
@@ -778,7 +885,7 @@ __global__ void __launch_bounds__(kStreamThreads, (StreamDefault<T, BR, BC>::kCt
   pdl_trigger();
   bool skipped = false;
   const double dot = stream_rows<T, BR, BC, typename StreamDefault<T, BR, BC>::type>(
-      m.tiles, m.n_tiles, m.pack, xf, epi, smem, &S->status, &S->done, &skipped);
+      m.tiles, m.n_tiles, m.pack, xf, epi, smem, &S->status, &S->done, m.ctl, &skipped);
   if (part && !skipped) write_part(dot, part, sh);
 }
 
@@ -838,7 +945,7 @@ __global__ void __launch_bounds__(kStreamThreads, (StreamDefault<TK, BS, BS>::kC
   bool skipped = false;
   const double dot = stream_rows<TK, BS, BS, typename StreamDefault<TK, BS, BS>::type>(
       m.tiles, m.n_tiles, m.pack, XPNewS<TK, TM>{z, p_old, rz_beta + 1},
-      EpiSpmvDotS<TK, TM>{z, p_old, rz_beta + 1, p_new, q}, smem, &S->status, &S->done, &skipped,
+      EpiSpmvDotS<TK, TM>{z, p_old, rz_beta + 1, p_new, q}, smem, &S->status, &S->done, m.ctl, &skipped,
       BetaHook{partA, nparts, first, par, S, sh, rz_beta});
   if (skipped) return;
   write_part(dot, partB, sh);
@@ -920,6 +1027,7 @@ struct Prec<double> {
   static double* cx(AmgHierarchy& h) { return h.cx64.p; }
   static PcgVecs<double>& pcg(SolverWork& w) { return w.p64; }
   static const double* fine_dinv(SolverWork& w) { return w.dinv64.p; }
+  static const double* fine_binv(SolverWork& w) { return w.binv64.p; }
 };
 template <>
 struct Prec<float> {
@@ -933,6 +1041,7 @@ struct Prec<float> {
   static float* cx(AmgHierarchy& h) { return h.cx32.p; }
   static PcgVecs<float>& pcg(SolverWork& w) { return w.p32; }
   static const float* fine_dinv(SolverWork& w) { return w.dinv32.p; }
+  static const float* fine_binv(SolverWork& w) { return w.binv32.p; }
 };
 
 template <int BS, typename T>
@@ -1070,6 +1179,20 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
 template <typename T>
 static int apply_prec(Solid* s, SolverWork& W, int precond, const T* r, T* z, PcgScalars* S, cudaStream_t st) {
   if (precond == 2) return vcycle<T>(s, *s->amg, W, 0, r, z, W.partA.p, S, st);
+  if (precond == 3) {
+    auto launch = [&](auto kern) {
+      const int g = resident_grid(kern, kThreads, (s->n_nodes + kThreads - 1) / kThreads);
+      W.npA = g;
+      kern<<<g, kThreads, 0, st>>>(s->n_nodes, r, Prec<T>::fine_binv(W), z, W.partA.p, S);
+    };
+    if (s->bs == 3)
+      launch(k_prec_block<3, T>);
+    else
+      launch(k_prec_block<6, T>);
+    W.launches++;
+    WN_CUDA(cudaGetLastError());
+    return 0;
+  }
   const int gp = resident_grid(k_prec_vec<T>, kThreads, (W.n + kThreads - 1) / kThreads);
   W.npA = gp;
   k_prec_vec<T><<<gp, kThreads, 0, st>>>(W.n, r, Prec<T>::fine_dinv(W), precond == 1 ? 1 : 0, z,
@@ -1430,7 +1553,8 @@ static int outer_loop(Solid* s, SolverWork& W, int mode, const double* F, double
 int solver_solve(Solid* s, const double* F, double* u, const wn_solve_params& prm, wn_solve_stats* stats,
                  cudaStream_t st) {
   WN_REQUIRE(s->assembled, WN_ESTATE, "solve: matrix not assembled");
-  WN_REQUIRE(prm.precond >= 0 && prm.precond <= 2, WN_EINVAL, "solve: precond must be 0 (none), 1 (jacobi), 2 (amg)");
+  WN_REQUIRE(prm.precond >= 0 && prm.precond <= 3, WN_EINVAL,
+             "solve: precond must be 0 (none), 1 (jacobi), 2 (amg) or 3 (block jacobi)");
   WN_REQUIRE(prm.precision >= 0 && prm.precision <= 2, WN_EINVAL,
              "solve: precision must be 0 (fp64), 1 (mixed: fp32 AMG in fp64 PCG) or 2 (fp32 PCG in fp64 refinement)");
   WN_REQUIRE(prm.max_iter > 0 && prm.rtol > 0.0, WN_EINVAL, "solve: max_iter > 0 and rtol > 0 required");
@@ -1448,6 +1572,21 @@ int solver_solve(Solid* s, const double* F, double* u, const wn_solve_params& pr
   k_fill_dinv<<<vec_grid(n), kThreads, 0, st>>>(s->n_nodes, s->bs, s->nnzb, s->diag_block.p, s->k64.p, W.dinv64.p,
                                                  W.dinv32.p);
   W.launches++;
+  if (prm.precond == 3) {  // block pseudo-inverses of the current values
+    const int64_t nb = s->n_nodes * s->bs * s->bs;
+    if (W.binv64.n != nb) {
+      WN_CHECK(W.binv64.alloc(nb));
+      WN_CHECK(W.binv32.alloc(nb));
+    }
+    if (s->bs == 3)
+      k_fill_block_pinv<3><<<grid_for(s->n_nodes, 1, 128, 8), 128, 0, st>>>(s->n_nodes, s->nnzb, s->diag_block.p,
+                                                                             s->k64.p, W.binv64.p, W.binv32.p);
+    else
+      k_fill_block_pinv<6><<<grid_for(s->n_nodes, 1, 128, 8), 128, 0, st>>>(s->n_nodes, s->nnzb, s->diag_block.p,
+                                                                             s->k64.p, W.binv64.p, W.binv32.p);
+    W.launches++;
+    WN_CUDA(cudaGetLastError());
+  }
   WN_CUDA(cudaEventRecord(W.ev0, st));
   W.npC = resident_grid(k_dot_self<double>, kThreads, (n + kThreads - 1) / kThreads);
   k_dot_self<double><<<W.npC, kThreads, 0, st>>>(n, F, W.partC.p);

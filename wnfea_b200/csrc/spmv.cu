@@ -63,30 +63,35 @@ template <typename T>
 __global__ void __launch_bounds__(kStreamThreads, (StreamDefault<T, 3, 3>::kCtasPerSm)) k_stream_spmv(const PackTile* __restrict__ tiles, int n_tiles,
                                                                    const unsigned char* __restrict__ pack,
                                                                    const T* __restrict__ x, T* __restrict__ y,
-                                                                   int* __restrict__ status) {
+                                                                   int* __restrict__ status, StreamCtl ctl) {
   extern __shared__ __align__(128) unsigned char smem[];
   stream_rows<T, 3, 3, typename StreamDefault<T, 3, 3>::type>(tiles, n_tiles, pack, XLoad<T, T>{x}, EpiY<T>{y},
-                                                               smem, status, nullptr);
+                                                               smem, status, nullptr, ctl);
 }
 
 template <typename T>
 static int launch_stream(const PackTile* tiles, int n_tiles, const unsigned char* pack, const T* x, T* y, int* status,
-                         cudaStream_t st) {
+                         StreamCtl ctl, cudaStream_t st) {
   if (!tiles || !pack || n_tiles == 0) return 0;
   auto kern = k_stream_spmv<T>;
   const int per_sm =
       stream_ctas_per_sm(reinterpret_cast<const void*>(kern), kStreamThreads, stream_smem_bytes<T, 3, 3>());
   if (per_sm < 1) return 0;
   const int grid = std::max(1, std::min(n_tiles, kNumSMs * per_sm));
-  kern<<<grid, kStreamThreads, stream_smem_bytes<T, 3, 3>(), st>>>(tiles, n_tiles, pack, x, y, status);
+  kern<<<grid, kStreamThreads, stream_smem_bytes<T, 3, 3>(), st>>>(tiles, n_tiles, pack, x, y, status, ctl);
   WN_CUDA(cudaGetLastError());
   return 1;
 }
 
 int launch_solid_spmv_stream(int precision, const PackTile* tiles, int n_tiles, const unsigned char* pack,
-                             const void* x, void* y, int* status, cudaStream_t st) {
-  if (precision == 0) return launch_stream<double>(tiles, n_tiles, pack, (const double*)x, (double*)y, status, st);
-  return launch_stream<float>(tiles, n_tiles, pack, (const float*)x, (float*)y, status, st);
+                             const void* x, void* y, int* status, unsigned long long wait_ns, int withhold,
+                             cudaStream_t st) {
+  StreamCtl ctl;
+  ctl.wait_ns = wait_ns;
+  ctl.withhold = withhold;
+  if (precision == 0)
+    return launch_stream<double>(tiles, n_tiles, pack, (const double*)x, (double*)y, status, ctl, st);
+  return launch_stream<float>(tiles, n_tiles, pack, (const float*)x, (float*)y, status, ctl, st);
 }
 
 int launch_solid_spmv_f64(int64_t n_rows, const int32_t* rp, const int32_t* ci, const double* v, int64_t nnzb,

@@ -200,7 +200,18 @@ __global__ void __launch_bounds__(256) k_pack_tiles(int n_tiles, const StreamTil
   }
 }
 
-constexpr unsigned long long kStreamWaitLimitNs = 4000000000ull;  // 4 s
+// Bounded waits of the pipeline.  ctl.wait_ns bounds every stage wait (consumers waiting for a
+// tile, the producer waiting for a free stage); the host sets it per matrix (default 4 s).  After
+// a failure the copies still in flight are drained with their own fixed limit, so a short
+// ctl.wait_ns never lets a CTA exit before its copies have landed.  ctl.withhold >= 0 is the
+// failure-detection test hook: the producer skips that tile's copy (nothing arms its stage), so
+// the consumers' wait for it must run out and the call must report WN_ETIMEOUT.
+constexpr unsigned long long kStreamWaitLimitNs = 4000000000ull;   // 4 s: default stage-wait limit
+constexpr unsigned long long kStreamDrainLimitNs = 4000000000ull;  // 4 s: drain of issued copies
+struct StreamCtl {
+  unsigned long long wait_ns = kStreamWaitLimitNs;
+  int withhold = -1;  // tile index withheld by the producer (tests only), -1: none
+};
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -248,29 +259,31 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
       : "memory");
 }
 
-// one thread: wait for the phase of `parity` to complete; false after the time limit or when
+// one thread: wait for the phase of `parity` to complete; false after limit_ns or when
 // `abort_flag` is raised (abort_flag may be null)
-__device__ __forceinline__ bool wait_thread(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+__device__ __forceinline__ bool wait_thread(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                            unsigned long long limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   for (uint32_t n = 1;; ++n) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((n & 63) == 0) {
       if (abort_flag && *abort_flag) return false;
-      if (global_ns() - t0 > kStreamWaitLimitNs) return false;
+      if (global_ns() - t0 > limit_ns) return false;
     }
   }
 }
 
 // a full warp: every lane polls, the warp leaves together (all lanes saw the phase complete,
 // or one lane saw the limit / the abort flag)
-__device__ __forceinline__ bool wait_warp(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+__device__ __forceinline__ bool wait_warp(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                          unsigned long long limit_ns) {
   if (__all_sync(0xffffffffu, mbar_try_wait(bar, parity))) return true;
   const unsigned long long t0 = global_ns();
   for (uint32_t n = 1;; ++n) {
     if (__all_sync(0xffffffffu, mbar_try_wait(bar, parity))) return true;
     if ((n & 63) == 0) {
-      const bool stop = *abort_flag != 0 || global_ns() - t0 > kStreamWaitLimitNs;
+      const bool stop = *abort_flag != 0 || global_ns() - t0 > limit_ns;
       if (__any_sync(0xffffffffu, stop)) return false;
     }
   }
@@ -305,12 +318,13 @@ __device__ __forceinline__ T pick_lane(const T (&a)[N], int l) {
 // The first stages' copies (the matrix only) are issued before pdl_wait(), so under a
 // programmatic dependent launch they overlap the predecessor's tail; then every thread runs
 // hook(), and when *done is set (read after the wait) the CTA lets those copies land and
-// returns with *skipped = true.
+// returns with *skipped = true.  Every warp of the CTA meets once more at the end; if any wait
+// ran out, one thread then waits (bounded) for the copies still in flight before the CTA exits.
 template <typename T, int BR, int BC, typename Cfg, typename XF, typename EPI, typename HOOK = NoHook>
 __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles, int n_tiles,
                                               const unsigned char* __restrict__ pack, const XF& xf, const EPI& epi,
-                                              unsigned char* smem, int* status, int* done, bool* skipped = nullptr,
-                                              const HOOK& hook = HOOK{}) {
+                                              unsigned char* smem, int* status, int* done, const StreamCtl ctl,
+                                              bool* skipped = nullptr, const HOOK& hook = HOOK{}) {
   constexpr int NV = BR * BC;
   constexpr int STAGES = Cfg::kStages;
   constexpr uint32_t SB = Cfg::template stage_bytes<T, NV>();
@@ -371,9 +385,9 @@ __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles
       }
       if (lane == 0) {
         const int s = j % STAGES;
-        if (j >= STAGES && !wait_thread(empty + s, (uint32_t)((j / STAGES - 1) & 1), abort_flag)) {
+        if (j >= STAGES && !wait_thread(empty + s, (uint32_t)((j / STAGES - 1) & 1), abort_flag, ctl.wait_ns)) {
           ok = false;
-        } else {
+        } else if (tb + j != ctl.withhold) {
           descs[s] = d;
           const uint32_t bytes = pack_bytes<T, NV>(d.w, d.y - d.x);
           mbar_arrive_expect_tx(full + s, bytes);
@@ -396,102 +410,109 @@ __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles
   hook();
   const bool skip = *skip_flag != 0;
   if (skipped) *skipped = skip;
+  // the copies issued so far (j tiles processed by the producer) into this CTA's stages: for each
+  // stage, wait (bounded) for the phase of the last tile actually copied into it
+  auto drain = [&]() {
+    for (int s = 0; s < STAGES && s < j; ++s) {
+      int t = s + STAGES * ((j - 1 - s) / STAGES);  // last tile processed into stage s
+      if (tb + t == ctl.withhold) t -= STAGES;        // withheld: its predecessor was the last copy
+      if (t >= 0) wait_thread(full + s, (uint32_t)((t / STAGES) & 1), nullptr, kStreamDrainLimitNs);
+    }
+  };
   if (skip) {  // let the copies already issued land before the CTA can exit
-    if (warp == NCW && lane == 0)
-      for (int s = 0; s < pre; ++s) wait_thread(full + s, 0u, nullptr);
+    if (warp == NCW && lane == 0) drain();
     return 0.0;
   }
 
+  const int gl = lane % G, grp = lane / G;
   if (warp == NCW) {
     issue(n_my);
-    if (lane == 0 && !ok) {
-      fail();
-      // let the copies already issued land before the CTA can exit
-      for (int s = 0; s < STAGES && s < j; ++s) wait_thread(full + s, (uint32_t)(((j - 1 - s) / STAGES) & 1), nullptr);
-    }
+    if (lane == 0 && !ok) fail();
     __syncwarp();
-    return 0.0;
-  }
-
-  // consumer warps
-  const int gl = lane % G, grp = lane / G;
-  for (j = 0; j < n_my; ++j) {
-    const int s = j % STAGES;
-    if (!wait_warp(full + s, (uint32_t)((j / STAGES) & 1), abort_flag)) {
-      if (lane == 0) fail();
-      break;
-    }
-    const unsigned char* st = stages + (size_t)s * SB;
-    const int4 d = descs[s];
-    const int r0 = d.x, nr = d.y - d.x, cntp = d.w;
-    const T* sv = reinterpret_cast<const T*>(st);
-    const int32_t* scol = reinterpret_cast<const int32_t*>(st + pack_col_off<T, NV>(cntp));
-    const uint16_t* srp = reinterpret_cast<const uint16_t*>(st + pack_row_off<T, NV>(cntp));
-    // warps take the tile's rows round-robin in passes of GPW * R rows (group g of a pass owns
-    // rows base + q GPW + g, q < R), starting from a warp that rotates per tile
-    const int wslot = (warp + j) % NCW;
-    for (int base = wslot * GPW * R; base < nr; base += NCW * GPW * R) {
-      int rs[R], re[R];
-      typename EPI::Pre pre[R];
-      T acc[R][BR];
-      int len = 0;
-#pragma unroll
-      for (int q = 0; q < R; ++q) {
-        const int lr = base + q * GPW + grp;
-        const bool active = lr < nr;
-        rs[q] = active ? srp[lr] : 0;
-        re[q] = active ? srp[lr + 1] : 0;
-        len = max(len, re[q] - rs[q]);
-        pre[q] = typename EPI::Pre{};
-        if (active && gl < BR) pre[q] = epi.load((int64_t)(r0 + lr) * BR + gl);
-#pragma unroll
-        for (int r = 0; r < BR; ++r) acc[q][r] = T(0);
+  } else {
+    // consumer warps
+    for (int jc = 0; jc < n_my; ++jc) {
+      const int s = jc % STAGES;
+      if (!wait_warp(full + s, (uint32_t)((jc / STAGES) & 1), abort_flag, ctl.wait_ns)) {
+        if (lane == 0) fail();
+        break;
       }
-      // U blocks of each of the R rows in flight per lane: their gathers are issued before the
-      // first multiply-add; each row's sum still runs over the lane's blocks in order
-      // (b, b + G, b + 2G, ...)
-      for (int o = gl; o < len; o += G * U) {
-        int col[R][U];
-        T xv[R][U][BC];
+      const unsigned char* st = stages + (size_t)s * SB;
+      const int4 d = descs[s];
+      const int r0 = d.x, nr = d.y - d.x, cntp = d.w;
+      const T* sv = reinterpret_cast<const T*>(st);
+      const int32_t* scol = reinterpret_cast<const int32_t*>(st + pack_col_off<T, NV>(cntp));
+      const uint16_t* srp = reinterpret_cast<const uint16_t*>(st + pack_row_off<T, NV>(cntp));
+      // warps take the tile's rows round-robin in passes of GPW * R rows (group g of a pass owns
+      // rows base + q GPW + g, q < R), starting from a warp that rotates per tile
+      const int wslot = (warp + jc) % NCW;
+      for (int base = wslot * GPW * R; base < nr; base += NCW * GPW * R) {
+        int rs[R], re[R];
+        typename EPI::Pre pre[R];
+        T acc[R][BR];
+        int len = 0;
 #pragma unroll
-        for (int q = 0; q < R; ++q)
+        for (int q = 0; q < R; ++q) {
+          const int lr = base + q * GPW + grp;
+          const bool active = lr < nr;
+          rs[q] = active ? srp[lr] : 0;
+          re[q] = active ? srp[lr + 1] : 0;
+          len = max(len, re[q] - rs[q]);
+          pre[q] = typename EPI::Pre{};
+          if (active && gl < BR) pre[q] = epi.load((int64_t)(r0 + lr) * BR + gl);
 #pragma unroll
-          for (int u = 0; u < U; ++u) col[q][u] = (rs[q] + o + u * G < re[q]) ? scol[rs[q] + o + u * G] : 0;
-#pragma unroll
-        for (int q = 0; q < R; ++q)
-#pragma unroll
-          for (int u = 0; u < U; ++u)
-#pragma unroll
-            for (int c = 0; c < BC; ++c) xv[q][u][c] = xf((int64_t)col[q][u] * BC + c);
-#pragma unroll
-        for (int q = 0; q < R; ++q)
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            const int b = rs[q] + o + u * G;
-            if (b < re[q]) {
-#pragma unroll
-              for (int r = 0; r < BR; ++r)
-#pragma unroll
-                for (int c = 0; c < BC; ++c) acc[q][r] = fma(sv[(r * BC + c) * cntp + b], xv[q][u][c], acc[q][r]);
-            }
-          }
-      }
-#pragma unroll
-      for (int q = 0; q < R; ++q) {
-#pragma unroll
-        for (int r = 0; r < BR; ++r) {
-          T v = acc[q][r];
-#pragma unroll
-          for (int o2 = G / 2; o2 > 0; o2 >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o2);
-          acc[q][r] = v;
+          for (int r = 0; r < BR; ++r) acc[q][r] = T(0);
         }
-        const int lr = base + q * GPW + grp;
-        if (lr < nr && gl < BR) dot += epi.store((int64_t)(r0 + lr) * BR + gl, pre[q], pick_lane<BR>(acc[q], gl));
+        // U blocks of each of the R rows in flight per lane: their gathers are issued before the
+        // first multiply-add; each row's sum still runs over the lane's blocks in order
+        // (b, b + G, b + 2G, ...)
+        for (int o = gl; o < len; o += G * U) {
+          int col[R][U];
+          T xv[R][U][BC];
+#pragma unroll
+          for (int q = 0; q < R; ++q)
+#pragma unroll
+            for (int u = 0; u < U; ++u) col[q][u] = (rs[q] + o + u * G < re[q]) ? scol[rs[q] + o + u * G] : 0;
+#pragma unroll
+          for (int q = 0; q < R; ++q)
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+              for (int c = 0; c < BC; ++c) xv[q][u][c] = xf((int64_t)col[q][u] * BC + c);
+#pragma unroll
+          for (int q = 0; q < R; ++q)
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              const int b = rs[q] + o + u * G;
+              if (b < re[q]) {
+#pragma unroll
+                for (int r = 0; r < BR; ++r)
+#pragma unroll
+                  for (int c = 0; c < BC; ++c) acc[q][r] = fma(sv[(r * BC + c) * cntp + b], xv[q][u][c], acc[q][r]);
+              }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+#pragma unroll
+          for (int r = 0; r < BR; ++r) {
+            T v = acc[q][r];
+#pragma unroll
+            for (int o2 = G / 2; o2 > 0; o2 >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o2);
+            acc[q][r] = v;
+          }
+          const int lr = base + q * GPW + grp;
+          if (lr < nr && gl < BR) dot += epi.store((int64_t)(r0 + lr) * BR + gl, pre[q], pick_lane<BR>(acc[q], gl));
+        }
       }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(empty + s);
     }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(empty + s);
   }
+  // every warp meets here; after a failure (some wait ran out, or the abort flag was raised)
+  // the producer's lane 0 waits for the copies it issued before the CTA can exit
+  __syncthreads();
+  if (*abort_flag && warp == NCW && lane == 0) drain();
   return dot;
 }
 

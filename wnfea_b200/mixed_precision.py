@@ -1,14 +1,22 @@
-"""Precision configuration (wnfea/solver/mixed_precision.py:23-106).
+"""Precision configuration (wnfea/solver/mixed_precision.py:23-122).
 
-``PrecisionConfig`` and the presets keep the reference's fields.  On this path they select
-the solver precision: ``enabled`` with ``inner_dtype = float32`` means FP32 inner PCG + AMG
-(FP32 values, FP32 accumulation, FP64 dot products) inside FP64 iterative refinement
-(``precision="mixed_fp32"``); ``FULL_FP64`` is the plain FP64 path.  The FP16
-``TRI_PRECISION`` preset is accepted and runs as ``MIXED_FP32`` (no FP16 V-cycle here).
+``PrecisionConfig``, the presets and the cast helpers keep the reference's fields and names.
+On this path a configuration selects the solver's ``precision`` argument
+(``solver_precision``):
+
+* ``enabled`` with ``inner_dtype = float32`` -> ``"mixed_fp32"``: FP64 PCG (FP64 SpMV, vectors
+  and dot products) preconditioned in FP32 (the AMG V-cycle with FP32 values, vectors and
+  accumulation and an FP64 coarsest inverse), inside the FP64 true-residual loop;
+* otherwise (``FULL_FP64``) -> ``"fp64"``.
+
+The reference's ``TRI_PRECISION`` adds an FP16 preconditioner for the early iterations
+(``use_tri_precision``).  This path has no FP16 V-cycle: asking a tri-precision configuration
+for its solver precision warns and selects ``"mixed_fp32"``.
 """
 
 from __future__ import annotations
 
+import warnings
 from dataclasses import dataclass
 
 import numpy as np
@@ -24,22 +32,52 @@ class PrecisionConfig:
     enabled: bool = True
 
     @property
+    def inner_eps_scale(self) -> float:
+        """sqrt(eps) of the inner dtype (mixed_precision.py:66-69)."""
+        return float(np.sqrt(np.finfo(self.inner_dtype).eps))
+
+    @property
+    def outer_eps_scale(self) -> float:
+        """sqrt(eps) of the outer dtype (mixed_precision.py:71-74)."""
+        return float(np.sqrt(np.finfo(self.outer_dtype).eps))
+
+    @property
     def working_dtype(self):
         return np.dtype(self.inner_dtype) if self.enabled else np.dtype(self.outer_dtype)
 
     @property
     def solver_precision(self) -> str:
         """The ``precision`` argument of solve_c3d10_pcg this configuration selects."""
+        if self.enabled and self.use_tri_precision:
+            warnings.warn("tri-precision (FP16 preconditioner) is not available on this path; "
+                          "the solve runs as mixed_fp32 (FP32 preconditioner in FP64 PCG)", UserWarning,
+                          stacklevel=2)
         return "mixed_fp32" if self.enabled and np.dtype(self.inner_dtype) == np.float32 else "fp64"
 
     def summary(self) -> str:
         if not self.enabled:
             return f"Uniform {np.dtype(self.outer_dtype).name} (mixed precision disabled)"
-        return (f"Mixed precision: inner={np.dtype(self.inner_dtype).name} (PCG/AMG), "
-                f"outer={np.dtype(self.outer_dtype).name} (residual/accumulation)")
+        inner = np.dtype(self.inner_dtype).name
+        outer = np.dtype(self.outer_dtype).name
+        if self.use_tri_precision:
+            return (f"Tri-precision requested: runs as inner={inner} preconditioner in {outer} PCG "
+                    f"(no FP16 V-cycle on this path)")
+        return f"Mixed precision: {outer} PCG/residual/dots, {inner} preconditioner (AMG V-cycle)"
 
 
 MIXED_FP32 = PrecisionConfig(inner_dtype=np.float32, outer_dtype=np.float64, enabled=True, use_tri_precision=False)
 TRI_PRECISION = PrecisionConfig(inner_dtype=np.float32, outer_dtype=np.float64, precond_coarse_dtype=np.float16,
                                 switch_tol=1e-2, use_tri_precision=True, enabled=True)
 FULL_FP64 = PrecisionConfig(inner_dtype=np.float64, outer_dtype=np.float64, enabled=False, use_tri_precision=False)
+
+
+def cast_to_inner(arr: np.ndarray, config: PrecisionConfig) -> np.ndarray:
+    """``arr`` in the configuration's working dtype (mixed_precision.py:109-114)."""
+    target = config.working_dtype
+    return arr if arr.dtype == target else arr.astype(target, copy=False)
+
+
+def cast_to_outer(arr: np.ndarray, config: PrecisionConfig) -> np.ndarray:
+    """``arr`` in the outer (accumulation) dtype (mixed_precision.py:117-122)."""
+    target = np.dtype(config.outer_dtype)
+    return arr if arr.dtype == target else arr.astype(target, copy=False)

@@ -54,7 +54,7 @@ def assemble_c3d10_sparse_3dof(model: FEAModel, apply_bcs: bool = True):
     return BSR3Matrix(system), F, fixed
 
 
-_PRECOND = {"none": 0, "jacobi": 1, "amg": 2}
+_PRECOND = {"none": 0, "jacobi": 1, "amg": 2, "block_jacobi": 3}
 _PRECISION = {"fp64": 0, "mixed_fp32": 1, "mixed_fp32_ir": 2}
 
 
@@ -63,7 +63,7 @@ def solve_c3d10_pcg(
     F: np.ndarray,
     rtol: float = 1e-6,
     max_iter: int = 2000,
-    preconditioner: str = "amg",
+    preconditioner: str = "jacobi",
     precision: str = "fp64",
     amg_params=None,
     inner_rtol: float = 0.0,
@@ -71,17 +71,20 @@ def solve_c3d10_pcg(
 ):
     """PCG on the GPU -> (u, iterations, final_rel_res, solve_time_sec) (solid_solver.py:197-308).
 
-    ``preconditioner``: "amg" (smoothed aggregation, default), "jacobi" (point Jacobi, the
-    reference's default) or "none".  ``precision``:
+    Defaults are the reference's (rtol 1e-6, 2000 iterations, point Jacobi, FP64).
+    ``preconditioner``: "jacobi" (point Jacobi, :228-236), "block_jacobi" (pseudo-inverse of
+    every 3x3 node block, :237-258), "none", or "amg" (smoothed-aggregation AMG V-cycle; no
+    reference counterpart for solids, and the fast choice for large meshes).  ``precision``:
 
-    * "fp64"          -- FP64 matrix, vectors, V-cycle;
-    * "mixed_fp32"    -- FP64 PCG (FP64 SpMV, vectors, dots) preconditioned by an FP32 AMG
-                         V-cycle (FP32 values, vectors and accumulation; FP64 coarsest
-                         inverse), inside the FP64 true-residual loop;
-    * "mixed_fp32_ir" -- the reference's mixed mode (:271-300): FP32 PCG (FP32 SpMV) inside
-                         FP64 iterative refinement.  Converges slowly once cond(K) * 6e-8
-                         approaches 1 (an FP32 SpMV cannot resolve smooth displacement
-                         fields: K u cancels ~8 digits per row); fine for small meshes.
+    * "fp64"          -- FP64 matrix, vectors, dots and preconditioner;
+    * "mixed_fp32"    -- FP64 PCG (FP64 SpMV, vectors and dots) with the preconditioner in FP32
+                         (for "amg": FP32 V-cycle values, vectors and accumulation, FP64
+                         coarsest inverse), inside the FP64 true-residual loop;
+    * "mixed_fp32_ir" -- the scheme of the reference's mixed mode (:271-300): FP32 PCG (FP32
+                         SpMV, FP32 preconditioner, FP64 dots) inside FP64 iterative
+                         refinement.  Converges slowly once cond(K) * 6e-8 approaches 1 (an
+                         FP32 SpMV cannot resolve smooth displacement fields: K u cancels ~8
+                         digits per row); fine for small meshes.
 
     All modes stop on the true FP64 residual ||F - K u|| <= rtol ||F||.  The returned
     iteration count is the real one (the reference stores scipy's ``info`` there,
@@ -142,10 +145,10 @@ def solve_c3d10_system(
     method: str = "auto",
     rtol: float = 1e-6,
     max_iter: int = 2000,
-    preconditioner: str = "amg",
+    preconditioner: str = "jacobi",
     precision: str = "fp64",
 ):
-    """Unified solve -> (u, stats) (solid_solver.py:132-194).
+    """Unified solve -> (u, stats) (solid_solver.py:132-194); defaults are the reference's.
 
     ``method``: "pcg" (GPU PCG), "auto" (the same: the GPU path has no size threshold), or
     "direct" -- the reference's SuperLU branch (:164-183) has no GPU counterpart here and
