@@ -1,14 +1,14 @@
-"""Benchmark of the C3D10 solve path on B200 -- one JSON line on stdout (rank 0).
+"""Benchmark of the C3D10 solve path on B200 -- one JSON line on stdout (rank 0); the full
+per-workload detail goes to stderr as one more JSON object.
 
-Workload (default): the 200,340-element structured C3D10 I-beam (L = 4 m, 337,585 nodes,
-1,012,755 DOFs, seeded 5 % corner jitter, root clamped, 50 kN tip shear), assembled on the
-GPU, smoothed-aggregation AMG built once; one *step* is one solve K u = F to a true relative
-residual of 1e-8:
+Workload (default, the headline): the 200,340-element structured C3D10 I-beam (L = 4 m,
+337,585 nodes, 1,012,755 DOFs, seeded 5 % corner jitter, root clamped, 50 kN tip shear),
+assembled on the GPU, smoothed-aggregation AMG built once; one *step* is one solve K u = F to a
+true relative residual of 1e-8:
 
 * ``value``  -- DOF/s of the mixed-precision solve (FP64 PCG with an FP32 AMG V-cycle, FP64
                 dots and coarsest solve, stopped on the true FP64 residual), device-resident
                 F/u, CUDA events on the launching stream;
-* ``fp64``   -- the same with the plain FP64 AMG-PCG, for the mixed vs FP64 ratio;
 * ``e2e``    -- the same metric through the public API ``solve_c3d10_system`` with host
                 (numpy) F and u, the host<->device copies inside the timed region;
 * ``roofline`` -- the fine-level FP32 BSR3 SpMV (the kernel class that every fused V-cycle
@@ -16,11 +16,17 @@ residual of 1e-8:
                 event-timed launch duration vs the measured HBM copy bandwidth;
 * ``cpu_baseline`` -- the reference's own CPU algorithm for this solve (scipy ``cg`` with the
                 point-Jacobi preconditioner, solid_solver.py:197-266, restated in the oracle),
-                timed on a bounded sample of iterations on this host and extrapolated to the
-                iteration count that algorithm needs at this size (measured by the GPU
-                Jacobi-PCG, which reproduces scipy's count).
+                timed on a bounded sample of iterations on this host and multiplied by the
+                iteration count the reference's own solve needed on this I-beam (a recorded
+                run of the reference, tests/golden/ibeam_reference_jacobi.json).
 
-``--impl reference`` runs only that CPU baseline, as the reference arm.  With N > 1 GPUs
+The line ends with the other precision modes and preconditioners on the same I-beam (FP64 AMG,
+the FP32-SpMV refinement of the reference's mixed scheme, GPU point-Jacobi PCG -- the
+reference's algorithm), the 480-element cantilever, the 10 x 10 co-rotational frame (10 load
+steps of Newton), the 32 batched load cases, the 162,000-element adjoint block, assembly and
+internal force, so that every configuration's headline number is in the line.
+
+``--impl reference`` runs only the CPU baseline, as the reference arm.  With N > 1 GPUs
 (torchrun) every rank solves its own replica (the solve does not shard): weak scaling,
 value = sum over ranks of DOF/s, timed as the max over ranks.
 """
@@ -28,6 +34,7 @@ value = sum over ranks of DOF/s, timed as the max over ranks.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -43,10 +50,30 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "C3D10 solve time & DOF/s, mixed vs FP64 GPU at rel.res 1e-8; adjoint grad ms"
-# Jacobi-PCG iterations to rel. res 1e-8 on the default I-beam, measured on a B200 by this
-# script's GPU arm (``jacobi_pcg_iterations`` in its output); used by the CPU-only
-# reference arm, which cannot afford to run the solve to convergence.
-JACOBI_ITERS_IBEAM = 48507
+# the reference's own Jacobi-PCG solve of the default I-beam, run to convergence on one host
+# core by tests/golden/make_ibeam_reference.py (iteration count, seconds per iteration)
+REFERENCE_RUN = ROOT / "tests" / "golden" / "ibeam_reference_jacobi.json"
+# measured here with the reference's own code (solid_solver.py) on the 480-element cantilever
+# and the 10 x 10 frame: context figures for the cantilever and frame lines
+REF_PROBE = {"c1_jacobi_pcg_s": 0.150, "c1_spsolve_s": 0.0187, "c2_jfnk_10_steps_s": 4.39}
+
+
+def _r(v, n=4):
+    """v rounded to n significant digits (keeps the JSON line short)."""
+    if v is None or isinstance(v, (bool, int, str)):
+        return v
+    if isinstance(v, dict):
+        return {k: _r(x, n) for k, x in v.items()}
+    if isinstance(v, (list, tuple)):
+        return [_r(x, n) for x in v]
+    v = float(v)
+    return float(f"{v:.{n}g}") if np.isfinite(v) else None
+
+
+def reference_run():
+    if REFERENCE_RUN.exists():
+        return json.loads(REFERENCE_RUN.read_text())
+    return None
 
 
 def parse():
@@ -67,7 +94,8 @@ def parse():
     ap.add_argument("--cases", type=int, default=32, help="load cases of the batched (multi-RHS) solve")
     ap.add_argument("--order", choices=["native", "scrambled", "rcm"], default="native",
                     help="profiling mode: node numbering -- the generator's, a seeded random one, or RCM of that")
-    ap.add_argument("--only", choices=["solve-mixed", "solve-fp64", "solve-multi", "spmv32", "spmv64", "frame"],
+    ap.add_argument("--only", choices=["solve-mixed", "solve-fp64", "solve-multi", "spmv32", "spmv64", "frame",
+                                       "assemble"],
                     default=None,
                     help="profiling mode: run only this operation (warmup + steps times) and print its time")
     return ap.parse_args()
@@ -115,6 +143,11 @@ def run_only(args):
             _lib.call("wn_solve_device", s.handle, F.data_ptr(), u.data_ptr(), prm, stt, st)
             info.update(iterations=stt.iterations, outer=stt.outer_iterations, rel_res=stt.rel_res,
                         device_ms=stt.solve_seconds * 1e3)
+    elif args.only == "assemble":
+        d_props = torch.from_numpy(np.ascontiguousarray(s.props)).cuda()
+
+        def op():
+            _lib.call("wn_assemble_c3d10_device", s.handle, d_props.data_ptr(), 1, st)
     else:
         prec = 1 if args.only == "spmv32" else 0
         dt = torch.float32 if prec else torch.float64
@@ -254,31 +287,51 @@ def cpu_jacobi_sample(Kcsr, F, iters):
 
 
 def run_reference(args):
+    """The reference arm: the reference's CPU solve algorithm (oracle restatement of
+    solve_c3d10_pcg's default branch -- scipy cg + point Jacobi, solid_solver.py:197-266) on the
+    host cores, on the same I-beam.  Each step times a bounded sample of ``--cpu-iters``
+    iterations on the full matrix; the solve time is that rate times the iteration count the
+    reference's own solve needed on this I-beam (a recorded run to convergence, see
+    REFERENCE_RUN).  The 480-element cantilever is solved to convergence for real (Jacobi-PCG
+    and scipy's direct solve)."""
     import scipy.sparse as sp  # noqa: F401
+    from scipy.sparse.linalg import spsolve
 
     from oracle import solid
+    from wnfea_b200.mesh import generate_c3d10_kuhn_block
     from wnfea_b200.model import solid_element_props, solid_fixed_dofs, solid_load_vector
 
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    ref = reference_run()
+    if args.slices != 315 or ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "no recorded reference Jacobi-PCG run for this I-beam "
+                                                              f"({args.slices} slices)"}))
+        return
     m, meta = build_model(args.slices)
     ndof = meta["n_dofs"]
     K, F, _ = solid.assemble(m.mesh_nodes, m.solid_elements, solid_element_props(m), solid_load_vector(m),
                              solid_fixed_dofs(m))
-    its = JACOBI_ITERS_IBEAM if (args.slices == 315 and JACOBI_ITERS_IBEAM) else None
+    its = int(ref["iterations"])
     per_iter = []
     for _ in range(args.warmup):
         cpu_jacobi_sample(K, F, 2)
     for _ in range(args.steps):
         per_iter.append(cpu_jacobi_sample(K, F, args.cpu_iters))
     t_it = statistics.median(per_iter)
-    if its is None:
-        line = {"impl": "reference", "unavailable": "Jacobi-PCG iteration count for this size not measured yet"}
-        print(json.dumps(line))
-        return
     solve_s = t_it * its
     v = ndof / solve_s
+    # the cantilever, for real
+    mc, _ = generate_c3d10_kuhn_block()
+    Kc, Fc, _ = solid.assemble(mc.mesh_nodes, mc.solid_elements, solid_element_props(mc), solid_load_vector(mc),
+                               solid_fixed_dofs(mc))
+    c1 = []
+    for _ in range(3):
+        _, c1_its, c1_rel, c1_s = solid.pcg(Kc, Fc, rtol=1e-8, max_iter=20000, preconditioner="jacobi")
+        t0 = time.perf_counter()
+        spsolve(Kc.tocsc(), Fc)
+        c1.append((c1_s, time.perf_counter() - t0))
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "DOF/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": solve_s * 1e3, "higher_is_better": True, "scaling": "weak",
@@ -286,8 +339,14 @@ def run_reference(args):
         "config": {"workload": f"C3D10 I-beam {meta['n_elements']} el / {ndof} DOFs, Jacobi-PCG (scipy cg) to 1e-8",
                    "l2": "inputs larger than L2"},
         "cpu_baseline": {"value": v, "unit": "DOF/s", "cores": 1, "kind": "port",
-                         "sample": f"{args.cpu_iters} scipy cg iterations per step, x {its} iterations"},
+                         "sample": f"{args.cpu_iters} scipy cg + Jacobi iterations on the full matrix per step "
+                                   f"({t_it * 1e3:.1f} ms/iter, sparse products single-threaded) x {its} iterations, "
+                                   "the count of the reference's own solve_c3d10_pcg run to 1e-8 on this I-beam"},
         "e2e": {"value": v, "unit": "DOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_run": {"iterations": its, "s_per_iteration": _r(ref["s_per_iteration"]),
+                          "solve_s": _r(ref["solve_s"]), "true_rel_res": _r(ref["true_rel_res"])},
+        "c1": {"workload": "480-el cantilever, 3075 DOFs, run to convergence", "jacobi_pcg_s": _r(min(c[0] for c in c1)),
+               "jacobi_pcg_iterations": c1_its, "rel_res": _r(c1_rel), "spsolve_s": _r(min(c[1] for c in c1))},
     }
     print(json.dumps(line))
 
@@ -491,6 +550,71 @@ def adjoint_workload(args, stream):
             "mixed_vs_fp64_gradient_max_rel_diff": float(np.max(np.abs(g_mixed - g64)) / np.max(np.abs(g64)))}
 
 
+def cantilever_workload(stream):
+    """BASELINE's 480-element cantilever (1 x 0.1 x 0.1 m, 20 x 2 x 2 hexes x 6 tets, root
+    clamped, -1000 N tip load): AMG-PCG FP64 and mixed to 1e-8 (device-resident, CUDA events),
+    the GPU point-Jacobi PCG (the reference's algorithm), and the public API call with host
+    buffers."""
+    import torch
+
+    from wnfea_b200 import _lib
+    from wnfea_b200.mesh import generate_c3d10_kuhn_block
+    from wnfea_b200.solid_solver import assemble_c3d10_sparse_3dof, solve_c3d10_system
+
+    m, _ = generate_c3d10_kuhn_block()
+    K, F_np, _ = assemble_c3d10_sparse_3dof(m)
+    s = K.system
+    s.amg_setup()
+    F = torch.from_numpy(F_np).cuda()
+    u = torch.empty_like(F)
+    sptr = stream.cuda_stream
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"dofs": int(F.numel())}
+    for name, precond, prec in (("amg_fp64", 2, 0), ("amg_mixed", 2, 1), ("jacobi_fp64", 1, 0)):
+        prm = _lib.SolveParams(1e-8, 20000, precond, prec, 0.0, 10, 8, 1)
+        st = _lib.SolveStats()
+        for _ in range(3):
+            _lib.call("wn_solve_device", s.handle, F.data_ptr(), u.data_ptr(), prm, st, sptr)
+        reps = 10
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            _lib.call("wn_solve_device", s.handle, F.data_ptr(), u.data_ptr(), prm, st, sptr)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[name] = {"ms": e0.elapsed_time(e1) / reps, "its": st.iterations, "rel_res": st.rel_res,
+                     "status": st.status}
+    solve_c3d10_system(K, F_np, method="pcg", rtol=1e-8, preconditioner="amg")
+    t0 = time.perf_counter()
+    for _ in range(10):
+        solve_c3d10_system(K, F_np, method="pcg", rtol=1e-8, preconditioner="amg")
+    out["api_amg_fp64_host_ms"] = (time.perf_counter() - t0) * 100.0
+    return out
+
+
+def frame_newton_workload():
+    """BASELINE's co-rotational frame: 10 x 10 nodes at 1 m, 180 beams (0.1 x 0.1 m, E = 200 GPa),
+    corners clamped, seeded z-loads U[-5, 5] kN; 10 load increments of Newton with the GPU
+    consistent tangent, at the reference's default tolerances (|R| < 1e-5) and tightened
+    (relative 1e-12)."""
+    from wnfea_b200.beam import solve_nonlinear_jfnk
+    from wnfea_b200.frames import generate_frame_grid
+
+    out = {}
+    for name, tol_rel, tol_abs in (("default_tol", 1e-5, 1e-5), ("tight_tol", 1e-12, 1e-8)):
+        best = None
+        for _ in range(3):
+            m = generate_frame_grid()
+            st = {}
+            t0 = time.perf_counter()
+            U = solve_nonlinear_jfnk(m, n_load_steps=10, tol_rel=tol_rel, tol_abs=tol_abs, verbose=False, stats=st)
+            dt = time.perf_counter() - t0
+            if best is None or dt < best["s"]:
+                best = {"s": dt, "newton": st["newton_iterations"], "max_uz": float(np.abs(U.reshape(-1, 6)[:, 2]).max())}
+        out[name] = best
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -511,25 +635,36 @@ def run_ours(args):
 
     m, meta = build_model(args.slices)
     ndof = meta["n_dofs"]
+    n_el = meta["n_elements"]
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
+    peak, peak_kind = measured_peaks()
 
     # assembly (device time)
     t0 = time.perf_counter()
     K, F_np, fixed = assemble_c3d10_sparse_3dof(m)
     t_asm_wall = time.perf_counter() - t0
     s = K.system
+    nb, n_nodes = s.nnzb, s.n_nodes
     props = np.ascontiguousarray(s.props)
     d_props = torch.from_numpy(props).cuda()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    for _ in range(2):
-        _lib.call("wn_assemble_c3d10_device", s.handle, d_props.data_ptr(), 1, sptr)
-    ev[0].record(stream)
-    for _ in range(3):
-        _lib.call("wn_assemble_c3d10_device", s.handle, d_props.data_ptr(), 1, sptr)
-    ev[1].record(stream)
-    torch.cuda.synchronize()
-    assembly_ms = ev[0].elapsed_time(ev[1]) / 3
+
+    def event_ms(fn, reps, warm=2):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for _ in range(reps):
+            fn()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]) / reps
+
+    assembly_ms = event_ms(lambda: _lib.call("wn_assemble_c3d10_device", s.handle, d_props.data_ptr(), 1, sptr), 5)
+    # algorithmic bytes of one assembly: FP64 values written, element->block map, connectivity,
+    # coordinates and element properties read
+    asm_bytes = nb * 9 * 8 + n_el * 100 * 4 + n_el * 40 + n_nodes * 24 + n_el * 16
     t0 = time.perf_counter()
     s.amg_setup()
     setup_s = time.perf_counter() - t0
@@ -538,13 +673,13 @@ def run_ours(args):
     u = torch.empty_like(F)
     rtol = 1e-8
 
-    def solve(precision, precond=2, max_iter=2000):
-        prm = _lib.SolveParams(rtol, max_iter, precond, precision, 0.0, 10, 8, 1)
+    def solve(precision, precond=2, max_iter=2000, max_outer=10):
+        prm = _lib.SolveParams(rtol, max_iter, precond, precision, 0.0, max_outer, 8, 1)
         st = _lib.SolveStats()
         _lib.call("wn_solve_device", s.handle, F.data_ptr(), u.data_ptr(), prm, st, sptr)
         return st
 
-    def timed(precision):
+    def timed(precision, steps):
         for _ in range(args.warmup):
             solve(precision)
         torch.cuda.synchronize()
@@ -555,7 +690,7 @@ def run_ours(args):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with ClockSampler(local) as clk:
             e0.record(stream)
-            for _ in range(args.steps):
+            for _ in range(steps):
                 st = solve(precision)
                 launches += st.kernel_launches
                 iters.append(st.iterations)
@@ -565,91 +700,151 @@ def run_ours(args):
                     raise RuntimeError(f"solve did not converge: status {st.status}")
             e1.record(stream)
             torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / args.steps
+        ms = e0.elapsed_time(e1) / steps
         if dist:
             t = torch.tensor([ms], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
         return ms, launches, iters, outer, max(rels), clk.summary()
 
-    ms_mixed, launches, it_m, out_m, rel_m, clocks = timed(1)
+    ms_mixed, launches, it_m, out_m, rel_m, clocks = timed(1, args.steps)
+    bytes_mixed = solve(1).algorithmic_bytes
     u_mixed = u.clone()
-    ms_64, launches64, it_64, _, rel_64, clocks64 = timed(0)
+    ms_64, launches64, it_64, out_64, rel_64, clocks64 = timed(0, args.steps)
+    bytes_64 = solve(0).algorithmic_bytes
+
+    # one more solve of each precision with an event after every kernel: in-solve durations and
+    # algorithmic bytes per kernel class (launches on this stream; graphs off for this solve)
+    def profiled(precision):
+        prm = _lib.SolveParams(rtol, 2000, 2, precision, 0.0, 10, 8, 1, 1)
+        st = _lib.SolveStats()
+        _lib.call("wn_solve_device", s.handle, F.data_ptr(), u.data_ptr(), prm, st, sptr)
+        n = C.c_int()
+        _lib.call("wn_solve_profile", s.handle, 0, C.byref(n), None, None, None, None)
+        k = n.value
+        names = C.create_string_buffer(48 * k)
+        cnt, pms, pby = np.zeros(k, dtype=np.int64), np.zeros(k), np.zeros(k)
+        _lib.call("wn_solve_profile", s.handle, k, C.byref(n), names, _lib.ptr(cnt), _lib.ptr(pms), _lib.ptr(pby))
+        rows = {names.raw[48 * i:48 * i + 48].split(b"\0", 1)[0].decode(): (int(cnt[i]), pms[i], pby[i])
+                for i in range(k)}
+        return rows, st.solve_seconds * 1e3
+
+    prof_mixed, prof_mixed_ms = profiled(1)
+    prof_64, prof_64_ms = profiled(0)
     u_diff = float(torch.linalg.norm(u - u_mixed) / torch.linalg.norm(u))
+    # host check of the returned FP64 u: ||F - K u|| / ||F|| in FP64 on the host with the GPU's
+    # own assembled matrix (independent arithmetic; the oracle comparison lives in the tests)
+    Kc = K.tocsr()
+    host_rel = {}
+    for name, uu in (("mixed", u_mixed), ("fp64", u)):
+        un = uu.cpu().numpy()
+        host_rel[name] = float(np.linalg.norm(F_np - Kc @ un) / np.linalg.norm(F_np))
 
     # end to end through the public API with host buffers
-    for _ in range(1):
-        solve_c3d10_system(K, F_np, method="pcg", rtol=rtol, precision="mixed_fp32")
+    solve_c3d10_system(K, F_np, method="pcg", rtol=rtol, preconditioner="amg", precision="mixed_fp32")
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        u_np, st = solve_c3d10_system(K, F_np, method="pcg", rtol=rtol, precision="mixed_fp32")
+        u_np, st = solve_c3d10_system(K, F_np, method="pcg", rtol=rtol, preconditioner="amg", precision="mixed_fp32")
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t0) / args.steps
+
+    # the other modes on the same I-beam, each solved once (after one warm-up for the graphs)
+    modes = {}
+    for name, precision, precond, max_iter in (("fp32_ir", 2, 2, 5000), ("jacobi_fp64", 0, 1, 200000),
+                                               ("block_jacobi_fp64", 0, 3, 200000)):
+        if rank != 0 or (args.skip_jacobi and precond != 2):
+            continue
+        solve(precision, precond, max_iter)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = solve(precision, precond, max_iter)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        modes[name] = {"ms": e0.elapsed_time(e1), "its": st.iterations, "outer": st.outer_iterations,
+                       "rel_res": st.rel_res, "status": st.status}
 
     # adjoint gradient (dC/dE per element, dC/dF) on the converged field
     gE = torch.empty(s.n_el, dtype=torch.float64, device="cuda")
     gF = torch.empty_like(F)
-    for _ in range(3):
-        _lib.call("wn_adjoint_compliance_device", s.handle, u.data_ptr(), gE.data_ptr(), gF.data_ptr(), sptr)
-    ev[0].record(stream)
-    for _ in range(10):
-        _lib.call("wn_adjoint_compliance_device", s.handle, u.data_ptr(), gE.data_ptr(), gF.data_ptr(), sptr)
-    ev[1].record(stream)
-    torch.cuda.synchronize()
-    adjoint_ms = ev[0].elapsed_time(ev[1]) / 10
+    adjoint_ms = event_ms(lambda: _lib.call("wn_adjoint_compliance_device", s.handle, u.data_ptr(), gE.data_ptr(),
+                                            gF.data_ptr(), sptr), 10)
+    adj_bytes = n_nodes * 24 * 2 + n_el * (40 + 8 + 8) + 3 * n_nodes * 8
 
     fint = internal_force(m, s, stream)
+    fint_bytes = n_nodes * 24 * 3 + n_el * (40 + 16)
     multi = None if args.skip_multi else batched_cases(args, m, s, stream, ms_mixed)
     adjoint = None if args.skip_adjoint else adjoint_workload(args, stream)
     frame_res = None if args.skip_frame else frame_workload(args, stream)
+    c1 = cantilever_workload(stream) if rank == 0 else None
+    c2 = frame_newton_workload() if rank == 0 else None
 
     # roofline: fine-level BSR3 SpMV, FP32 and FP64, event-timed on this stream
-    nb, n_nodes = s.nnzb, s.n_nodes
     x64 = torch.randn(3 * n_nodes, dtype=torch.float64, device="cuda")
     y64 = torch.empty_like(x64)
     x32, y32 = x64.float(), torch.empty(3 * n_nodes, dtype=torch.float32, device="cuda")
 
     def spmv_ms(prec, x, y, reps=50):
-        for _ in range(5):
-            _lib.call("wn_spmv_solid_device", s.handle, prec, x.data_ptr(), y.data_ptr(), sptr)
-        ev[0].record(stream)
-        for _ in range(reps):
-            _lib.call("wn_spmv_solid_device", s.handle, prec, x.data_ptr(), y.data_ptr(), sptr)
-        ev[1].record(stream)
-        torch.cuda.synchronize()
-        return ev[0].elapsed_time(ev[1]) / reps
+        return event_ms(lambda: _lib.call("wn_spmv_solid_device", s.handle, prec, x.data_ptr(), y.data_ptr(), sptr),
+                        reps, warm=5)
 
     def spmv_bytes(sz):
         return nb * (9 * sz + 4) + 4 * (n_nodes + 1) + 2 * 3 * n_nodes * sz
 
-    peak, peak_kind = measured_peaks()
     t32 = spmv_ms(1, x32, y32)
     t64 = spmv_ms(0, x64, y64)
     ach32 = spmv_bytes(4) / (t32 * 1e-3) / 1e9
     ach64 = spmv_bytes(8) / (t64 * 1e-3) / 1e9
 
-    jacobi_iters = None
-    if not args.skip_jacobi and rank == 0:
-        st = solve(0, precond=1, max_iter=200000)
-        jacobi_iters = st.iterations if st.status == 0 else None
-
     cpu = None
-    if not args.skip_cpu and rank == 0 and world == 1:
-        Kc = K.tocsr()
-        t_it = cpu_jacobi_sample(Kc, F_np, args.cpu_iters)
-        its = jacobi_iters or JACOBI_ITERS_IBEAM
-        if its:
-            cpu = {"value": ndof / (t_it * its), "unit": "DOF/s", "cores": 1, "kind": "port",
-                   "sample": f"{args.cpu_iters} iterations of scipy cg + Jacobi on the full matrix "
-                             f"({t_it * 1e3:.1f} ms/iter, 1 thread), x {its} iterations to 1e-8",
-                   "solve_s": t_it * its}
+    ref = reference_run()
+    if not args.skip_cpu and rank == 0 and world == 1 and ref is not None and args.slices == 315:
+        t_it = cpu_jacobi_sample(Kc, F_np, args.cpu_iters)  # the same matrix, exported as scipy CSR
+        its = int(ref["iterations"])
+        cpu = {"value": ndof / (t_it * its), "unit": "DOF/s", "cores": 1, "kind": "port",
+               "sample": f"{args.cpu_iters} iterations of scipy cg + Jacobi on the full matrix "
+                         f"({t_it * 1e3:.1f} ms/iter, 1 thread) x {its} iterations (the reference's own "
+                         "solve_c3d10_pcg run to 1e-8 on this I-beam)",
+               "solve_s": t_it * its}
 
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
+    gbs = lambda b, ms: b / (ms * 1e-3) / 1e9  # noqa: E731
     value = world * ndof / (ms_mixed * 1e-3)
+
+    def prof_summary(rows):
+        """per kernel class: launches, ms per launch, fraction of the measured HBM peak, share of the
+        profiled solve's kernel time"""
+        tot = sum(v[1] for v in rows.values())
+        return {k: {"n": v[0], "ms_each": v[1] / v[0], "frac": gbs(v[2], v[1]) / peak if v[1] > 0 else None,
+                    "share": v[1] / tot} for k, v in sorted(rows.items(), key=lambda kv: -kv[1][1])}
+
+    def fine_f32(rows):
+        """the FP32 fine-matrix passes of the V-cycle together (pre / Chebyshev / residual / post)"""
+        sel = [v for k, v in rows.items() if k.startswith("l0.") and k.split(".")[1] in
+               ("pre_smooth", "pre_cheb", "residual", "post_smooth", "post_cheb")]
+        b, t = sum(v[2] for v in sel), sum(v[1] for v in sel)
+        return gbs(b, t) / peak if t > 0 else None
+
+    in_solve = {"whole_solve_mixed": gbs(bytes_mixed, ms_mixed) / peak, "whole_solve_fp64": gbs(bytes_64, ms_64) / peak,
+                "pcg_spmv_dot_f64": gbs(prof_mixed["pcg_spmv_dot"][2], prof_mixed["pcg_spmv_dot"][1]) / peak,
+                "fine_vcycle_f32": fine_f32(prof_mixed), "fine_vcycle_f64": fine_f32(prof_64)}
+    details = {
+        "iterations": {"mixed_inner": it_m[-1], "mixed_outer": out_m[-1], "fp64": it_64[-1], "fp64_outer": out_64[-1]},
+        "rel_res": {"mixed": rel_m, "fp64": rel_64}, "host_rel_res": host_rel, "u_rel_diff_mixed_vs_fp64": u_diff,
+        "fp64": {"ms_per_step": ms_64, "clocks": clocks64, "launches": launches64},
+        "algorithmic_bytes_per_solve": {"mixed": bytes_mixed, "fp64": bytes_64},
+        "profile_mixed": prof_summary(prof_mixed), "profile_fp64": prof_summary(prof_64),
+        "profiled_solve_ms": {"mixed": prof_mixed_ms, "fp64": prof_64_ms},
+        "modes": modes, "assembly_ms": assembly_ms, "assembly_algorithmic_bytes": asm_bytes,
+        "assembly_wall_s_first_call": t_asm_wall, "amg_setup_s": setup_s, "adjoint_grad_ms_ibeam": adjoint_ms,
+        "adjoint": adjoint, "multi_rhs": multi, "internal_force": fint, "beam_frame": frame_res, "c1": c1, "c2": c2,
+        "roofline_fp64_spmv": {"achieved": ach64, "frac": ach64 / peak, "launch_ms": t64,
+                               "algorithmic_bytes": spmv_bytes(8)},
+    }
+    sys.stderr.write(json.dumps(details) + "\n")
     line = {
         "metric": METRIC,
         "value": value,
@@ -661,42 +856,42 @@ def run_ours(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32 (AMG, SpMV, vectors) + f64 (residual, dots, coarse Cholesky)",
+        "dtype": "f64 PCG/SpMV/dots + f32 AMG V-cycle + f64 coarsest inverse",
         "data": "synthetic",
         "config": {
-            "workload": f"C3D10 I-beam {meta['n_elements']} el / {meta['n_nodes']} nodes / {ndof} DOFs, "
-                        "FP64 PCG + FP32 SA-AMG V-cycle to true rel.res 1e-8",
-            "elements": meta["n_elements"], "dofs": ndof, "nnz_blocks": nb, "rtol": rtol,
-            "preconditioner": "smoothed-aggregation AMG, Chebyshev(2)", "parallelism": f"replicas x{world}",
-            "l2": "inputs larger than L2 (FP32 K 0.31 GB, FP64 K 0.61 GB per step)",
+            "workload": f"C3D10 I-beam {n_el} el / {ndof} DOFs, FP64 PCG + FP32 SA-AMG V-cycle to true rel.res 1e-8",
+            "nnz_blocks": nb, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (FP64 K 0.61 GB, FP32 K 0.31 GB per step)",
         },
-        "iterations": {"mixed_inner": it_m[-1], "mixed_outer": out_m[-1], "fp64": it_64[-1]},
-        "rel_res": {"mixed": rel_m, "fp64": rel_64},
-        "fp64": {"value": world * ndof / (ms_64 * 1e-3), "ms_per_step": ms_64, "clocks": clocks64},
-        "speedup_mixed_vs_fp64": ms_64 / ms_mixed,
-        "u_rel_diff_mixed_vs_fp64": u_diff,
-        "assembly_ms": assembly_ms,
-        "assembly_wall_s_first_call": t_asm_wall,
-        "amg_setup_s": setup_s,
-        "adjoint_grad_ms": adjoint["grad_kernel_ms"] if adjoint else None,
-        "adjoint_grad_ms_ibeam_field": adjoint_ms,
-        "adjoint": adjoint,
-        "multi_rhs": multi,
-        "internal_force": fint,
-        "beam_frame": frame_res,
-        "jacobi_pcg_iterations": jacobi_iters,
-        "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak,
+        "roofline": {"bound": "hbm", "achieved": _r(ach32), "peak": peak, "unit": "GB/s", "frac": _r(ach32 / peak),
                      "traffic": ncu_traffic("k_stream_spmv_f32_ibeam200k.txt"), "peak_kind": peak_kind,
-                     "kernel": "k_stream_spmv<float> (fine-level FP32 BSR3 SpMV streamed from the tile-major "
-                               "pack by bulk async copies)",
-                     "algorithmic_bytes": spmv_bytes(4), "launch_ms": t32},
-        "roofline_fp64_spmv": {"achieved": ach64, "frac": ach64 / peak, "launch_ms": t64,
-                               "algorithmic_bytes": spmv_bytes(8)},
-        "cpu_baseline": cpu,
+                     "kernel": "k_stream_spmv<float> fine FP32 BSR3 SpMV", "algorithmic_bytes": spmv_bytes(4),
+                     "launch_ms": _r(t32)},
+        "cpu_baseline": _r(cpu),
         "e2e": {"value": world * ndof / e2e_s, "unit": "DOF/s", "h2d_bytes_per_step": 8 * ndof,
                 "d2h_bytes_per_step": 8 * ndof, "api": "solve_c3d10_system(K, F numpy) -> u numpy"},
         "gpu_launches": launches,
         "clocks": clocks,
+        # ---- every configuration's headline, compact (details on stderr) ----
+        "in_solve_frac_of_hbm": _r(in_solve, 3),
+        "kernels_frac_of_hbm": _r({"spmv_f64": ach64 / peak, "assembly": gbs(asm_bytes, assembly_ms) / peak,
+                                   "assembly_ms": assembly_ms, "fint": gbs(fint_bytes, fint["device_ms"]) / peak,
+                                   "adjoint": gbs(adj_bytes, adjoint_ms) / peak}, 3),
+        "amg_setup_s": _r(setup_s, 3),
+        "c1_cantilever": _r({k: (v["ms"] if isinstance(v, dict) else v) for k, v in c1.items()}, 3) if c1 else None,
+        "c1_ref_probe_s": {"jacobi_pcg": REF_PROBE["c1_jacobi_pcg_s"], "spsolve": REF_PROBE["c1_spsolve_s"]},
+        "c2_frame_newton_s": _r({k: v["s"] for k, v in c2.items()}, 3) if c2 else None,
+        "c2_ref_probe_s": REF_PROBE["c2_jfnk_10_steps_s"],
+        "c4_multi_rhs": _r({"ms_per_case": multi["ms_per_case"], "its": multi["batched_iterations"],
+                            "max_rel_res": multi["max_case_rel_res"]}, 3) if multi else None,
+        "c5_adjoint": _r({"grad_ms": adjoint["grad_kernel_ms"], "solve_ms": adjoint["forward_solve_ms"],
+                          "fd_max_rel_err": adjoint["fd_check"]["max_rel_err"]}, 3) if adjoint else None,
+        "modes_ms_its": {k: [_r(v["ms"]), v["its"], v["outer"], _r(v["rel_res"], 3)] for k, v in modes.items()},
+        "host_rel_res": _r(host_rel, 3),
+        "iterations": [it_m[-1], out_m[-1], it_64[-1], out_64[-1]],
+        "rel_res": _r([rel_m, rel_64], 3),
+        "fp64_ms": _r(ms_64),
+        "speedup_mixed_vs_fp64": _r(ms_64 / ms_mixed),
     }
     print(json.dumps(line))
     if dist:

@@ -74,6 +74,18 @@ int wn_solid_get_map(void* h, int32_t* emap);
  * (nnzb entries) and optionally emap (n_el*100) to fill them. */
 int wn_bsr3_pattern_host(int64_t n_nodes, int64_t n_el, const int32_t* conn, int64_t* nnzb, int32_t* row_ptr,
                          int32_t* col_idx, int32_t* emap);
+/* Host-only plan of the tile-owner assembly (no device work; for tests and inspection).  The
+ * block rows are cut into the row tiles of the streamed fine matrix (WN_STREAM_TILE_BLOCKS /
+ * _ROWS); per tile: its incident elements (ascending), and per block its contributions in the
+ * assembly's summation order (element ascending) as slot << 8 | a << 4 | b (slot = index in the
+ * tile's element list, (a, b) = element-local node pair), and the tile's blocks by descending
+ * contribution count (perm[b0 + k] = local index).  Call with tiles == NULL to get the sizes;
+ * *n_tiles = 0 when the mesh takes the element-scratch assembly instead (a tile with more than
+ * 200 incident elements, or a row over the tile capacity).  Sizes: tiles 4 n_tiles, el_ptr
+ * n_tiles + 1, el *n_el_entries, contrib 100 n_el, perm nnzb. */
+int wn_assembly_plan_host(int64_t n_nodes, int64_t n_el, const int32_t* conn, int64_t* n_tiles, int* ne_max,
+                          int64_t* n_el_entries, int32_t* tiles, int32_t* el_ptr, int32_t* el, uint16_t* contrib,
+                          uint16_t* perm);
 /* Dirichlet mask over the 3*n_nodes DOFs (host, 1 = FIXED, NULL = none).  FIXED DOFs get
  * zero rows/columns and diagonal 1 and a zero load (solid_solver.py:95-127). */
 int wn_solid_set_fixed(void* h, const uint8_t* fixed_mask);
@@ -198,6 +210,8 @@ typedef struct wn_solve_params {
   int max_outer;      /* mixed: refinement steps (<= 0: 10)                           */
   int chunk;          /* iterations per CUDA-graph replay / host convergence check    */
   int use_graph;      /* 1 = replay captured chunks as a CUDA graph                   */
+  int profile;        /* 1 = time every kernel of this solve with CUDA events (graphs
+                         off; read back with wn_solve_profile); 0 = normal          */
 } wn_solve_params;
 
 typedef struct wn_solve_stats {
@@ -212,6 +226,9 @@ typedef struct wn_solve_stats {
   double solve_seconds;  /* device time of the solve (CUDA events)                   */
   double setup_seconds;  /* wall time of the last AMG setup                          */
   int64_t kernel_launches; /* kernels issued by the solve (graph replays counted per kernel) */
+  double algorithmic_bytes; /* unique bytes read + written by the kernels that did their work
+                               (matrices, vectors; single-RHS solves): divided by
+                               solve_seconds, the solve's achieved memory bandwidth       */
 } wn_solve_stats;
 
 /* Device pointers F, u (3 n_nodes).  Returns 0 even when not converged: check
@@ -220,6 +237,11 @@ int wn_solve_device(void* h, const double* d_F, double* d_u, const wn_solve_para
                     uintptr_t stream);
 /* Host buffers F, u (copies in and out). */
 int wn_solve(void* h, const double* F, double* u, const wn_solve_params* params, wn_solve_stats* stats);
+/* Per kernel class of the last solve run with params.profile = 1 (e.g. "l0.pre_smooth" for the
+ * fine-level first smoothing step, "pcg_spmv_dot", "coarse"): launches that did their work,
+ * their summed CUDA-event durations (ms) and algorithmic bytes.  names: capacity x 48 chars
+ * (NUL-terminated); *n_rows = number of classes (may exceed capacity). */
+int wn_solve_profile(void* h, int capacity, int* n_rows, char* names, int64_t* counts, double* ms, double* bytes);
 
 /* Linear 6-DOF-per-node systems (beam frames; the reference's GPU AMG-PCG of
  * BlockBeamAMGPreconditioner.solve_pcg -> hip_solve_pcg_amg, fast_kernels.py:598-663 and

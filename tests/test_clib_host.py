@@ -71,3 +71,79 @@ def test_pattern_rejects_bad_node_index():
     with pytest.raises(_lib.WnError) as e:
         pattern_host(conn, len(m.mesh_nodes))
     assert e.value.code == -3
+
+
+def assembly_plan_host(conn, n_nodes):
+    conn = np.ascontiguousarray(conn, dtype=np.int32)
+    nt, nemax, nel = C.c_int64(), C.c_int(), C.c_int64()
+    _lib.call("wn_assembly_plan_host", n_nodes, len(conn), _lib.ptr(conn), C.byref(nt), C.byref(nemax), C.byref(nel),
+              None, None, None, None, None)
+    tiles = np.empty((nt.value, 4), dtype=np.int32)
+    el_ptr = np.empty(nt.value + 1, dtype=np.int32)
+    el = np.empty(nel.value, dtype=np.int32)
+    contrib = np.empty(len(conn) * 100, dtype=np.uint16)
+    rp, ci, _ = pattern_host(conn, n_nodes)
+    perm = np.empty(len(ci), dtype=np.uint16)
+    _lib.call("wn_assembly_plan_host", n_nodes, len(conn), _lib.ptr(conn), C.byref(nt), C.byref(nemax), C.byref(nel),
+              _lib.ptr(tiles), _lib.ptr(el_ptr), _lib.ptr(el), _lib.ptr(contrib), _lib.ptr(perm))
+    return tiles, el_ptr, el, contrib, perm, nemax.value, rp, ci
+
+
+@pytest.mark.parametrize("which", ["c1", "ibeam-shuffled"])
+def test_assembly_plan_rebuilds_the_oracle_matrix(which):
+    """The tile-owner assembly's plan: tiles cover every block row once and match the streamed
+    engine's tiling; each tile lists exactly the elements incident to its rows; perm is a
+    permutation of the tile's blocks by descending contribution count; and summing, per block in
+    the plan's order, the oracle's element blocks named by (slot, a, b) reproduces the oracle's
+    assembled K (no Dirichlet BCs), with blocks (i, j) and (j, i) exact transposes."""
+    from oracle import c3d10
+
+    from wnfea_b200.model import solid_element_props
+
+    if which == "c1":
+        m, _ = generate_c3d10_kuhn_block()
+    else:
+        m, _ = generate_c3d10_ibeam_structured(n_slices=5, length=4.0 * 5 / 315, seed=2)
+        perm_nodes = np.random.default_rng(3).permutation(len(m.mesh_nodes))
+        inv = np.empty_like(perm_nodes)
+        inv[perm_nodes] = np.arange(len(perm_nodes))
+        m.mesh_nodes = m.mesh_nodes[perm_nodes].copy()
+        m.solid_elements = inv[m.solid_elements].astype(np.int32)
+    conn = np.ascontiguousarray(m.solid_elements, dtype=np.int32)
+    n = len(m.mesh_nodes)
+    tiles, el_ptr, el, contrib, perm, nemax, rp, ci = assembly_plan_host(conn, n)
+    assert len(tiles) > 1 and tiles[0, 0] == 0 and tiles[-1, 1] == n
+    assert np.array_equal(tiles[1:, 0], tiles[:-1, 1]) and np.array_equal(tiles[:, 2], rp[tiles[:, 0]])
+    assert np.array_equal(tiles[:, 3], rp[tiles[:, 1]])
+    nt_stream = C.c_int64()
+    _lib.call("wn_stream_tiles_host", n, _lib.ptr(rp), None, 0, C.byref(nt_stream))
+    st = np.empty((nt_stream.value, 4), dtype=np.int32)
+    _lib.call("wn_stream_tiles_host", n, _lib.ptr(rp), _lib.ptr(st), nt_stream.value, C.byref(nt_stream))
+    assert np.array_equal(st, tiles)
+    node_tile = np.repeat(np.arange(len(tiles)), tiles[:, 1] - tiles[:, 0])
+    for t in range(len(tiles)):
+        mine = np.flatnonzero((node_tile[conn] == t).any(axis=1))
+        assert np.array_equal(el[el_ptr[t]:el_ptr[t + 1]], mine)
+    assert nemax == np.diff(el_ptr).max()
+    Ke = c3d10.element_stiffness_batch(m.mesh_nodes[conn], solid_element_props(m))
+    gptr = np.concatenate([[0], np.cumsum(np.bincount(pattern_host(conn, n)[2].ravel(), minlength=len(ci)))])
+    vals = np.zeros((len(ci), 3, 3))
+    for t in range(len(tiles)):
+        b0, b1 = tiles[t, 2], tiles[t, 3]
+        assert np.array_equal(np.sort(perm[b0:b1]), np.arange(b1 - b0))
+        counts = np.diff(gptr[b0:b1 + 1])[perm[b0:b1]]
+        assert np.all(np.diff(counts) <= 0)
+        els = el[el_ptr[t]:el_ptr[t + 1]]
+        for b in range(b0, b1):
+            last = -1
+            for q in range(gptr[b], gptr[b + 1]):
+                code = int(contrib[q])
+                e, a, bb = els[code >> 8], (code >> 4) & 15, code & 15
+                assert e > last  # element order
+                last = e
+                vals[b] += Ke[e, 3 * a:3 * a + 3, 3 * bb:3 * bb + 3]
+    K = solid.bsr3_to_csr(rp, ci, vals)
+    assert abs(K - K.T).max() == 0.0
+    Ko, _, _ = solid.assemble(m.mesh_nodes, conn, solid_element_props(m), apply_bcs=False)
+    D = (K - Ko).tocsr()
+    assert np.abs(D.data).max(initial=0.0) <= 1e-14 * np.abs(Ko.data).max()

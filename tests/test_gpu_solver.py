@@ -246,3 +246,31 @@ def test_tiny_mesh_hierarchy_without_levels():
     assert stm["status"] == 0
     Ur = spsolve(Ko.tocsc(), Fm)
     assert np.linalg.norm(U - Ur) <= 1e-8 * np.linalg.norm(Ur)
+
+
+def test_profiled_solve_accounts_every_kernel():
+    """params.profile: the same solve with an event after every kernel.  The solution is bitwise
+    the normal one; the per-class algorithmic bytes add up to the solve's algorithmic_bytes (the
+    classes count exactly the launches that did their work); the classes name the V-cycle stages
+    per level, the PCG kernels and the outer-residual kernels."""
+    m = _ibeam(12, seed=4)
+    K, F, _ = assemble_c3d10_sparse_3dof(m)
+    s = K.system
+    s.amg_setup()
+    for precision in (0, 1):
+        u0, st0 = s.solve(F, rtol=1e-8, precision=precision)
+        u1, st1 = s.solve(F, rtol=1e-8, precision=precision, profile=True)
+        assert st0["status"] == 0 and st1["status"] == 0
+        assert np.array_equal(u0, u1) and st0["iterations"] == st1["iterations"]
+        assert st0["algorithmic_bytes"] > 0 and abs(st1["algorithmic_bytes"] - st0["algorithmic_bytes"]) <= (
+            1e-12 * st0["algorithmic_bytes"])
+        prof = s.profile_table()
+        for name in ("pcg_spmv_dot", "pcg_update", "l0.pre_smooth", "l0.residual", "l0.restrict", "l0.prolong",
+                     "l0.post_smooth", "l0.post_cheb", "coarse", "outer_residual"):
+            assert name in prof, (name, sorted(prof))
+        its = st1["iterations"]
+        assert prof["pcg_spmv_dot"][0] == its and prof["pcg_update"][0] == its
+        assert prof["coarse"][0] == its  # the initial apply plus one per iteration but the last
+        total = sum(v[2] for v in prof.values())
+        assert abs(total - st1["algorithmic_bytes"]) <= 1e-9 * total
+        assert 0 < sum(v[1] for v in prof.values()) <= st1["solve_seconds"] * 1e3 * 1.01

@@ -50,6 +50,7 @@ class SolveParams(C.Structure):
         ("max_outer", C.c_int),
         ("chunk", C.c_int),
         ("use_graph", C.c_int),
+        ("profile", C.c_int),
     ]
 
 
@@ -65,6 +66,7 @@ class SolveStats(C.Structure):
         ("solve_seconds", C.c_double),
         ("setup_seconds", C.c_double),
         ("kernel_launches", C.c_int64),
+        ("algorithmic_bytes", C.c_double),
     ]
 
 
@@ -91,6 +93,7 @@ SIGNATURES: dict[str, tuple] = {
     "wn_spmv_solid_device": (_I, [_P, _I, _P, _P, _U]),
     "wn_solid_set_stream": (_I, [_P, _I]),
     "wn_solid_stream_status": (_I, [_P, _I, _PI]),
+    "wn_assembly_plan_host": (_I, [_I64, _I64, _P, C.POINTER(_I64), _PI, C.POINTER(_I64), _P, _P, _P, _P, _P]),
     "wn_solid_stream_test_hook": (_I, [_P, _I64, _I]),
     "wn_stream_tiles_host": (_I, [_I64, _P, _P, _I64, C.POINTER(_I64)]),
     "wn_spmv_bsr_f64_device": (_I, [_I, _I, _I64, _P, _P, _P, _P, _P, _D, _D, _U]),
@@ -119,6 +122,7 @@ SIGNATURES: dict[str, tuple] = {
     "wn_amg_host_coarse": (_I, [_P, _PI64, _P, _P]),
     "wn_solve_device": (_I, [_P, _P, _P, C.POINTER(SolveParams), C.POINTER(SolveStats), _U]),
     "wn_solve": (_I, [_P, _P, _P, C.POINTER(SolveParams), C.POINTER(SolveStats)]),
+    "wn_solve_profile": (_I, [_P, _I, _PI, _P, _P, _P, _P]),
     "wn_bsr6_system_create": (_I, [_I64, _P, _P, _P, _P, _P, C.POINTER(_P)]),
     "wn_beam_linear_system": (_I, [_P, C.POINTER(_P)]),
     "wn_solve_multi_device": (_I, [_P, _I, _P, _P, C.POINTER(SolveParams), C.POINTER(SolveStats), _P, _P, _U]),

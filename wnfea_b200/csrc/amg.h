@@ -1,6 +1,8 @@
 // Device-resident AMG hierarchy and solver workspace.
 #pragma once
 
+#include <string>
+
 #include <cuda_runtime.h>
 
 #include <array>
@@ -136,12 +138,39 @@ struct SolverWork {
   int64_t launches = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaStream_t own = nullptr;  // used when the caller passes the legacy default stream
+  // Launch accounting of the current solve.  bytes: algorithmic bytes (unique reads + writes)
+  // of the kernels that did their work; the PCG iterations are counted from the device-side
+  // iteration count, so kernels that returned early after convergence are not counted.
+  double bytes = 0.0;
+  double iter_core_bytes = 0.0, iter_prec_bytes = 0.0;  // one iteration: SpMV/update/check, M^-1
+  // Profile mode (wn_solve_params.profile): graphs off, an event after every launch; each
+  // launch's duration is the time between its event and the previous one
+  struct Note {
+    const char* kind;  // kernel class; with level >= 0 reported as "l<level>.<kind>"
+    int level;
+    double bytes;
+    int iter;   // PCG iteration of the launch (-1: outside the iterations)
+    bool prec;  // part of the iteration's preconditioner apply
+    bool valid;
+  };
+  bool profile = false;
+  int cur_iter = -1;
+  bool cur_prec = false;
+  std::vector<Note> notes;
+  std::vector<cudaEvent_t> note_events;  // note_events[i]: after launch i; [0] is the start mark
+  struct ProfileRow {
+    std::string name;
+    int64_t count = 0;
+    double ms = 0.0, bytes = 0.0;
+  };
+  std::vector<ProfileRow> last_profile;  // aggregated per kernel class after a profiled solve
   ~SolverWork() {
     for (auto& a : graphs)
       for (auto& g : a) g.reset();
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (own) cudaStreamDestroy(own);
+    for (cudaEvent_t e : note_events) cudaEventDestroy(e);
   }
 };
 

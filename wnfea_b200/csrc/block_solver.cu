@@ -1439,6 +1439,7 @@ int solver_solve_multi(Solid* s, int n_rhs, const double* F, double* U, const wn
     stats->rel_res = worst;
     stats->solve_seconds = ms * 1e-3;
     stats->kernel_launches = W.launches;
+    stats->algorithmic_bytes = 0.0;  // not counted for the batched solve
     stats->setup_seconds = s->amg ? s->amg->setup_seconds : 0.0;
     stats->n_levels = s->amg ? (int)s->amg->levels.size() + 1 : 0;
   }

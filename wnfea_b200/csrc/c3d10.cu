@@ -163,6 +163,126 @@ __global__ void gather_assemble_kernel(int64_t nnzb, const int32_t* __restrict__
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// Tile-owner assembly (no per-element scratch in global memory).  One CTA per row tile of
+// the fine matrix (the tiles of its tile-major packs):
+//   phase 1: for every element incident to the tile's rows (the plan's list) and every
+//            Gauss point, the Cartesian derivatives dN/dx (3 x 10) and w|J| lambda, w|J| mu
+//            into shared memory (element stride kAsmElStride doubles: an odd number of 8-byte
+//            words, so lanes reading different elements hit different banks);
+//   phase 2: one thread per block of the tile, in the plan's order of descending contribution
+//            count (lanes of a warp carry blocks of similar cost), sums the block's
+//            contributions in element order (the gather order), each computed from shared
+//            memory as K_pq = sum_g w (lam v_p v_q^T + mu v_q v_p^T + mu (v_p . v_q) I) with
+//            p = min(a, b), q = max(a, b) and transposed when a > b -- so blocks (i, j) and
+//            (j, i) add bitwise-transposed terms in the same order and K is exactly
+//            symmetric -- applies the Dirichlet rows / columns and writes the FP64 and FP32
+//            component-major values and, when given, the FP64 / FP32 pack segments of the tile.
+// ---------------------------------------------------------------------------------------
+constexpr int kAsmThreads = 256;
+constexpr int kAsmGpStride = 32;                  // 30 derivatives + w lam + w mu
+constexpr int kAsmElStride = 4 * kAsmGpStride + 1;  // 129 doubles per element
+
+__global__ void __launch_bounds__(kAsmThreads, 2) assemble_tiles_kernel(
+    const AsmTileArgs A, const double* __restrict__ nodes, const int32_t* __restrict__ conn,
+    const double* __restrict__ props, const uint8_t* __restrict__ fixed, int64_t nnzb, double* __restrict__ k64,
+    float* __restrict__ k32, int* __restrict__ flags) {
+  extern __shared__ double s_el[];
+  const int t = blockIdx.x;
+  const int4 T = reinterpret_cast<const int4*>(A.tiles)[t];  // r0, r1, b0, b1
+  const int e_beg = A.el_ptr[t], ne = A.el_ptr[t + 1] - e_beg;
+  for (int item = threadIdx.x; item < ne * 4; item += kAsmThreads) {
+    const int k = item >> 2, g = item & 3;
+    const int64_t e = A.el[e_beg + k];
+    double X[10][3];
+    load_coords(nodes, conn, e, X);
+    double dndx[3][10];
+    const double det = gp_cartesian(g, X, dndx);
+    if (!(det > 0.0)) atomicOr(flags, 1);
+    double lam, mu;
+    lame(props[e * 2], props[e * 2 + 1], lam, mu);
+    double* d = s_el + k * kAsmElStride + g * kAsmGpStride;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int a = 0; a < 10; ++a) d[i * 10 + a] = dndx[i][a];
+    const double w = kWeight * det;
+    d[30] = w * lam;
+    d[31] = w * mu;
+  }
+  __syncthreads();
+  const int nb = T.w - T.z;
+  for (int kk = threadIdx.x; kk < nb; kk += kAsmThreads) {
+    const int j = A.perm[T.z + kk];  // local block index
+    const int64_t b = T.z + j;
+    double acc[9];
+#pragma unroll
+    for (int m = 0; m < 9; ++m) acc[m] = 0.0;
+    const int32_t q0 = A.gptr[b], q1 = A.gptr[b + 1];
+    for (int32_t q = q0; q < q1; ++q) {
+      const int code = A.contrib[q];
+      const int slot = code >> 8, ea = (code >> 4) & 15, eb = code & 15;
+      const int p = min(ea, eb), r = max(ea, eb);
+      double M[9];
+#pragma unroll
+      for (int m = 0; m < 9; ++m) M[m] = 0.0;
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {
+        const double* d = s_el + slot * kAsmElStride + g * kAsmGpStride;
+        const double vp0 = d[p], vp1 = d[10 + p], vp2 = d[20 + p];
+        const double vq0 = d[r], vq1 = d[10 + r], vq2 = d[20 + r];
+        const double wl = d[30], wm = d[31];
+        const double lp0 = wl * vp0, lp1 = wl * vp1, lp2 = wl * vp2;
+        const double mp0 = wm * vp0, mp1 = wm * vp1, mp2 = wm * vp2;
+        const double dg = mp0 * vq0 + mp1 * vq1 + mp2 * vq2;
+        // entry (i, j): lam vp_i vq_j + mu vp_j vq_i (+ mu vp . vq on the diagonal)
+        M[0] += lp0 * vq0 + mp0 * vq0 + dg;
+        M[1] += lp0 * vq1 + mp1 * vq0;
+        M[2] += lp0 * vq2 + mp2 * vq0;
+        M[3] += lp1 * vq0 + mp0 * vq1;
+        M[4] += lp1 * vq1 + mp1 * vq1 + dg;
+        M[5] += lp1 * vq2 + mp2 * vq1;
+        M[6] += lp2 * vq0 + mp0 * vq2;
+        M[7] += lp2 * vq1 + mp1 * vq2;
+        M[8] += lp2 * vq2 + mp2 * vq2 + dg;
+      }
+      if (ea <= eb) {
+#pragma unroll
+        for (int m = 0; m < 9; ++m) acc[m] += M[m];
+      } else {
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int jj = 0; jj < 3; ++jj) acc[i * 3 + jj] += M[jj * 3 + i];
+      }
+    }
+    const int64_t r0 = (int64_t)A.block_row[b] * 3, c0 = (int64_t)A.col_idx[b] * 3;
+    if (fixed) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj)
+          if (fixed[r0 + i] | fixed[c0 + jj]) acc[i * 3 + jj] = (r0 + i == c0 + jj) ? 1.0 : 0.0;
+    }
+#pragma unroll
+    for (int m = 0; m < 9; ++m) {
+      k64[m * nnzb + b] = acc[m];
+      k32[m * nnzb + b] = (float)acc[m];
+    }
+    if (A.p64) {
+      const int4 d64 = reinterpret_cast<const int4*>(A.d64)[t];  // r0, r1, seg, cntp
+      const int4 d32 = reinterpret_cast<const int4*>(A.d32)[t];
+      double* v64 = reinterpret_cast<double*>(A.p64 + (size_t)d64.z * 128);
+      float* v32 = reinterpret_cast<float*>(A.p32 + (size_t)d32.z * 128);
+#pragma unroll
+      for (int m = 0; m < 9; ++m) {
+        v64[m * d64.w + j] = acc[m];
+        v32[m * d32.w + j] = (float)acc[m];
+      }
+    }
+  }
+}
+
 // Matrix-free element forces f_e = Ke u_e (= sum_g w|J| B^T C B u_e, c3d10.py:252-283) for
 // DOF stride `stride` (3 for the solid path, 6 for the reference's mixed-DOF layout of
 // kernels.cpp:244-376).  If fe_out: writes f_e (n_el x 30).  If energy_out: writes
@@ -312,6 +432,24 @@ __global__ void nodal_average_kernel(int64_t n_nodes, const int64_t* __restrict_
 // ---------------------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------------------
+int launch_assemble_tiles(const AsmTileArgs& A, int n_tiles, int ne_max, const double* nodes, const int32_t* conn,
+                          const double* props, const uint8_t* fixed, int64_t nnzb, double* k64, float* k32, int* flags,
+                          cudaStream_t st) {
+  if (n_tiles == 0) return 0;
+  const size_t smem = (size_t)ne_max * kAsmElStride * sizeof(double);
+  static int configured_bytes[64] = {0};  // per device: the largest dynamic size allowed so far
+  int dev = 0;
+  WN_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) dev = 0;
+  if ((int)smem > configured_bytes[dev] && smem > 48 * 1024) {
+    WN_CUDA(cudaFuncSetAttribute(assemble_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured_bytes[dev] = (int)smem;
+  }
+  assemble_tiles_kernel<<<n_tiles, kAsmThreads, smem, st>>>(A, nodes, conn, props, fixed, nnzb, k64, k32, flags);
+  WN_CUDA(cudaGetLastError());
+  return 0;
+}
+
 int launch_ke_upper(int64_t n_el, int64_t n_nodes, const double* nodes, const int32_t* conn, const double* props,
                     double* out, int* flags, cudaStream_t st) {
   if (n_el == 0) return 0;

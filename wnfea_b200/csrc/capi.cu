@@ -225,7 +225,35 @@ int wn_solid_create(int64_t n_nodes, int64_t n_el, const double* nodes, const in
   st = st ? st : s->diag_block.upload(pat.diag_block);
   st = st ? st : s->emap.upload(pat.emap);
   st = st ? st : s->gptr.upload(pat.gather_ptr);
-  st = st ? st : s->gsrc.upload(pat.gather_src);
+  {
+    // tile-owner assembly when every tile's incident elements fit in shared memory (200 of them,
+    // 206 KB); the tiles are those of the streamed fine matrix
+    AssemblyPlan plan;
+    std::vector<StreamTile> stiles;
+    const bool ok = build_assembly_plan(pat, n_el, kStreamCap, kStreamRowCap, 200, plan) == 0 &&
+                    build_stream_tiles(pat.row_ptr.data(), n_nodes, stiles) && stiles.size() == plan.tiles.size();
+    bool same = ok;
+    for (size_t t = 0; same && t < stiles.size(); ++t)
+      same = stiles[t].r0 == plan.tiles[t].r0 && stiles[t].r1 == plan.tiles[t].r1;
+    if (same && plan.n_tiles > 0) {
+      s->asm_tiles = plan.n_tiles;
+      s->asm_ne_max = plan.ne_max;
+      std::vector<int32_t> tl(plan.tiles.size() * 4);
+      for (size_t t = 0; t < plan.tiles.size(); ++t) {
+        tl[4 * t] = plan.tiles[t].r0;
+        tl[4 * t + 1] = plan.tiles[t].r1;
+        tl[4 * t + 2] = plan.tiles[t].b0;
+        tl[4 * t + 3] = plan.tiles[t].b1;
+      }
+      st = st ? st : s->asm_tile.upload(tl);
+      st = st ? st : s->asm_el_ptr.upload(plan.el_ptr);
+      st = st ? st : s->asm_el.upload(plan.el);
+      st = st ? st : s->asm_perm.upload(plan.perm);
+      st = st ? st : s->asm_contrib.upload(plan.contrib);
+    } else {
+      st = st ? st : s->gsrc.upload(pat.gather_src);
+    }
+  }
   st = st ? st : s->inc_ptr.upload(pat.inc_ptr);
   st = st ? st : s->inc_ea.upload(pat.inc_ea);
   st = st ? st : s->flags.alloc(16);
@@ -249,6 +277,39 @@ int wn_solid_create(int64_t n_nodes, int64_t n_el, const double* nodes, const in
   s->h_diag_block = std::move(pat.diag_block);
   s->h_fixed.assign(n_nodes * 3, 0);
   *out_handle = s;
+  return 0;
+}
+
+int wn_assembly_plan_host(int64_t n_nodes, int64_t n_el, const int32_t* conn, int64_t* n_tiles, int* ne_max,
+                          int64_t* n_el_entries, int32_t* tiles, int32_t* el_ptr, int32_t* el, uint16_t* contrib,
+                          uint16_t* perm) {
+  WN_REQUIRE(n_tiles && ne_max && n_el_entries && (conn || n_el == 0) && n_nodes > 0 && n_el >= 0, WN_EINVAL,
+             "wn_assembly_plan_host: bad argument");
+  Bsr3Pattern pat;
+  int rc = build_bsr3_pattern(n_nodes, n_el, conn, pat);
+  WN_REQUIRE(rc != -3, WN_EMESH, "wn_assembly_plan_host: element node index out of range");
+  WN_REQUIRE(rc == 0, WN_EINVAL, "wn_assembly_plan_host: pattern construction failed (%d)", rc);
+  AssemblyPlan plan;
+  if (build_assembly_plan(pat, n_el, kStreamCap, kStreamRowCap, 200, plan) != 0) {
+    *n_tiles = 0;
+    *ne_max = 0;
+    *n_el_entries = 0;
+    return 0;
+  }
+  *n_tiles = plan.n_tiles;
+  *ne_max = plan.ne_max;
+  *n_el_entries = (int64_t)plan.el.size();
+  if (tiles)
+    for (int t = 0; t < plan.n_tiles; ++t) {
+      tiles[4 * t] = plan.tiles[t].r0;
+      tiles[4 * t + 1] = plan.tiles[t].r1;
+      tiles[4 * t + 2] = plan.tiles[t].b0;
+      tiles[4 * t + 3] = plan.tiles[t].b1;
+    }
+  if (el_ptr) std::copy(plan.el_ptr.begin(), plan.el_ptr.end(), el_ptr);
+  if (el) std::copy(plan.el.begin(), plan.el.end(), el);
+  if (contrib) std::copy(plan.contrib.begin(), plan.contrib.end(), contrib);
+  if (perm) std::copy(plan.perm.begin(), plan.perm.end(), perm);
   return 0;
 }
 
@@ -330,15 +391,33 @@ int wn_assemble_c3d10_device(void* h, const double* d_props, int apply_bcs, uint
   cudaStream_t st = (cudaStream_t)stream;
   WN_CHECK(s->props.alloc(s->n_el * 2));
   if (s->n_el) WN_CUDA(cudaMemcpyAsync(s->props.p, d_props, s->props.bytes(), cudaMemcpyDeviceToDevice, st));
-  WN_CHECK(s->ke.alloc(s->n_el * 55 * 9));
   WN_CHECK(s->k64.alloc(s->nnzb * 9));
   WN_CHECK(s->k32.alloc(s->nnzb * 9));
   WN_CUDA(cudaMemsetAsync(s->flags.p, 0, sizeof(int), st));
-  WN_CHECK(launch_ke_upper(s->n_el, s->n_nodes, s->nodes.p, s->conn.p, s->props.p, s->ke.p, s->flags.p, st));
-  WN_CHECK(launch_gather_assemble(s->nnzb, s->gptr.p, s->gsrc.p, s->ke.p, s->block_row.p, s->col_idx.p,
-                                  apply_bcs ? s->fixed.p : nullptr, s->k64.p, s->k32.p, st));
-  // tile-major copies for the streamed fine-level kernels
-  if (s->stream_fine) WN_CHECK(s->fine.pack(s->row_ptr.p, s->col_idx.p, s->k32.p, s->k64.p, s->nnzb, st));
+  if (s->asm_tiles > 0) {
+    // tile-owner assembly: values and, when the packs exist with their structure, the packs'
+    // values too, in one kernel with no element scratch
+    const bool fused = s->stream_fine && s->fine.n_tiles == s->asm_tiles && s->fine.structure &&
+                       s->fine.p64.p && s->fine.p32.p;
+    AsmTileArgs A{s->asm_tile.p, s->asm_el_ptr.p, s->asm_el.p, s->asm_perm.p, s->gptr.p, s->asm_contrib.p,
+                  s->block_row.p, s->col_idx.p,
+                  fused ? reinterpret_cast<const int32_t*>(s->fine.d64.p) : nullptr,
+                  fused ? reinterpret_cast<const int32_t*>(s->fine.d32.p) : nullptr,
+                  fused ? s->fine.p64.p : nullptr, fused ? s->fine.p32.p : nullptr};
+    WN_CHECK(launch_assemble_tiles(A, s->asm_tiles, s->asm_ne_max, s->nodes.p, s->conn.p, s->props.p,
+                                   apply_bcs ? s->fixed.p : nullptr, s->nnzb, s->k64.p, s->k32.p, s->flags.p, st));
+    if (fused)
+      s->fine.packed = true;
+    else if (s->stream_fine)  // first assembly: build the packs (structure and values) from the arrays
+      WN_CHECK(s->fine.pack(s->row_ptr.p, s->col_idx.p, s->k32.p, s->k64.p, s->nnzb, st));
+  } else {
+    WN_CHECK(s->ke.alloc(s->n_el * 55 * 9));
+    WN_CHECK(launch_ke_upper(s->n_el, s->n_nodes, s->nodes.p, s->conn.p, s->props.p, s->ke.p, s->flags.p, st));
+    WN_CHECK(launch_gather_assemble(s->nnzb, s->gptr.p, s->gsrc.p, s->ke.p, s->block_row.p, s->col_idx.p,
+                                    apply_bcs ? s->fixed.p : nullptr, s->k64.p, s->k32.p, st));
+    // tile-major copies for the streamed fine-level kernels
+    if (s->stream_fine) WN_CHECK(s->fine.pack(s->row_ptr.p, s->col_idx.p, s->k32.p, s->k64.p, s->nnzb, st));
+  }
   int flag = 0;
   WN_CHECK(read_flag(s, st, &flag));
   WN_REQUIRE(flag == 0, WN_EMESH, "wn_assemble_c3d10: non-positive Jacobian determinant in a C3D10 element");

@@ -188,6 +188,11 @@ int wn_solve(void* h, const double* F, double* u, const wn_solve_params* params,
   return 0;
 }
 
+int wn_solve_profile(void* h, int capacity, int* n_rows, char* names, int64_t* counts, double* ms, double* bytes) {
+  WN_REQUIRE(h && n_rows && capacity >= 0, WN_EINVAL, "wn_solve_profile: bad argument");
+  return solver_profile(reinterpret_cast<Solid*>(h), capacity, n_rows, names, counts, ms, bytes);
+}
+
 int wn_solve_multi_device(void* h, int n_rhs, const double* d_F, double* d_U, const wn_solve_params* params,
                           wn_solve_stats* stats, int* case_iters, double* case_rel_res, uintptr_t stream) {
   WN_REQUIRE(h && params && n_rhs >= 0 && (n_rhs == 0 || (d_F && d_U)), WN_EINVAL,

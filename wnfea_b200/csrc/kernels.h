@@ -8,6 +8,27 @@
 namespace wn {
 
 // c3d10.cu
+// tile-owner assembly (assemble_tiles_kernel): device arrays of an AssemblyPlan (pattern.h) and,
+// when the packs of the streamed fine matrix use the same tiles, their descriptors and buffers
+// (p64 == nullptr: no packs written)
+struct AsmTileArgs {
+  const int32_t* tiles;      // n_tiles x 4: r0, r1, b0, b1
+  const int32_t* el_ptr;     // n_tiles + 1
+  const int32_t* el;         // incident elements per tile
+  const uint16_t* perm;      // nnzb
+  const int32_t* gptr;       // nnzb + 1
+  const uint16_t* contrib;   // n_el * 100
+  const int32_t* block_row;  // nnzb
+  const int32_t* col_idx;    // nnzb
+  const int32_t* d64;        // pack descriptors (n_tiles x 4: r0, r1, seg, cntp) or null
+  const int32_t* d32;
+  unsigned char* p64;        // packs or null
+  unsigned char* p32;
+};
+// flags bit 0: det J <= 0.  Dynamic shared memory: ne_max elements of 129 doubles.
+int launch_assemble_tiles(const AsmTileArgs& A, int n_tiles, int ne_max, const double* nodes, const int32_t* conn,
+                          const double* props, const uint8_t* fixed, int64_t nnzb, double* k64, float* k32, int* flags,
+                          cudaStream_t st);
 // flags: bit 0 = det J <= 0, bit 1 = node index outside [0, n_nodes) (that element: zero Ke)
 int launch_ke_upper(int64_t n_el, int64_t n_nodes, const double* nodes, const int32_t* conn, const double* props,
                     double* out, int* flags, cudaStream_t st);

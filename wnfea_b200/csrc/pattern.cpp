@@ -18,7 +18,7 @@
 
 namespace wn {
 
-static void parallel_for(int64_t n, int nthreads, const std::function<void(int64_t, int64_t)>& fn) {
+void parallel_for(int64_t n, int nthreads, const std::function<void(int64_t, int64_t)>& fn) {
   if (nthreads <= 1 || n < 4096) {
     fn(0, n);
     return;
@@ -139,6 +139,72 @@ int build_bsr3_pattern(int64_t n_nodes, int64_t n_el, const int32_t* conn, Bsr3P
           out.gather_src[pos[blk]++] = (int32_t)((e * 55 + tri) * 2 + (ia > ib ? 1 : 0));
         }
   }
+  return 0;
+}
+
+// Tile-owner assembly plan.  Tiles: whole block rows, at most tile_blocks blocks and tile_rows
+// rows each, greedy in row order (the tiling of the streamed fine matrix).
+int build_assembly_plan(const Bsr3Pattern& pat, int64_t n_el, int tile_blocks, int tile_rows, int ne_cap,
+                        AssemblyPlan& out) {
+  out = AssemblyPlan();
+  const int64_t n = pat.n_nodes;
+  const int32_t* rp = pat.row_ptr.data();
+  for (int64_t r = 0; r < n;) {
+    const int64_t r0 = r;
+    if (rp[r + 1] - rp[r] > tile_blocks) return 1;
+    while (r < n && r - r0 < tile_rows && rp[r + 1] - rp[r0] <= tile_blocks) ++r;
+    out.tiles.push_back({(int32_t)r0, (int32_t)r, rp[r0], rp[r]});
+  }
+  const int64_t nt = (int64_t)out.tiles.size();
+  if (nt >= (int64_t)INT32_MAX || ne_cap > 256) return 1;
+  out.n_tiles = (int)nt;
+  // incident elements per tile: the elements of the incidence lists of its rows
+  std::vector<std::vector<int32_t>> els(nt);
+  std::vector<int> over(nt, 0);
+  const int nth = host_threads();
+  parallel_for(nt, nth, [&](int64_t a, int64_t b) {
+    for (int64_t t = a; t < b; ++t) {
+      std::vector<int32_t>& v = els[t];
+      for (int64_t q = pat.inc_ptr[out.tiles[t].r0]; q < pat.inc_ptr[out.tiles[t].r1]; ++q) v.push_back(pat.inc_ea[q] / 10);
+      std::sort(v.begin(), v.end());
+      v.erase(std::unique(v.begin(), v.end()), v.end());
+      if ((int)v.size() > ne_cap) over[t] = 1;
+    }
+  });
+  for (int64_t t = 0; t < nt; ++t) {
+    if (over[t]) return 1;
+    out.ne_max = std::max(out.ne_max, (int)els[t].size());
+  }
+  out.el_ptr.assign(nt + 1, 0);
+  for (int64_t t = 0; t < nt; ++t) out.el_ptr[t + 1] = out.el_ptr[t] + (int32_t)els[t].size();
+  out.el.resize(out.el_ptr[nt]);
+  out.contrib.resize(pat.gather_src.size());
+  out.perm.resize(pat.nnzb);
+  parallel_for(nt, nth, [&](int64_t a, int64_t b) {
+    std::vector<std::pair<int32_t, int32_t>> order;
+    for (int64_t t = a; t < b; ++t) {
+      const std::vector<int32_t>& v = els[t];
+      std::copy(v.begin(), v.end(), out.el.begin() + out.el_ptr[t]);
+      const AssemblyTile& T = out.tiles[t];
+      order.clear();
+      for (int32_t blk = T.b0; blk < T.b1; ++blk) {
+        for (int32_t q = pat.gather_ptr[blk]; q < pat.gather_ptr[blk + 1]; ++q) {
+          const int32_t src = pat.gather_src[q];  // (e * 55 + tri) * 2 + transposed
+          const int32_t e = (src >> 1) / 55, tri = (src >> 1) % 55;
+          int lo = 0;
+          while (tri_index(lo + 1, lo + 1) <= tri) ++lo;  // tri_index(lo, lo) <= tri < tri_index(lo + 1, lo + 1)
+          const int hi = lo + (tri - tri_index(lo, lo));
+          const int ea = (src & 1) ? hi : lo, eb = (src & 1) ? lo : hi;
+          const int slot = (int)(std::lower_bound(v.begin(), v.end(), e) - v.begin());
+          out.contrib[q] = (uint16_t)((slot << 8) | (ea << 4) | eb);
+        }
+        order.push_back({pat.gather_ptr[blk + 1] - pat.gather_ptr[blk], blk - T.b0});
+      }
+      std::stable_sort(order.begin(), order.end(), [](const std::pair<int32_t, int32_t>& x,
+                                                     const std::pair<int32_t, int32_t>& y) { return x.first > y.first; });
+      for (size_t k = 0; k < order.size(); ++k) out.perm[T.b0 + k] = (uint16_t)order[k].second;
+    }
+  });
   return 0;
 }
 

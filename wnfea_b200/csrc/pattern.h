@@ -28,5 +28,32 @@ struct Bsr3Pattern {
 
 int build_bsr3_pattern(int64_t n_nodes, int64_t n_el, const int32_t* conn, Bsr3Pattern& out);
 int host_threads();
+void parallel_for(int64_t n, int nthreads, const std::function<void(int64_t, int64_t)>& fn);
+
+// Plan of the tile-owner assembly (c3d10.cu assemble_tiles_kernel): the block rows are cut into
+// the row tiles of the streamed fine matrix; the CTA of a tile computes the Cartesian shape
+// derivatives of every element incident to its rows once (shared memory) and then sums each of
+// its blocks' contributions, in element order, in registers -- no per-element scratch in
+// global memory.
+struct AssemblyTile {
+  int32_t r0, r1, b0, b1;  // block rows [r0, r1) holding blocks [b0, b1)
+};
+struct AssemblyPlan {
+  int n_tiles = 0;
+  int ne_max = 0;                 // most distinct elements incident to one tile
+  std::vector<AssemblyTile> tiles;
+  std::vector<int32_t> el_ptr;    // n_tiles + 1
+  std::vector<int32_t> el;        // the tile's incident elements, ascending
+  // per block, its contributions in the gather order (gather_ptr): slot << 8 | a << 4 | b with
+  // slot the element's index in its tile's list and (a, b) the element-local node pair
+  std::vector<uint16_t> contrib;  // n_el * 100
+  // per tile, its local block indices by descending contribution count (lanes of a warp then
+  // carry blocks of similar cost): perm[b0 + k] = local index of the k-th block
+  std::vector<uint16_t> perm;     // nnzb
+};
+// 0: plan made; 1: the row tiles cannot be made (a row over the tile capacity) or a tile has
+// more than ne_cap incident elements (the caller keeps the element-scratch assembly).
+int build_assembly_plan(const Bsr3Pattern& pat, int64_t n_el, int tile_blocks, int tile_rows, int ne_cap,
+                        AssemblyPlan& out);
 
 }  // namespace wn

@@ -36,7 +36,11 @@ struct Solid {
   DArray<double> props;     // n_el x 2  [E, nu]
   // pattern + maps
   DArray<int32_t> row_ptr, col_idx, block_row, diag_block;
-  DArray<int32_t> emap, gptr, gsrc;
+  DArray<int32_t> emap, gptr, gsrc;  // gsrc: only for the element-scratch assembly (no plan)
+  // tile-owner assembly plan (pattern.h AssemblyPlan); asm_tiles == 0: element-scratch assembly
+  int asm_tiles = 0, asm_ne_max = 0;
+  DArray<int32_t> asm_tile, asm_el_ptr, asm_el;
+  DArray<uint16_t> asm_perm, asm_contrib;
   DArray<int64_t> inc_ptr;
   DArray<int32_t> inc_ea;
   // values

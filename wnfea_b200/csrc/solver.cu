@@ -21,6 +21,8 @@
 //     Every mode runs inside an FP64 refinement loop whose residual r = F - K u uses the FP64
 //     matrix with compensated arithmetic.
 #include <chrono>
+#include <map>
+#include <string>
 #include <type_traits>
 #include <cmath>
 #include <cstring>
@@ -1013,6 +1015,28 @@ static void level_spmv(const DevBsr& M, const StreamMat& Ms, const T* vals, cons
 static inline int rows_grid(int64_t n_rows) { return grid_for(n_rows, 32, kThreads, 8); }
 static inline int vec_grid(int64_t n) { return grid_for(n, 1, kThreads, 8); }
 
+// ---------------------------------------------------------------------------------------
+// launch accounting: algorithmic bytes per launch (unique reads + writes of the kernel's
+// arrays) and, in profile mode, an event after the launch
+// ---------------------------------------------------------------------------------------
+// one pass over a block matrix: values, column indices, row pointers
+static double mat_bytes(int64_t nnzb, int br, int bc, int64_t n_rows, int value_bytes) {
+  return (double)nnzb * (br * bc * value_bytes + 4) + 4.0 * (double)(n_rows + 1);
+}
+
+static void note(SolverWork& W, cudaStream_t st, const char* kind, int level, double bytes) {
+  W.bytes += bytes;
+  if (!W.profile) return;
+  const size_t i = W.notes.size();
+  while (W.note_events.size() < i + 2) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    W.note_events.push_back(e);
+  }
+  cudaEventRecord(W.note_events[i + 1], st);
+  W.notes.push_back({kind, level, bytes, W.cur_iter, W.cur_prec, true});
+}
+
 template <typename T>
 struct Prec;
 template <>
@@ -1068,11 +1092,13 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
     k_coarse<T><<<resident_grid(k_coarse<T>, kThreads, (H.n_coarse + rows_per_cta - 1) / rows_per_cta), kThreads, 0,
                   st>>>(H.n_coarse, H.coarse_inv.p, b, out, S);
     W.launches++;
+    note(W, st, "coarse", -1, (double)H.n_coarse * H.n_coarse * 8 + 2.0 * H.n_coarse * sizeof(T));
     if (part) {  // a hierarchy without levels: the PCG's r . z comes from here
       const int g = resident_grid(k_dot_pair<T>, kThreads, (H.n_coarse + kThreads - 1) / kThreads);
       W.npA = g;
       k_dot_pair<T><<<g, kThreads, 0, st>>>(H.n_coarse, b, out, part, S);
       W.launches++;
+      note(W, st, "dot", -1, 2.0 * H.n_coarse * sizeof(T));
     }
     WN_CUDA(cudaGetLastError());
     return 0;
@@ -1087,6 +1113,13 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
   const T it = (T)L.inv_theta;
   const int64_t sd = (lvl == 0) ? s->nnzb : 0;  // component stride of the fine matrix
   const int64_t work = (nr * 32 + kThreads - 1) / kThreads;
+  // algorithmic bytes: the level matrix, one level vector, the transfer operators
+  const double Vb = (double)nr * L.bs * sizeof(T);
+  const double Ab = mat_bytes(lvl == 0 ? s->nnzb : L.A.nnzb, L.bs, L.bs, nr, sizeof(T));
+  const int64_t nc_dofs = (lvl + 1 < nlev) ? H.levels[lvl + 1].n_nodes * H.levels[lvl + 1].bs : H.n_coarse;
+  const double Vc = (double)nc_dofs * sizeof(T);
+  const double Rb = mat_bytes(L.R.nnzb, L.R.br, L.R.bc, L.R.n_rows, sizeof(T));
+  const double Pb = mat_bytes(L.P.nnzb, L.P.br, L.P.bc, L.P.n_rows, sizeof(T));
   auto run = [&](auto bs_tag) -> int {
     constexpr int BS = decltype(bs_tag)::value;
     auto rg = [&](auto kern) { return resident_grid(kern, kThreads, work); };
@@ -1106,6 +1139,7 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
       k_pre_first<BS, T><<<rg(k_pre_first<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, deg, c1, c2,
                                                                       V.x.p, V.r.p, V.d.p, V.res.p, S);
     W.launches++;
+    note(W, st, "pre_smooth", lvl, Ab + (deg == 1 ? 4 : 5) * Vb);
     T* din = V.d.p;
     T* dout = V.d2.p;
     for (int k = 2; k < deg; ++k) {
@@ -1116,6 +1150,7 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
         k_cheb_step<BS, T><<<rg(k_cheb_step<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout, V.r.p,
                                                                         V.x.p, ck1, ck2, b, nullptr, S);
       W.launches++;
+      note(W, st, "pre_cheb", lvl, Ab + 7 * Vb);
       std::swap(din, dout);
     }
     if (deg >= 2) {
@@ -1123,6 +1158,7 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
                                             nullptr)))
         k_residual<BS, T><<<rg(k_residual<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, V.x.p, V.res.p, S);
       W.launches++;
+      note(W, st, "residual", lvl, Ab + 3 * Vb);
     }
     // restriction b_c = R res
     DevLevel* Ln = lvl + 1 < nlev ? &H.levels[lvl + 1] : nullptr;
@@ -1130,10 +1166,12 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
     T* xc = Ln ? Prec<T>::vecs(*Ln).x2.p : Prec<T>::cx(H);
     level_spmv<6, BS, T>(L.R, L.Rs, Prec<T>::Rv(L), V.res.p, bc, 0, S, st);
     W.launches++;
+    note(W, st, "restrict", lvl, Rb + Vb + Vc);
     WN_CHECK(vcycle<T>(s, H, W, lvl + 1, bc, xc, nullptr, S, st));
     // prolongation x += P x_c
     level_spmv<BS, 6, T>(L.P, L.Ps, Prec<T>::Pv(L), xc, V.x.p, 1, S, st);
     W.launches++;
+    note(W, st, "prolong", lvl, Pb + Vc + 2 * Vb);
     // post-smoothing: result in `out`
     double* part_last = (deg == 1) ? part : nullptr;
     int gpf = 0;
@@ -1146,6 +1184,7 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
     }
     if (part_last) W.npA = gpf;
     W.launches++;
+    note(W, st, "post_smooth", lvl, Ab + 6 * Vb);
     din = V.d.p;
     dout = V.d2.p;
     for (int k = 1; k < deg; ++k) {
@@ -1161,6 +1200,7 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
       }
       if (pk) W.npA = gcs;
       W.launches++;
+      note(W, st, "post_cheb", lvl, Ab + (pk ? 8 : 7) * Vb);
       std::swap(din, dout);
     }
     return 0;
@@ -1190,6 +1230,7 @@ static int apply_prec(Solid* s, SolverWork& W, int precond, const T* r, T* z, Pc
     else
       launch(k_prec_block<6, T>);
     W.launches++;
+    note(W, st, "block_jacobi", -1, (2.0 + s->bs) * W.n * sizeof(T));
     WN_CUDA(cudaGetLastError());
     return 0;
   }
@@ -1198,6 +1239,7 @@ static int apply_prec(Solid* s, SolverWork& W, int precond, const T* r, T* z, Pc
   k_prec_vec<T><<<gp, kThreads, 0, st>>>(W.n, r, Prec<T>::fine_dinv(W), precond == 1 ? 1 : 0, z,
                                                          W.partA.p, S);
   W.launches++;
+  note(W, st, precond == 1 ? "jacobi" : "copy", -1, (precond == 1 ? 3.0 : 2.0) * W.n * sizeof(T));
   WN_CUDA(cudaGetLastError());
   return 0;
 }
@@ -1260,14 +1302,25 @@ static int pcg_iteration(Solid* s, SolverWork& W, int precond, int k, PcgScalars
                                                    p_new, B.q, W.partA.p, W.partB.p, W.npA, k == 0, par, S);
     return g;
   };
+  const double b_start = W.bytes;
   const int gsd = s->bs == 3 ? spmv_dot(std::integral_constant<int, 3>{}) : spmv_dot(std::integral_constant<int, 6>{});
+  const double nK = (double)W.n * sizeof(TK), nM = (double)W.n * sizeof(TM);
+  note(W, st, "pcg_spmv_dot", -1, mat_bytes(s->nnzb, s->bs, s->bs, s->n_nodes, sizeof(TK)) + nM + 3 * nK);
   W.npB = gsd;
   k_update<TK, TM><<<gup, kThreads, 0, st>>>(W.n, B.x, B.r, B.rm, p_new, B.q, W.partB.p, W.partC.p, W.npB, par, S);
+  note(W, st, "pcg_update", -1, 6 * nK + (B.rm ? nM : 0.0));
   W.npC = gup;
   k_check<<<1, kThreads, 0, st>>>(S, W.partC.p, W.npC);
+  note(W, st, "pcg_check", -1, 0.0);
   W.launches += 3;
   WN_CUDA(cudaGetLastError());
-  return apply_prec<TM>(s, W, precond, prec_input(B), B.z, S, st);
+  const double b_mid = W.bytes;
+  W.cur_prec = true;
+  const int rc = apply_prec<TM>(s, W, precond, prec_input(B), B.z, S, st);
+  W.cur_prec = false;
+  W.iter_core_bytes = b_mid - b_start;
+  W.iter_prec_bytes = W.bytes - b_mid;
+  return rc;
 }
 
 // PCG on the fine matrix: solves A x = b from x = 0 to ||r|| <= rtol ||b||.  The first chunk
@@ -1279,16 +1332,25 @@ static int pcg_solve(Solid* s, SolverWork& W, int mode, const TK* b, double rtol
   PcgBufs<TK, TM> B = pcg_bufs<TK, TM>(s, W);
   WN_CUDA(cudaMemsetAsync(B.p0, 0, W.n * sizeof(TK), st));  // iteration 0: p = z + 0 * p_old
   WN_CUDA(cudaMemsetAsync(B.p1, 0, W.n * sizeof(TK), st));
+  const size_t note0 = W.notes.size();
+  W.cur_iter = -1;
   W.npC = resident_grid(k_init_vecs<TK, TM>, kThreads, (W.n + kThreads - 1) / kThreads);
   k_init_vecs<TK, TM><<<W.npC, kThreads, 0, st>>>(W.n, b, B.x, B.r, B.rm, W.partC.p);
+  note(W, st, "pcg_init", -1, 3.0 * W.n * sizeof(TK) + (B.rm ? (double)W.n * sizeof(TM) : 0.0));
   k_init_scalars<<<1, kThreads, 0, st>>>(S, W.partC.p, W.npC, rtol, max_iter);
+  note(W, st, "pcg_check", -1, 0.0);
   W.launches += 2;
   WN_CUDA(cudaGetLastError());
   WN_CHECK(apply_prec<TM>(s, W, precond, prec_input(B), B.z, S, st));
+  const double bytes_before_iterations = W.bytes;
   chunk = std::max(2, chunk + (chunk & 1));  // even: the parity pattern repeats per chunk
+  if (W.profile) use_graph = 0;  // every launch timed by its own event
   GraphCache& G = W.graphs[mode][precond];
   const int64_t key = chunk;
-  for (int k = 0; k < chunk && k < max_iter; ++k) WN_CHECK((pcg_iteration<TK, TM>(s, W, precond, k, S, st)));
+  for (int k = 0; k < chunk && k < max_iter; ++k) {
+    W.cur_iter = k;
+    WN_CHECK((pcg_iteration<TK, TM>(s, W, precond, k, S, st)));
+  }
   int k0 = chunk;
   while (true) {
     WN_CUDA(cudaMemcpyAsync(hS, S, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
@@ -1299,6 +1361,8 @@ static int pcg_solve(Solid* s, SolverWork& W, int mode, const TK* b, double rtol
         G.reset();
         cudaGraph_t graph;
         const int64_t before = W.launches;
+        const double bytes_before = W.bytes;
+        const double core = W.iter_core_bytes, prec = W.iter_prec_bytes;
         WN_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         int rc = 0;
         // the iteration count and max_iter live on the device (k_check) and the chunk is
@@ -1314,13 +1378,29 @@ static int pcg_solve(Solid* s, SolverWork& W, int mode, const TK* b, double rtol
         G.stream = st;
         G.kernels = W.launches - before;
         W.launches = before;
+        W.bytes = bytes_before;  // captured, not run
+        W.iter_core_bytes = core;
+        W.iter_prec_bytes = prec;
       }
       WN_CUDA(cudaGraphLaunch(G.exec, st));
       W.launches += G.kernels;
     } else {
-      for (int k = 0; k < chunk; ++k) WN_CHECK((pcg_iteration<TK, TM>(s, W, precond, k0 + k, S, st)));
+      for (int k = 0; k < chunk; ++k) {
+        W.cur_iter = k0 + k;
+        WN_CHECK((pcg_iteration<TK, TM>(s, W, precond, k0 + k, S, st)));
+      }
     }
     k0 += chunk;
+  }
+  W.cur_iter = -1;
+  // bytes of the iterations that ran: I products / updates / checks and I - 1 preconditioner
+  // applies (the last check ends the loop before its apply); launches past the device-side
+  // end of the loop return at once and count nothing
+  const int I = hS->iters;
+  W.bytes = bytes_before_iterations + I * W.iter_core_bytes + std::max(I - 1, 0) * W.iter_prec_bytes;
+  for (size_t i = note0; i < W.notes.size(); ++i) {
+    SolverWork::Note& nt = W.notes[i];
+    if (nt.iter >= I || (nt.prec && nt.iter == I - 1)) nt.valid = false;
   }
   return 0;
 }
@@ -1473,7 +1553,10 @@ static int true_residual(Solid* s, SolverWork& W, const double* F, float* r32, c
     launch(k_outer_residual_dd<3>);
   else
     launch(k_outer_residual_dd<6>);
+  note(W, st, "outer_residual", -1,
+       mat_bytes(s->nnzb, s->bs, s->bs, s->n_nodes, 8) + 4.0 * W.n * 8 + (r32 ? 4.0 * W.n : 0.0));
   k_reduce_rr<<<1, kThreads, 0, st>>>(W.scal.p + 1, W.partC.p, W.npC);
+  note(W, st, "reduce", -1, 0.0);
   W.launches += 2;
   WN_CUDA(cudaGetLastError());
   PcgScalars h;
@@ -1544,6 +1627,7 @@ static int outer_loop(Solid* s, SolverWork& W, int mode, const double* F, double
     }
     PcgBufs<TK, TM> B = pcg_bufs<TK, TM>(s, W);
     k_accumulate<TK><<<vec_grid(n), kThreads, 0, st>>>(n, W.u64.p, W.ulo.p, B.x);
+    note(W, st, "accumulate", -1, 4.0 * n * 8 + (double)n * sizeof(TK));
     W.launches++;
     WN_CUDA(cudaGetLastError());
   }
@@ -1569,8 +1653,20 @@ int solver_solve(Solid* s, const double* F, double* u, const wn_solve_params& pr
   const int64_t n = W.n;
   const int chunk = prm.chunk > 0 ? prm.chunk : 8;
   PcgScalars hS{};
+  W.bytes = 0.0;
+  W.profile = prm.profile != 0;
+  W.notes.clear();
+  W.cur_iter = -1;
+  W.cur_prec = false;
+  if (W.profile && W.note_events.empty()) {
+    cudaEvent_t e = nullptr;
+    WN_CUDA(cudaEventCreate(&e));
+    W.note_events.push_back(e);
+  }
+  if (W.profile) WN_CUDA(cudaEventRecord(W.note_events[0], st));
   k_fill_dinv<<<vec_grid(n), kThreads, 0, st>>>(s->n_nodes, s->bs, s->nnzb, s->diag_block.p, s->k64.p, W.dinv64.p,
                                                  W.dinv32.p);
+  note(W, st, "fill_dinv", -1, 20.0 * n);
   W.launches++;
   if (prm.precond == 3) {  // block pseudo-inverses of the current values
     const int64_t nb = s->n_nodes * s->bs * s->bs;
@@ -1584,13 +1680,16 @@ int solver_solve(Solid* s, const double* F, double* u, const wn_solve_params& pr
     else
       k_fill_block_pinv<6><<<grid_for(s->n_nodes, 1, 128, 8), 128, 0, st>>>(s->n_nodes, s->nnzb, s->diag_block.p,
                                                                              s->k64.p, W.binv64.p, W.binv32.p);
+    note(W, st, "fill_block_pinv", -1, 20.0 * nb);
     W.launches++;
     WN_CUDA(cudaGetLastError());
   }
   WN_CUDA(cudaEventRecord(W.ev0, st));
   W.npC = resident_grid(k_dot_self<double>, kThreads, (n + kThreads - 1) / kThreads);
   k_dot_self<double><<<W.npC, kThreads, 0, st>>>(n, F, W.partC.p);
+  note(W, st, "dot", -1, 8.0 * n);
   k_reduce_rr<<<1, kThreads, 0, st>>>(W.scal.p + 1, W.partC.p, W.npC);
+  note(W, st, "reduce", -1, 0.0);
   W.launches += 2;
   WN_CUDA(cudaMemcpyAsync(&hS, W.scal.p + 1, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
   WN_CUDA(cudaStreamSynchronize(st));
@@ -1616,6 +1715,27 @@ int solver_solve(Solid* s, const double* F, double* u, const wn_solve_params& pr
   WN_CUDA(cudaEventSynchronize(W.ev1));
   float ms = 0.f;
   WN_CUDA(cudaEventElapsedTime(&ms, W.ev0, W.ev1));
+  if (W.profile) {  // per kernel class: launches that did their work, event-timed durations
+    W.last_profile.clear();
+    std::map<std::string, size_t> row_of;
+    for (size_t i = 0; i < W.notes.size(); ++i) {
+      const SolverWork::Note& nt = W.notes[i];
+      if (!nt.valid) continue;
+      float t = 0.f;
+      WN_CUDA(cudaEventElapsedTime(&t, W.note_events[i], W.note_events[i + 1]));
+      const std::string name = nt.level >= 0 ? "l" + std::to_string(nt.level) + "." + nt.kind : std::string(nt.kind);
+      auto it = row_of.find(name);
+      if (it == row_of.end()) {
+        it = row_of.emplace(name, W.last_profile.size()).first;
+        W.last_profile.push_back(SolverWork::ProfileRow{name, 0, 0.0, 0.0});
+      }
+      SolverWork::ProfileRow& r = W.last_profile[it->second];
+      r.count++;
+      r.ms += t;
+      r.bytes += nt.bytes;
+    }
+    W.profile = false;
+  }
   if (stats) {
     stats->iterations = total_iters;
     stats->outer_iterations = outer;
@@ -1625,6 +1745,23 @@ int solver_solve(Solid* s, const double* F, double* u, const wn_solve_params& pr
     stats->kernel_launches = W.launches;
     stats->setup_seconds = s->amg ? s->amg->setup_seconds : 0.0;
     stats->n_levels = s->amg ? (int)s->amg->levels.size() + 1 : 0;
+    stats->algorithmic_bytes = W.bytes;
+  }
+  return 0;
+}
+
+int solver_profile(Solid* s, int capacity, int* n_rows, char* names, int64_t* counts, double* ms, double* bytes) {
+  WN_REQUIRE(s->work, WN_ESTATE, "solve profile: no solve has run on this handle");
+  const auto& P = s->work->last_profile;
+  *n_rows = (int)P.size();
+  for (int i = 0; i < capacity && i < (int)P.size(); ++i) {
+    if (names) {
+      std::strncpy(names + (size_t)i * 48, P[i].name.c_str(), 47);
+      names[(size_t)i * 48 + 47] = 0;
+    }
+    if (counts) counts[i] = P[i].count;
+    if (ms) ms[i] = P[i].ms;
+    if (bytes) bytes[i] = P[i].bytes;
   }
   return 0;
 }

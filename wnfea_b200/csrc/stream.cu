@@ -32,6 +32,7 @@ static int plan_shape(StreamMat& m, const int32_t* h_rp, int64_t n_rows) {
 void StreamMat::clear() {
   n_tiles = 0;
   packed = false;
+  structure = false;
   plan.release();
   d32.release();
   d64.release();
@@ -73,6 +74,7 @@ int StreamMat::pack(const int32_t* rp, const int32_t* ci, const float* v32, cons
   else if (nv == 18) WN_CHECK(pack_shape<18>(*this, rp, ci, v32, v64, stride, st));
   else return 0;
   packed = true;
+  structure = true;
   return 0;
 }
 

@@ -20,6 +20,7 @@ struct StreamMat {
   DArray<unsigned char> p32, p64;
   int64_t size32 = 0, size64 = 0;
   bool packed = false;  // the packs hold the current values
+  bool structure = false;  // the packs hold the column indices and row starts (set by pack())
   StreamCtl ctl;         // wait limit of the streamed kernels on this matrix (and the test hook)
   // Tile plan and descriptors of a br x bc matrix from its host row pointer (shapes 3x3, 6x6,
   // 3x6, 6x3; others are left unstreamed).  Packs are allocated by pack().

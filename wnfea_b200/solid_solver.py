@@ -173,6 +173,8 @@ def solve_c3d10_system(
         "levels": st["n_levels"],
         "status": st["status"],
         "dof_per_s": K.shape[0] / st["solve_seconds"] if st["solve_seconds"] > 0 else float("inf"),
+        "algorithmic_bytes": st["algorithmic_bytes"],
+        "achieved_GBps": st["algorithmic_bytes"] / st["solve_seconds"] / 1e9 if st["solve_seconds"] > 0 else 0.0,
     }
     return u, stats
 

@@ -101,14 +101,30 @@ class SolidSystem:
 
     def solve(self, F: np.ndarray, rtol: float = 1e-8, max_iter: int = 2000, precond: int = 2,
               precision: int = 0, inner_rtol: float = 0.0, max_outer: int = 10, chunk: int = 8,
-              use_graph: bool = True):
-        """Solve K u = F on the GPU (host buffers); returns (u, stats dict)."""
+              use_graph: bool = True, profile: bool = False):
+        """Solve K u = F on the GPU (host buffers); returns (u, stats dict).  ``profile``: time
+        every kernel with CUDA events (read back with ``profile_table()``)."""
         F = np.ascontiguousarray(F, dtype=np.float64)
         u = np.empty_like(F)
-        prm = _lib.SolveParams(rtol, max_iter, precond, precision, inner_rtol, max_outer, chunk, int(use_graph))
+        prm = _lib.SolveParams(rtol, max_iter, precond, precision, inner_rtol, max_outer, chunk, int(use_graph),
+                               int(profile))
         st = _lib.SolveStats()
         call("wn_solve", self._h, ptr(F), ptr(u), C.byref(prm), C.byref(st))
         return u, {f: getattr(st, f) for f, _ in _lib.SolveStats._fields_}
+
+    def profile_table(self) -> dict:
+        """{kernel class: (launches, ms, algorithmic bytes)} of the last profiled solve."""
+        n = C.c_int()
+        call("wn_solve_profile", self._h, 0, C.byref(n), None, None, None, None)
+        k = n.value
+        names = C.create_string_buffer(48 * max(k, 1))
+        counts = np.zeros(k, dtype=np.int64)
+        ms = np.zeros(k)
+        by = np.zeros(k)
+        call("wn_solve_profile", self._h, k, C.byref(n), names, ptr(counts), ptr(ms), ptr(by))
+        raw = names.raw
+        return {raw[48 * i:48 * i + 48].split(b"\0", 1)[0].decode(): (int(counts[i]), float(ms[i]), float(by[i]))
+                for i in range(k)}
 
     def solve_multi(self, F: np.ndarray, rtol: float = 1e-8, max_iter: int = 2000, precond: int = 2,
                     precision: int = 1, max_outer: int = 10, chunk: int = 8, use_graph: bool = True):
