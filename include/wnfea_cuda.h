@@ -150,6 +150,9 @@ typedef struct wn_amg_params {
   double stream_min_mb;    /* level matrices / transfer operators of at least this many MB
                               in FP32 are streamed from tile-major packs, smaller ones stay
                               L2-resident on the register row kernels; < 0: none     (4)    */
+  int setup_on_device;     /* 1: diagonal, power iterations, prolongator and Galerkin
+                              products on the GPU (aggregation and the per-aggregate QR on
+                              the host); 0: the whole setup on the host               (1)    */
 } wn_amg_params;
 
 /* Defaults above. */

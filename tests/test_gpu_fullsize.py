@@ -7,7 +7,8 @@ full configurations that the benchmark times and check, against the oracle's FP6
 restatement of the reference (solid_solver.py:26-129, 311-365; c3d10.py:219-318):
 
 * the BSR3 pattern and element->block map bit for bit, and the assembled K (with BCs) entry by
-  entry (<= 1e-14 of max |K|, the summation-order tolerance of the small-mesh tests);
+  entry through K - K_oracle (<= 1e-14 of max |K|, the summation-order tolerance of the
+  small-mesh tests);
 * the true residual ||F - K u|| / ||F|| of the GPU's FP64 u in 80-bit host arithmetic with the
   oracle's K, for the FP64 and the mixed solve (and 4 of the 32 batched cases), at the requested
   1e-8 or at the FP64 rounding level of K u;
@@ -80,8 +81,12 @@ def test_fullsize_pattern_map_and_matrix(ibeam):
     _lib.call("wn_solid_get_map", s.handle, _lib.ptr(emap))
     assert np.array_equal(emap, oemap)
     Kc = K.tocsr()
-    assert np.array_equal(Kc.indptr, Ko.indptr) and np.array_equal(Kc.indices, Ko.indices)
-    assert np.abs(Kc.data - Ko.data).max() <= 1e-14 * np.abs(Ko.data).max()
+    # entries whose exact value is zero (couplings that cancel by symmetry) may come out as exact
+    # zeros in one summation order and as ~1e-17 in the other, so eliminate_zeros can keep a few
+    # thousand more or fewer of them: compare through the difference
+    D = (Kc - Ko).tocsr()
+    assert np.abs(D.data).max(initial=0.0) <= 1e-14 * np.abs(Ko.data).max()
+    assert abs(Kc.nnz - Ko.nnz) <= 1e-3 * Ko.nnz
     assert np.array_equal(F, Fo)
 
 

@@ -35,6 +35,7 @@ class AmgParams(C.Structure):
         ("smooth_prolongator", C.c_int),
         ("power_iters", C.c_int),
         ("stream_min_mb", C.c_double),
+        ("setup_on_device", C.c_int),
     ]
 
 

@@ -1,6 +1,7 @@
 """Smoothed-aggregation AMG of the C3D10 path: parameters, hierarchy export, host-only setup.
 
-The hierarchy itself is built by the library (host C++ setup, GPU apply).  This module
+The hierarchy itself is built by the library (GPU setup with host aggregation by default, or
+the whole setup in host C++; GPU apply).  This module
 exposes its knobs (``AMGParams`` = ``wn_amg_params``) and reads a hierarchy back as scipy
 matrices, for inspection and for the parity tests.  The reference's counterpart is the
 beam-only ``BlockBeamAMGPreconditioner`` (wnfea/solver/amg_preconditioner.py:147-661);
@@ -32,6 +33,7 @@ class AMGParams:
     smooth_prolongator: int = 1
     power_iters: int = 15
     stream_min_mb: float = 4.0
+    setup_on_device: int = 1
 
     def to_c(self) -> _lib.AmgParams:
         return _lib.AmgParams(**{f.name: getattr(self, f.name) for f in fields(self)})

@@ -60,6 +60,8 @@ struct DevLevel {
   StreamMat As, Ps, Rs;
   LevelVecs<double> v64;
   LevelVecs<float> v32;
+  // host row pointers of A (levels >= 1), P and R when the hierarchy was built on the device
+  std::vector<int32_t> h_A_rp, h_P_rp, h_R_rp;
 };
 
 struct AmgHierarchy {
@@ -71,6 +73,8 @@ struct AmgHierarchy {
   DArray<float> cb32, cx32;   // (FP32 path)
   int degree = 2;
   double setup_seconds = 0.0;
+  bool device_built = false;  // levels made by amg_build_device (host.levels hold no matrices
+  bool host_synced = false;   // until amg_sync_host copies them down)
   uint64_t id = 0;  // unique per setup (workspaces sized for a hierarchy compare it)
 };
 

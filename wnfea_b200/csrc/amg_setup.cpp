@@ -43,6 +43,7 @@ wn_amg_params amg_default_params() {
   p.smooth_prolongator = 1;
   p.power_iters = 15;
   p.stream_min_mb = 4.0;
+  p.setup_on_device = 1;
   return p;
 }
 
@@ -181,60 +182,11 @@ int64_t aggregate(const View& A, double theta, std::vector<int32_t>& agg) {
   const int64_t n = A.n_rows;
   const int bsz = A.br * A.bc;
   std::vector<double> nrm(A.rp[n]);
-  std::vector<double> dn(n, 0.0);
   par_rows(n, [&](int64_t a, int64_t b, int) {
     for (int64_t i = a; i < b; ++i)
-      for (int32_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-        nrm[k] = block_fro(A.v + (int64_t)k * bsz, bsz);
-        if (A.ci[k] == i) dn[i] = nrm[k];
-      }
+      for (int32_t k = A.rp[i]; k < A.rp[i + 1]; ++k) nrm[k] = block_fro(A.v + (int64_t)k * bsz, bsz);
   });
-  std::vector<uint8_t> strong(A.rp[n], 0);
-  std::vector<uint8_t> has_strong(n, 0);
-  par_rows(n, [&](int64_t a, int64_t b, int) {
-    for (int64_t i = a; i < b; ++i)
-      for (int32_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-        const int32_t j = A.ci[k];
-        if (j != i && nrm[k] > 0.0 && nrm[k] >= theta * std::sqrt(dn[i] * dn[j])) {
-          strong[k] = 1;
-          has_strong[i] = 1;
-        }
-      }
-  });
-  agg.assign(n, -1);
-  int64_t na = 0;
-  for (int64_t i = 0; i < n; ++i) {  // pass 1: roots whose strong neighbourhood is free
-    if (agg[i] >= 0 || !has_strong[i]) continue;
-    bool free_all = true;
-    for (int32_t k = A.rp[i]; k < A.rp[i + 1] && free_all; ++k)
-      if (strong[k] && agg[A.ci[k]] >= 0) free_all = false;
-    if (!free_all) continue;
-    agg[i] = (int32_t)na;
-    for (int32_t k = A.rp[i]; k < A.rp[i + 1]; ++k)
-      if (strong[k]) agg[A.ci[k]] = (int32_t)na;
-    ++na;
-  }
-  std::vector<int32_t> pass2(agg);
-  for (int64_t i = 0; i < n; ++i) {  // pass 2: join the strongest aggregated neighbour
-    if (agg[i] >= 0 || !has_strong[i]) continue;
-    double best = -1.0;
-    int32_t ba = -1;
-    for (int32_t k = A.rp[i]; k < A.rp[i + 1]; ++k)
-      if (strong[k] && agg[A.ci[k]] >= 0 && nrm[k] > best) {
-        best = nrm[k];
-        ba = agg[A.ci[k]];
-      }
-    pass2[i] = ba;
-  }
-  agg.swap(pass2);
-  for (int64_t i = 0; i < n; ++i) {  // pass 3: leftovers with strong links form new aggregates
-    if (agg[i] >= 0 || !has_strong[i]) continue;
-    agg[i] = (int32_t)na;
-    for (int32_t k = A.rp[i]; k < A.rp[i + 1]; ++k)
-      if (strong[k] && agg[A.ci[k]] < 0) agg[A.ci[k]] = (int32_t)na;
-    ++na;
-  }
-  return na;
+  return aggregate_norms(n, A.rp, A.ci, nrm.data(), theta, agg);
 }
 
 // thin Householder QR of the m x 6 column-major matrix a: Q (m x 6, column-major), R (6x6)
@@ -434,15 +386,70 @@ void symmetrize(HostBsr& A) {
 
 }  // namespace
 
-int amg_build(const wn_amg_params& prm, int64_t n0, int bs0, const int32_t* rp0, const int32_t* ci0,
-              const double* v0, const double* coords, const uint8_t* fixed, HostHierarchy& out) {
-  out = HostHierarchy();
-  out.params = prm;
-  WN_REQUIRE(n0 > 0 && rp0 && ci0 && v0 && coords && (bs0 == 3 || bs0 == 6), WN_EINVAL, "amg_build: bad argument");
-  // near-null space on level 0: the 6 rigid-body modes, zero on fixed DOFs.  Rows ux, uy, uz
-  // (and for 6-DOF nodes rx, ry, rz); columns tx, ty, tz, rx, ry, rz (the layout of
-  // amg_preconditioner.py:30-69): a rotation w moves a node by w x X and turns it by w.
-  std::vector<double> B((size_t)n0 * bs0 * 6, 0.0);
+// Three-pass greedy aggregation (Vanek-Mandel-Brezina) on the strong block graph, given the
+// Frobenius norm of every block: (i, j) is strong if |A_ij| >= theta sqrt(|A_ii| |A_jj|).
+// Pass 1 makes roots of nodes whose strong neighbourhood is still free; pass 2 joins each left
+// node to its strongest aggregated neighbour; pass 3 turns the leftovers with strong links into
+// new aggregates.  Nodes without strong links (fully fixed nodes) stay unaggregated (-1).
+int64_t aggregate_norms(int64_t n, const int32_t* rp, const int32_t* ci, const double* nrm, double theta,
+                        std::vector<int32_t>& agg) {
+  std::vector<double> dn(n, 0.0);
+  for (int64_t i = 0; i < n; ++i)
+    for (int32_t k = rp[i]; k < rp[i + 1]; ++k)
+      if (ci[k] == i) dn[i] = nrm[k];
+  std::vector<uint8_t> strong(rp[n], 0);
+  std::vector<uint8_t> has_strong(n, 0);
+  par_rows(n, [&](int64_t a, int64_t b, int) {
+    for (int64_t i = a; i < b; ++i)
+      for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
+        const int32_t j = ci[k];
+        if (j != i && nrm[k] > 0.0 && nrm[k] >= theta * std::sqrt(dn[i] * dn[j])) {
+          strong[k] = 1;
+          has_strong[i] = 1;
+        }
+      }
+  });
+  agg.assign(n, -1);
+  int64_t na = 0;
+  for (int64_t i = 0; i < n; ++i) {  // pass 1: roots whose strong neighbourhood is free
+    if (agg[i] >= 0 || !has_strong[i]) continue;
+    bool free_all = true;
+    for (int32_t k = rp[i]; k < rp[i + 1] && free_all; ++k)
+      if (strong[k] && agg[ci[k]] >= 0) free_all = false;
+    if (!free_all) continue;
+    agg[i] = (int32_t)na;
+    for (int32_t k = rp[i]; k < rp[i + 1]; ++k)
+      if (strong[k]) agg[ci[k]] = (int32_t)na;
+    ++na;
+  }
+  std::vector<int32_t> pass2(agg);
+  for (int64_t i = 0; i < n; ++i) {  // pass 2: join the strongest aggregated neighbour
+    if (agg[i] >= 0 || !has_strong[i]) continue;
+    double best = -1.0;
+    int32_t ba = -1;
+    for (int32_t k = rp[i]; k < rp[i + 1]; ++k)
+      if (strong[k] && agg[ci[k]] >= 0 && nrm[k] > best) {
+        best = nrm[k];
+        ba = agg[ci[k]];
+      }
+    pass2[i] = ba;
+  }
+  agg.swap(pass2);
+  for (int64_t i = 0; i < n; ++i) {  // pass 3: leftovers with strong links form new aggregates
+    if (agg[i] >= 0 || !has_strong[i]) continue;
+    agg[i] = (int32_t)na;
+    for (int32_t k = rp[i]; k < rp[i + 1]; ++k)
+      if (strong[k] && agg[ci[k]] < 0) agg[ci[k]] = (int32_t)na;
+    ++na;
+  }
+  return na;
+}
+
+// Near-null space of level 0: the 6 rigid-body modes, zero on fixed DOFs.  Rows ux, uy, uz (and
+// for 6-DOF nodes rx, ry, rz); columns tx, ty, tz, rx, ry, rz (the layout of
+// amg_preconditioner.py:30-69): a rotation w moves a node by w x X and turns it by w.
+void near_null_space(int64_t n0, int bs0, const double* coords, const uint8_t* fixed, std::vector<double>& B) {
+  B.assign((size_t)n0 * bs0 * 6, 0.0);
   for (int64_t i = 0; i < n0; ++i) {
     const double X = coords[i * 3], Y = coords[i * 3 + 1], Z = coords[i * 3 + 2];
     double* b = &B[(size_t)i * bs0 * 6];
@@ -453,102 +460,51 @@ int amg_build(const wn_amg_params& prm, int64_t n0, int bs0, const int32_t* rp0,
       for (int c = 0; c < 6; ++c) b[r * 6 + c] = fx ? 0.0 : m[r][c];
     }
   }
-  View A{bs0, bs0, n0, n0, rp0, ci0, v0};
-  HostBsr Aown;
-  int bs = bs0;
-  int64_t n = n0;
-  for (int lvl = 0;; ++lvl) {
-    const int64_t ndof = n * bs;
-    if (ndof <= prm.coarse_size || lvl >= prm.max_levels - 1) break;
-    HostLevel L;
-    L.bs = bs;
-    L.n_nodes = n;
-    L.dinv = inv_diag(A);
-    L.rho = power_rho(A, L.dinv, prm.power_iters);
-    L.n_agg = aggregate(A, prm.strength_theta, L.agg);
-    if (L.n_agg == 0 || L.n_agg * 6 >= (int64_t)(0.8 * ndof)) break;  // coarsening stalled
-    // tentative prolongator: per aggregate QR of its near-null-space rows
-    std::vector<int32_t> cnt(L.n_agg + 1, 0);
+}
+
+// Tentative prolongator: per aggregate, a thin QR of its members' near-null-space rows;
+// Qnode (n x bs x 6) = each node's block of Q, Bc (n_agg x 36) = the R factors (the coarse
+// near-null space).
+void tentative_prolongator(int64_t n, int bs, int64_t n_agg, const std::vector<int32_t>& agg,
+                           const std::vector<double>& B, std::vector<double>& Qnode, std::vector<double>& Bc) {
+  std::vector<int32_t> cnt(n_agg + 1, 0);
+  for (int64_t i = 0; i < n; ++i)
+    if (agg[i] >= 0) cnt[agg[i] + 1]++;
+  for (int64_t a = 0; a < n_agg; ++a) cnt[a + 1] += cnt[a];
+  std::vector<int32_t> members(cnt[n_agg]);
+  {
+    std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1);
     for (int64_t i = 0; i < n; ++i)
-      if (L.agg[i] >= 0) cnt[L.agg[i] + 1]++;
-    for (int64_t a = 0; a < L.n_agg; ++a) cnt[a + 1] += cnt[a];
-    std::vector<int32_t> members(cnt[L.n_agg]);
-    {
-      std::vector<int32_t> pos(cnt.begin(), cnt.end() - 1);
-      for (int64_t i = 0; i < n; ++i)
-        if (L.agg[i] >= 0) members[pos[L.agg[i]]++] = (int32_t)i;
-    }
-    std::vector<double> Qnode((size_t)n * bs * 6, 0.0);  // tentative block of each node
-    std::vector<double> Bc((size_t)L.n_agg * 36, 0.0);
-    par_rows(L.n_agg, [&](int64_t a0, int64_t a1, int) {
-      std::vector<double> mat, q;
-      for (int64_t a = a0; a < a1; ++a) {
-        const int cntn = cnt[a + 1] - cnt[a];
-        const int m = cntn * bs;
-        mat.assign((size_t)m * 6, 0.0);
-        for (int t = 0; t < cntn; ++t) {
-          const int32_t node = members[cnt[a] + t];
-          for (int r = 0; r < bs; ++r)
-            for (int c = 0; c < 6; ++c) mat[(size_t)c * m + t * bs + r] = B[((size_t)node * bs + r) * 6 + c];
-        }
-        double R[36];
-        qr6(m, mat, q, R);
-        for (int t = 0; t < cntn; ++t) {
-          const int32_t node = members[cnt[a] + t];
-          for (int r = 0; r < bs; ++r)
-            for (int c = 0; c < 6; ++c) Qnode[((size_t)node * bs + r) * 6 + c] = q[(size_t)c * m + t * bs + r];
-        }
-        std::copy(R, R + 36, &Bc[(size_t)a * 36]);
-      }
-    });
-    // (smoothed) prolongator rows
-    std::vector<std::vector<int32_t>> rc(n);
-    std::vector<std::vector<double>> rv(n);
-    const double w = prm.smooth_prolongator ? prm.prolong_omega / L.rho : 0.0;
-    par_rows(n, [&](int64_t a0, int64_t a1, int) {
-      RowAcc acc;
-      acc.init(L.n_agg, bs * 6);
-      for (int64_t i = a0; i < a1; ++i) {
-        if (L.agg[i] >= 0) {
-          double* s = acc.slot(L.agg[i]);
-          for (int k = 0; k < bs * 6; ++k) s[k] += Qnode[(size_t)i * bs * 6 + k];
-        }
-        if (w != 0.0) {
-          for (int32_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-            const int32_t j = A.ci[k];
-            if (L.agg[j] < 0) continue;
-            const double* ab = A.v + (size_t)k * bs * bs;
-            const double* qj = &Qnode[(size_t)j * bs * 6];
-            double* s = acc.slot(L.agg[j]);
-            for (int r = 0; r < bs; ++r) {
-              const double f = -w * L.dinv[i * bs + r];
-              for (int c = 0; c < bs; ++c) {
-                const double av = ab[r * bs + c];
-                if (av == 0.0) continue;
-                for (int t = 0; t < 6; ++t) s[r * 6 + t] += f * av * qj[c * 6 + t];
-              }
-            }
-          }
-        }
-        acc.flush(rc[i], rv[i]);
-      }
-    });
-    rows_to_bsr(bs, 6, n, L.n_agg, rc, rv, L.P);
-    transpose(view(L.P), L.R);
-    // Galerkin product A_c = R (A P)
-    HostBsr AP, Ac;
-    spgemm(A, view(L.P), AP);
-    spgemm(view(L.R), view(AP), Ac);
-    symmetrize(Ac);
-    if (lvl > 0) L.A = std::move(Aown);
-    out.levels.push_back(std::move(L));
-    Aown = std::move(Ac);
-    A = view(Aown);
-    B.swap(Bc);
-    bs = 6;
-    n = out.levels.back().n_agg;
+      if (agg[i] >= 0) members[pos[agg[i]]++] = (int32_t)i;
   }
-  // coarsest level: dense FP64, Cholesky, explicit inverse A^-1 = L^-T L^-1
+  Qnode.assign((size_t)n * bs * 6, 0.0);
+  Bc.assign((size_t)n_agg * 36, 0.0);
+  par_rows(n_agg, [&](int64_t a0, int64_t a1, int) {
+    std::vector<double> mat, q;
+    for (int64_t a = a0; a < a1; ++a) {
+      const int cntn = cnt[a + 1] - cnt[a];
+      const int m = cntn * bs;
+      mat.assign((size_t)m * 6, 0.0);
+      for (int t = 0; t < cntn; ++t) {
+        const int32_t node = members[cnt[a] + t];
+        for (int r = 0; r < bs; ++r)
+          for (int c = 0; c < 6; ++c) mat[(size_t)c * m + t * bs + r] = B[((size_t)node * bs + r) * 6 + c];
+      }
+      double R[36];
+      qr6(m, mat, q, R);
+      for (int t = 0; t < cntn; ++t) {
+        const int32_t node = members[cnt[a] + t];
+        for (int r = 0; r < bs; ++r)
+          for (int c = 0; c < 6; ++c) Qnode[((size_t)node * bs + r) * 6 + c] = q[(size_t)c * m + t * bs + r];
+      }
+      std::copy(R, R + 36, &Bc[(size_t)a * 36]);
+    }
+  });
+}
+
+// Coarsest level: the n x n block matrix (bs x bs row-major blocks) made dense in FP64, its
+// Cholesky factor and the explicit inverse A^-1 = L^-T L^-1 (into out.coarse_A / coarse_inv).
+int dense_coarse(int64_t n, int bs, const int32_t* rp, const int32_t* ci, const double* v, HostHierarchy& out) {
   const int64_t nc = n * bs;
   WN_REQUIRE(nc <= 20000, WN_ETOOBIG, "amg_build: coarsest level too large (%lld DOFs); raise max_levels",
              (long long)nc);
@@ -556,10 +512,10 @@ int amg_build(const wn_amg_params& prm, int64_t n0, int bs0, const int32_t* rp0,
   std::vector<double>& D = out.coarse_A;
   D.assign((size_t)nc * nc, 0.0);
   for (int64_t i = 0; i < n; ++i)
-    for (int32_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-      const double* blk = A.v + (size_t)k * bs * bs;
+    for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
+      const double* blk = v + (size_t)k * bs * bs;
       for (int r = 0; r < bs; ++r)
-        for (int c = 0; c < bs; ++c) D[(size_t)(i * bs + r) * nc + A.ci[k] * bs + c] = blk[r * bs + c];
+        for (int c = 0; c < bs; ++c) D[(size_t)(i * bs + r) * nc + ci[k] * bs + c] = blk[r * bs + c];
     }
   // unaggregated-only systems can leave zero rows: give them a unit diagonal
   for (int64_t i = 0; i < nc; ++i) {
@@ -605,6 +561,103 @@ int amg_build(const wn_amg_params& prm, int64_t n0, int bs0, const int32_t* rp0,
   });
   for (int64_t i = 0; i < nc; ++i)
     for (int64_t j = 0; j < i; ++j) out.coarse_inv[(size_t)i * nc + j] = out.coarse_inv[(size_t)j * nc + i];
+  return WN_OK;
+}
+
+// WN_AMG_TRACE=1 in the environment: phase times of the setup on stderr
+struct PhaseTrace {
+  bool on;
+  std::chrono::steady_clock::time_point t;
+  PhaseTrace() : on(std::getenv("WN_AMG_TRACE") != nullptr), t(std::chrono::steady_clock::now()) {}
+  void mark(const char* what, int lvl) {
+    if (!on) return;
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "amg_build: level %d %-12s %8.3f s\n", lvl, what,
+                 std::chrono::duration<double>(now - t).count());
+    t = now;
+  }
+};
+
+int amg_build(const wn_amg_params& prm, int64_t n0, int bs0, const int32_t* rp0, const int32_t* ci0,
+              const double* v0, const double* coords, const uint8_t* fixed, HostHierarchy& out) {
+  PhaseTrace tr;
+  out = HostHierarchy();
+  out.params = prm;
+  WN_REQUIRE(n0 > 0 && rp0 && ci0 && v0 && coords && (bs0 == 3 || bs0 == 6), WN_EINVAL, "amg_build: bad argument");
+  std::vector<double> B;
+  near_null_space(n0, bs0, coords, fixed, B);
+  View A{bs0, bs0, n0, n0, rp0, ci0, v0};
+  HostBsr Aown;
+  int bs = bs0;
+  int64_t n = n0;
+  for (int lvl = 0;; ++lvl) {
+    const int64_t ndof = n * bs;
+    if (ndof <= prm.coarse_size || lvl >= prm.max_levels - 1) break;
+    HostLevel L;
+    L.bs = bs;
+    L.n_nodes = n;
+    L.dinv = inv_diag(A);
+    L.rho = power_rho(A, L.dinv, prm.power_iters);
+    tr.mark("rho", lvl);
+    L.n_agg = aggregate(A, prm.strength_theta, L.agg);
+    tr.mark("aggregate", lvl);
+    if (L.n_agg == 0 || L.n_agg * 6 >= (int64_t)(0.8 * ndof)) break;  // coarsening stalled
+    // tentative prolongator: per aggregate QR of its near-null-space rows
+    std::vector<double> Qnode, Bc;
+    tentative_prolongator(n, bs, L.n_agg, L.agg, B, Qnode, Bc);
+    tr.mark("tentative", lvl);
+    // (smoothed) prolongator rows
+    std::vector<std::vector<int32_t>> rc(n);
+    std::vector<std::vector<double>> rv(n);
+    const double w = prm.smooth_prolongator ? prm.prolong_omega / L.rho : 0.0;
+    par_rows(n, [&](int64_t a0, int64_t a1, int) {
+      RowAcc acc;
+      acc.init(L.n_agg, bs * 6);
+      for (int64_t i = a0; i < a1; ++i) {
+        if (L.agg[i] >= 0) {
+          double* s = acc.slot(L.agg[i]);
+          for (int k = 0; k < bs * 6; ++k) s[k] += Qnode[(size_t)i * bs * 6 + k];
+        }
+        if (w != 0.0) {
+          for (int32_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+            const int32_t j = A.ci[k];
+            if (L.agg[j] < 0) continue;
+            const double* ab = A.v + (size_t)k * bs * bs;
+            const double* qj = &Qnode[(size_t)j * bs * 6];
+            double* s = acc.slot(L.agg[j]);
+            for (int r = 0; r < bs; ++r) {
+              const double f = -w * L.dinv[i * bs + r];
+              for (int c = 0; c < bs; ++c) {
+                const double av = ab[r * bs + c];
+                if (av == 0.0) continue;
+                for (int t = 0; t < 6; ++t) s[r * 6 + t] += f * av * qj[c * 6 + t];
+              }
+            }
+          }
+        }
+        acc.flush(rc[i], rv[i]);
+      }
+    });
+    rows_to_bsr(bs, 6, n, L.n_agg, rc, rv, L.P);
+    transpose(view(L.P), L.R);
+    tr.mark("prolongator", lvl);
+    // Galerkin product A_c = R (A P)
+    HostBsr AP, Ac;
+    spgemm(A, view(L.P), AP);
+    tr.mark("A*P", lvl);
+    spgemm(view(L.R), view(AP), Ac);
+    tr.mark("R*(AP)", lvl);
+    symmetrize(Ac);
+    if (lvl > 0) L.A = std::move(Aown);
+    out.levels.push_back(std::move(L));
+    Aown = std::move(Ac);
+    A = view(Aown);
+    B.swap(Bc);
+    bs = 6;
+    n = out.levels.back().n_agg;
+  }
+  WN_CHECK(dense_coarse(n, bs, A.rp, A.ci, A.v, out));
+  tr.mark("coarse", -1);
   // the last coarse matrix (BSR) is kept for tests through coarse_A only
   return WN_OK;
 }

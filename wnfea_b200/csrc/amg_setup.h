@@ -43,4 +43,15 @@ int amg_build(const wn_amg_params& prm, int64_t n0, int bs0, const int32_t* rp0,
 
 wn_amg_params amg_default_params();
 
+// Pieces shared by the host setup above and the device setup (amg_device.cu):
+// greedy aggregation from block norms (-1 = unaggregated); the rigid-body near-null space of
+// level 0; the tentative prolongator (per-aggregate QR: Qnode n x bs x 6, Bc n_agg x 36); the
+// dense coarsest level (out.n_coarse, coarse_A, coarse_inv).
+int64_t aggregate_norms(int64_t n, const int32_t* rp, const int32_t* ci, const double* nrm, double theta,
+                        std::vector<int32_t>& agg);
+void near_null_space(int64_t n0, int bs0, const double* coords, const uint8_t* fixed, std::vector<double>& B);
+void tentative_prolongator(int64_t n, int bs, int64_t n_agg, const std::vector<int32_t>& agg,
+                           const std::vector<double>& B, std::vector<double>& Qnode, std::vector<double>& Bc);
+int dense_coarse(int64_t n, int bs, const int32_t* rp, const int32_t* ci, const double* v, HostHierarchy& out);
+
 }  // namespace wn

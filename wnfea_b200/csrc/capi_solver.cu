@@ -2,6 +2,7 @@
 #include <cstring>
 
 #include "amg.h"
+#include "amg_device.h"
 #include "common.cuh"
 #include "solid.h"
 #include "solver.h"
@@ -19,7 +20,9 @@ struct HostAmgHandle {
 // says which by the entry point used.  Solid handles carry the hierarchy in s->amg->host.
 HostHierarchy* host_of_solid(void* h) {
   Solid* s = reinterpret_cast<Solid*>(h);
-  return s->amg ? &s->amg->host : nullptr;
+  if (!s->amg) return nullptr;
+  if (amg_sync_host(*s->amg) != 0) return nullptr;  // device-built levels: copies made on demand
+  return &s->amg->host;
 }
 
 int export_matrix(HostHierarchy* H, int level, int which, int* br, int* bc, int64_t* n_rows, int64_t* n_cols,
@@ -76,7 +79,7 @@ int wn_amg_info(void* h, int* n_levels, int* bs, int64_t* n_nodes, int64_t* nnzb
   for (int l = 0; l < L && l < 16; ++l) {
     if (bs) bs[l] = H.levels[l].bs;
     if (n_nodes) n_nodes[l] = H.levels[l].n_nodes;
-    if (nnzb) nnzb[l] = l == 0 ? s->nnzb : H.levels[l].A.nnzb();
+    if (nnzb) nnzb[l] = l == 0 ? s->nnzb : s->amg->levels[l].A.nnzb;
   }
   if (n_coarse) *n_coarse = H.n_coarse;
   if (setup_seconds) *setup_seconds = s->amg->setup_seconds;

@@ -28,6 +28,7 @@
 #include <cstring>
 
 #include "amg.h"
+#include "amg_device.h"
 #include "common.cuh"
 #include "eft.cuh"
 #include "kernels.h"
@@ -1472,24 +1473,33 @@ int solver_setup(Solid* s, const wn_amg_params& prm) {
   WN_REQUIRE(prm.smoother_degree >= 1 && prm.smoother_degree <= 8, WN_EINVAL, "AMG setup: smoother_degree in [1, 8]");
   WN_REQUIRE(prm.max_levels >= 1 && prm.max_levels <= 16, WN_EINVAL, "AMG setup: max_levels in [1, 16]");
   const auto t0 = std::chrono::steady_clock::now();
-  const int nb = s->bs * s->bs;
-  std::vector<double> soa(s->nnzb * nb), vals(s->nnzb * nb);
-  WN_CUDA(cudaMemcpy(soa.data(), s->k64.p, soa.size() * sizeof(double), cudaMemcpyDeviceToHost));
-  if (s->bs == 3) {
-    for (int64_t b = 0; b < s->nnzb; ++b)  // component-major on the device -> row-major blocks
-      for (int k = 0; k < 9; ++k) vals[b * 9 + k] = soa[k * s->nnzb + b];
-  } else {
-    vals.swap(soa);  // 6x6 blocks are stored row-major already
-  }
-  std::vector<double>().swap(soa);
   std::unique_ptr<AmgHierarchy> H(new AmgHierarchy());
-  const uint8_t* fixed = s->bcs_applied ? s->h_fixed.data() : nullptr;
-  WN_CHECK(amg_build(prm, s->n_nodes, s->bs, s->h_row_ptr.data(), s->h_col_idx.data(), vals.data(), s->h_nodes.data(),
-                     fixed, H->host));
+  // device setup first (1 = a row beyond its shared-memory capacities: the host builder then)
+  int dev_rc = 1;
+  if (prm.setup_on_device) {
+    dev_rc = amg_build_device(s, prm, *H);
+    WN_CHECK(dev_rc < 0 || dev_rc > 1 ? dev_rc : 0);
+    if (dev_rc == 1) H.reset(new AmgHierarchy());
+  }
+  if (dev_rc != 0) {
+    const int nb = s->bs * s->bs;
+    std::vector<double> soa(s->nnzb * nb), vals(s->nnzb * nb);
+    WN_CUDA(cudaMemcpy(soa.data(), s->k64.p, soa.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    if (s->bs == 3) {
+      for (int64_t b = 0; b < s->nnzb; ++b)  // component-major on the device -> row-major blocks
+        for (int k = 0; k < 9; ++k) vals[b * 9 + k] = soa[k * s->nnzb + b];
+    } else {
+      vals.swap(soa);  // 6x6 blocks are stored row-major already
+    }
+    std::vector<double>().swap(soa);
+    const uint8_t* fixed = s->bcs_applied ? s->h_fixed.data() : nullptr;
+    WN_CHECK(amg_build(prm, s->n_nodes, s->bs, s->h_row_ptr.data(), s->h_col_idx.data(), vals.data(),
+                       s->h_nodes.data(), fixed, H->host));
+    H->levels.resize(H->host.levels.size());
+  }
   H->degree = prm.smoother_degree;
   static uint64_t next_id = 0;
   H->id = ++next_id;
-  H->levels.resize(H->host.levels.size());
   for (size_t l = 0; l < H->host.levels.size(); ++l) {
     const HostLevel& h = H->host.levels[l];
     DevLevel& L = H->levels[l];
@@ -1498,29 +1508,33 @@ int solver_setup(Solid* s, const wn_amg_params& prm) {
     if (l == 0) {
       L.a_rp = s->row_ptr.p;
       L.a_ci = s->col_idx.p;
-    } else {
-      WN_CHECK(L.A.upload(h.A));
     }
-    WN_CHECK(L.dinv64.upload(h.dinv));
-    std::vector<float> f(h.dinv.begin(), h.dinv.end());
-    WN_CHECK(L.dinv32.upload(f));
+    if (!H->device_built) {
+      if (l > 0) WN_CHECK(L.A.upload(h.A));
+      WN_CHECK(L.dinv64.upload(h.dinv));
+      std::vector<float> f(h.dinv.begin(), h.dinv.end());
+      WN_CHECK(L.dinv32.upload(f));
+      WN_CHECK(L.P.upload(h.P));
+      WN_CHECK(L.R.upload(h.R));
+      if (l > 0) L.h_A_rp = h.A.rp;
+      L.h_P_rp = h.P.rp;
+      L.h_R_rp = h.R.rp;
+    }
     L.rho = h.rho;
     cheb_coefficients(prm, L);
-    WN_CHECK(L.P.upload(h.P));
-    WN_CHECK(L.R.upload(h.R));
     // matrices of at least stream_min_mb MB (FP32) are streamed from tile-major packs (on the
     // 1M-DOF I-beam: level 1 and the transfers of levels 0-1, 24-142 MB; streaming level 2 and
     // the level-1 transfers too, at 4 MB rather than 32 MB, took 0.8 ms off a 47 ms solve)
-    auto stream_if_large = [&](StreamMat& m, const HostBsr& hb, const DevBsr& db) -> int {
+    auto stream_if_large = [&](StreamMat& m, const std::vector<int32_t>& h_rp, const DevBsr& db) -> int {
       if (prm.stream_min_mb < 0.0 ||
-          (double)(hb.nnzb() * hb.br * hb.bc * (int64_t)sizeof(float)) < prm.stream_min_mb * 1048576.0)
+          (double)(db.nnzb * db.br * db.bc * (int64_t)sizeof(float)) < prm.stream_min_mb * 1048576.0)
         return 0;
-      WN_CHECK(m.make_plan(hb.rp.data(), hb.n_rows, hb.br, hb.bc));
+      WN_CHECK(m.make_plan(h_rp.data(), db.n_rows, db.br, db.bc));
       return m.pack(db.rp.p, db.ci.p, db.v32.p, db.v64.p, 0, 0);
     };
-    if (l > 0) WN_CHECK(stream_if_large(L.As, h.A, L.A));
-    WN_CHECK(stream_if_large(L.Ps, h.P, L.P));
-    WN_CHECK(stream_if_large(L.Rs, h.R, L.R));
+    if (l > 0) WN_CHECK(stream_if_large(L.As, L.h_A_rp, L.A));
+    WN_CHECK(stream_if_large(L.Ps, L.h_P_rp, L.P));
+    WN_CHECK(stream_if_large(L.Rs, L.h_R_rp, L.R));
     WN_CHECK(L.v64.alloc(h.n_nodes * h.bs));
     WN_CHECK(L.v32.alloc(h.n_nodes * h.bs));
   }
