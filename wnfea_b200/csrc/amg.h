@@ -94,7 +94,9 @@ struct PcgScalars {
 template <typename T>
 struct PcgVecs {
   DArray<T> x, r, z, p0, p1, q;
+  DArray<T> d0;  // D^-1 r / theta_0 of the fine level, written by the update for the next V-cycle
   int alloc(int64_t n) {
+    WN_CHECK(d0.alloc(n));
     WN_CHECK(x.alloc(n));
     WN_CHECK(r.alloc(n));
     WN_CHECK(z.alloc(n));

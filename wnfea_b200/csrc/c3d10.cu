@@ -14,6 +14,7 @@
 #include "c3d10.cuh"
 #include "common.cuh"
 #include "kernels.h"
+#include "wnfea_cuda.h"
 
 namespace wn {
 
@@ -211,13 +212,20 @@ __global__ void __launch_bounds__(kAsmThreads, 2) assemble_tiles_kernel(
     d[31] = w * mu;
   }
   __syncthreads();
+  // phase 2: each thread sums the contributions of up to two blocks (a tile holds at most
+  // 2 kAsmThreads blocks) in registers
   const int nb = T.w - T.z;
-  for (int kk = threadIdx.x; kk < nb; kk += kAsmThreads) {
-    const int j = A.perm[T.z + kk];  // local block index
-    const int64_t b = T.z + j;
-    double acc[9];
+  double acc[2][9];
+  int jloc[2] = {-1, -1};
 #pragma unroll
-    for (int m = 0; m < 9; ++m) acc[m] = 0.0;
+  for (int h = 0; h < 2; ++h) {
+    const int kk = threadIdx.x + h * kAsmThreads;
+#pragma unroll
+    for (int m = 0; m < 9; ++m) acc[h][m] = 0.0;
+    if (kk >= nb) continue;
+    const int j = A.perm[T.z + kk];  // local block index
+    jloc[h] = j;
+    const int64_t b = T.z + j;
     const int32_t q0 = A.gptr[b], q1 = A.gptr[b + 1];
     for (int32_t q = q0; q < q1; ++q) {
       const int code = A.contrib[q];
@@ -248,39 +256,47 @@ __global__ void __launch_bounds__(kAsmThreads, 2) assemble_tiles_kernel(
       }
       if (ea <= eb) {
 #pragma unroll
-        for (int m = 0; m < 9; ++m) acc[m] += M[m];
+        for (int m = 0; m < 9; ++m) acc[h][m] += M[m];
       } else {
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
-          for (int jj = 0; jj < 3; ++jj) acc[i * 3 + jj] += M[jj * 3 + i];
+          for (int jj = 0; jj < 3; ++jj) acc[h][i * 3 + jj] += M[jj * 3 + i];
       }
     }
-    const int64_t r0 = (int64_t)A.block_row[b] * 3, c0 = (int64_t)A.col_idx[b] * 3;
     if (fixed) {
+      const int64_t r0 = (int64_t)A.block_row[b] * 3, c0 = (int64_t)A.col_idx[b] * 3;
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int jj = 0; jj < 3; ++jj)
-          if (fixed[r0 + i] | fixed[c0 + jj]) acc[i * 3 + jj] = (r0 + i == c0 + jj) ? 1.0 : 0.0;
-    }
-#pragma unroll
-    for (int m = 0; m < 9; ++m) {
-      k64[m * nnzb + b] = acc[m];
-      k32[m * nnzb + b] = (float)acc[m];
-    }
-    if (A.p64) {
-      const int4 d64 = reinterpret_cast<const int4*>(A.d64)[t];  // r0, r1, seg, cntp
-      const int4 d32 = reinterpret_cast<const int4*>(A.d32)[t];
-      double* v64 = reinterpret_cast<double*>(A.p64 + (size_t)d64.z * 128);
-      float* v32 = reinterpret_cast<float*>(A.p32 + (size_t)d32.z * 128);
-#pragma unroll
-      for (int m = 0; m < 9; ++m) {
-        v64[m * d64.w + j] = acc[m];
-        v32[m * d32.w + j] = (float)acc[m];
-      }
+          if (fixed[r0 + i] | fixed[c0 + jj]) acc[h][i * 3 + jj] = (r0 + i == c0 + jj) ? 1.0 : 0.0;
     }
   }
+  // phase 3: the tile's blocks staged in shared memory in local order (over the element data,
+  // which every thread has finished reading), then written coalesced, component by component
+  __syncthreads();
+  double* stage = s_el;  // nb x 9 (odd stride: consecutive blocks hit different banks)
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+    if (jloc[h] >= 0)
+#pragma unroll
+      for (int m = 0; m < 9; ++m) stage[jloc[h] * 9 + m] = acc[h][m];
+  __syncthreads();
+  const int4 d64 = A.p64 ? reinterpret_cast<const int4*>(A.d64)[t] : make_int4(0, 0, 0, 0);  // r0, r1, seg, cntp
+  const int4 d32 = A.p64 ? reinterpret_cast<const int4*>(A.d32)[t] : make_int4(0, 0, 0, 0);
+  double* v64 = A.p64 ? reinterpret_cast<double*>(A.p64 + (size_t)d64.z * 128) : nullptr;
+  float* v32 = A.p64 ? reinterpret_cast<float*>(A.p32 + (size_t)d32.z * 128) : nullptr;
+  for (int m = 0; m < 9; ++m)
+    for (int j = threadIdx.x; j < nb; j += kAsmThreads) {
+      const double v = stage[j * 9 + m];
+      k64[m * nnzb + T.z + j] = v;
+      k32[m * nnzb + T.z + j] = (float)v;
+      if (v64) {
+        v64[m * d64.w + j] = v;
+        v32[m * d32.w + j] = (float)v;
+      }
+    }
 }
 
 // Matrix-free element forces f_e = Ke u_e (= sum_g w|J| B^T C B u_e, c3d10.py:252-283) for
@@ -436,7 +452,10 @@ int launch_assemble_tiles(const AsmTileArgs& A, int n_tiles, int ne_max, const d
                           const double* props, const uint8_t* fixed, int64_t nnzb, double* k64, float* k32, int* flags,
                           cudaStream_t st) {
   if (n_tiles == 0) return 0;
-  const size_t smem = (size_t)ne_max * kAsmElStride * sizeof(double);
+  // element data of the tile, then (same space) its finished blocks: at most
+  // WN_STREAM_TILE_BLOCKS x 9 doubles
+  static_assert(WN_STREAM_TILE_BLOCKS <= 2 * kAsmThreads, "two blocks per thread in the assembly");
+  const size_t smem = std::max((size_t)ne_max * kAsmElStride, (size_t)WN_STREAM_TILE_BLOCKS * 9) * sizeof(double);
   static int configured_bytes[64] = {0};  // per device: the largest dynamic size allowed so far
   int dev = 0;
   WN_CUDA(cudaGetDevice(&dev));

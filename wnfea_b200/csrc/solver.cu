@@ -540,7 +540,8 @@ __global__ void __launch_bounds__(kThreads) k_update(int64_t n, TK* __restrict__
                                                      TM* __restrict__ rm, const TK* __restrict__ p,
                                                      const TK* __restrict__ q, const double* __restrict__ partB,
                                                      double* __restrict__ partC, int nparts, int par,
-                                                     PcgScalars* __restrict__ S) {
+                                                     PcgScalars* __restrict__ S, TM* __restrict__ d0,
+                                                     const TM* __restrict__ dinv, TM inv_theta) {
   pdl_trigger();  // dependents launched programmatically may start their prologue
   __shared__ double sh[kThreads / 32];
   if (S->done) return;
@@ -560,6 +561,9 @@ __global__ void __launch_bounds__(kThreads) k_update(int64_t n, TK* __restrict__
     const TK ri = r[i] - a * q[i];
     r[i] = ri;
     if (rm) rm[i] = (TM)ri;
+    // the next V-cycle's first smoothing input (x_j = D^-1 b_j / theta with b = r in the
+    // preconditioner's precision), so that its streamed kernel gathers one vector, not two
+    if (d0) d0[i] = dinv[i] * (TM)ri * inv_theta;
     s += (double)ri * (double)ri;
   }
   write_part(s, partC, sh);
@@ -1086,7 +1090,7 @@ static void level_A(Solid* s, DevLevel& L, int lvl, const int32_t*& rp, const in
 // part (if not null) receives the partials of b . out.
 template <typename T>
 static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b, T* out, double* part,
-                  PcgScalars* S, cudaStream_t st) {
+                  PcgScalars* S, cudaStream_t st, const T* d0 = nullptr) {
   const int nlev = (int)H.levels.size();
   if (lvl == nlev) {  // coarsest
     constexpr int rows_per_cta = (kThreads / 32) / kCoarseWarpsPerRow;
@@ -1134,9 +1138,12 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
     const StreamMat& Am = (lvl == 0) ? s->fine : L.As;
     const bool stream = Am.packed;
     const T c1 = deg >= 2 ? (T)L.c1[0] : T(0), c2 = deg >= 2 ? (T)L.c2[0] : T(0);
-    if (!(stream && launch_stream_rows<T, BS, BS>(Am, XD0<T>{b, dinv, it},
-                                          EpiPreFirst<T>{b, dinv, it, deg, c1, c2, V.x.p, V.r.p, V.d.p, V.res.p},
-                                          nullptr, S, st, nullptr)))
+    // d0 (level 0, from the PCG update): the first step's input D^-1 b / theta precomputed
+    const EpiPreFirst<T> epi_pre{b, dinv, it, deg, c1, c2, V.x.p, V.r.p, V.d.p, V.res.p};
+    const bool pre_streamed =
+        stream && (d0 ? launch_stream_rows<T, BS, BS>(Am, XLoad<T, T>{d0}, epi_pre, nullptr, S, st, nullptr)
+                      : launch_stream_rows<T, BS, BS>(Am, XD0<T>{b, dinv, it}, epi_pre, nullptr, S, st, nullptr));
+    if (!pre_streamed)
       k_pre_first<BS, T><<<rg(k_pre_first<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, deg, c1, c2,
                                                                       V.x.p, V.r.p, V.d.p, V.res.p, S);
     W.launches++;
@@ -1218,8 +1225,9 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
 
 // z = M r with partials of r . z into partA
 template <typename T>
-static int apply_prec(Solid* s, SolverWork& W, int precond, const T* r, T* z, PcgScalars* S, cudaStream_t st) {
-  if (precond == 2) return vcycle<T>(s, *s->amg, W, 0, r, z, W.partA.p, S, st);
+static int apply_prec(Solid* s, SolverWork& W, int precond, const T* r, T* z, PcgScalars* S, cudaStream_t st,
+                      const T* d0 = nullptr) {
+  if (precond == 2) return vcycle<T>(s, *s->amg, W, 0, r, z, W.partA.p, S, st, d0);
   if (precond == 3) {
     auto launch = [&](auto kern) {
       const int g = resident_grid(kern, kThreads, (s->n_nodes + kThreads - 1) / kThreads);
@@ -1308,8 +1316,13 @@ static int pcg_iteration(Solid* s, SolverWork& W, int precond, int k, PcgScalars
   const double nK = (double)W.n * sizeof(TK), nM = (double)W.n * sizeof(TM);
   note(W, st, "pcg_spmv_dot", -1, mat_bytes(s->nnzb, s->bs, s->bs, s->n_nodes, sizeof(TK)) + nM + 3 * nK);
   W.npB = gsd;
-  k_update<TK, TM><<<gup, kThreads, 0, st>>>(W.n, B.x, B.r, B.rm, p_new, B.q, W.partB.p, W.partC.p, W.npB, par, S);
-  note(W, st, "pcg_update", -1, 6 * nK + (B.rm ? nM : 0.0));
+  // with the AMG preconditioner, the update also writes the fine level's first smoothing input
+  const bool pre_input = precond == 2 && !s->amg->levels.empty();
+  TM* d0 = pre_input ? Prec<TM>::pcg(W).d0.p : nullptr;
+  const TM it0 = pre_input ? (TM)s->amg->levels[0].inv_theta : TM(0);
+  k_update<TK, TM><<<gup, kThreads, 0, st>>>(W.n, B.x, B.r, B.rm, p_new, B.q, W.partB.p, W.partC.p, W.npB, par, S, d0,
+                                             Prec<TM>::fine_dinv(W), it0);
+  note(W, st, "pcg_update", -1, 6 * nK + (B.rm ? nM : 0.0) + (d0 ? 2 * nM : 0.0));
   W.npC = gup;
   k_check<<<1, kThreads, 0, st>>>(S, W.partC.p, W.npC);
   note(W, st, "pcg_check", -1, 0.0);
@@ -1317,7 +1330,7 @@ static int pcg_iteration(Solid* s, SolverWork& W, int precond, int k, PcgScalars
   WN_CUDA(cudaGetLastError());
   const double b_mid = W.bytes;
   W.cur_prec = true;
-  const int rc = apply_prec<TM>(s, W, precond, prec_input(B), B.z, S, st);
+  const int rc = apply_prec<TM>(s, W, precond, prec_input(B), B.z, S, st, d0);
   W.cur_prec = false;
   W.iter_core_bytes = b_mid - b_start;
   W.iter_prec_bytes = W.bytes - b_mid;
