@@ -110,3 +110,28 @@ def test_ibeam_mixed_batch_matches_fp64():
     e64 = np.linalg.norm(U64 - Ur, axis=0) / np.linalg.norm(Ur, axis=0)
     e32 = np.linalg.norm(U32 - Ur, axis=0) / np.linalg.norm(Ur, axis=0)
     assert e64.max() < 1e-8 and e32.max() < 1e-6
+
+
+def test_streamed_fine_level_matches_register_kernels():
+    """The batched fine level streamed from the tile-major pack (the default) and the register
+    row kernels (streaming off): the same per-case arithmetic in the same order, so the row
+    products agree bit for bit and the solves differ only by the order in which the per-CTA dot
+    partials are summed."""
+    from wnfea_b200 import _lib
+
+    m = _ibeam(20, seed=8)
+    K, _, _ = assemble_c3d10_sparse_3dof(m)
+    s = K.system
+    s.amg_setup()
+    F = tip_load_cases(m.mesh_nodes, n_cases=32, seed=4)
+    F[np.asarray(solid_fixed_dofs(m), dtype=np.int64), :] = 0.0
+    for precision in (0, 1):
+        U1, st1 = s.solve_multi(F, rtol=1e-9, precision=precision)
+        _lib.call("wn_solid_set_stream", s.handle, 0)
+        try:
+            U0, st0 = s.solve_multi(F, rtol=1e-9, precision=precision)
+        finally:
+            _lib.call("wn_solid_set_stream", s.handle, 1)
+        assert st1["status"] == 0 and st0["status"] == 0
+        assert np.abs(st1["case_iterations"] - st0["case_iterations"]).max() <= 1
+        assert np.linalg.norm(U1 - U0) <= 1e-9 * np.linalg.norm(U0)

@@ -544,6 +544,299 @@ __global__ void __launch_bounds__(kThreads) kb_post_first(int64_t n_rows, const 
   if (part) write_case_parts<T>(dot, part);
 }
 
+// ---------------------------------------------------------------------------------------
+// streamed fine level (3x3 blocks): the fine matrix comes from its tile-major pack through the
+// shared-memory stage ring of stream.cuh (stream_pipeline).  Per tile, a group of 8 lanes per
+// block row (4 rows per warp), lane l owning 4 of the 32 cases; the group walks its row's
+// blocks in order, two blocks' x gathers in flight, and reads each block's 9 values from the
+// stage (the 8 lanes of a group read the same word: a shared-memory broadcast, where the
+// register kernels above load the values coalesced and pass them round with shuffles).  The
+// per-case arithmetic and the order of every multiply-add are those of the register kernels,
+// so both paths give the same bits.
+// ---------------------------------------------------------------------------------------
+// the fine matrix in one precision as the streamed kernels see it
+struct BView {
+  const PackTile* tiles;
+  int n_tiles;
+  const unsigned char* pack;
+  StreamCtl ctl;
+};
+template <typename T>
+BView bview(const StreamMat& m) {
+  if constexpr (sizeof(T) == 4)
+    return {m.d32.p, m.n_tiles, m.p32.p, m.ctl};
+  else
+    return {m.d64.p, m.n_tiles, m.p64.p, m.ctl};
+}
+
+// the per-case partial sums of a CTA of NW warps (cf. write_case_parts)
+template <typename M, int NW>
+__device__ __forceinline__ void write_case_parts_nw(double (&d)[4], double* __restrict__ part) {
+  __shared__ double sh[NW][kBatch];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    d[k] += __shfl_xor_sync(0xffffffffu, d[k], 8);
+    d[k] += __shfl_xor_sync(0xffffffffu, d[k], 16);
+  }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane < 8)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) sh[w][case_of<M>(lane, k)] = d[k];
+  __syncthreads();
+  if (threadIdx.x < kBatch) {
+    double s = 0.0;
+    for (int k = 0; k < NW; ++k) s += sh[k][threadIdx.x];
+    part[(int64_t)blockIdx.x * kBatch + threadIdx.x] = s;
+  }
+}
+
+// The tile body: rows of the 3x3 fine matrix against DOF-major n x 32 vectors; per row DOF i,
+// pre = epi.load(i, l) before the product and epi.store(i, l, pre, acc, dot) after it
+template <typename T, typename XF, typename EPI, typename HOOK>
+__device__ __forceinline__ void batch_stream_rows(const BView& m, const XF& xf, const EPI& epi, unsigned char* smem,
+                                                  BlockScalars* S, bool* skipped, const HOOK& hook,
+                                                  double (&dot)[4]) {
+  using Cfg = typename StreamDefault<T, 3, 3>::type;
+  constexpr int NCW = Cfg::kWarps;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int l = lane & 7, grp = lane >> 3;
+  auto body = [&](int jc, const unsigned char* st, const int4 d, double&) {
+    const int r0 = d.x, nr = d.y - d.x, cntp = d.w;
+    const T* sv = reinterpret_cast<const T*>(st);
+    const int32_t* scol = reinterpret_cast<const int32_t*>(st + pack_col_off<T, 9>(cntp));
+    const uint16_t* srp = reinterpret_cast<const uint16_t*>(st + pack_row_off<T, 9>(cntp));
+    // warps take the tile's rows in passes of 4, starting from a warp that rotates per tile
+    const int wslot = (warp + jc) % NCW;
+    for (int base = wslot * 4; base < nr; base += NCW * 4) {
+      const int lr = base + grp;
+      if (lr >= nr) continue;  // no warp-wide operation below: the groups run independently
+      const int rs = srp[lr], re = srp[lr + 1];
+      const int64_t i0 = (int64_t)(r0 + lr) * 3;
+      typename EPI::Pre pre[3];
+#pragma unroll
+      for (int r = 0; r < 3; ++r) pre[r] = epi.load(i0 + r, l);
+      T acc[3][4];
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc[r][k] = T(0);
+      auto fma_block = [&](int b, const C4<T> (&x)[3]) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const T a = sv[(r * 3 + c) * cntp + b];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) acc[r][k] = fma(a, x[c].v[k], acc[r][k]);
+          }
+      };
+      int b = rs;
+      // two blocks' gathers in flight in FP32; one in FP64 (registers: two CTAs per SM)
+      for (; sizeof(T) == 4 && b + 1 < re; b += 2) {
+        const int64_t ca = scol[b], cb = scol[b + 1];
+        C4<T> xa[3], xb[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          xa[c] = xf(ca * 3 + c, l);
+          xb[c] = xf(cb * 3 + c, l);
+        }
+        fma_block(b, xa);
+        fma_block(b + 1, xb);
+      }
+      for (; b < re; ++b) {
+        const int64_t ca = scol[b];
+        C4<T> xa[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) xa[c] = xf(ca * 3 + c, l);
+        fma_block(b, xa);
+      }
+#pragma unroll
+      for (int r = 0; r < 3; ++r) epi.store(i0 + r, l, pre[r], acc[r], dot);
+    }
+  };
+  stream_pipeline<T, 9, Cfg>(m.tiles, m.n_tiles, m.pack, smem, &S->status, &S->done, m.ctl, skipped, hook, body);
+}
+
+// epilogues of the streamed fine-level kernels (the arithmetic of kb_pre_first, kb_cheb_step,
+// kb_residual, kb_post_first and kb_spmv_dot); like those kernels they read the row's own
+// operands after the row product (no registers held across it)
+struct BNoPre {};
+template <typename T>
+struct BEpiPreFirst {
+  const T* __restrict__ b;
+  const T* __restrict__ dinv;
+  T inv_theta;
+  int deg;
+  T c1, c2;
+  T *__restrict__ x, *__restrict__ r, *__restrict__ d, *__restrict__ res;
+  using Pre = BNoPre;
+  __device__ __forceinline__ Pre load(int64_t, int) const { return {}; }
+  __device__ __forceinline__ void store(int64_t i, int l, const Pre&, const T (&acc)[4], double (&)[4]) const {
+    const int64_t o = i * kBatch;
+    const T di = dinv[i];
+    const C4<T> bi = ldc<T>(b + o, l);
+    C4<T> xo, ro, dd;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const T t = acc[k];
+      const T d0 = di * bi.v[k] * inv_theta;
+      if (deg == 1) {
+        xo.v[k] = d0;
+        ro.v[k] = bi.v[k] - t;
+      } else {
+        const T r1 = di * bi.v[k] - di * t;
+        const T d1 = c1 * d0 + c2 * r1;
+        xo.v[k] = d0 + d1;
+        ro.v[k] = r1;
+        dd.v[k] = d1;
+      }
+    }
+    stc<T>(x + o, l, xo);
+    if (deg == 1) {
+      stc<T>(res + o, l, ro);
+    } else {
+      stc<T>(r + o, l, ro);
+      stc<T>(d + o, l, dd);
+    }
+  }
+};
+template <typename T>
+struct BEpiCheb {  // r -= D^-1 A d_in; d_out = c1 d_in + c2 r; x += d_out; dot: b . x
+  const T* __restrict__ dinv;
+  const T* __restrict__ d_in;
+  T *__restrict__ d_out, *__restrict__ r, *__restrict__ x;
+  T c1, c2;
+  const T* __restrict__ b;
+  int want_dot;
+  using Pre = BNoPre;
+  __device__ __forceinline__ Pre load(int64_t, int) const { return {}; }
+  __device__ __forceinline__ void store(int64_t i, int l, const Pre&, const T (&acc)[4], double (&dot)[4]) const {
+    const int64_t o = i * kBatch;
+    const T di = dinv[i];
+    const C4<T> rv = ldc<T>(r + o, l), dv = ldc<T>(d_in + o, l), xv = ldc<T>(x + o, l);
+    C4<T> ro, dn, xn;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      ro.v[k] = rv.v[k] - di * acc[k];
+      dn.v[k] = c1 * dv.v[k] + c2 * ro.v[k];
+      xn.v[k] = xv.v[k] + dn.v[k];
+    }
+    stc<T>(r + o, l, ro);
+    stc<T>(d_out + o, l, dn);
+    stc<T>(x + o, l, xn);
+    if (want_dot) {
+      const C4<T> bv = ldc<T>(b + o, l);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) dot[k] += (double)bv.v[k] * (double)xn.v[k];
+    }
+  }
+};
+template <typename T>
+struct BEpiResidual {  // res = b - A x
+  const T* __restrict__ b;
+  T* __restrict__ res;
+  using Pre = BNoPre;
+  __device__ __forceinline__ Pre load(int64_t, int) const { return {}; }
+  __device__ __forceinline__ void store(int64_t i, int l, const Pre&, const T (&acc)[4], double (&)[4]) const {
+    const C4<T> bv = ldc<T>(b + i * kBatch, l);
+    C4<T> ro;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ro.v[k] = bv.v[k] - acc[k];
+    stc<T>(res + i * kBatch, l, ro);
+  }
+};
+template <typename T>
+struct BEpiPostFirst {  // r0 = D^-1 (b - A x), d0 = r0 / theta, x2 = x + d0; dot: b . x2
+  const T* __restrict__ b;
+  const T* __restrict__ dinv;
+  T inv_theta;
+  const T* __restrict__ x;
+  T *__restrict__ x2, *__restrict__ r, *__restrict__ d;
+  int want_dot;
+  using Pre = BNoPre;
+  __device__ __forceinline__ Pre load(int64_t, int) const { return {}; }
+  __device__ __forceinline__ void store(int64_t i, int l, const Pre&, const T (&acc)[4], double (&dot)[4]) const {
+    const int64_t o = i * kBatch;
+    const T di = dinv[i];
+    const C4<T> bv = ldc<T>(b + o, l), xv = ldc<T>(x + o, l);
+    C4<T> ro, dd, xn;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      ro.v[k] = di * (bv.v[k] - acc[k]);
+      dd.v[k] = ro.v[k] * inv_theta;
+      xn.v[k] = xv.v[k] + dd.v[k];
+      if (want_dot) dot[k] += (double)bv.v[k] * (double)xn.v[k];
+    }
+    stc<T>(r + o, l, ro);
+    stc<T>(d + o, l, dd);
+    stc<T>(x2 + o, l, xn);
+  }
+};
+template <typename TM>
+struct BEpiSpmvDot {  // p_new = z + beta p_old; q = A p_new; dot: p_new . q
+  BPNew<TM> pf;
+  double *__restrict__ p_new, *__restrict__ q;
+  using Pre = BNoPre;
+  __device__ __forceinline__ Pre load(int64_t, int) const { return {}; }
+  __device__ __forceinline__ void store(int64_t i, int l, const Pre&, const double (&acc)[4],
+                                        double (&dot)[4]) const {
+    const int64_t o = i * kBatch;
+    const C4<double> pv = pf(i, l);
+    C4<double> qv;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      qv.v[k] = acc[k];
+      dot[k] += pv.v[k] * qv.v[k];
+    }
+    stc<double>(p_new + o, l, pv);
+    stc<double>(q + o, l, qv);
+  }
+};
+
+// the streamed fine-level kernel: a persistent CTA per tile run; part (if set) receives the
+// per-case partials of the epilogue's dot
+template <typename T>
+struct BStreamCtas {
+  static constexpr int value = 2;
+};
+template <typename T, typename XF, typename EPI>
+__global__ void __launch_bounds__(kStreamThreads, BStreamCtas<T>::value)
+    kbs_rows(BView m, XF xf, EPI epi, double* __restrict__ part, BlockScalars* __restrict__ S) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  bool skipped = false;
+  double dot[4] = {0.0, 0.0, 0.0, 0.0};
+  batch_stream_rows<T>(m, xf, epi, smem, S, &skipped, NoHook{}, dot);
+  if (part && !skipped) write_case_parts_nw<T, kStreamThreads / 32>(dot, part);
+}
+// the PCG product with the FP64 pack: p_new = z + beta p_old on the fly, its case map is the
+// FP64 one (cases 2l, 2l+1, 16+2l, 17+2l)
+template <typename TM>
+__global__ void __launch_bounds__(kStreamThreads, 2)
+    kbs_spmv_dot(BView m, const TM* __restrict__ z, const double* __restrict__ p_old, double* __restrict__ p_new,
+                 double* __restrict__ q, double* __restrict__ partB, BlockScalars* __restrict__ S) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  bool skipped = false;
+  double dot[4] = {0.0, 0.0, 0.0, 0.0};
+  const int l = threadIdx.x & 7;
+  const BPNew<TM> pf{z, p_old, case_scalars<double>(S->beta, l)};
+  batch_stream_rows<double>(m, pf, BEpiSpmvDot<TM>{pf, p_new, q}, smem, S, &skipped, NoHook{}, dot);
+  if (!skipped) write_case_parts_nw<double, kStreamThreads / 32>(dot, partB);
+}
+
+// launch a streamed fine-level kernel; the grid (one persistent wave), 0 if it cannot run here
+template <typename T, typename K, typename... Args>
+int launch_bs(K kern, const StreamMat& m, cudaStream_t st, Args... args) {
+  if (!m.packed || m.br != 3 || m.bc != 3) return 0;
+  const size_t smem = stream_smem_bytes<T, 3, 3>();
+  const int per_sm = stream_ctas_per_sm(reinterpret_cast<const void*>(kern), kStreamThreads, smem);
+  if (per_sm < 1) return 0;
+  const int g = std::max(1, std::min(m.n_tiles, kNumSMs * per_sm));
+  if (g > BlockWork::kMaxParts) return 0;
+  kern<<<g, kStreamThreads, smem, st>>>(args...);
+  if (cudaGetLastError() != cudaSuccess) return 0;
+  return g;
+}
+
 // y = A x or y += A x for the block-contiguous transfer operators (BR x BC blocks)
 template <int BR, int BC, typename T, int S>
 __global__ void __launch_bounds__(kThreads) kb_level_spmv(int64_t n_rows, const int32_t* __restrict__ rp,
@@ -1037,7 +1330,8 @@ void batch_level_spmv(const DevBsr& M, const T* vals, const T* x, T* y, int accu
 // one batched V-cycle at level lvl: out = V(b); part (if set) receives b . out per case
 template <typename T>
 int batch_vcycle(Solid* s, AmgHierarchy& H, BlockWork& W, int lvl, const T* b, T* out, double* part,
-                 const int* done, cudaStream_t st) {
+                 BlockScalars* S, cudaStream_t st) {
+  const int* done = &S->done;
   const int nlev = (int)H.levels.size();
   if (lvl == nlev) {
     kb_coarse<T><<<resident_grid(kb_coarse<T>, kThreads, (H.n_coarse * 32 + kThreads - 1) / kThreads), kThreads, 0,
@@ -1061,27 +1355,39 @@ int batch_vcycle(Solid* s, AmgHierarchy& H, BlockWork& W, int lvl, const T* b, T
   const int64_t sd = (lvl == 0) ? s->nnzb : 0;
   auto run = [&](auto bs_tag) -> int {
     constexpr int BS = decltype(bs_tag)::value;
-    constexpr int S = (BS == 3) ? 1 : 4;  // coarse 6x6 levels: rows of ~50-250 blocks, one warp each
-    const int work = rows_work(nr * S);
+    constexpr int SG = (BS == 3) ? 1 : 4;  // coarse 6x6 levels: rows of ~50-250 blocks, one warp each
+    const int work = rows_work(nr * SG);
     auto rg = [&](auto kern) { return resident_grid(kern, kThreads, work); };
     const int32_t* rp = lvl == 0 ? s->row_ptr.p : L.A.rp.p;
     const int32_t* ci = lvl == 0 ? s->col_idx.p : L.A.ci.p;
     const T* av = lvl == 0 ? BPrec<T>::A0(s) : BPrec<T>::Av(L);
     const T c1 = deg >= 2 ? (T)L.c1[0] : T(0), c2 = deg >= 2 ? (T)L.c2[0] : T(0);
-    kb_pre_first<BS, T, S><<<rg(kb_pre_first<BS, T, S>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, deg, c1, c2,
-                                                                      V.x.p, V.r.p, V.d.p, V.res.p, done);
+    // the fine level streams its matrix from the tile-major pack when it has one
+    const bool fine_stream = lvl == 0 && BS == 3 && s->fine.packed;
+    const BView fv = bview<T>(s->fine);
+    auto streamed = [&](auto xf, auto epi, double* part_out) -> int {
+      return launch_bs<T>(kbs_rows<T, decltype(xf), decltype(epi)>, s->fine, st, fv, xf, epi, part_out, S);
+    };
+    if (!(fine_stream && streamed(BD0<T, T>{b, dinv, it},
+                                  BEpiPreFirst<T>{b, dinv, it, deg, c1, c2, V.x.p, V.r.p, V.d.p, V.res.p}, nullptr)))
+      kb_pre_first<BS, T, SG><<<rg(kb_pre_first<BS, T, SG>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, deg, c1,
+                                                                        c2, V.x.p, V.r.p, V.d.p, V.res.p, done);
     W.launches++;
     T* din = V.d.p;
     T* dout = V.d2.p;
     for (int k = 2; k < deg; ++k) {
-      kb_cheb_step<BS, T, S><<<rg(kb_cheb_step<BS, T, S>), kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout, V.r.p,
-                                                                        V.x.p, (T)L.c1[k - 1], (T)L.c2[k - 1], b,
-                                                                        nullptr, done);
+      const T ck1 = (T)L.c1[k - 1], ck2 = (T)L.c2[k - 1];
+      if (!(fine_stream &&
+            streamed(BLoad<T, T>{din}, BEpiCheb<T>{dinv, din, dout, V.r.p, V.x.p, ck1, ck2, b, 0}, nullptr)))
+        kb_cheb_step<BS, T, SG><<<rg(kb_cheb_step<BS, T, SG>), kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout,
+                                                                          V.r.p, V.x.p, ck1, ck2, b, nullptr, done);
       W.launches++;
       std::swap(din, dout);
     }
     if (deg >= 2) {
-      kb_residual<BS, T, S><<<rg(kb_residual<BS, T, S>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, V.x.p, V.res.p, done);
+      if (!(fine_stream && streamed(BLoad<T, T>{V.x.p}, BEpiResidual<T>{b, V.res.p}, nullptr)))
+        kb_residual<BS, T, SG><<<rg(kb_residual<BS, T, SG>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, V.x.p, V.res.p,
+                                                                         done);
       W.launches++;
     }
     const bool last = lvl + 1 >= nlev;
@@ -1089,23 +1395,36 @@ int batch_vcycle(Solid* s, AmgHierarchy& H, BlockWork& W, int lvl, const T* b, T
     T* xc = last ? BPrec<T>::cx(W) : BPrec<T>::lv(W, lvl + 1).x2.p;
     batch_level_spmv<6, BS, T>(L.R, BPrec<T>::Rv(L), V.res.p, bc, 0, done, st);
     W.launches++;
-    WN_CHECK(batch_vcycle<T>(s, H, W, lvl + 1, bc, xc, nullptr, done, st));
+    WN_CHECK(batch_vcycle<T>(s, H, W, lvl + 1, bc, xc, nullptr, S, st));
     batch_level_spmv<BS, 6, T>(L.P, BPrec<T>::Pv(L), xc, V.x.p, 1, done, st);
     W.launches++;
     double* part_last = (deg == 1) ? part : nullptr;
-    const int gpf = rg(kb_post_first<BS, T, S>);
+    int gpf = fine_stream ? streamed(BLoad<T, T>{V.x.p},
+                                     BEpiPostFirst<T>{b, dinv, it, V.x.p, out, V.r.p, V.d.p, part_last != nullptr},
+                                     part_last)
+                          : 0;
+    if (gpf == 0) {
+      gpf = rg(kb_post_first<BS, T, SG>);
+      kb_post_first<BS, T, SG><<<gpf, kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, V.x.p, out, V.r.p, V.d.p,
+                                                     part_last, done);
+    }
     if (part_last) W.npA = gpf;
-    kb_post_first<BS, T, S><<<gpf, kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, V.x.p, out, V.r.p, V.d.p,
-                                                   part_last, done);
     W.launches++;
     din = V.d.p;
     dout = V.d2.p;
     for (int k = 1; k < deg; ++k) {
       double* pk = (k == deg - 1) ? part : nullptr;
-      const int gcs = rg(kb_cheb_step<BS, T, S>);
+      const T ck1 = (T)L.c1[k - 1], ck2 = (T)L.c2[k - 1];
+      int gcs = fine_stream ? streamed(BLoad<T, T>{din}, BEpiCheb<T>{dinv, din, dout, V.r.p, out, ck1, ck2, b,
+                                                                     pk != nullptr},
+                                       pk)
+                            : 0;
+      if (gcs == 0) {
+        gcs = rg(kb_cheb_step<BS, T, SG>);
+        kb_cheb_step<BS, T, SG><<<gcs, kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout, V.r.p, out, ck1, ck2, b,
+                                                      pk, done);
+      }
       if (pk) W.npA = gcs;
-      kb_cheb_step<BS, T, S><<<gcs, kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout, V.r.p, out,
-                                                    (T)L.c1[k - 1], (T)L.c2[k - 1], b, pk, done);
       W.launches++;
       std::swap(din, dout);
     }
@@ -1118,8 +1437,9 @@ int batch_vcycle(Solid* s, AmgHierarchy& H, BlockWork& W, int lvl, const T* b, T
 
 // z = M r for all cases, partA = r . z per case
 template <typename TM>
-int batch_prec(Solid* s, BlockWork& W, int precond, const TM* r, TM* z, const int* done, cudaStream_t st) {
-  if (precond == 2) return batch_vcycle<TM>(s, *s->amg, W, 0, r, z, W.partA.p, done, st);
+int batch_prec(Solid* s, BlockWork& W, int precond, const TM* r, TM* z, BlockScalars* S, cudaStream_t st) {
+  const int* done = &S->done;
+  if (precond == 2) return batch_vcycle<TM>(s, *s->amg, W, 0, r, z, W.partA.p, S, st);
   const int g = resident_grid(kb_prec_vec<TM>, kThreads, quads_work(W.n));
   W.npA = g;
   kb_prec_vec<TM><<<g, kThreads, 0, st>>>(W.n, r, BPrec<TM>::fine_dinv(W), precond == 1 ? 1 : 0, z, W.partA.p,
@@ -1143,9 +1463,14 @@ int batch_iteration(Solid* s, BlockWork& W, int precond, int k, BlockScalars* S,
   const int par = k & 1;
   double* p_new = par ? W.p1.p : W.p0.p;
   double* p_old = par ? W.p0.p : W.p1.p;
-  const int gsd = resident_grid(kb_spmv_dot<TM>, kThreads, rows_work(s->n_nodes));
-  kb_spmv_dot<TM><<<gsd, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, s->nnzb,
-                                            BPrec<TM>::z(W), p_old, p_new, W.q.p, W.partB.p, S);
+  // the fine FP64 matrix streamed from its pack when it has one, else the register kernel
+  int gsd = launch_bs<double>(kbs_spmv_dot<TM>, s->fine, st, bview<double>(s->fine), (const TM*)BPrec<TM>::z(W),
+                              (const double*)p_old, p_new, W.q.p, W.partB.p, S);
+  if (gsd == 0) {
+    gsd = resident_grid(kb_spmv_dot<TM>, kThreads, rows_work(s->n_nodes));
+    kb_spmv_dot<TM><<<gsd, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, s->nnzb,
+                                              BPrec<TM>::z(W), p_old, p_new, W.q.p, W.partB.p, S);
+  }
   W.npB = gsd;
   kb_alpha<<<1, kThreads, 0, st>>>(S, W.partB.p, W.npB);
   const int gup = resident_grid(kb_update<TM>, kThreads, quads_work(W.n));
@@ -1154,7 +1479,7 @@ int batch_iteration(Solid* s, BlockWork& W, int precond, int k, BlockScalars* S,
   kb_check<<<1, kThreads, 0, st>>>(S, W.partC.p, W.npC);
   W.launches += 4;
   WN_CUDA(cudaGetLastError());
-  WN_CHECK(batch_prec<TM>(s, W, precond, prec_input<TM>(W), BPrec<TM>::z(W), &S->done, st));
+  WN_CHECK(batch_prec<TM>(s, W, precond, prec_input<TM>(W), BPrec<TM>::z(W), S, st));
   kb_beta<<<1, kThreads, 0, st>>>(S, W.partA.p, W.npA, 0);
   W.launches++;
   WN_CUDA(cudaGetLastError());
@@ -1173,7 +1498,7 @@ int batch_pcg(Solid* s, BlockWork& W, int vmode, const double* b, int max_iter, 
   kb_init_scalars<<<1, kThreads, 0, st>>>(S, W.partC.p, W.npC, W.rtol_cols.p, max_iter);
   W.launches += 2;
   WN_CUDA(cudaGetLastError());
-  WN_CHECK(batch_prec<TM>(s, W, precond, prec_input<TM>(W), BPrec<TM>::z(W), &S->done, st));
+  WN_CHECK(batch_prec<TM>(s, W, precond, prec_input<TM>(W), BPrec<TM>::z(W), S, st));
   kb_beta<<<1, kThreads, 0, st>>>(S, W.partA.p, W.npA, 1);
   W.launches++;
   chunk = std::max(2, chunk + (chunk & 1));  // even: the parity pattern repeats per chunk

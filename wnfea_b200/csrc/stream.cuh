@@ -310,30 +310,26 @@ __device__ __forceinline__ T pick_lane(const T (&a)[N], int l) {
   return v;
 }
 
-// The engine.  Every thread of a CTA of Cfg::kThreads threads calls it once (dynamic shared
-// memory of stream_smem_bytes<T, BR, BC, Cfg>()); the pack was built from a plan with Cfg's
-// capacities.  Per row DOF i = BR row + c of the CTA's tiles the owning lane (c < BR <= G)
-// calls pre = epi.load(i) before the row product and dot += epi.store(i, pre, (A x)_i) after
-// it, with x_j = xf(j) (j = BC col + c).  Returns the thread's dot sum (0 for the producer).
+// The tile pipeline.  Every thread of a CTA of Cfg::kThreads threads calls it once (dynamic
+// shared memory of stream_smem_bytes<T, BR, BC, Cfg>()); the pack was built from a plan with
+// Cfg's capacities (NV = BR * BC values per block).  The producer warp streams the CTA's run of
+// tiles into the stage ring; every consumer warp calls body(jc, stage, desc, dot) for each tile jc
+// of the run (stage = the tile's image in shared memory, desc = rows r0, r1 / segment /
+// cntp), adding its dot contributions to the consumer's running sum, which is returned (0 for
+// the producer).
 // The first stages' copies (the matrix only) are issued before pdl_wait(), so under a
 // programmatic dependent launch they overlap the predecessor's tail; then every thread runs
 // hook(), and when *done is set (read after the wait) the CTA lets those copies land and
 // returns with *skipped = true.  Every warp of the CTA meets once more at the end; if any wait
 // ran out, one thread then waits (bounded) for the copies still in flight before the CTA exits.
-template <typename T, int BR, int BC, typename Cfg, typename XF, typename EPI, typename HOOK = NoHook>
-__device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles, int n_tiles,
-                                              const unsigned char* __restrict__ pack, const XF& xf, const EPI& epi,
-                                              unsigned char* smem, int* status, int* done, const StreamCtl ctl,
-                                              bool* skipped = nullptr, const HOOK& hook = HOOK{}) {
-  constexpr int NV = BR * BC;
+template <typename T, int NV, typename Cfg, typename BODY, typename HOOK>
+__device__ __forceinline__ double stream_pipeline(const PackTile* __restrict__ tiles, int n_tiles,
+                                                  const unsigned char* __restrict__ pack, unsigned char* smem,
+                                                  int* status, int* done, const StreamCtl ctl, bool* skipped,
+                                                  const HOOK& hook, BODY& body) {
   constexpr int STAGES = Cfg::kStages;
   constexpr uint32_t SB = Cfg::template stage_bytes<T, NV>();
-  constexpr int G = Cfg::kG;
-  constexpr int U = Cfg::kUnroll;
-  constexpr int R = Cfg::kRpg;
-  constexpr int GPW = 32 / G;  // row groups per warp
   constexpr int NCW = Cfg::kWarps;
-  static_assert(BR <= G, "a lane per row DOF");
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + STAGES;
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + 256);
@@ -424,7 +420,6 @@ __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles
     return 0.0;
   }
 
-  const int gl = lane % G, grp = lane / G;
   if (warp == NCW) {
     issue(n_my);
     if (lane == 0 && !ok) fail();
@@ -437,74 +432,7 @@ __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles
         if (lane == 0) fail();
         break;
       }
-      const unsigned char* st = stages + (size_t)s * SB;
-      const int4 d = descs[s];
-      const int r0 = d.x, nr = d.y - d.x, cntp = d.w;
-      const T* sv = reinterpret_cast<const T*>(st);
-      const int32_t* scol = reinterpret_cast<const int32_t*>(st + pack_col_off<T, NV>(cntp));
-      const uint16_t* srp = reinterpret_cast<const uint16_t*>(st + pack_row_off<T, NV>(cntp));
-      // warps take the tile's rows round-robin in passes of GPW * R rows (group g of a pass owns
-      // rows base + q GPW + g, q < R), starting from a warp that rotates per tile
-      const int wslot = (warp + jc) % NCW;
-      for (int base = wslot * GPW * R; base < nr; base += NCW * GPW * R) {
-        int rs[R], re[R];
-        typename EPI::Pre pre[R];
-        T acc[R][BR];
-        int len = 0;
-#pragma unroll
-        for (int q = 0; q < R; ++q) {
-          const int lr = base + q * GPW + grp;
-          const bool active = lr < nr;
-          rs[q] = active ? srp[lr] : 0;
-          re[q] = active ? srp[lr + 1] : 0;
-          len = max(len, re[q] - rs[q]);
-          pre[q] = typename EPI::Pre{};
-          if (active && gl < BR) pre[q] = epi.load((int64_t)(r0 + lr) * BR + gl);
-#pragma unroll
-          for (int r = 0; r < BR; ++r) acc[q][r] = T(0);
-        }
-        // U blocks of each of the R rows in flight per lane: their gathers are issued before the
-        // first multiply-add; each row's sum still runs over the lane's blocks in order
-        // (b, b + G, b + 2G, ...)
-        for (int o = gl; o < len; o += G * U) {
-          int col[R][U];
-          T xv[R][U][BC];
-#pragma unroll
-          for (int q = 0; q < R; ++q)
-#pragma unroll
-            for (int u = 0; u < U; ++u) col[q][u] = (rs[q] + o + u * G < re[q]) ? scol[rs[q] + o + u * G] : 0;
-#pragma unroll
-          for (int q = 0; q < R; ++q)
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-#pragma unroll
-              for (int c = 0; c < BC; ++c) xv[q][u][c] = xf((int64_t)col[q][u] * BC + c);
-#pragma unroll
-          for (int q = 0; q < R; ++q)
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-              const int b = rs[q] + o + u * G;
-              if (b < re[q]) {
-#pragma unroll
-                for (int r = 0; r < BR; ++r)
-#pragma unroll
-                  for (int c = 0; c < BC; ++c) acc[q][r] = fma(sv[(r * BC + c) * cntp + b], xv[q][u][c], acc[q][r]);
-              }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < R; ++q) {
-#pragma unroll
-          for (int r = 0; r < BR; ++r) {
-            T v = acc[q][r];
-#pragma unroll
-            for (int o2 = G / 2; o2 > 0; o2 >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o2);
-            acc[q][r] = v;
-          }
-          const int lr = base + q * GPW + grp;
-          if (lr < nr && gl < BR) dot += epi.store((int64_t)(r0 + lr) * BR + gl, pre[q], pick_lane<BR>(acc[q], gl));
-        }
-      }
+      body(jc, stages + (size_t)s * SB, descs[s], dot);
       __syncwarp();
       if (lane == 0) mbar_arrive(empty + s);
     }
@@ -514,6 +442,96 @@ __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles
   __syncthreads();
   if (*abort_flag && warp == NCW && lane == 0) drain();
   return dot;
+}
+
+// The row engine: y-rows of A x with G lanes per block row (lane l taking the row's blocks
+// l, l + G, ...; U blocks in flight per lane, R rows per lane group), for every row DOF
+// i = BR row + c of the CTA's tiles the owning lane (c < BR <= G) calls pre = epi.load(i) before
+// the row product and dot += epi.store(i, pre, (A x)_i) after it, with x_j = xf(j)
+// (j = BC col + c).  Returns the thread's dot sum (0 for the producer).
+template <typename T, int BR, int BC, typename Cfg, typename XF, typename EPI, typename HOOK = NoHook>
+__device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles, int n_tiles,
+                                              const unsigned char* __restrict__ pack, const XF& xf, const EPI& epi,
+                                              unsigned char* smem, int* status, int* done, const StreamCtl ctl,
+                                              bool* skipped = nullptr, const HOOK& hook = HOOK{}) {
+  constexpr int NV = BR * BC;
+  constexpr int G = Cfg::kG;
+  constexpr int U = Cfg::kUnroll;
+  constexpr int R = Cfg::kRpg;
+  constexpr int GPW = 32 / G;  // row groups per warp
+  constexpr int NCW = Cfg::kWarps;
+  static_assert(BR <= G, "a lane per row DOF");
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gl = lane % G, grp = lane / G;
+  auto body = [&](int jc, const unsigned char* st, const int4 d, double& dot) {
+    const int r0 = d.x, nr = d.y - d.x, cntp = d.w;
+    const T* sv = reinterpret_cast<const T*>(st);
+    const int32_t* scol = reinterpret_cast<const int32_t*>(st + pack_col_off<T, NV>(cntp));
+    const uint16_t* srp = reinterpret_cast<const uint16_t*>(st + pack_row_off<T, NV>(cntp));
+    // warps take the tile's rows round-robin in passes of GPW * R rows (group g of a pass owns
+    // rows base + q GPW + g, q < R), starting from a warp that rotates per tile
+    const int wslot = (warp + jc) % NCW;
+    for (int base = wslot * GPW * R; base < nr; base += NCW * GPW * R) {
+      int rs[R], re[R];
+      typename EPI::Pre pre[R];
+      T acc[R][BR];
+      int len = 0;
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int lr = base + q * GPW + grp;
+        const bool active = lr < nr;
+        rs[q] = active ? srp[lr] : 0;
+        re[q] = active ? srp[lr + 1] : 0;
+        len = max(len, re[q] - rs[q]);
+        pre[q] = typename EPI::Pre{};
+        if (active && gl < BR) pre[q] = epi.load((int64_t)(r0 + lr) * BR + gl);
+#pragma unroll
+        for (int r = 0; r < BR; ++r) acc[q][r] = T(0);
+      }
+      // U blocks of each of the R rows in flight per lane: their gathers are issued before the
+      // first multiply-add; each row's sum still runs over the lane's blocks in order
+      // (b, b + G, b + 2G, ...)
+      for (int o = gl; o < len; o += G * U) {
+        int col[R][U];
+        T xv[R][U][BC];
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+#pragma unroll
+          for (int u = 0; u < U; ++u) col[q][u] = (rs[q] + o + u * G < re[q]) ? scol[rs[q] + o + u * G] : 0;
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int c = 0; c < BC; ++c) xv[q][u][c] = xf((int64_t)col[q][u] * BC + c);
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int b = rs[q] + o + u * G;
+            if (b < re[q]) {
+#pragma unroll
+              for (int r = 0; r < BR; ++r)
+#pragma unroll
+                for (int c = 0; c < BC; ++c) acc[q][r] = fma(sv[(r * BC + c) * cntp + b], xv[q][u][c], acc[q][r]);
+            }
+          }
+      }
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+#pragma unroll
+        for (int r = 0; r < BR; ++r) {
+          T v = acc[q][r];
+#pragma unroll
+          for (int o2 = G / 2; o2 > 0; o2 >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o2);
+          acc[q][r] = v;
+        }
+        const int lr = base + q * GPW + grp;
+        if (lr < nr && gl < BR) dot += epi.store((int64_t)(r0 + lr) * BR + gl, pre[q], pick_lane<BR>(acc[q], gl));
+      }
+    }
+  };
+  return stream_pipeline<T, NV, Cfg>(tiles, n_tiles, pack, smem, status, done, ctl, skipped, hook, body);
 }
 
 #endif  // __CUDACC__
