@@ -7,8 +7,10 @@ full configurations that the benchmark times and check, against the oracle's FP6
 restatement of the reference (solid_solver.py:26-129, 311-365; c3d10.py:219-318):
 
 * the BSR3 pattern and element->block map bit for bit, and the assembled K (with BCs) entry by
-  entry through K - K_oracle (<= 1e-14 of max |K|, the summation-order tolerance of the
-  small-mesh tests);
+  entry through K - K_oracle: <= 1e-14 of max |K| (the summation-order tolerance of the
+  small-mesh tests) against the oracle's element matrices formed translation-invariantly, and
+  <= 1e-12 against the reference's absolute-coordinate form (whose own rounding on this 4 m
+  beam is 1.0e-13 of max |K|);
 * the true residual ||F - K u|| / ||F|| of the GPU's FP64 u in 80-bit host arithmetic with the
   oracle's K, for the FP64 and the mixed solve (and 4 of the 32 batched cases), at the requested
   1e-8 or at the FP64 rounding level of K u;
@@ -27,7 +29,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from oracle import solid
+from oracle import c3d10, solid
 from wnfea_b200 import _lib
 from wnfea_b200.mesh import generate_c3d10_ibeam_structured, generate_c3d10_pressure_block, tip_load_cases
 from wnfea_b200.model import solid_element_props, solid_fixed_dofs, solid_load_vector
@@ -81,11 +83,21 @@ def test_fullsize_pattern_map_and_matrix(ibeam):
     _lib.call("wn_solid_get_map", s.handle, _lib.ptr(emap))
     assert np.array_equal(emap, oemap)
     Kc = K.tocsr()
-    # entries whose exact value is zero (couplings that cancel by symmetry) may come out as exact
+    # Entries whose exact value is zero (couplings that cancel by symmetry) may come out as exact
     # zeros in one summation order and as ~1e-17 in the other, so eliminate_zeros can keep a few
-    # thousand more or fewer of them: compare through the difference
-    D = (Kc - Ko).tocsr()
-    assert np.abs(D.data).max(initial=0.0) <= 1e-14 * np.abs(Ko.data).max()
+    # thousand more or fewer of them: compare through the difference.
+    # The reference forms J from absolute coordinates (c3d10.py:109-137); on this 4 m beam of
+    # 1 cm elements that cancellation alone moves its element matrices by up to 3.6e-13 (1.0e-13
+    # of max |K| assembled, measured against the same elements taken relative to their first
+    # node).  The GPU forms J from relative coordinates, so: <= 1e-14 against the oracle
+    # evaluated the same translation-invariant way, <= 1e-12 against the reference's own form.
+    Ke_rel = c3d10.element_stiffness_batch(m.mesh_nodes[m.solid_elements] - m.mesh_nodes[m.solid_elements][:, :1],
+                                           solid_element_props(m))
+    Kr, _, _ = solid.assemble(m.mesh_nodes, m.solid_elements, solid_element_props(m), solid_load_vector(m),
+                              solid_fixed_dofs(m), Ke=Ke_rel)
+    for Kref, tol in ((Kr, 1e-14), (Ko, 1e-12)):
+        D = (Kc - Kref).tocsr()
+        assert np.abs(D.data).max(initial=0.0) <= tol * np.abs(Kref.data).max(), tol
     assert abs(Kc.nnz - Ko.nnz) <= 1e-3 * Ko.nnz
     assert np.array_equal(F, Fo)
 

@@ -43,6 +43,10 @@ __device__ __forceinline__ double gp_cartesian(int g, const double X[10][3], dou
   gauss_point(g, xi, eta, zeta);
   double dn[3][10];
   natural_derivs(xi, eta, zeta, dn);
+  // J = dN/dxi X with X taken relative to node 0: the same matrix (the derivatives of the shape
+  // functions sum to zero), without the cancellation of absolute coordinates -- an element 4 m
+  // from the origin with 1 cm edges would lose about three digits of J (c3d10.py:109-137 uses
+  // the absolute coordinates; its Ke there carries relative errors up to ~4e-13)
   double J[3][3];
 #pragma unroll
   for (int k = 0; k < 3; ++k)
@@ -50,7 +54,7 @@ __device__ __forceinline__ double gp_cartesian(int g, const double X[10][3], dou
     for (int j = 0; j < 3; ++j) {
       double s = 0.0;
 #pragma unroll
-      for (int a = 0; a < 10; ++a) s = fma(dn[k][a], X[a][j], s);
+      for (int a = 1; a < 10; ++a) s = fma(dn[k][a], X[a][j] - X[0][j], s);
       J[k][j] = s;
     }
   const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
