@@ -108,9 +108,13 @@ int wn_solid_device_arrays(void* h, const double** k64, const float** k32, const
 /* y = K x for the assembled matrix: precision 0 = FP64 values/accumulation, 1 = FP32
  * values/accumulation (x, y are float then).  Device pointers. */
 int wn_spmv_solid_device(void* h, int precision, const void* x, void* y, uintptr_t stream);
-/* Streamed fine-level kernels on (enable != 0, the default) or off.  Off drops the tile plan and
- * the FP32 / FP64 tile-major packs (about 1 GB per million DOFs) and runs the fine level on the
- * register row kernels; on rebuilds them (and packs the current values).  Synchronises. */
+/* Streamed fine-level kernels: enable 1 (the default) streams the fine level of single-case
+ * solves from the tile-major packs, 2 also that of the batched (wn_solve_multi) solves, 0 turns
+ * streaming off: it drops the tile plan and the FP32 / FP64 packs (about 1 GB per million DOFs)
+ * and runs the fine level on the register row kernels; 1 or 2 rebuild them (and pack the
+ * current values).  The batched solves default to the register kernels: with 32 cases per
+ * block a row's cost is the gather of the x rows it touches, not the block values the packs
+ * save.  Synchronises. */
 int wn_solid_set_stream(void* h, int enable);
 /* Status word of the streamed fine-matrix products of wn_spmv_solid_device: WN_OK, or
  * WN_ETIMEOUT when a bounded pipeline wait of a call since the last reset ran out of time (the

@@ -113,10 +113,11 @@ def test_ibeam_mixed_batch_matches_fp64():
 
 
 def test_streamed_fine_level_matches_register_kernels():
-    """The batched fine level streamed from the tile-major pack (the default) and the register
-    row kernels (streaming off): the same per-case arithmetic in the same order, so the row
-    products agree bit for bit and the solves differ only by the order in which the per-CTA dot
-    partials are summed."""
+    """The batched fine level streamed from the tile-major pack (streaming mode 2) and the
+    register row kernels (the default, mode 1; and with streaming off, mode 0): the same per-case
+    arithmetic in the same order, so the row products agree bit for bit and the solves differ
+    only by the order in which the per-CTA dot partials are summed.  Switching modes between
+    solves re-captures the batched solver's graphs (the packs are freed and rebuilt)."""
     from wnfea_b200 import _lib
 
     m = _ibeam(20, seed=8)
@@ -127,11 +128,17 @@ def test_streamed_fine_level_matches_register_kernels():
     F[np.asarray(solid_fixed_dofs(m), dtype=np.int64), :] = 0.0
     for precision in (0, 1):
         U1, st1 = s.solve_multi(F, rtol=1e-9, precision=precision)
-        _lib.call("wn_solid_set_stream", s.handle, 0)
+        _lib.call("wn_solid_set_stream", s.handle, 2)
         try:
+            U2, st2 = s.solve_multi(F, rtol=1e-9, precision=precision)
+            _lib.call("wn_solid_set_stream", s.handle, 0)
             U0, st0 = s.solve_multi(F, rtol=1e-9, precision=precision)
         finally:
             _lib.call("wn_solid_set_stream", s.handle, 1)
-        assert st1["status"] == 0 and st0["status"] == 0
-        assert np.abs(st1["case_iterations"] - st0["case_iterations"]).max() <= 1
-        assert np.linalg.norm(U1 - U0) <= 1e-9 * np.linalg.norm(U0)
+        U1b, st1b = s.solve_multi(F, rtol=1e-9, precision=precision)
+        for st in (st0, st1, st2, st1b):
+            assert st["status"] == 0
+        assert np.array_equal(U1, U1b)
+        for U, st in ((U2, st2), (U0, st0)):
+            assert np.abs(st["case_iterations"] - st1["case_iterations"]).max() <= 1
+            assert np.linalg.norm(U - U1) <= 1e-9 * np.linalg.norm(U1)

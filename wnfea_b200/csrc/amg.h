@@ -112,6 +112,7 @@ struct GraphCache {
   cudaStream_t stream = nullptr;
   int64_t key = -1;
   int64_t kernels = 0;  // kernels per replay
+  uint64_t fine_epoch = 0;  // StreamMat::epoch of the fine matrix at capture
   ~GraphCache() {
     if (exec) cudaGraphExecDestroy(exec);
   }

@@ -1363,7 +1363,7 @@ int batch_vcycle(Solid* s, AmgHierarchy& H, BlockWork& W, int lvl, const T* b, T
     const T* av = lvl == 0 ? BPrec<T>::A0(s) : BPrec<T>::Av(L);
     const T c1 = deg >= 2 ? (T)L.c1[0] : T(0), c2 = deg >= 2 ? (T)L.c2[0] : T(0);
     // the fine level streams its matrix from the tile-major pack when it has one
-    const bool fine_stream = lvl == 0 && BS == 3 && s->fine.packed;
+    const bool fine_stream = lvl == 0 && BS == 3 && s->fine.packed && s->stream_batched;
     const BView fv = bview<T>(s->fine);
     auto streamed = [&](auto xf, auto epi, double* part_out) -> int {
       return launch_bs<T>(kbs_rows<T, decltype(xf), decltype(epi)>, s->fine, st, fv, xf, epi, part_out, S);
@@ -1463,9 +1463,12 @@ int batch_iteration(Solid* s, BlockWork& W, int precond, int k, BlockScalars* S,
   const int par = k & 1;
   double* p_new = par ? W.p1.p : W.p0.p;
   double* p_old = par ? W.p0.p : W.p1.p;
-  // the fine FP64 matrix streamed from its pack when it has one, else the register kernel
-  int gsd = launch_bs<double>(kbs_spmv_dot<TM>, s->fine, st, bview<double>(s->fine), (const TM*)BPrec<TM>::z(W),
-                              (const double*)p_old, p_new, W.q.p, W.partB.p, S);
+  // the fine FP64 matrix streamed from its pack when batched streaming is on, else the
+  // register kernel
+  int gsd = s->stream_batched ? launch_bs<double>(kbs_spmv_dot<TM>, s->fine, st, bview<double>(s->fine),
+                                                  (const TM*)BPrec<TM>::z(W), (const double*)p_old, p_new, W.q.p,
+                                                  W.partB.p, S)
+                              : 0;
   if (gsd == 0) {
     gsd = resident_grid(kb_spmv_dot<TM>, kThreads, rows_work(s->n_nodes));
     kb_spmv_dot<TM><<<gsd, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, s->nnzb,
@@ -1510,7 +1513,7 @@ int batch_pcg(Solid* s, BlockWork& W, int vmode, const double* b, int max_iter, 
     WN_CUDA(cudaStreamSynchronize(st));
     if (hS->done || k0 >= max_iter) break;
     if (use_graph) {
-      if (G.key != key || G.stream != st || !G.exec) {
+      if (G.key != key || G.stream != st || !G.exec || G.fine_epoch != s->fine.epoch) {
         G.reset();
         cudaGraph_t graph;
         const int64_t before = W.launches;
@@ -1525,6 +1528,7 @@ int batch_pcg(Solid* s, BlockWork& W, int vmode, const double* b, int max_iter, 
         WN_CUDA(e);
         G.key = key;
         G.stream = st;
+        G.fine_epoch = s->fine.epoch;
         G.kernels = W.launches - before;
         W.launches = before;
       }

@@ -227,7 +227,7 @@ int wn_solid_create(int64_t n_nodes, int64_t n_el, const double* nodes, const in
   st = st ? st : s->gptr.upload(pat.gather_ptr);
   {
     // tile-owner assembly when every tile's incident elements fit in shared memory (200 of them,
-    // 206 KB); the tiles are those of the streamed fine matrix
+    // 203 KB); the tiles are those of the streamed fine matrix
     AssemblyPlan plan;
     std::vector<StreamTile> stiles;
     const bool ok = build_assembly_plan(pat, n_el, kStreamCap, kStreamRowCap, 200, plan) == 0 &&
@@ -483,8 +483,12 @@ int wn_solid_set_stream(void* h, int enable) {
   WN_REQUIRE(s->bs == 3, WN_ESTATE, "wn_solid_set_stream: not a C3D10 system");
   WN_CHECK(select_device(s));
   WN_CUDA(cudaDeviceSynchronize());
+  WN_REQUIRE(enable >= 0 && enable <= 2, WN_EINVAL, "wn_solid_set_stream: enable %d not 0, 1 or 2", enable);
   s->stream_fine = enable != 0;
+  s->stream_batched = enable == 2;
   // captured PCG chunks hold the launches (and pack pointers) of the current path: drop them
+  // (the batched solver's on the epoch change)
+  ++s->fine.epoch;
   if (s->work)
     for (auto& a : s->work->graphs)
       for (auto& g : a) g.reset();
@@ -518,7 +522,9 @@ int wn_solid_stream_test_hook(void* h, int64_t wait_limit_ns, int withhold_tile)
   WN_CUDA(cudaDeviceSynchronize());
   s->fine.ctl.wait_ns = wait_limit_ns > 0 ? (unsigned long long)wait_limit_ns : kStreamWaitLimitNs;
   s->fine.ctl.withhold = withhold_tile >= 0 ? withhold_tile : -1;
-  // captured PCG chunks carry the old control values as kernel parameters: drop them
+  // captured PCG chunks (single and batched) carry the old control values as kernel
+  // parameters: drop them
+  ++s->fine.epoch;
   if (s->work)
     for (auto& a : s->work->graphs)
       for (auto& g : a) g.reset();

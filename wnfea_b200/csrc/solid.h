@@ -54,6 +54,7 @@ struct Solid {
   // pattern, FP32 / FP64 tile-major packs refreshed by every assembly
   StreamMat fine;
   bool stream_fine = true;  // wn_solid_set_stream: plan and packs kept (else the register kernels)
+  bool stream_batched = false;  // wn_solid_set_stream(2): the batched solves stream the fine level too
   bool assembled = false;
   bool bcs_applied = false;
   std::unique_ptr<AmgHierarchy> amg;

@@ -1371,7 +1371,7 @@ static int pcg_solve(Solid* s, SolverWork& W, int mode, const TK* b, double rtol
     WN_CUDA(cudaStreamSynchronize(st));
     if (hS->done || k0 >= max_iter) break;
     if (use_graph) {
-      if (G.key != key || G.stream != st || !G.exec) {
+      if (G.key != key || G.stream != st || !G.exec || G.fine_epoch != s->fine.epoch) {
         G.reset();
         cudaGraph_t graph;
         const int64_t before = W.launches;
@@ -1390,6 +1390,7 @@ static int pcg_solve(Solid* s, SolverWork& W, int mode, const TK* b, double rtol
         WN_CUDA(e);
         G.key = key;
         G.stream = st;
+        G.fine_epoch = s->fine.epoch;
         G.kernels = W.launches - before;
         W.launches = before;
         W.bytes = bytes_before;  // captured, not run

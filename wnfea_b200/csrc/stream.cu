@@ -30,6 +30,7 @@ static int plan_shape(StreamMat& m, const int32_t* h_rp, int64_t n_rows) {
 }
 
 void StreamMat::clear() {
+  ++epoch;
   n_tiles = 0;
   packed = false;
   structure = false;
@@ -66,8 +67,10 @@ int StreamMat::pack(const int32_t* rp, const int32_t* ci, const float* v32, cons
                     cudaStream_t st) {
   packed = false;
   if (n_tiles == 0) return 0;
+  const unsigned char *old32 = p32.p, *old64 = p64.p;
   WN_CHECK(p32.alloc(size32));
   WN_CHECK(p64.alloc(size64));
+  if (p32.p != old32 || p64.p != old64) ++epoch;
   const int nv = br * bc;
   if (nv == 9) WN_CHECK(pack_shape<9>(*this, rp, ci, v32, v64, stride, st));
   else if (nv == 36) WN_CHECK(pack_shape<36>(*this, rp, ci, v32, v64, stride, st));

@@ -22,6 +22,9 @@ struct StreamMat {
   bool packed = false;  // the packs hold the current values
   bool structure = false;  // the packs hold the column indices and row starts (set by pack())
   StreamCtl ctl;         // wait limit of the streamed kernels on this matrix (and the test hook)
+  // changes whenever the plan or pack buffers are released or reallocated: a captured graph
+  // holds their addresses and is replayed only while the epoch it was captured at is current
+  uint64_t epoch = 0;
   // Tile plan and descriptors of a br x bc matrix from its host row pointer (shapes 3x3, 6x6,
   // 3x6, 6x3; others are left unstreamed).  Packs are allocated by pack().
   int make_plan(const int32_t* h_rp, int64_t n_rows, int br, int bc);

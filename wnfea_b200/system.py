@@ -69,10 +69,12 @@ class SolidSystem:
         call("wn_solid_get_map", self._h, ptr(m))
         return m
 
-    def set_streaming(self, enable: bool) -> None:
-        """Streamed fine-level kernels (tile-major packs, the default) on or off; off frees the
-        packs (about 1 GB per million DOFs) and runs the fine level on the register row kernels."""
-        call("wn_solid_set_stream", self._h, int(bool(enable)))
+    def set_streaming(self, enable: bool, batched: bool = False) -> None:
+        """Streamed fine-level kernels (tile-major packs, the default for single-case solves) on or
+        off; off frees the packs (about 1 GB per million DOFs) and runs the fine level on the
+        register row kernels.  ``batched`` streams the fine level of the 32-case solves too (they
+        default to the register kernels)."""
+        call("wn_solid_set_stream", self._h, (2 if batched else 1) if enable else 0)
 
     # -- assembly ---------------------------------------------------------------------------
     def set_fixed(self, fixed_dofs) -> None:
