@@ -86,6 +86,13 @@ int wn_bsr3_pattern_host(int64_t n_nodes, int64_t n_el, const int32_t* conn, int
 int wn_assembly_plan_host(int64_t n_nodes, int64_t n_el, const int32_t* conn, int64_t* n_tiles, int* ne_max,
                           int64_t* n_el_entries, int32_t* tiles, int32_t* el_ptr, int32_t* el, uint16_t* contrib,
                           uint16_t* perm);
+/* The work split of the tile-owner assembly (host; chunk_ptr n_tiles + 1, n_split n_tiles,
+ * chunks n_chunks; NULL outputs skipped): blocks with more than *chunk_len contributions (the
+ * first n_split[t] of tile t's order) are summed in chunks, chunks[k] = local block |
+ * first contribution << 9 | length << 19 | first chunk of its block << 25; *max_codes is the
+ * most contributions of one tile.  All zero when the mesh takes the element-scratch assembly. */
+int wn_assembly_chunks_host(int64_t n_nodes, int64_t n_el, const int32_t* conn, int* chunk_len, int* max_codes,
+                            int64_t* n_chunks, int32_t* chunk_ptr, uint32_t* chunks, int32_t* n_split);
 /* Dirichlet mask over the 3*n_nodes DOFs (host, 1 = FIXED, NULL = none).  FIXED DOFs get
  * zero rows/columns and diagonal 1 and a zero load (solid_solver.py:95-127). */
 int wn_solid_set_fixed(void* h, const uint8_t* fixed_mask);
@@ -116,6 +123,12 @@ int wn_spmv_solid_device(void* h, int precision, const void* x, void* y, uintptr
  * block a row's cost is the gather of the x rows it touches, not the block values the packs
  * save.  Synchronises. */
 int wn_solid_set_stream(void* h, int enable);
+/* Batched solves (wn_solve_multi*): the FP32 fine-level passes with each row tile's x slice
+ * (the 32 cases of the tile's column nodes) staged in shared memory (enable != 0), or the
+ * register row kernels gathering x through L1/L2 (0, the default: on the 1M-DOF I-beam the
+ * staged passes are slower, 312 vs 270 ms per 32-case batch).  The same arithmetic in the same
+ * order: the row products are bitwise the same.  Synchronises. */
+int wn_solid_set_batch_staging(void* h, int enable);
 /* Status word of the streamed fine-matrix products of wn_spmv_solid_device: WN_OK, or
  * WN_ETIMEOUT when a bounded pipeline wait of a call since the last reset ran out of time (the
  * y of that call is not valid).  Synchronises the device; reset != 0 clears the word. */

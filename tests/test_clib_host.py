@@ -147,3 +147,79 @@ def test_assembly_plan_rebuilds_the_oracle_matrix(which):
     Ko, _, _ = solid.assemble(m.mesh_nodes, conn, solid_element_props(m), apply_bcs=False)
     D = (K - Ko).tocsr()
     assert np.abs(D.data).max(initial=0.0) <= 1e-14 * np.abs(Ko.data).max()
+
+
+def assembly_chunks_host(conn, n_nodes, n_tiles):
+    conn = np.ascontiguousarray(conn, dtype=np.int32)
+    C_len, max_codes, n_chunks = C.c_int(), C.c_int(), C.c_int64()
+    _lib.call("wn_assembly_chunks_host", n_nodes, len(conn), _lib.ptr(conn), C.byref(C_len), C.byref(max_codes),
+              C.byref(n_chunks), None, None, None)
+    chunk_ptr = np.empty(n_tiles + 1, dtype=np.int32)
+    chunks = np.empty(max(n_chunks.value, 1), dtype=np.uint32)
+    n_split = np.empty(n_tiles, dtype=np.int32)
+    _lib.call("wn_assembly_chunks_host", n_nodes, len(conn), _lib.ptr(conn), C.byref(C_len), C.byref(max_codes),
+              C.byref(n_chunks), _lib.ptr(chunk_ptr), _lib.ptr(chunks), _lib.ptr(n_split))
+    return C_len.value, max_codes.value, chunk_ptr, chunks[:n_chunks.value], n_split
+
+
+@pytest.mark.parametrize("which", ["c1", "ibeam-shuffled", "ibeam60"])
+def test_assembly_work_items_cover_every_block(which):
+    """The assembly kernel's work items, replayed on the host with the kernel's own index
+    arithmetic (256 threads, three rounds): every block of a tile is summed exactly once --
+    unsplit blocks by one thread, split blocks (more than chunk_len contributions) as chunks
+    of at most chunk_len consecutive contributions that tile the block's list, cut by its count
+    alone (so blocks (i, j) and (j, i) alike) and combined from the first chunk's thread --
+    the chunk slots stay below 32 and the contribution codes inside max_codes."""
+    if which == "c1":
+        m, _ = generate_c3d10_kuhn_block()
+    elif which == "ibeam60":
+        m, _ = generate_c3d10_ibeam_structured(n_slices=60, length=4.0 * 60 / 315, seed=0)
+    else:
+        m, _ = generate_c3d10_ibeam_structured(n_slices=5, length=4.0 * 5 / 315, seed=2)
+        perm_nodes = np.random.default_rng(3).permutation(len(m.mesh_nodes))
+        inv = np.empty_like(perm_nodes)
+        inv[perm_nodes] = np.arange(len(perm_nodes))
+        m.mesh_nodes = m.mesh_nodes[perm_nodes].copy()
+        m.solid_elements = inv[m.solid_elements].astype(np.int32)
+    conn = np.ascontiguousarray(m.solid_elements, dtype=np.int32)
+    n = len(m.mesh_nodes)
+    tiles, el_ptr, el, contrib, perm, nemax, rp, ci = assembly_plan_host(conn, n)
+    clen, max_codes, chunk_ptr, chunks, n_split = assembly_chunks_host(conn, n, len(tiles))
+    gptr = np.concatenate([[0], np.cumsum(np.bincount(pattern_host(conn, n)[2].ravel(), minlength=len(ci)))])
+    count = np.diff(gptr)
+    assert 1 <= clen <= 63 or clen == 1024
+    T, x = 256, np.arange(256)
+    n_split_blocks = 0
+    for t in range(len(tiles)):
+        b0, b1 = int(tiles[t, 2]), int(tiles[t, 3])
+        nb = b1 - b0
+        c0, NH, H = int(chunk_ptr[t]), int(chunk_ptr[t + 1] - chunk_ptr[t]), int(n_split[t])
+        L = nb - H
+        assert 0 <= H and NH <= 32 and (H == 0) == (NH == 0) and NH >= 2 * H
+        assert gptr[b1] - gptr[b0] <= max_codes
+        loc = perm[b0:b1].astype(np.int64)
+        cnt = count[b0 + loc]
+        assert np.all(cnt[:H] > clen) and np.all(cnt[H:] <= clen)
+        n0 = min(L, T - NH)
+        ranks = [x[NH:][x[NH:] - NH < L] - NH]
+        k1 = n0 + (T - 1 - x)
+        ranks.append(k1[k1 < L])
+        k2 = n0 + T + x[:NH]
+        ranks.append(k2[k2 < L])
+        assert np.array_equal(np.sort(np.concatenate(ranks)), np.arange(L))
+        ch = chunks[c0:c0 + NH].astype(np.int64)
+        cj, off, ln, first = ch & 511, (ch >> 9) & 1023, (ch >> 19) & 63, (ch >> 25) & 1
+        y = 0
+        for i in range(H):
+            j = int(loc[i])
+            c = int(count[b0 + j])
+            nchunk = -(-c // clen)
+            want = [c // nchunk + (1 if mm < c % nchunk else 0) for mm in range(nchunk)]
+            assert first[y] == 1 and np.all(cj[y:y + nchunk] == j) and np.all(first[y + 1:y + nchunk] == 0)
+            assert list(ln[y:y + nchunk]) == want
+            assert list(off[y:y + nchunk]) == list(np.concatenate([[0], np.cumsum(want)[:-1]]))
+            y += nchunk
+            n_split_blocks += 1
+        assert y == NH
+    if which == "ibeam60":
+        assert n_split_blocks > 0 and clen == 6

@@ -4,9 +4,10 @@ builder (setup_on_device = 0, and the host-only wn_amg_setup_host).
 Both builders share the aggregation and the per-aggregate QR (host code); the device builder
 runs the diagonal, the power iterations, the smoothed prolongator, the transpose and the two
 Galerkin products on the GPU with the host builder's summation order.  Checked per level: the
-prolongator and restriction patterns identical and R = P^T exactly, the values of P, R and the
-coarse operators A_l against the host builder's, rho, 1/diag and the coarsest inverse; A_c
-against scipy's R (A P); and a solve with each hierarchy (same iteration count).
+values of P, R and the coarse operators A_l against the host builder's (patterns equal up to
+blocks whose terms cancel to an exact zero in one rounding and not the other), R = P^T
+exactly, rho, 1/diag and the coarsest inverse; A_c against scipy's R (A P); and a solve with
+each hierarchy (iteration counts within rounding noise).
 """
 
 from __future__ import annotations
@@ -45,14 +46,18 @@ def test_device_setup_matches_host_builder(which):
         assert lh.bs == ld.bs and lh.n_nodes == ld.n_nodes
         assert abs(lh.rho - ld.rho) <= 1e-12 * lh.rho
         np.testing.assert_allclose(ld.dinv, lh.dinv, rtol=1e-13, atol=0)
+        # Both builders drop all-zero blocks; a block whose terms cancel exactly can come out as
+        # 0 in one summation order and as ~1e-17 in the other, so the patterns may differ by such
+        # blocks: compare through the difference (a block present on one side only counts with
+        # its full size) and bound the count of differing blocks.
         for a, b in ((ld.P, lh.P), (ld.R, lh.R)):
-            assert np.array_equal(a.indptr, b.indptr) and np.array_equal(a.indices, b.indices)
             assert _close(a, b, 1e-12)
+            assert abs(a.nnz - b.nnz) <= 0.01 * b.nnz
         # R = P^T exactly (blocks transposed)
         assert abs(sp.csr_matrix(ld.R) - sp.csr_matrix(ld.P).T).max() == 0.0
         if lh.A is not None:
-            assert np.array_equal(ld.A.indptr, lh.A.indptr) and np.array_equal(ld.A.indices, lh.A.indices)
             assert _close(ld.A, lh.A, 1e-12)
+            assert abs(ld.A.nnz - lh.A.nnz) <= 0.01 * lh.A.nnz
     # the Galerkin product of level 0 against scipy, and the coarsest inverse
     A0 = K.to_bsr().tocsr()
     P0, R0 = sp.csr_matrix(Hd.levels[0].P), sp.csr_matrix(Hd.levels[0].R)

@@ -83,6 +83,28 @@ def test_assembly_is_bit_reproducible():
     assert np.array_equal(v1, s.values())
 
 
+@pytest.mark.parametrize("which", ["c1", "ibeam20"])
+def test_assembled_matrix_is_exactly_symmetric(which):
+    """K == K^T bit for bit, with and without the Dirichlet rows / columns: blocks (i, j) and
+    (j, i) sum transposed terms in the same order, diagonal blocks are symmetric, and the split
+    blocks (the vertex nodes' diagonal blocks, summed in chunks by several threads) are cut and
+    combined alike; the graded modulus makes every element's lam, mu differ."""
+    m = generate_c3d10_kuhn_block()[0] if which == "c1" else generate_c3d10_ibeam_structured(
+        n_slices=20, length=4.0 * 20 / 315, seed=5)[0]
+    props = solid_element_props(m)
+    props[:, 0] *= np.exp(np.random.default_rng(1).uniform(-1, 1, len(props)))
+    s = SolidSystem(m.mesh_nodes, m.solid_elements)
+    s.set_fixed(solid_fixed_dofs(m))
+    for bcs in (False, True):
+        s.assemble(props, apply_bcs=bcs)
+        rp, ci = s.pattern()
+        K = solid.bsr3_to_csr(rp, ci, s.values())
+        assert abs(K - K.T).max() == 0.0, bcs
+        ovals = solid.bsr3_from_csr(solid.assemble(m.mesh_nodes, m.solid_elements, props, apply_bcs=False)[0], rp, ci)
+        if not bcs:
+            np.testing.assert_allclose(s.values(), ovals, rtol=0, atol=1e-14 * np.abs(ovals).max())
+
+
 def test_jittered_ibeam_assembly_matches_oracle():
     m, _ = generate_c3d10_ibeam_structured(n_slices=12, length=4.0 * 12 / 315, seed=3)
     props = solid_element_props(m)

@@ -113,11 +113,13 @@ def test_ibeam_mixed_batch_matches_fp64():
 
 
 def test_streamed_fine_level_matches_register_kernels():
-    """The batched fine level streamed from the tile-major pack (streaming mode 2) and the
-    register row kernels (the default, mode 1; and with streaming off, mode 0): the same per-case
-    arithmetic in the same order, so the row products agree bit for bit and the solves differ
-    only by the order in which the per-CTA dot partials are summed.  Switching modes between
-    solves re-captures the batched solver's graphs (the packs are freed and rebuilt)."""
+    """The batched fine level on its three paths: the register row kernels (the default), x
+    staged per row tile in shared memory (staging on) and streamed from the tile-major pack
+    (streaming mode 2).  Each runs the same per-case arithmetic in the same order, so the row
+    products agree bit for bit and the solves differ only by the order in which the per-CTA dot
+    partials are summed.  Switching paths between solves re-captures the batched solver's
+    graphs (streaming off frees the packs, mode 2 rebuilds them), and returning to the default
+    reproduces its first result exactly."""
     from wnfea_b200 import _lib
 
     m = _ibeam(20, seed=8)
@@ -128,17 +130,20 @@ def test_streamed_fine_level_matches_register_kernels():
     F[np.asarray(solid_fixed_dofs(m), dtype=np.int64), :] = 0.0
     for precision in (0, 1):
         U1, st1 = s.solve_multi(F, rtol=1e-9, precision=precision)
-        _lib.call("wn_solid_set_stream", s.handle, 2)
         try:
+            _lib.call("wn_solid_set_stream", s.handle, 2)
             U2, st2 = s.solve_multi(F, rtol=1e-9, precision=precision)
             _lib.call("wn_solid_set_stream", s.handle, 0)
             U0, st0 = s.solve_multi(F, rtol=1e-9, precision=precision)
+            _lib.call("wn_solid_set_batch_staging", s.handle, 1)
+            Ur, str_ = s.solve_multi(F, rtol=1e-9, precision=precision)
         finally:
+            _lib.call("wn_solid_set_batch_staging", s.handle, 0)
             _lib.call("wn_solid_set_stream", s.handle, 1)
         U1b, st1b = s.solve_multi(F, rtol=1e-9, precision=precision)
-        for st in (st0, st1, st2, st1b):
+        for st in (st0, st1, st2, str_, st1b):
             assert st["status"] == 0
         assert np.array_equal(U1, U1b)
-        for U, st in ((U2, st2), (U0, st0)):
+        for U, st in ((U2, st2), (U0, st0), (Ur, str_)):
             assert np.abs(st["case_iterations"] - st1["case_iterations"]).max() <= 1
             assert np.linalg.norm(U - U1) <= 1e-9 * np.linalg.norm(U1)

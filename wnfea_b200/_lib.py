@@ -93,8 +93,10 @@ SIGNATURES: dict[str, tuple] = {
     "wn_solid_device_arrays": (_I, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
     "wn_spmv_solid_device": (_I, [_P, _I, _P, _P, _U]),
     "wn_solid_set_stream": (_I, [_P, _I]),
+    "wn_solid_set_batch_staging": (_I, [_P, _I]),
     "wn_solid_stream_status": (_I, [_P, _I, _PI]),
     "wn_assembly_plan_host": (_I, [_I64, _I64, _P, C.POINTER(_I64), _PI, C.POINTER(_I64), _P, _P, _P, _P, _P]),
+    "wn_assembly_chunks_host": (_I, [_I64, _I64, _P, _PI, _PI, C.POINTER(_I64), _P, _P, _P]),
     "wn_solid_stream_test_hook": (_I, [_P, _I64, _I]),
     "wn_stream_tiles_host": (_I, [_I64, _P, _P, _I64, C.POINTER(_I64)]),
     "wn_spmv_bsr_f64_device": (_I, [_I, _I, _I64, _P, _P, _P, _P, _P, _D, _D, _U]),

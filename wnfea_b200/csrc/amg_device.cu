@@ -120,13 +120,17 @@ __global__ void ks_divide(int64_t n, double* __restrict__ v, double d) {
     v[i] /= d;
 }
 
+// Frobenius norm of every block, bitwise the host builder's block_fro (the same explicit fused
+// multiply-adds in the same order): the aggregation compares these norms, and on regular meshes
+// many neighbours' blocks have equal norms, so a last-bit difference would break those ties
+// differently and change the aggregates
 __global__ void ks_block_norms(DMat A, double* __restrict__ nrm) {
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < A.nnzb; k += (int64_t)gridDim.x * blockDim.x) {
     double s = 0.0;
     for (int r = 0; r < A.br; ++r)
       for (int c = 0; c < A.bc; ++c) {
         const double b = A.at(k, r, c);
-        s += b * b;
+        s = fma(b, b, s);
       }
     nrm[k] = sqrt(s);
   }

@@ -171,9 +171,11 @@ double power_rho(const View& A, const std::vector<double>& dinv, int iters) {
   return lam;
 }
 
+// explicit fused multiply-adds (whatever the compiler's contraction setting), bitwise the device
+// builder's ks_block_norms: the aggregation breaks ties between equal norms by order
 double block_fro(const double* b, int n) {
   double s = 0.0;
-  for (int k = 0; k < n; ++k) s += b[k] * b[k];
+  for (int k = 0; k < n; ++k) s = std::fma(b[k], b[k], s);
   return std::sqrt(s);
 }
 

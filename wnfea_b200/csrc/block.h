@@ -74,6 +74,12 @@ struct BlockWork {
   DArray<float> cb32, cx32;
   DArray<double> cb64, cx64;
   uint64_t hierarchy_id = 0;        // the AmgHierarchy the level vectors were sized for
+  // x-tiles of the fine level (block_solver.cu build_x_tiles): runs of rows whose blocks name at
+  // most 256 columns; per tile its sorted columns, per block its column's index among them
+  DArray<int32_t> xt_rows, xt_col_ptr, xt_cols;
+  DArray<uint8_t> xt_lcol;
+  int xt_n = 0;         // tiles (0: no plan)
+  bool xt_tried = false;
   GraphCache graphs[2][3];          // [V-cycle precision 0 fp64 / 1 fp32][preconditioner]
   int64_t launches = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;

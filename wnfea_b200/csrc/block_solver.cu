@@ -837,6 +837,230 @@ int launch_bs(K kern, const StreamMat& m, cudaStream_t st, Args... args) {
   return g;
 }
 
+// ---------------------------------------------------------------------------------------
+// fine level with each tile's x slice staged in shared memory (the default for the batched
+// fine level).  An x-tile is a run of whole block rows whose blocks name at most kXTileCols
+// distinct column nodes (the plan in BlockWork: per tile the sorted column list, per block its
+// column as an 8-bit index into that list).  The CTA first writes the x values of the tile's
+// columns -- xf(i, l) for the 32 cases of each of their DOFs, the same functor and arithmetic
+// as the register kernels' gathers -- into shared memory with coalesced 16-byte loads, many in
+// flight at once; then 8-lane groups run the rows exactly as batch_row_staged does (stages of 8
+// blocks, values component-major and coalesced, broadcast by shuffles; the same order of every
+// multiply-add, so the same bits) but read each block's x from shared memory by its local
+// column.  A gathered x row served 2-3 blocks of the tile from L1/L2 before (the tiles' column
+// lists hold 2.8 M rows against 8.5 M blocks on the I-beam), and the gathers' latency was what
+// bound the batched sweeps.
+// ---------------------------------------------------------------------------------------
+constexpr int kXTileCols = 256;  // columns per x-tile: the 8-bit local column index
+struct XTiles {
+  const int32_t* rows;     // n_tiles + 1 block-row starts
+  const int32_t* col_ptr;  // n_tiles + 1
+  const int32_t* cols;     // per tile its distinct column nodes, ascending
+  const uint8_t* lcol;     // nnzb: the block's column as an index into its tile's list
+  int n_tiles;
+};
+
+// How an x functor's slice is staged: the functor's source rows are copied as they are
+// (cp.async, 16 bytes per lane, no register round trip) and the functor's arithmetic, if any,
+// is applied when a value is read -- the same expression on the same operands, so the same bits.
+template <typename XF>
+struct XStage;
+template <>
+struct XStage<BLoad<float, float>> {
+  static constexpr bool kDinv = false;
+  static __device__ __forceinline__ const float* src(const BLoad<float, float>& f) { return f.x; }
+  static __device__ __forceinline__ const float* dinv(const BLoad<float, float>&) { return nullptr; }
+  static __device__ __forceinline__ float scale(const BLoad<float, float>&) { return 1.0f; }
+};
+template <>
+struct XStage<BD0<float, float>> {  // dinv_i b_i / theta
+  static constexpr bool kDinv = true;
+  static __device__ __forceinline__ const float* src(const BD0<float, float>& f) { return f.b; }
+  static __device__ __forceinline__ const float* dinv(const BD0<float, float>& f) { return f.dinv; }
+  static __device__ __forceinline__ float scale(const BD0<float, float>& f) { return f.inv_theta; }
+};
+
+template <bool kDinv>
+struct XsLoad {  // x of local DOF u (local column * 3 + component) from the staged slice
+  const float* xs;
+  const float* sd;  // staged dinv (BD0)
+  float it;
+  __device__ __forceinline__ C4<float> operator()(int64_t u, int l) const {
+    C4<float> v = ldc<float>(xs + u * kBatch, l);
+    if constexpr (kDinv) {
+      const float di = sd[u];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) v.v[k] = di * v.v[k] * it;  // BD0's expression
+    }
+    return v;
+  }
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// batch_row_staged for the 3x3 component-major fine matrix with 8-bit local columns
+template <typename T, typename XL, typename FA>
+__device__ __forceinline__ void batch_row_xs(const int32_t* __restrict__ rp, const uint8_t* __restrict__ lcol,
+                                             const T* __restrict__ av, int64_t stride, int64_t row, bool active,
+                                             int l, const XL& xload, const FA& fmacc) {
+  constexpr unsigned kFull = 0xffffffffu;
+  constexpr int TPG = Tpg<T>::value;
+  using XV = decltype(xload(int64_t(0), 0));
+  const int gbase = threadIdx.x & 24;
+  int32_t q0 = 0, q1 = 0;
+  if (active) {
+    q0 = __ldg(rp + row);
+    q1 = __ldg(rp + row + 1);
+  }
+  const int nst = (q1 - q0 + 7) >> 3;
+  const int wst = __reduce_max_sync(kFull, nst);
+  for (int it = 0; it < wst; ++it) {
+    const int32_t qb = q0 + it * 8;
+    const int cnt = q1 - qb;
+    const int32_t q = qb + l;
+    const int mcol = (l < cnt) ? (int)__ldg(lcol + q) : 0;
+    T mv[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) mv[e] = (l < cnt) ? __ldg(av + (int64_t)e * stride + q) : T(0);
+#pragma unroll
+    for (int g = 0; g < 8; g += TPG) {
+      XV xv[TPG][3];
+#pragma unroll
+      for (int u = 0; u < TPG; ++u) {
+        const int col = __shfl_sync(kFull, mcol, gbase | (g + u));
+#pragma unroll
+        for (int c = 0; c < 3; ++c) xv[u][c] = xload((int64_t)col * 3 + c, l);
+      }
+#pragma unroll
+      for (int u = 0; u < TPG; ++u) {
+        const int t = g + u;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) fmacc(r, __shfl_sync(kFull, mv[r * 3 + c], gbase | t), xv[u][c]);
+      }
+    }
+  }
+}
+
+template <typename XF, typename EPI>
+__global__ void __launch_bounds__(kThreads, 2) kbx_rows(XTiles xt, const int32_t* __restrict__ rp,
+                                                        const float* __restrict__ av, int64_t stride, XF xf, EPI epi,
+                                                        double* __restrict__ part, const int* __restrict__ done) {
+  if (*done) return;
+  using XS = XStage<XF>;
+  extern __shared__ __align__(16) unsigned char xsm[];
+  float* xs = reinterpret_cast<float*>(xsm);  // kXTileCols x 3 DOFs x 32 cases
+  __shared__ int32_t s_cols[kXTileCols];
+  __shared__ float s_dinv[XS::kDinv ? kXTileCols * 3 : 1];
+  const int warp = threadIdx.x >> 5, grp = (threadIdx.x & 31) >> 3, l = threadIdx.x & 7;
+  const float* src = XS::src(xf);
+  double dot[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int t = blockIdx.x; t < xt.n_tiles; t += gridDim.x) {
+    const int c0 = xt.col_ptr[t], nc = xt.col_ptr[t + 1] - c0;
+    for (int k = threadIdx.x; k < nc; k += kThreads) s_cols[k] = xt.cols[c0 + k];
+    __syncthreads();
+    // the slice: 8 chunks of 16 bytes per DOF row (32 cases), all copies in flight at once
+    for (int idx = threadIdx.x; idx < nc * 24; idx += kThreads) {
+      const int u = idx >> 3, ch = idx & 7;
+      const int64_t dof = (int64_t)s_cols[u / 3] * 3 + u % 3;
+      cp_async16(xs + u * kBatch + ch * 4, src + dof * kBatch + ch * 4);
+    }
+    if constexpr (XS::kDinv)
+      for (int u = threadIdx.x; u < nc * 3; u += kThreads) s_dinv[u] = XS::dinv(xf)[(int64_t)s_cols[u / 3] * 3 + u % 3];
+    cp_async_wait_all();
+    __syncthreads();
+    const int r0 = xt.rows[t], r1 = xt.rows[t + 1];
+    for (int base = r0 + warp * 4; base < r1; base += (kThreads >> 5) * 4) {  // warp-uniform bound
+      const int row = base + grp;
+      float acc[3][4];
+      batch_row_xs<float>(rp, xt.lcol, av, stride, row, row < r1, l, XsLoad<XS::kDinv>{xs, s_dinv, XS::scale(xf)},
+                          FmaAcc<3, float>(acc));
+      if (row >= r1) continue;
+#pragma unroll
+      for (int r = 0; r < 3; ++r) epi.store((int64_t)row * 3 + r, l, epi.load((int64_t)row * 3 + r, l), acc[r], dot);
+    }
+    __syncthreads();  // the slice is rewritten for the next tile
+  }
+  if (part) write_case_parts<float>(dot, part);
+}
+
+// host plan of the x-tiles: greedy runs of whole rows with at most kXTileCols distinct columns
+int build_x_tiles(Solid* s, BlockWork& W) {
+  W.xt_tried = true;
+  const int64_t n = s->n_nodes;
+  const std::vector<int32_t>& rp = s->h_row_ptr;
+  const std::vector<int32_t>& ci = s->h_col_idx;
+  if (s->bs != 3 || (int64_t)rp.size() != n + 1 || (int64_t)ci.size() != s->nnzb) return 0;
+  std::vector<int32_t> rows{0}, col_ptr{0}, cols;
+  std::vector<uint8_t> lcol(s->nnzb);
+  std::vector<int32_t> stamp(n, -1), local(n, 0);
+  std::vector<int32_t> cur;
+  int tile = 0;
+  for (int64_t r = 0; r < n;) {
+    cur.clear();
+    const int64_t r0 = r;
+    while (r < n) {
+      int add = 0;  // columns of row r new to the tile (a row names each column once)
+      for (int32_t q = rp[r]; q < rp[r + 1]; ++q) add += stamp[ci[q]] != tile;
+      if ((int)cur.size() + add > kXTileCols) break;
+      for (int32_t q = rp[r]; q < rp[r + 1]; ++q)
+        if (stamp[ci[q]] != tile) {
+          stamp[ci[q]] = tile;
+          cur.push_back(ci[q]);
+        }
+      ++r;
+    }
+    if (r == r0) return 0;  // one row names more than kXTileCols columns: no plan
+    std::sort(cur.begin(), cur.end());
+    for (size_t k = 0; k < cur.size(); ++k) local[cur[k]] = (int32_t)k;
+    for (int32_t q = rp[r0]; q < rp[r]; ++q) lcol[q] = (uint8_t)local[ci[q]];
+    cols.insert(cols.end(), cur.begin(), cur.end());
+    rows.push_back((int32_t)r);
+    col_ptr.push_back((int32_t)cols.size());
+    ++tile;
+  }
+  WN_CHECK(W.xt_rows.upload(rows));
+  WN_CHECK(W.xt_col_ptr.upload(col_ptr));
+  WN_CHECK(W.xt_cols.upload(cols));
+  WN_CHECK(W.xt_lcol.upload(lcol));
+  W.xt_n = tile;
+  return 0;
+}
+
+// launch a staged-x fine-level kernel (persistent grid); the grid, 0 if no plan, no fit or not
+// an FP32 pass with a stageable x functor (an FP64 slice, 192 KB, would leave one CTA per SM)
+template <typename XF>
+struct Stageable : std::false_type {};
+template <>
+struct Stageable<BLoad<float, float>> : std::true_type {};
+template <>
+struct Stageable<BD0<float, float>> : std::true_type {};
+
+template <typename T, typename XF, typename EPI>
+int launch_bx(Solid* s, BlockWork& W, const T* av, XF xf, EPI epi, double* part, const int* done, cudaStream_t st) {
+  if constexpr (!std::is_same<T, float>::value || !Stageable<XF>::value) {
+    return 0;
+  } else {
+    if (!s->batch_stage_x || W.xt_n == 0) return 0;
+    const size_t smem = (size_t)kXTileCols * 3 * kBatch * sizeof(float);
+    auto kern = kbx_rows<XF, EPI>;
+    const int per_sm = stream_ctas_per_sm(reinterpret_cast<const void*>(kern), kThreads, smem);
+    if (per_sm < 1) return 0;
+    const int g = std::max(1, std::min(W.xt_n, std::min(kNumSMs * per_sm, BlockWork::kMaxParts)));
+    kern<<<g, kThreads, smem, st>>>(XTiles{W.xt_rows.p, W.xt_col_ptr.p, W.xt_cols.p, W.xt_lcol.p, W.xt_n},
+                                    s->row_ptr.p, av, s->nnzb, xf, epi, part, done);
+    if (cudaGetLastError() != cudaSuccess) return 0;
+    return g;
+  }
+}
+
 // y = A x or y += A x for the block-contiguous transfer operators (BR x BC blocks)
 template <int BR, int BC, typename T, int S>
 __global__ void __launch_bounds__(kThreads) kb_level_spmv(int64_t n_rows, const int32_t* __restrict__ rp,
@@ -1365,10 +1589,16 @@ int batch_vcycle(Solid* s, AmgHierarchy& H, BlockWork& W, int lvl, const T* b, T
     // the fine level streams its matrix from the tile-major pack when it has one
     const bool fine_stream = lvl == 0 && BS == 3 && s->fine.packed && s->stream_batched;
     const BView fv = bview<T>(s->fine);
+    // the fine level: streamed from the pack when batched streaming is on, else with each
+    // tile's x slice staged in shared memory (when the plan exists), else the register kernels
     auto streamed = [&](auto xf, auto epi, double* part_out) -> int {
-      return launch_bs<T>(kbs_rows<T, decltype(xf), decltype(epi)>, s->fine, st, fv, xf, epi, part_out, S);
+      int g = fine_stream ? launch_bs<T>(kbs_rows<T, decltype(xf), decltype(epi)>, s->fine, st, fv, xf, epi,
+                                         part_out, S)
+                          : 0;
+      if (g == 0 && lvl == 0 && BS == 3) g = launch_bx<T>(s, W, av, xf, epi, part_out, done, st);
+      return g;
     };
-    if (!(fine_stream && streamed(BD0<T, T>{b, dinv, it},
+    if (!(streamed(BD0<T, T>{b, dinv, it},
                                   BEpiPreFirst<T>{b, dinv, it, deg, c1, c2, V.x.p, V.r.p, V.d.p, V.res.p}, nullptr)))
       kb_pre_first<BS, T, SG><<<rg(kb_pre_first<BS, T, SG>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, deg, c1,
                                                                         c2, V.x.p, V.r.p, V.d.p, V.res.p, done);
@@ -1377,15 +1607,14 @@ int batch_vcycle(Solid* s, AmgHierarchy& H, BlockWork& W, int lvl, const T* b, T
     T* dout = V.d2.p;
     for (int k = 2; k < deg; ++k) {
       const T ck1 = (T)L.c1[k - 1], ck2 = (T)L.c2[k - 1];
-      if (!(fine_stream &&
-            streamed(BLoad<T, T>{din}, BEpiCheb<T>{dinv, din, dout, V.r.p, V.x.p, ck1, ck2, b, 0}, nullptr)))
+      if (!streamed(BLoad<T, T>{din}, BEpiCheb<T>{dinv, din, dout, V.r.p, V.x.p, ck1, ck2, b, 0}, nullptr))
         kb_cheb_step<BS, T, SG><<<rg(kb_cheb_step<BS, T, SG>), kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout,
                                                                           V.r.p, V.x.p, ck1, ck2, b, nullptr, done);
       W.launches++;
       std::swap(din, dout);
     }
     if (deg >= 2) {
-      if (!(fine_stream && streamed(BLoad<T, T>{V.x.p}, BEpiResidual<T>{b, V.res.p}, nullptr)))
+      if (!streamed(BLoad<T, T>{V.x.p}, BEpiResidual<T>{b, V.res.p}, nullptr))
         kb_residual<BS, T, SG><<<rg(kb_residual<BS, T, SG>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, V.x.p, V.res.p,
                                                                          done);
       W.launches++;
@@ -1399,10 +1628,8 @@ int batch_vcycle(Solid* s, AmgHierarchy& H, BlockWork& W, int lvl, const T* b, T
     batch_level_spmv<BS, 6, T>(L.P, BPrec<T>::Pv(L), xc, V.x.p, 1, done, st);
     W.launches++;
     double* part_last = (deg == 1) ? part : nullptr;
-    int gpf = fine_stream ? streamed(BLoad<T, T>{V.x.p},
-                                     BEpiPostFirst<T>{b, dinv, it, V.x.p, out, V.r.p, V.d.p, part_last != nullptr},
-                                     part_last)
-                          : 0;
+    int gpf = streamed(BLoad<T, T>{V.x.p},
+                       BEpiPostFirst<T>{b, dinv, it, V.x.p, out, V.r.p, V.d.p, part_last != nullptr}, part_last);
     if (gpf == 0) {
       gpf = rg(kb_post_first<BS, T, SG>);
       kb_post_first<BS, T, SG><<<gpf, kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, V.x.p, out, V.r.p, V.d.p,
@@ -1415,10 +1642,8 @@ int batch_vcycle(Solid* s, AmgHierarchy& H, BlockWork& W, int lvl, const T* b, T
     for (int k = 1; k < deg; ++k) {
       double* pk = (k == deg - 1) ? part : nullptr;
       const T ck1 = (T)L.c1[k - 1], ck2 = (T)L.c2[k - 1];
-      int gcs = fine_stream ? streamed(BLoad<T, T>{din}, BEpiCheb<T>{dinv, din, dout, V.r.p, out, ck1, ck2, b,
-                                                                     pk != nullptr},
-                                       pk)
-                            : 0;
+      int gcs = streamed(BLoad<T, T>{din}, BEpiCheb<T>{dinv, din, dout, V.r.p, out, ck1, ck2, b, pk != nullptr},
+                         pk);
       if (gcs == 0) {
         gcs = rg(kb_cheb_step<BS, T, SG>);
         kb_cheb_step<BS, T, SG><<<gcs, kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout, V.r.p, out, ck1, ck2, b,
@@ -1469,6 +1694,7 @@ int batch_iteration(Solid* s, BlockWork& W, int precond, int k, BlockScalars* S,
                                                   (const TM*)BPrec<TM>::z(W), (const double*)p_old, p_new, W.q.p,
                                                   W.partB.p, S)
                               : 0;
+
   if (gsd == 0) {
     gsd = resident_grid(kb_spmv_dot<TM>, kThreads, rows_work(s->n_nodes));
     kb_spmv_dot<TM><<<gsd, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, s->nnzb,
@@ -1606,6 +1832,7 @@ int ensure_block_work(Solid* s, int vmode, int precond) {
     WN_CUDA(cudaEventCreate(&W.ev0));
     WN_CUDA(cudaEventCreate(&W.ev1));
   }
+  if (!W.xt_tried) WN_CHECK(build_x_tiles(s, W));
   return 0;
 }
 

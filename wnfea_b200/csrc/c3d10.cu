@@ -14,6 +14,7 @@
 #include "c3d10.cuh"
 #include "common.cuh"
 #include "kernels.h"
+#include "pattern.h"
 #include "wnfea_cuda.h"
 
 namespace wn {
@@ -167,128 +168,250 @@ __global__ void gather_assemble_kernel(int64_t nnzb, const int32_t* __restrict__
 // ---------------------------------------------------------------------------------------
 // Tile-owner assembly (no per-element scratch in global memory).  One CTA per row tile of
 // the fine matrix (the tiles of its tile-major packs):
+//   phase 0: the tile's contribution codes into shared memory, and each thread's three work
+//            items (below) from the plan, loads in flight during phase 1;
 //   phase 1: for every element incident to the tile's rows (the plan's list) and every
-//            Gauss point, the Cartesian derivatives dN/dx (3 x 10) and w|J| lambda, w|J| mu
-//            into shared memory (element stride kAsmElStride doubles: an odd number of 8-byte
-//            words, so lanes reading different elements hit different banks);
-//   phase 2: one thread per block of the tile, in the plan's order of descending contribution
-//            count (lanes of a warp carry blocks of similar cost), sums the block's
-//            contributions in element order (the gather order), each computed from shared
-//            memory as K_pq = sum_g w (lam v_p v_q^T + mu v_q v_p^T + mu (v_p . v_q) I) with
-//            p = min(a, b), q = max(a, b) and transposed when a > b -- so blocks (i, j) and
-//            (j, i) add bitwise-transposed terms in the same order and K is exactly
-//            symmetric -- applies the Dirichlet rows / columns and writes the FP64 and FP32
+//            Gauss point, the Cartesian derivatives dN/dx (3 x 10) and w|J| into shared memory,
+//            lam and mu beside them.  A warp takes one Gauss point for 32 elements, so the
+//            natural derivatives are compile-time constants (gp_cartesian_rel) and the 32
+//            lanes store to 32 distinct banks (element stride kAsmElStride: odd in 8-byte words);
+//   phase 2: with v = dN/dx at a Gauss point, an element's block is
+//            K_ab = lam S + mu S^T + mu tr(S) I for S = sum_g w v_a v_b^T (the isotropic
+//            B^T C B of c3d10.py:244-246 summed over the Gauss points); a work item sums
+//            A = sum_e lam_e S_e and B = sum_e mu_e S_e over a run of the block's contributions
+//            in element order (the gather order), and the block is K = A + B^T + tr(B) I.  S is
+//            computed for (p, r) = (min, max) of the element's local node pair and transposed
+//            when a > b, and S_pp is mirrored from its upper triangle, so blocks (i, j) and
+//            (j, i) add bitwise-transposed terms in the same order, diagonal blocks come out
+//            symmetric and K is exactly symmetric.
+//            Work items, in three rounds of one item per thread: round 0 gives the chunks of
+//            the tile's split blocks (more than the plan's chunk_len contributions: the
+//            diagonal blocks of vertex nodes) to threads 0 .. NH-1, which leave their A and B in
+//            chunk slots, and the heaviest other blocks to the rest; round 1 the next 256
+//            blocks in reverse thread order (a thread with a heavy block in round 0 gets a light
+//            one now); round 2 the remainder to threads 0 .. NH-1.  A thread holds at most two
+//            finished blocks.  The chunk sums of a split block are then added in chunk order;
+//            blocks are cut by their contribution count alone, so (i, j) and (j, i) alike.
+//            Then the Dirichlet rows / columns;
+//   phase 3: the tile's blocks staged in shared memory and written coalesced: FP64 and FP32
 //            component-major values and, when given, the FP64 / FP32 pack segments of the tile.
 // ---------------------------------------------------------------------------------------
 constexpr int kAsmThreads = 256;
-constexpr int kAsmGpStride = 32;                  // 30 derivatives + w lam + w mu
-constexpr int kAsmElStride = 4 * kAsmGpStride + 1;  // 129 doubles per element
+constexpr int kAsmGpStride = 31;                  // 30 derivatives + w|J|
+constexpr int kAsmElStride = 4 * kAsmGpStride + 1;  // 125 doubles per element (odd)
 
-__global__ void __launch_bounds__(kAsmThreads, 2) assemble_tiles_kernel(
-    const AsmTileArgs A, const double* __restrict__ nodes, const int32_t* __restrict__ conn,
-    const double* __restrict__ props, const uint8_t* __restrict__ fixed, int64_t nnzb, double* __restrict__ k64,
-    float* __restrict__ k32, int* __restrict__ flags) {
-  extern __shared__ double s_el[];
-  const int t = blockIdx.x;
-  const int4 T = reinterpret_cast<const int4*>(A.tiles)[t];  // r0, r1, b0, b1
-  const int e_beg = A.el_ptr[t], ne = A.el_ptr[t + 1] - e_beg;
-  for (int item = threadIdx.x; item < ne * 4; item += kAsmThreads) {
-    const int k = item >> 2, g = item & 3;
-    const int64_t e = A.el[e_beg + k];
-    double X[10][3];
-    load_coords(nodes, conn, e, X);
-    double dndx[3][10];
-    const double det = gp_cartesian(g, X, dndx);
-    if (!(det > 0.0)) atomicOr(flags, 1);
-    double lam, mu;
-    lame(props[e * 2], props[e * 2 + 1], lam, mu);
-    double* d = s_el + k * kAsmElStride + g * kAsmGpStride;
+// shared-memory layout (doubles): [0, el_area) element data, later the staged blocks;
+// [el_area, el_area + 18 kAsmChunkSlots) chunk sums; then the tile's contribution codes
+__host__ __device__ constexpr int64_t asm_el_area(int ne_max) {
+  return (int64_t)ne_max * (kAsmElStride + 2) > (int64_t)WN_STREAM_TILE_BLOCKS * 9
+             ? (int64_t)ne_max * (kAsmElStride + 2)
+             : (int64_t)WN_STREAM_TILE_BLOCKS * 9;
+}
+
+struct AsmItem {
+  int j = -1;      // local block, -1: none
+  int qa = 0, qb = 0;  // contributions [qa, qb) (global indices)
+};
+
+// A and B of a work item: sum over contributions q in [qa, qb) of lam S and mu S
+__device__ __forceinline__ void asm_item_sums(const double* __restrict__ s_el, const double* __restrict__ s_lm,
+                                              const uint16_t* __restrict__ s_codes, int qbase, int qa, int qb,
+                                              double (&As)[9], double (&Bs)[9]) {
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
+  for (int m = 0; m < 9; ++m) As[m] = Bs[m] = 0.0;
+  for (int q = qa; q < qb; ++q) {
+    const int code = s_codes[q - qbase];
+    const int slot = code >> 8, ea = (code >> 4) & 15, eb = code & 15;
+    const int p = min(ea, eb), r = max(ea, eb);
+    const double* d = s_el + slot * kAsmElStride;
+    double S[9];
 #pragma unroll
-      for (int a = 0; a < 10; ++a) d[i * 10 + a] = dndx[i][a];
-    const double w = kWeight * det;
-    d[30] = w * lam;
-    d[31] = w * mu;
-  }
-  __syncthreads();
-  // phase 2: each thread sums the contributions of up to two blocks (a tile holds at most
-  // 2 kAsmThreads blocks) in registers
-  const int nb = T.w - T.z;
-  double acc[2][9];
-  int jloc[2] = {-1, -1};
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int kk = threadIdx.x + h * kAsmThreads;
-#pragma unroll
-    for (int m = 0; m < 9; ++m) acc[h][m] = 0.0;
-    if (kk >= nb) continue;
-    const int j = A.perm[T.z + kk];  // local block index
-    jloc[h] = j;
-    const int64_t b = T.z + j;
-    const int32_t q0 = A.gptr[b], q1 = A.gptr[b + 1];
-    for (int32_t q = q0; q < q1; ++q) {
-      const int code = A.contrib[q];
-      const int slot = code >> 8, ea = (code >> 4) & 15, eb = code & 15;
-      const int p = min(ea, eb), r = max(ea, eb);
-      double M[9];
-#pragma unroll
-      for (int m = 0; m < 9; ++m) M[m] = 0.0;
-#pragma unroll
-      for (int g = 0; g < 4; ++g) {
-        const double* d = s_el + slot * kAsmElStride + g * kAsmGpStride;
-        const double vp0 = d[p], vp1 = d[10 + p], vp2 = d[20 + p];
-        const double vq0 = d[r], vq1 = d[10 + r], vq2 = d[20 + r];
-        const double wl = d[30], wm = d[31];
-        const double lp0 = wl * vp0, lp1 = wl * vp1, lp2 = wl * vp2;
-        const double mp0 = wm * vp0, mp1 = wm * vp1, mp2 = wm * vp2;
-        const double dg = mp0 * vq0 + mp1 * vq1 + mp2 * vq2;
-        // entry (i, j): lam vp_i vq_j + mu vp_j vq_i (+ mu vp . vq on the diagonal)
-        M[0] += lp0 * vq0 + mp0 * vq0 + dg;
-        M[1] += lp0 * vq1 + mp1 * vq0;
-        M[2] += lp0 * vq2 + mp2 * vq0;
-        M[3] += lp1 * vq0 + mp0 * vq1;
-        M[4] += lp1 * vq1 + mp1 * vq1 + dg;
-        M[5] += lp1 * vq2 + mp2 * vq1;
-        M[6] += lp2 * vq0 + mp0 * vq2;
-        M[7] += lp2 * vq1 + mp1 * vq2;
-        M[8] += lp2 * vq2 + mp2 * vq2 + dg;
-      }
-      if (ea <= eb) {
-#pragma unroll
-        for (int m = 0; m < 9; ++m) acc[h][m] += M[m];
+    for (int g = 0; g < 4; ++g) {
+      const double* dg = d + g * kAsmGpStride;
+      const double w = dg[30];
+      const double wp0 = w * dg[p], wp1 = w * dg[10 + p], wp2 = w * dg[20 + p];
+      const double vr0 = dg[r], vr1 = dg[10 + r], vr2 = dg[20 + r];
+      if (g == 0) {
+        S[0] = wp0 * vr0; S[1] = wp0 * vr1; S[2] = wp0 * vr2;
+        S[3] = wp1 * vr0; S[4] = wp1 * vr1; S[5] = wp1 * vr2;
+        S[6] = wp2 * vr0; S[7] = wp2 * vr1; S[8] = wp2 * vr2;
       } else {
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-          for (int jj = 0; jj < 3; ++jj) acc[h][i * 3 + jj] += M[jj * 3 + i];
+        S[0] = fma(wp0, vr0, S[0]); S[1] = fma(wp0, vr1, S[1]); S[2] = fma(wp0, vr2, S[2]);
+        S[3] = fma(wp1, vr0, S[3]); S[4] = fma(wp1, vr1, S[4]); S[5] = fma(wp1, vr2, S[5]);
+        S[6] = fma(wp2, vr0, S[6]); S[7] = fma(wp2, vr1, S[7]); S[8] = fma(wp2, vr2, S[8]);
       }
     }
-    if (fixed) {
-      const int64_t r0 = (int64_t)A.block_row[b] * 3, c0 = (int64_t)A.col_idx[b] * 3;
+    if (p == r) {  // S_pp symmetric: its lower triangle from the upper
+      S[3] = S[1];
+      S[6] = S[2];
+      S[7] = S[5];
+    }
+    const double lam = s_lm[2 * slot], mu = s_lm[2 * slot + 1];
+    if (ea <= eb) {
+#pragma unroll
+      for (int m = 0; m < 9; ++m) {
+        As[m] = fma(lam, S[m], As[m]);
+        Bs[m] = fma(mu, S[m], Bs[m]);
+      }
+    } else {
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int jj = 0; jj < 3; ++jj)
-          if (fixed[r0 + i] | fixed[c0 + jj]) acc[h][i * 3 + jj] = (r0 + i == c0 + jj) ? 1.0 : 0.0;
+        for (int jj = 0; jj < 3; ++jj) {
+          As[i * 3 + jj] = fma(lam, S[jj * 3 + i], As[i * 3 + jj]);
+          Bs[i * 3 + jj] = fma(mu, S[jj * 3 + i], Bs[i * 3 + jj]);
+        }
+    }
+  }
+}
+
+// K = A + B^T + tr(B) I, then the Dirichlet rows / columns of block b
+__device__ __forceinline__ void asm_finish(const AsmTileArgs& A, const uint8_t* __restrict__ fixed, int64_t b,
+                                           const double (&As)[9], const double (&Bs)[9], double (&out)[9]) {
+  const double trB = Bs[0] + Bs[4] + Bs[8];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int jj = 0; jj < 3; ++jj) out[i * 3 + jj] = As[i * 3 + jj] + Bs[jj * 3 + i] + (i == jj ? trB : 0.0);
+  if (fixed) {
+    const int64_t r0 = (int64_t)A.block_row[b] * 3, c0 = (int64_t)A.col_idx[b] * 3;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int jj = 0; jj < 3; ++jj)
+        if (fixed[r0 + i] | fixed[c0 + jj]) out[i * 3 + jj] = (r0 + i == c0 + jj) ? 1.0 : 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(kAsmThreads, 2) assemble_tiles_kernel(
+    const AsmTileArgs A, int el_area, const double* __restrict__ nodes, const int32_t* __restrict__ conn,
+    const double* __restrict__ props, const uint8_t* __restrict__ fixed, int64_t nnzb, double* __restrict__ k64,
+    float* __restrict__ k32, int* __restrict__ flags) {
+  extern __shared__ double s_el[];
+  double* s_part = s_el + el_area;  // kAsmChunkSlots x (A 9, B 9)
+  uint16_t* s_codes = reinterpret_cast<uint16_t*>(s_part + 18 * kAsmChunkSlots);
+  const int t = blockIdx.x, x = threadIdx.x;
+  const int4 T = reinterpret_cast<const int4*>(A.tiles)[t];  // r0, r1, b0, b1
+  const int e_beg = A.el_ptr[t], ne = A.el_ptr[t + 1] - e_beg;
+  double* s_lm = s_el + ne * kAsmElStride;  // lam, mu per element
+  const int nb = T.w - T.z;
+  // phase 0
+  const int qbase = A.gptr[T.z], ncodes = A.gptr[T.w] - qbase;
+  for (int i = x; i < ncodes; i += kAsmThreads) s_codes[i] = A.contrib[qbase + i];
+  const int c0 = A.chunk_ptr[t], NH = A.chunk_ptr[t + 1] - c0, H = A.n_split[t], L = nb - H;
+  const int n0 = min(L, kAsmThreads - NH);  // light blocks of round 0
+  AsmItem it[3];
+  bool first = false;  // round 0 holds the first chunk of a split block
+  if (x < NH) {
+    const uint32_t c = A.chunks[c0 + x];
+    it[0].j = (int)(c & 511u);
+    it[0].qa = A.gptr[T.z + it[0].j] + (int)((c >> 9) & 1023u);
+    it[0].qb = it[0].qa + (int)((c >> 19) & 63u);
+    first = (c >> 25) & 1u;
+  } else if (x - NH < L) {
+    it[0].j = A.perm[T.z + H + (x - NH)];
+  }
+  {
+    const int k1 = n0 + (kAsmThreads - 1 - x), k2 = n0 + kAsmThreads + x;
+    if (k1 < L) it[1].j = A.perm[T.z + H + k1];
+    if (x < NH && k2 < L) it[2].j = A.perm[T.z + H + k2];
+  }
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+    if (it[r].j >= 0 && !(r == 0 && x < NH)) {
+      it[r].qa = A.gptr[T.z + it[r].j];
+      it[r].qb = A.gptr[T.z + it[r].j + 1];
+    }
+  // phase 1
+  {
+    const int warp = x >> 5, lane = x & 31;
+    const int n_items = ((ne + 31) >> 5) * 4;  // (32-element group, Gauss point)
+    for (int wi = warp; wi < n_items; wi += kAsmThreads / 32) {
+      const int g = wi & 3, k = (wi >> 2) * 32 + lane;
+      if (k >= ne) continue;
+      const int64_t e = A.el[e_beg + k];
+      double Xr[10][3];
+      load_coords(nodes, conn, e, Xr);
+#pragma unroll
+      for (int a = 1; a < 10; ++a)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Xr[a][j] -= Xr[0][j];
+      double dndx[3][10];
+      double det;
+      switch (g) {  // warp-uniform
+        case 0: det = gp_cartesian_rel<0>(Xr, dndx); break;
+        case 1: det = gp_cartesian_rel<1>(Xr, dndx); break;
+        case 2: det = gp_cartesian_rel<2>(Xr, dndx); break;
+        default: det = gp_cartesian_rel<3>(Xr, dndx); break;
+      }
+      if (!(det > 0.0)) atomicOr(flags, 1);
+      double* d = s_el + k * kAsmElStride + g * kAsmGpStride;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int a = 0; a < 10; ++a) d[i * 10 + a] = dndx[i][a];
+      d[30] = kWeight * det;
+      if (g == 0) {
+        double lam, mu;
+        lame(props[e * 2], props[e * 2 + 1], lam, mu);
+        s_lm[2 * k] = lam;
+        s_lm[2 * k + 1] = mu;
+      }
+    }
+  }
+  __syncthreads();
+  // phase 2: rounds 0 and 2 finish into fin[0], round 1 into fin[1] (a thread has a light
+  // block in round 0 or in round 2, not both); split-block chunks leave A and B in slot x
+  double fin[2][9];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    if (it[r].j < 0) continue;
+    double As[9], Bs[9];
+    asm_item_sums(s_el, s_lm, s_codes, qbase, it[r].qa, it[r].qb, As, Bs);
+    if (r == 0 && x < NH) {
+#pragma unroll
+      for (int m = 0; m < 9; ++m) {
+        s_part[x * 18 + m] = As[m];
+        s_part[x * 18 + 9 + m] = Bs[m];
+      }
+    } else {
+      asm_finish(A, fixed, T.z + it[r].j, As, Bs, fin[r == 1 ? 1 : 0]);
     }
   }
   // phase 3: the tile's blocks staged in shared memory in local order (over the element data,
   // which every thread has finished reading), then written coalesced, component by component
   __syncthreads();
   double* stage = s_el;  // nb x 9 (odd stride: consecutive blocks hit different banks)
+  if (first) {  // the chunk sums of this split block, in chunk order
+    double As[9], Bs[9];
 #pragma unroll
-  for (int h = 0; h < 2; ++h)
-    if (jloc[h] >= 0)
+    for (int m = 0; m < 9; ++m) {
+      As[m] = s_part[x * 18 + m];
+      Bs[m] = s_part[x * 18 + 9 + m];
+    }
+    for (int y = x + 1; y < NH && !((A.chunks[c0 + y] >> 25) & 1u); ++y)
 #pragma unroll
-      for (int m = 0; m < 9; ++m) stage[jloc[h] * 9 + m] = acc[h][m];
+      for (int m = 0; m < 9; ++m) {
+        As[m] += s_part[y * 18 + m];
+        Bs[m] += s_part[y * 18 + 9 + m];
+      }
+    double out[9];
+    asm_finish(A, fixed, T.z + it[0].j, As, Bs, out);
+#pragma unroll
+    for (int m = 0; m < 9; ++m) stage[it[0].j * 9 + m] = out[m];
+  }
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+    if (it[r].j >= 0 && !(r == 0 && x < NH))
+#pragma unroll
+      for (int m = 0; m < 9; ++m) stage[it[r].j * 9 + m] = fin[r == 1 ? 1 : 0][m];
   __syncthreads();
   const int4 d64 = A.p64 ? reinterpret_cast<const int4*>(A.d64)[t] : make_int4(0, 0, 0, 0);  // r0, r1, seg, cntp
   const int4 d32 = A.p64 ? reinterpret_cast<const int4*>(A.d32)[t] : make_int4(0, 0, 0, 0);
   double* v64 = A.p64 ? reinterpret_cast<double*>(A.p64 + (size_t)d64.z * 128) : nullptr;
   float* v32 = A.p64 ? reinterpret_cast<float*>(A.p32 + (size_t)d32.z * 128) : nullptr;
   for (int m = 0; m < 9; ++m)
-    for (int j = threadIdx.x; j < nb; j += kAsmThreads) {
+    for (int j = x; j < nb; j += kAsmThreads) {
       const double v = stage[j * 9 + m];
       k64[m * nnzb + T.z + j] = v;
       k32[m * nnzb + T.z + j] = (float)v;
@@ -448,14 +571,20 @@ __global__ void nodal_average_kernel(int64_t n_nodes, const int64_t* __restrict_
 // ---------------------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------------------
-int launch_assemble_tiles(const AsmTileArgs& A, int n_tiles, int ne_max, const double* nodes, const int32_t* conn,
-                          const double* props, const uint8_t* fixed, int64_t nnzb, double* k64, float* k32, int* flags,
-                          cudaStream_t st) {
+size_t assemble_tiles_smem(int ne_max, int max_codes) {
+  return (size_t)(asm_el_area(ne_max) + 18 * kAsmChunkSlots) * sizeof(double) + ((size_t)max_codes * 2 + 7) / 8 * 8;
+}
+
+int launch_assemble_tiles(const AsmTileArgs& A, int n_tiles, int ne_max, int max_codes, const double* nodes,
+                          const int32_t* conn, const double* props, const uint8_t* fixed, int64_t nnzb, double* k64,
+                          float* k32, int* flags, cudaStream_t st) {
   if (n_tiles == 0) return 0;
-  // element data of the tile, then (same space) its finished blocks: at most
-  // WN_STREAM_TILE_BLOCKS x 9 doubles
+  // element data of the tile (derivatives, then lam and mu), later (same space) its finished
+  // blocks, at most WN_STREAM_TILE_BLOCKS x 9 doubles; the chunk sums; the contribution codes
   static_assert(WN_STREAM_TILE_BLOCKS <= 2 * kAsmThreads, "two blocks per thread in the assembly");
-  const size_t smem = std::max((size_t)ne_max * kAsmElStride, (size_t)WN_STREAM_TILE_BLOCKS * 9) * sizeof(double);
+  const int64_t el_area = asm_el_area(ne_max);
+  const size_t smem = assemble_tiles_smem(ne_max, max_codes);
+  WN_REQUIRE(smem <= kAsmSmemLimit, WN_ETOOBIG, "assembly: %zu bytes of shared memory per tile", smem);
   static int configured_bytes[64] = {0};  // per device: the largest dynamic size allowed so far
   int dev = 0;
   WN_CUDA(cudaGetDevice(&dev));
@@ -464,7 +593,8 @@ int launch_assemble_tiles(const AsmTileArgs& A, int n_tiles, int ne_max, const d
     WN_CUDA(cudaFuncSetAttribute(assemble_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     configured_bytes[dev] = (int)smem;
   }
-  assemble_tiles_kernel<<<n_tiles, kAsmThreads, smem, st>>>(A, nodes, conn, props, fixed, nnzb, k64, k32, flags);
+  assemble_tiles_kernel<<<n_tiles, kAsmThreads, smem, st>>>(A, (int)el_area, nodes, conn, props, fixed, nnzb, k64,
+                                                            k32, flags);
   WN_CUDA(cudaGetLastError());
   return 0;
 }

@@ -226,11 +226,12 @@ int wn_solid_create(int64_t n_nodes, int64_t n_el, const double* nodes, const in
   st = st ? st : s->emap.upload(pat.emap);
   st = st ? st : s->gptr.upload(pat.gather_ptr);
   {
-    // tile-owner assembly when every tile's incident elements fit in shared memory (200 of them,
-    // 203 KB); the tiles are those of the streamed fine matrix
+    // tile-owner assembly when every tile's incident elements and contribution codes fit in
+    // shared memory (at most 200 elements); the tiles are those of the streamed fine matrix
     AssemblyPlan plan;
     std::vector<StreamTile> stiles;
     const bool ok = build_assembly_plan(pat, n_el, kStreamCap, kStreamRowCap, 200, plan) == 0 &&
+                    assemble_tiles_smem(plan.ne_max, plan.max_codes) <= kAsmSmemLimit &&
                     build_stream_tiles(pat.row_ptr.data(), n_nodes, stiles) && stiles.size() == plan.tiles.size();
     bool same = ok;
     for (size_t t = 0; same && t < stiles.size(); ++t)
@@ -238,6 +239,7 @@ int wn_solid_create(int64_t n_nodes, int64_t n_el, const double* nodes, const in
     if (same && plan.n_tiles > 0) {
       s->asm_tiles = plan.n_tiles;
       s->asm_ne_max = plan.ne_max;
+      s->asm_max_codes = plan.max_codes;
       std::vector<int32_t> tl(plan.tiles.size() * 4);
       for (size_t t = 0; t < plan.tiles.size(); ++t) {
         tl[4 * t] = plan.tiles[t].r0;
@@ -250,6 +252,9 @@ int wn_solid_create(int64_t n_nodes, int64_t n_el, const double* nodes, const in
       st = st ? st : s->asm_el.upload(plan.el);
       st = st ? st : s->asm_perm.upload(plan.perm);
       st = st ? st : s->asm_contrib.upload(plan.contrib);
+      st = st ? st : s->asm_chunk_ptr.upload(plan.chunk_ptr);
+      st = st ? st : s->asm_n_split.upload(plan.n_split);
+      st = st ? st : s->asm_chunks.upload(plan.chunks);
     } else {
       st = st ? st : s->gsrc.upload(pat.gather_src);
     }
@@ -310,6 +315,30 @@ int wn_assembly_plan_host(int64_t n_nodes, int64_t n_el, const int32_t* conn, in
   if (el) std::copy(plan.el.begin(), plan.el.end(), el);
   if (contrib) std::copy(plan.contrib.begin(), plan.contrib.end(), contrib);
   if (perm) std::copy(plan.perm.begin(), plan.perm.end(), perm);
+  return 0;
+}
+
+int wn_assembly_chunks_host(int64_t n_nodes, int64_t n_el, const int32_t* conn, int* chunk_len, int* max_codes,
+                            int64_t* n_chunks, int32_t* chunk_ptr, uint32_t* chunks, int32_t* n_split) {
+  WN_REQUIRE(chunk_len && max_codes && n_chunks && (conn || n_el == 0) && n_nodes > 0 && n_el >= 0, WN_EINVAL,
+             "wn_assembly_chunks_host: bad argument");
+  Bsr3Pattern pat;
+  int rc = build_bsr3_pattern(n_nodes, n_el, conn, pat);
+  WN_REQUIRE(rc != -3, WN_EMESH, "wn_assembly_chunks_host: element node index out of range");
+  WN_REQUIRE(rc == 0, WN_EINVAL, "wn_assembly_chunks_host: pattern construction failed (%d)", rc);
+  AssemblyPlan plan;
+  if (build_assembly_plan(pat, n_el, kStreamCap, kStreamRowCap, 200, plan) != 0) {
+    *chunk_len = 0;
+    *max_codes = 0;
+    *n_chunks = 0;
+    return 0;
+  }
+  *chunk_len = plan.chunk_len;
+  *max_codes = plan.max_codes;
+  *n_chunks = (int64_t)plan.chunks.size();
+  if (chunk_ptr) std::copy(plan.chunk_ptr.begin(), plan.chunk_ptr.end(), chunk_ptr);
+  if (chunks) std::copy(plan.chunks.begin(), plan.chunks.end(), chunks);
+  if (n_split) std::copy(plan.n_split.begin(), plan.n_split.end(), n_split);
   return 0;
 }
 
@@ -403,9 +432,11 @@ int wn_assemble_c3d10_device(void* h, const double* d_props, int apply_bcs, uint
                   s->block_row.p, s->col_idx.p,
                   fused ? reinterpret_cast<const int32_t*>(s->fine.d64.p) : nullptr,
                   fused ? reinterpret_cast<const int32_t*>(s->fine.d32.p) : nullptr,
-                  fused ? s->fine.p64.p : nullptr, fused ? s->fine.p32.p : nullptr};
-    WN_CHECK(launch_assemble_tiles(A, s->asm_tiles, s->asm_ne_max, s->nodes.p, s->conn.p, s->props.p,
-                                   apply_bcs ? s->fixed.p : nullptr, s->nnzb, s->k64.p, s->k32.p, s->flags.p, st));
+                  fused ? s->fine.p64.p : nullptr, fused ? s->fine.p32.p : nullptr,
+                  s->asm_chunk_ptr.p, s->asm_chunks.p, s->asm_n_split.p};
+    WN_CHECK(launch_assemble_tiles(A, s->asm_tiles, s->asm_ne_max, s->asm_max_codes, s->nodes.p, s->conn.p,
+                                   s->props.p, apply_bcs ? s->fixed.p : nullptr, s->nnzb, s->k64.p, s->k32.p,
+                                   s->flags.p, st));
     if (fused)
       s->fine.packed = true;
     else if (s->stream_fine)  // first assembly: build the packs (structure and values) from the arrays
@@ -501,6 +532,16 @@ int wn_solid_set_stream(void* h, int enable) {
     WN_CHECK(s->fine.pack(s->row_ptr.p, s->col_idx.p, s->k32.p, s->k64.p, s->nnzb, 0));
     WN_CUDA(cudaDeviceSynchronize());
   }
+  return 0;
+}
+
+int wn_solid_set_batch_staging(void* h, int enable) {
+  WN_REQUIRE(h, WN_EINVAL, "wn_solid_set_batch_staging: null handle");
+  Solid* s = as_solid(h);
+  WN_CHECK(select_device(s));
+  WN_CUDA(cudaDeviceSynchronize());
+  s->batch_stage_x = enable != 0;
+  ++s->fine.epoch;  // captured batched chunks hold the launches of the other path
   return 0;
 }
 

@@ -24,11 +24,17 @@ struct AsmTileArgs {
   const int32_t* d32;
   unsigned char* p64;        // packs or null
   unsigned char* p32;
+  const int32_t* chunk_ptr;  // n_tiles + 1 (AssemblyPlan::chunk_ptr)
+  const uint32_t* chunks;    // AssemblyPlan::chunks
+  const int32_t* n_split;    // n_tiles
 };
-// flags bit 0: det J <= 0.  Dynamic shared memory: ne_max elements of 129 doubles.
-int launch_assemble_tiles(const AsmTileArgs& A, int n_tiles, int ne_max, const double* nodes, const int32_t* conn,
-                          const double* props, const uint8_t* fixed, int64_t nnzb, double* k64, float* k32, int* flags,
-                          cudaStream_t st);
+// flags bit 0: det J <= 0.  Dynamic shared memory: ne_max elements of 127 doubles (at least
+// the tile's 512 x 9 staged blocks), 32 chunk sums of 18 doubles, max_codes 16-bit codes.
+size_t assemble_tiles_smem(int ne_max, int max_codes);
+constexpr size_t kAsmSmemLimit = 227 * 1024;  // dynamic shared memory of one CTA on sm_100
+int launch_assemble_tiles(const AsmTileArgs& A, int n_tiles, int ne_max, int max_codes, const double* nodes,
+                          const int32_t* conn, const double* props, const uint8_t* fixed, int64_t nnzb, double* k64,
+                          float* k32, int* flags, cudaStream_t st);
 // flags: bit 0 = det J <= 0, bit 1 = node index outside [0, n_nodes) (that element: zero Ke)
 int launch_ke_upper(int64_t n_el, int64_t n_nodes, const double* nodes, const int32_t* conn, const double* props,
                     double* out, int* flags, cudaStream_t st);

@@ -205,6 +205,56 @@ int build_assembly_plan(const Bsr3Pattern& pat, int64_t n_el, int tile_blocks, i
       for (size_t k = 0; k < order.size(); ++k) out.perm[T.b0 + k] = (uint16_t)order[k].second;
     }
   });
+  // chunk length: the smallest of the candidates whose chunks fit the kernel's slots in every
+  // tile (heavy blocks are the diagonal blocks of vertex nodes; 6 on the structured I-beam)
+  int32_t max_count = 0;
+  for (int64_t blk = 0; blk < pat.nnzb; ++blk)
+    max_count = std::max(max_count, pat.gather_ptr[blk + 1] - pat.gather_ptr[blk]);
+  if (max_count > 1023) return 1;  // 10-bit chunk offsets
+  const int candidates[] = {6, 8, 12, 16, 24, 32, 48, 63};
+  out.chunk_len = 1024;  // no split block
+  for (int C : candidates) {
+    if (C >= max_count) break;
+    int worst = 0;
+    for (int64_t t = 0; t < nt && worst <= kAsmChunkSlots; ++t) {
+      int nc = 0;
+      for (int32_t blk = out.tiles[t].b0; blk < out.tiles[t].b1; ++blk) {
+        const int32_t c = pat.gather_ptr[blk + 1] - pat.gather_ptr[blk];
+        if (c > C) nc += (c + C - 1) / C;
+      }
+      worst = std::max(worst, nc);
+    }
+    if (worst <= kAsmChunkSlots) {
+      out.chunk_len = C;
+      break;
+    }
+  }
+  out.chunk_ptr.assign(nt + 1, 0);
+  out.n_split.assign(nt, 0);
+  out.chunks.clear();
+  for (int64_t t = 0; t < nt; ++t) {
+    const AssemblyTile& T = out.tiles[t];
+    out.max_codes = std::max(out.max_codes, pat.gather_ptr[T.b1] - pat.gather_ptr[T.b0]);
+    int h = 0;
+    for (int32_t k = 0; k < T.b1 - T.b0; ++k) {
+      const int32_t j = out.perm[T.b0 + k];
+      const int32_t c = pat.gather_ptr[T.b0 + j + 1] - pat.gather_ptr[T.b0 + j];
+      if (c <= out.chunk_len) break;  // perm is by descending count: the rest are not split
+      ++h;
+      // c contributions in n near-equal chunks: the first c % n of them one longer
+      const int32_t n = (c + out.chunk_len - 1) / out.chunk_len, base = c / n, extra = c % n;
+      int32_t off = 0;
+      for (int32_t m = 0; m < n; ++m) {
+        const int32_t len = base + (m < extra ? 1 : 0);
+        out.chunks.push_back((uint32_t)j | ((uint32_t)off << 9) | ((uint32_t)len << 19) | ((m == 0 ? 1u : 0u) << 25));
+        off += len;
+      }
+    }
+    out.n_split[t] = h;
+    out.chunk_ptr[t + 1] = (int32_t)out.chunks.size();
+    out.max_chunks = std::max(out.max_chunks, out.chunk_ptr[t + 1] - out.chunk_ptr[t]);
+  }
+  if (out.max_chunks > kAsmChunkSlots) return 1;
   return 0;
 }
 

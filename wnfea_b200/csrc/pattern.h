@@ -50,7 +50,21 @@ struct AssemblyPlan {
   // per tile, its local block indices by descending contribution count (lanes of a warp then
   // carry blocks of similar cost): perm[b0 + k] = local index of the k-th block
   std::vector<uint16_t> perm;     // nnzb
+  // Blocks with more than chunk_len contributions ("split" blocks; they lead perm) are summed
+  // in chunks of at most chunk_len consecutive contributions by different threads and the
+  // chunk sums added in chunk order.  Whether a block is split and where its chunks start
+  // depend on its contribution count alone, so blocks (i, j) and (j, i) are cut alike.
+  int chunk_len = 0;
+  int max_chunks = 0;             // most chunks in one tile (<= kAsmChunkSlots)
+  int max_codes = 0;              // most contributions in one tile
+  std::vector<int32_t> chunk_ptr; // n_tiles + 1
+  // per tile, the chunks of its split blocks in perm order: local block | first contribution
+  // (offset in the block's list) << 9 | length << 19 | first chunk of its block << 25
+  std::vector<uint32_t> chunks;
+  std::vector<int32_t> n_split;   // per tile: its split blocks (perm[b0 .. b0 + n_split))
 };
+// chunk-sum slots of the assembly kernel's shared memory (one per chunk of a tile)
+constexpr int kAsmChunkSlots = 32;
 // 0: plan made; 1: the row tiles cannot be made (a row over the tile capacity) or a tile has
 // more than ne_cap incident elements (the caller keeps the element-scratch assembly).
 int build_assembly_plan(const Bsr3Pattern& pat, int64_t n_el, int tile_blocks, int tile_rows, int ne_cap,

@@ -38,9 +38,10 @@ struct Solid {
   DArray<int32_t> row_ptr, col_idx, block_row, diag_block;
   DArray<int32_t> emap, gptr, gsrc;  // gsrc: only for the element-scratch assembly (no plan)
   // tile-owner assembly plan (pattern.h AssemblyPlan); asm_tiles == 0: element-scratch assembly
-  int asm_tiles = 0, asm_ne_max = 0;
-  DArray<int32_t> asm_tile, asm_el_ptr, asm_el;
+  int asm_tiles = 0, asm_ne_max = 0, asm_max_codes = 0;
+  DArray<int32_t> asm_tile, asm_el_ptr, asm_el, asm_chunk_ptr, asm_n_split;
   DArray<uint16_t> asm_perm, asm_contrib;
+  DArray<uint32_t> asm_chunks;
   DArray<int64_t> inc_ptr;
   DArray<int32_t> inc_ea;
   // values
@@ -55,6 +56,7 @@ struct Solid {
   StreamMat fine;
   bool stream_fine = true;  // wn_solid_set_stream: plan and packs kept (else the register kernels)
   bool stream_batched = false;  // wn_solid_set_stream(2): the batched solves stream the fine level too
+  bool batch_stage_x = false;   // wn_solid_set_batch_staging: batched fine level with x staged per tile
   bool assembled = false;
   bool bcs_applied = false;
   std::unique_ptr<AmgHierarchy> amg;
