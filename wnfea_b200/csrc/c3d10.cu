@@ -208,6 +208,13 @@ __host__ __device__ constexpr int64_t asm_el_area(int ne_max) {
              : (int64_t)WN_STREAM_TILE_BLOCKS * 9;
 }
 
+// doubles of the space shared by the chunk sums (phase 2 on) and the incident elements'
+// connectivity (phases 0-1)
+__host__ __device__ constexpr int64_t asm_union_doubles(int ne_max) {
+  return (int64_t)18 * kAsmChunkSlots > ((int64_t)ne_max * 10 + 1) / 2 ? (int64_t)18 * kAsmChunkSlots
+                                                                      : ((int64_t)ne_max * 10 + 1) / 2;
+}
+
 struct AsmItem {
   int j = -1;      // local block, -1: none
   int qa = 0, qb = 0;  // contributions [qa, qb) (global indices)
@@ -288,22 +295,25 @@ __global__ void __launch_bounds__(kAsmThreads, 2) assemble_tiles_kernel(
     const double* __restrict__ props, const uint8_t* __restrict__ fixed, int64_t nnzb, double* __restrict__ k64,
     float* __restrict__ k32, int* __restrict__ flags) {
   extern __shared__ double s_el[];
-  double* s_part = s_el + el_area;  // kAsmChunkSlots x (A 9, B 9)
-  uint16_t* s_codes = reinterpret_cast<uint16_t*>(s_part + 18 * kAsmChunkSlots);
+  double* s_part = s_el + el_area;                           // kAsmChunkSlots x (A 9, B 9), phase 2 on
+  int32_t* s_conn = reinterpret_cast<int32_t*>(s_part);      // the same space, phases 0-1: ne x 10
+  uint16_t* s_codes = reinterpret_cast<uint16_t*>(s_el + el_area + asm_union_doubles(A.ne_max));
+  __shared__ uint32_t s_chunk[kAsmChunkSlots];
   const int t = blockIdx.x, x = threadIdx.x;
   const int4 T = reinterpret_cast<const int4*>(A.tiles)[t];  // r0, r1, b0, b1
-  const int e_beg = A.el_ptr[t], ne = A.el_ptr[t + 1] - e_beg;
+  const int4 H0 = reinterpret_cast<const int4*>(A.hdr)[2 * t];
+  const int4 H1 = reinterpret_cast<const int4*>(A.hdr)[2 * t + 1];
+  const int e_beg = H0.x, ne = H0.y, c0 = H0.z, NH = H0.w, H = H1.x, qbase = H1.y, ncodes = H1.z;
   double* s_lm = s_el + ne * kAsmElStride;  // lam, mu per element
-  const int nb = T.w - T.z;
-  // phase 0
-  const int qbase = A.gptr[T.z], ncodes = A.gptr[T.w] - qbase;
-  for (int i = x; i < ncodes; i += kAsmThreads) s_codes[i] = A.contrib[qbase + i];
-  const int c0 = A.chunk_ptr[t], NH = A.chunk_ptr[t + 1] - c0, H = A.n_split[t], L = nb - H;
+  const int nb = T.w - T.z, L = nb - H;
+  // phase 0: work items, incident elements (connectivity, lam, mu), codes -- loads in flight
+  // together, each at most two dependent steps from the tile header
   const int n0 = min(L, kAsmThreads - NH);  // light blocks of round 0
   AsmItem it[3];
   bool first = false;  // round 0 holds the first chunk of a split block
   if (x < NH) {
     const uint32_t c = A.chunks[c0 + x];
+    s_chunk[x] = c;
     it[0].j = (int)(c & 511u);
     it[0].qa = A.gptr[T.z + it[0].j] + (int)((c >> 9) & 1023u);
     it[0].qb = it[0].qa + (int)((c >> 19) & 63u);
@@ -322,6 +332,35 @@ __global__ void __launch_bounds__(kAsmThreads, 2) assemble_tiles_kernel(
       it[r].qa = A.gptr[T.z + it[r].j];
       it[r].qb = A.gptr[T.z + it[r].j + 1];
     }
+  for (int k = x; k < ne; k += kAsmThreads) {
+    const int64_t e = A.el[e_beg + k];
+    int32_t cn[10];
+#pragma unroll
+    for (int a = 0; a < 10; ++a) cn[a] = conn[e * 10 + a];
+    double lam, mu;
+    lame(props[e * 2], props[e * 2 + 1], lam, mu);
+#pragma unroll
+    for (int a = 0; a < 10; ++a) s_conn[k * 10 + a] = cn[a];
+    s_lm[2 * k] = lam;
+    s_lm[2 * k + 1] = mu;
+  }
+  {
+    constexpr int kDeep = 8;  // codes per thread loaded before any is stored
+    for (int i0 = x; i0 < ncodes; i0 += kAsmThreads * kDeep) {
+      uint16_t v[kDeep];
+#pragma unroll
+      for (int j = 0; j < kDeep; ++j) {
+        const int i = i0 + j * kAsmThreads;
+        v[j] = i < ncodes ? A.contrib[qbase + i] : (uint16_t)0;
+      }
+#pragma unroll
+      for (int j = 0; j < kDeep; ++j) {
+        const int i = i0 + j * kAsmThreads;
+        if (i < ncodes) s_codes[i] = v[j];
+      }
+    }
+  }
+  __syncthreads();
   // phase 1
   {
     const int warp = x >> 5, lane = x & 31;
@@ -329,9 +368,14 @@ __global__ void __launch_bounds__(kAsmThreads, 2) assemble_tiles_kernel(
     for (int wi = warp; wi < n_items; wi += kAsmThreads / 32) {
       const int g = wi & 3, k = (wi >> 2) * 32 + lane;
       if (k >= ne) continue;
-      const int64_t e = A.el[e_beg + k];
       double Xr[10][3];
-      load_coords(nodes, conn, e, Xr);
+#pragma unroll
+      for (int a = 0; a < 10; ++a) {
+        const int64_t nd = s_conn[k * 10 + a];
+        Xr[a][0] = nodes[nd * 3 + 0];
+        Xr[a][1] = nodes[nd * 3 + 1];
+        Xr[a][2] = nodes[nd * 3 + 2];
+      }
 #pragma unroll
       for (int a = 1; a < 10; ++a)
 #pragma unroll
@@ -351,15 +395,9 @@ __global__ void __launch_bounds__(kAsmThreads, 2) assemble_tiles_kernel(
 #pragma unroll
         for (int a = 0; a < 10; ++a) d[i * 10 + a] = dndx[i][a];
       d[30] = kWeight * det;
-      if (g == 0) {
-        double lam, mu;
-        lame(props[e * 2], props[e * 2 + 1], lam, mu);
-        s_lm[2 * k] = lam;
-        s_lm[2 * k + 1] = mu;
-      }
     }
   }
-  __syncthreads();
+  __syncthreads();  // s_conn is dead from here on (its space holds the chunk sums)
   // phase 2: rounds 0 and 2 finish into fin[0], round 1 into fin[1] (a thread has a light
   // block in round 0 or in round 2, not both); split-block chunks leave A and B in slot x
   double fin[2][9];
@@ -389,7 +427,7 @@ __global__ void __launch_bounds__(kAsmThreads, 2) assemble_tiles_kernel(
       As[m] = s_part[x * 18 + m];
       Bs[m] = s_part[x * 18 + 9 + m];
     }
-    for (int y = x + 1; y < NH && !((A.chunks[c0 + y] >> 25) & 1u); ++y)
+    for (int y = x + 1; y < NH && !((s_chunk[y] >> 25) & 1u); ++y)
 #pragma unroll
       for (int m = 0; m < 9; ++m) {
         As[m] += s_part[y * 18 + m];
@@ -410,16 +448,28 @@ __global__ void __launch_bounds__(kAsmThreads, 2) assemble_tiles_kernel(
   const int4 d32 = A.p64 ? reinterpret_cast<const int4*>(A.d32)[t] : make_int4(0, 0, 0, 0);
   double* v64 = A.p64 ? reinterpret_cast<double*>(A.p64 + (size_t)d64.z * 128) : nullptr;
   float* v32 = A.p64 ? reinterpret_cast<float*>(A.p32 + (size_t)d32.z * 128) : nullptr;
-  for (int m = 0; m < 9; ++m)
-    for (int j = x; j < nb; j += kAsmThreads) {
-      const double v = stage[j * 9 + m];
-      k64[m * nnzb + T.z + j] = v;
-      k32[m * nnzb + T.z + j] = (float)v;
+  // nb <= 2 kAsmThreads: two blocks per thread and component, all shared-memory reads first
+#pragma unroll
+  for (int m = 0; m < 9; ++m) {
+    const int j0 = x, j1 = x + kAsmThreads;
+    const double a0 = j0 < nb ? stage[j0 * 9 + m] : 0.0, a1 = j1 < nb ? stage[j1 * 9 + m] : 0.0;
+    if (j0 < nb) {
+      k64[m * nnzb + T.z + j0] = a0;
+      k32[m * nnzb + T.z + j0] = (float)a0;
       if (v64) {
-        v64[m * d64.w + j] = v;
-        v32[m * d32.w + j] = (float)v;
+        v64[m * d64.w + j0] = a0;
+        v32[m * d32.w + j0] = (float)a0;
       }
     }
+    if (j1 < nb) {
+      k64[m * nnzb + T.z + j1] = a1;
+      k32[m * nnzb + T.z + j1] = (float)a1;
+      if (v64) {
+        v64[m * d64.w + j1] = a1;
+        v32[m * d32.w + j1] = (float)a1;
+      }
+    }
+  }
 }
 
 // Matrix-free element forces f_e = Ke u_e (= sum_g w|J| B^T C B u_e, c3d10.py:252-283) for
@@ -572,7 +622,8 @@ __global__ void nodal_average_kernel(int64_t n_nodes, const int64_t* __restrict_
 // host launchers
 // ---------------------------------------------------------------------------------------
 size_t assemble_tiles_smem(int ne_max, int max_codes) {
-  return (size_t)(asm_el_area(ne_max) + 18 * kAsmChunkSlots) * sizeof(double) + ((size_t)max_codes * 2 + 7) / 8 * 8;
+  return (size_t)(asm_el_area(ne_max) + asm_union_doubles(ne_max)) * sizeof(double) +
+         ((size_t)max_codes * 2 + 7) / 8 * 8;
 }
 
 int launch_assemble_tiles(const AsmTileArgs& A, int n_tiles, int ne_max, int max_codes, const double* nodes,

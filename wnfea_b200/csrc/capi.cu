@@ -248,12 +248,21 @@ int wn_solid_create(int64_t n_nodes, int64_t n_el, const double* nodes, const in
         tl[4 * t + 3] = plan.tiles[t].b1;
       }
       st = st ? st : s->asm_tile.upload(tl);
-      st = st ? st : s->asm_el_ptr.upload(plan.el_ptr);
+      std::vector<int32_t> hdr(plan.tiles.size() * 8, 0);
+      for (size_t t = 0; t < plan.tiles.size(); ++t) {
+        int32_t* h = &hdr[8 * t];
+        h[0] = plan.el_ptr[t];
+        h[1] = plan.el_ptr[t + 1] - plan.el_ptr[t];
+        h[2] = plan.chunk_ptr[t];
+        h[3] = plan.chunk_ptr[t + 1] - plan.chunk_ptr[t];
+        h[4] = plan.n_split[t];
+        h[5] = pat.gather_ptr[plan.tiles[t].b0];
+        h[6] = pat.gather_ptr[plan.tiles[t].b1] - pat.gather_ptr[plan.tiles[t].b0];
+      }
+      st = st ? st : s->asm_hdr.upload(hdr);
       st = st ? st : s->asm_el.upload(plan.el);
       st = st ? st : s->asm_perm.upload(plan.perm);
       st = st ? st : s->asm_contrib.upload(plan.contrib);
-      st = st ? st : s->asm_chunk_ptr.upload(plan.chunk_ptr);
-      st = st ? st : s->asm_n_split.upload(plan.n_split);
       st = st ? st : s->asm_chunks.upload(plan.chunks);
     } else {
       st = st ? st : s->gsrc.upload(pat.gather_src);
@@ -428,12 +437,12 @@ int wn_assemble_c3d10_device(void* h, const double* d_props, int apply_bcs, uint
     // values too, in one kernel with no element scratch
     const bool fused = s->stream_fine && s->fine.n_tiles == s->asm_tiles && s->fine.structure &&
                        s->fine.p64.p && s->fine.p32.p;
-    AsmTileArgs A{s->asm_tile.p, s->asm_el_ptr.p, s->asm_el.p, s->asm_perm.p, s->gptr.p, s->asm_contrib.p,
+    AsmTileArgs A{s->asm_tile.p, s->asm_hdr.p, s->asm_el.p, s->asm_perm.p, s->gptr.p, s->asm_contrib.p,
                   s->block_row.p, s->col_idx.p,
                   fused ? reinterpret_cast<const int32_t*>(s->fine.d64.p) : nullptr,
                   fused ? reinterpret_cast<const int32_t*>(s->fine.d32.p) : nullptr,
                   fused ? s->fine.p64.p : nullptr, fused ? s->fine.p32.p : nullptr,
-                  s->asm_chunk_ptr.p, s->asm_chunks.p, s->asm_n_split.p};
+                  s->asm_chunks.p, s->asm_ne_max};
     WN_CHECK(launch_assemble_tiles(A, s->asm_tiles, s->asm_ne_max, s->asm_max_codes, s->nodes.p, s->conn.p,
                                    s->props.p, apply_bcs ? s->fixed.p : nullptr, s->nnzb, s->k64.p, s->k32.p,
                                    s->flags.p, st));

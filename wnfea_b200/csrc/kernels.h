@@ -13,7 +13,9 @@ namespace wn {
 // (p64 == nullptr: no packs written)
 struct AsmTileArgs {
   const int32_t* tiles;      // n_tiles x 4: r0, r1, b0, b1
-  const int32_t* el_ptr;     // n_tiles + 1
+  // n_tiles x 8: first incident element, incident elements, first chunk, chunks; split blocks,
+  // first contribution, contributions, 0 (one load per tile for every per-tile scalar)
+  const int32_t* hdr;
   const int32_t* el;         // incident elements per tile
   const uint16_t* perm;      // nnzb
   const int32_t* gptr;       // nnzb + 1
@@ -24,12 +26,12 @@ struct AsmTileArgs {
   const int32_t* d32;
   unsigned char* p64;        // packs or null
   unsigned char* p32;
-  const int32_t* chunk_ptr;  // n_tiles + 1 (AssemblyPlan::chunk_ptr)
   const uint32_t* chunks;    // AssemblyPlan::chunks
-  const int32_t* n_split;    // n_tiles
+  int ne_max;                // most incident elements of a tile (shared-memory layout)
 };
 // flags bit 0: det J <= 0.  Dynamic shared memory: ne_max elements of 127 doubles (at least
-// the tile's 512 x 9 staged blocks), 32 chunk sums of 18 doubles, max_codes 16-bit codes.
+// the tile's 512 x 9 staged blocks); 32 chunk sums of 18 doubles, earlier the incident
+// elements' connectivity (ne_max x 10 int32); max_codes 16-bit codes.
 size_t assemble_tiles_smem(int ne_max, int max_codes);
 constexpr size_t kAsmSmemLimit = 227 * 1024;  // dynamic shared memory of one CTA on sm_100
 int launch_assemble_tiles(const AsmTileArgs& A, int n_tiles, int ne_max, int max_codes, const double* nodes,

@@ -39,7 +39,7 @@ struct Solid {
   DArray<int32_t> emap, gptr, gsrc;  // gsrc: only for the element-scratch assembly (no plan)
   // tile-owner assembly plan (pattern.h AssemblyPlan); asm_tiles == 0: element-scratch assembly
   int asm_tiles = 0, asm_ne_max = 0, asm_max_codes = 0;
-  DArray<int32_t> asm_tile, asm_el_ptr, asm_el, asm_chunk_ptr, asm_n_split;
+  DArray<int32_t> asm_tile, asm_hdr, asm_el;
   DArray<uint16_t> asm_perm, asm_contrib;
   DArray<uint32_t> asm_chunks;
   DArray<int64_t> inc_ptr;
