@@ -94,6 +94,9 @@ def parse():
     ap.add_argument("--cases", type=int, default=32, help="load cases of the batched (multi-RHS) solve")
     ap.add_argument("--order", choices=["native", "scrambled", "rcm"], default="native",
                     help="profiling mode: node numbering -- the generator's, a seeded random one, or RCM of that")
+    ap.add_argument("--batch-fine", choices=["register", "staged", "streamed"], default="register",
+                    help="profiling mode solve-multi: the batched fine level's path (register row kernels, x "
+                         "slices staged in shared memory, or streamed from the tile-major packs)")
     ap.add_argument("--only", choices=["solve-mixed", "solve-fp64", "solve-multi", "spmv32", "spmv64", "frame",
                                        "assemble"],
                     default=None,
@@ -123,6 +126,9 @@ def run_only(args):
         from wnfea_b200.mesh import tip_load_cases
 
         s.amg_setup()
+        s.set_batch_staging(args.batch_fine == "staged")
+        if args.batch_fine == "streamed":
+            s.set_streaming(True, batched=True)
         Fm = torch.from_numpy(tip_load_cases(m.mesh_nodes, n_cases=args.cases, seed=0)).cuda()
         Um = torch.empty_like(Fm)
         info = {}
@@ -168,7 +174,8 @@ def run_only(args):
     if args.only in ("solve-mixed", "solve-fp64"):
         out.update(info)
     if args.only == "solve-multi":
-        out.update({"cases": args.cases, "iterations": info["iterations"], "outer": info["outer_iterations"],
+        out.update({"batch_fine": args.batch_fine, "cases": args.cases, "iterations": info["iterations"],
+                    "outer": info["outer_iterations"],
                     "status": info["status"], "max_rel_res": info["rel_res"],
                     "device_ms": info["solve_seconds"] * 1e3,
                     "case_iterations": [int(v) for v in info["case_iterations"]]})
