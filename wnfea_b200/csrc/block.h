@@ -68,6 +68,9 @@ struct BlockWork {
   // preconditioner input / output in the V-cycle precision
   DArray<float> z32, r32;
   DArray<double> z64;
+  // the fine V-cycle's first smoothing input dinv r / theta, written by the PCG update
+  DArray<float> d0_32;
+  DArray<double> d0_64;
   // V-cycle vectors per level and the coarsest right-hand side / solution
   std::vector<BatchLevelVecs<float>> lv32;
   std::vector<BatchLevelVecs<double>> lv64;

@@ -389,10 +389,12 @@ struct Tpg {
 // batched V-cycle kernels (same arithmetic per case as the single-RHS smoother kernels);
 // vectors of type T use the case map of T
 // ---------------------------------------------------------------------------------------
-template <int BS, typename T, int S>
+// xf: the first smoothing step's x, dinv b / theta -- BD0 on the fly, or BLoad of the vector the
+// PCG update wrote (the same values)
+template <int BS, typename T, int S, typename XF>
 __global__ void __launch_bounds__(kThreads) kb_pre_first(int64_t n_rows, const int32_t* __restrict__ rp,
                                                          const int32_t* __restrict__ ci, const T* __restrict__ av,
-                                                         int64_t stride, const T* __restrict__ b,
+                                                         int64_t stride, XF xf, const T* __restrict__ b,
                                                          const T* __restrict__ dinv, T inv_theta, int deg, T c1, T c2,
                                                          T* __restrict__ x, T* __restrict__ r, T* __restrict__ d,
                                                          T* __restrict__ res, const int* __restrict__ done) {
@@ -400,7 +402,7 @@ __global__ void __launch_bounds__(kThreads) kb_pre_first(int64_t n_rows, const i
   BATCH_TEAM_LOOP(n_rows, S) {
     T acc[BS][4];
     batch_row_staged<BS, BS, BLayout<BS>::value, Tpg<T>::value, S, T>(rp, ci, av, stride, row, row < n_rows, l,
-                                                                BD0<T, T>{b, dinv, inv_theta}, FmaAcc<BS, T>(acc));
+                                                                xf, FmaAcc<BS, T>(acc));
     if (row >= n_rows || !lead) continue;
 #pragma unroll
     for (int rr = 0; rr < BS; ++rr) {
@@ -1276,7 +1278,8 @@ template <typename TM>
 __global__ void __launch_bounds__(kThreads) kb_update(int64_t n, double* __restrict__ x, double* __restrict__ r,
                                                       TM* __restrict__ rm, const double* __restrict__ p,
                                                       const double* __restrict__ q, double* __restrict__ partC,
-                                                      const BlockScalars* __restrict__ S) {
+                                                      const BlockScalars* __restrict__ S, TM* __restrict__ d0,
+                                                      const TM* __restrict__ dinv, TM inv_theta) {
   if (S->done) return;
   double dot[4] = {0.0, 0.0, 0.0, 0.0};
   {
@@ -1296,7 +1299,15 @@ __global__ void __launch_bounds__(kThreads) kb_update(int64_t n, double* __restr
       }
       stc<double>(x + o, l, xv);
       stc<double>(r + o, l, rv);
-      if (rm) stc<double>(rm + o, l, cvt4<TM>(rv));
+      const C4<TM> rt = cvt4<TM>(rv);
+      if (rm) stc<double>(rm + o, l, rt);
+      if (d0) {  // the V-cycle's first smoothing input, BD0's expression on the same values
+        const TM di = dinv[i];
+        C4<TM> dv;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dv.v[k] = di * rt.v[k] * inv_theta;
+        stc<double>(d0 + o, l, dv);
+      }
     }
   }
   write_case_parts<double>(dot, partC);
@@ -1519,6 +1530,7 @@ struct BPrec<float> {
   static const float* fine_dinv(BlockWork& W) { return W.dinv32.p; }
   static float* z(BlockWork& W) { return W.z32.p; }
   static float* rm(BlockWork& W) { return W.r32.p; }  // r in FP32 for the V-cycle
+  static float* d0(BlockWork& W) { return W.d0_32.p; }
 };
 template <>
 struct BPrec<double> {
@@ -1533,6 +1545,7 @@ struct BPrec<double> {
   static const double* fine_dinv(BlockWork& W) { return W.dinv64.p; }
   static double* z(BlockWork& W) { return W.z64.p; }
   static double* rm(BlockWork&) { return nullptr; }  // the V-cycle reads the FP64 r directly
+  static double* d0(BlockWork& W) { return W.d0_64.p; }
 };
 
 // long rows (>= 4 stages of 8 blocks on average) are shared by the 4 groups of a warp
@@ -1554,7 +1567,7 @@ void batch_level_spmv(const DevBsr& M, const T* vals, const T* x, T* y, int accu
 // one batched V-cycle at level lvl: out = V(b); part (if set) receives b . out per case
 template <typename T>
 int batch_vcycle(Solid* s, AmgHierarchy& H, BlockWork& W, int lvl, const T* b, T* out, double* part,
-                 BlockScalars* S, cudaStream_t st) {
+                 BlockScalars* S, cudaStream_t st, const T* d0 = nullptr) {
   const int* done = &S->done;
   const int nlev = (int)H.levels.size();
   if (lvl == nlev) {
@@ -1598,10 +1611,19 @@ int batch_vcycle(Solid* s, AmgHierarchy& H, BlockWork& W, int lvl, const T* b, T
       if (g == 0 && lvl == 0 && BS == 3) g = launch_bx<T>(s, W, av, xf, epi, part_out, done, st);
       return g;
     };
-    if (!(streamed(BD0<T, T>{b, dinv, it},
-                                  BEpiPreFirst<T>{b, dinv, it, deg, c1, c2, V.x.p, V.r.p, V.d.p, V.res.p}, nullptr)))
-      kb_pre_first<BS, T, SG><<<rg(kb_pre_first<BS, T, SG>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, deg, c1,
-                                                                        c2, V.x.p, V.r.p, V.d.p, V.res.p, done);
+    // the first step's x: dinv b / theta, read from d0 when the PCG update wrote it
+    const BEpiPreFirst<T> epf{b, dinv, it, deg, c1, c2, V.x.p, V.r.p, V.d.p, V.res.p};
+    if (d0 && lvl == 0) {
+      if (!streamed(BLoad<T, T>{d0}, epf, nullptr)) {
+        auto k = kb_pre_first<BS, T, SG, BLoad<T, T>>;
+        k<<<rg(k), kThreads, 0, st>>>(nr, rp, ci, av, sd, BLoad<T, T>{d0}, b, dinv, it, deg, c1, c2, V.x.p, V.r.p,
+                                      V.d.p, V.res.p, done);
+      }
+    } else if (!streamed(BD0<T, T>{b, dinv, it}, epf, nullptr)) {
+      auto k = kb_pre_first<BS, T, SG, BD0<T, T>>;
+      k<<<rg(k), kThreads, 0, st>>>(nr, rp, ci, av, sd, BD0<T, T>{b, dinv, it}, b, dinv, it, deg, c1, c2, V.x.p,
+                                    V.r.p, V.d.p, V.res.p, done);
+    }
     W.launches++;
     T* din = V.d.p;
     T* dout = V.d2.p;
@@ -1662,9 +1684,10 @@ int batch_vcycle(Solid* s, AmgHierarchy& H, BlockWork& W, int lvl, const T* b, T
 
 // z = M r for all cases, partA = r . z per case
 template <typename TM>
-int batch_prec(Solid* s, BlockWork& W, int precond, const TM* r, TM* z, BlockScalars* S, cudaStream_t st) {
+int batch_prec(Solid* s, BlockWork& W, int precond, const TM* r, TM* z, BlockScalars* S, cudaStream_t st,
+               const TM* d0 = nullptr) {
   const int* done = &S->done;
-  if (precond == 2) return batch_vcycle<TM>(s, *s->amg, W, 0, r, z, W.partA.p, S, st);
+  if (precond == 2) return batch_vcycle<TM>(s, *s->amg, W, 0, r, z, W.partA.p, S, st, d0);
   const int g = resident_grid(kb_prec_vec<TM>, kThreads, quads_work(W.n));
   W.npA = g;
   kb_prec_vec<TM><<<g, kThreads, 0, st>>>(W.n, r, BPrec<TM>::fine_dinv(W), precond == 1 ? 1 : 0, z, W.partA.p,
@@ -1702,13 +1725,17 @@ int batch_iteration(Solid* s, BlockWork& W, int precond, int k, BlockScalars* S,
   }
   W.npB = gsd;
   kb_alpha<<<1, kThreads, 0, st>>>(S, W.partB.p, W.npB);
+  // with the AMG preconditioner the update also writes the V-cycle's first smoothing input
+  TM* d0 = (precond == 2 && s->amg && !s->amg->levels.empty()) ? BPrec<TM>::d0(W) : nullptr;
+  const TM it0 = d0 ? (TM)s->amg->levels[0].inv_theta : TM(0);
   const int gup = resident_grid(kb_update<TM>, kThreads, quads_work(W.n));
-  kb_update<TM><<<gup, kThreads, 0, st>>>(W.n, W.x.p, W.r.p, BPrec<TM>::rm(W), p_new, W.q.p, W.partC.p, S);
+  kb_update<TM><<<gup, kThreads, 0, st>>>(W.n, W.x.p, W.r.p, BPrec<TM>::rm(W), p_new, W.q.p, W.partC.p, S, d0,
+                                          BPrec<TM>::fine_dinv(W), it0);
   W.npC = gup;
   kb_check<<<1, kThreads, 0, st>>>(S, W.partC.p, W.npC);
   W.launches += 4;
   WN_CUDA(cudaGetLastError());
-  WN_CHECK(batch_prec<TM>(s, W, precond, prec_input<TM>(W), BPrec<TM>::z(W), S, st));
+  WN_CHECK(batch_prec<TM>(s, W, precond, prec_input<TM>(W), BPrec<TM>::z(W), S, st, d0));
   kb_beta<<<1, kThreads, 0, st>>>(S, W.partA.p, W.npA, 0);
   W.launches++;
   WN_CUDA(cudaGetLastError());
@@ -1792,8 +1819,10 @@ int ensure_block_work(Solid* s, int vmode, int precond) {
   if (vmode == 1) {
     WN_CHECK(W.z32.alloc(nb));
     WN_CHECK(W.r32.alloc(nb));
+    if (precond == 2) WN_CHECK(W.d0_32.alloc(nb));
   } else {
     WN_CHECK(W.z64.alloc(nb));
+    if (precond == 2) WN_CHECK(W.d0_64.alloc(nb));
   }
   WN_CHECK(W.partA.alloc((int64_t)BlockWork::kMaxParts * kBatch));
   WN_CHECK(W.partB.alloc((int64_t)BlockWork::kMaxParts * kBatch));
