@@ -20,7 +20,16 @@ functions, so both sides see identical inputs.  Fixtures:
 * ``beam_frame.npz``      -- the 10x10 co-rotational frame: F_int at a seeded displacement
                              from compute_internal_forces_fast's NumPy path
                              (fast_kernels.py:451-537) and the 10-step JFNK solution of
-                             solve_nonlinear_jfnk (nonlinear_solver.py:159-376).
+                             solve_nonlinear_jfnk (nonlinear_solver.py:159-376);
+* ``structured_block.npz`` -- the reference's own mesh generator (generate_c3d10_structured_block,
+                             solid_generator.py:21-213) with the arguments of its test
+                             (tests/test_solid_bench.py:18-26): nodes, connectivity, clamped and
+                             loaded nodes with their loads, and on that mesh the reference's
+                             F, direct solution and stress field.
+
+    python tests/golden/make_golden.py /path/to/reference structured_block
+
+makes only the last one.
 """
 
 from __future__ import annotations
@@ -34,6 +43,31 @@ import numpy as np
 
 HERE = pathlib.Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
+
+
+def structured_block(ref: str) -> None:
+    builtins.Path = pathlib.Path
+    sys.path.insert(0, ref)
+    from scipy.sparse.linalg import spsolve
+    from wnfea.mesh.solid_generator import generate_c3d10_structured_block
+    from wnfea.solver.solid_solver import assemble_c3d10_sparse_3dof, compute_c3d10_stress_field
+
+    model, meta = generate_c3d10_structured_block(length=5.0, width=1.0, height=1.0, nx=10, ny=3, nz=3,
+                                                  tip_load_total=1000.0)
+    K, F, fixed = assemble_c3d10_sparse_3dof(model)
+    u = spsolve(K.tocsc(), F)
+    cell_sig, cell_vm, nodal_vm = compute_c3d10_stress_field(model, u)
+    np.savez_compressed(
+        HERE / "structured_block.npz",
+        nodes=np.asarray(model.mesh_nodes, dtype=np.float64),
+        conn=np.asarray(model.solid_elements, dtype=np.int32),
+        fixed_nodes=np.array([s.node_id for s in model.supports], dtype=np.int64),
+        load_nodes=np.array([ld.node_id for ld in model.loads], dtype=np.int64),
+        load_f=np.array([[ld.fx, ld.fy, ld.fz] for ld in model.loads], dtype=np.float64),
+        counts=np.array([meta["n_nodes"], meta["n_elements"], meta["n_dofs"], meta["root_nodes_fixed"],
+                         meta["tip_nodes_loaded"]], dtype=np.int64),
+        F=F, fixed=np.asarray(fixed, dtype=np.int64), u=u, cell_sig=cell_sig, cell_vm=cell_vm, nodal_vm=nodal_vm)
+    print("structured block", meta["n_elements"], "elements,", meta["n_dofs"], "DOFs")
 
 
 def main(ref: str) -> None:
@@ -170,4 +204,9 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref_dir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) > 2 and sys.argv[2] == "structured_block":
+        structured_block(ref_dir)
+    else:
+        main(ref_dir)
+        structured_block(ref_dir)

@@ -33,6 +33,7 @@ from .rcm import (
     permute_solution_to_original,
 )
 from .vtu import VTUExporter, export_vtu
+from .mesh import generate_c3d10_structured_block
 from .mixed_precision import FULL_FP64, MIXED_FP32, TRI_PRECISION, PrecisionConfig
 from .solid_solver import (
     assemble_c3d10_sparse_3dof,
@@ -51,5 +52,5 @@ __all__ = [
     "compute_internal_forces_fast", "prepare_batch_data", "solve_nonlinear_jfnk", "NonLinearConvergenceError",
     "BeamFrame", "ComplianceProblem", "Compliance",
     "apply_rcm_to_model", "compute_matrix_bandwidth", "compute_node_adjacency_matrix", "compute_rcm_order",
-    "permute_solution_to_original", "VTUExporter", "export_vtu",
+    "permute_solution_to_original", "VTUExporter", "export_vtu", "generate_c3d10_structured_block",
 ]

@@ -119,6 +119,66 @@ def check_positive_jacobians(coords: np.ndarray, conn: np.ndarray) -> float:
     return vmin
 
 
+# The reference's 5-tet splitting of a hex (solid_generator.py:66-80), corners numbered
+# 0 (i,j,k), 1 (i+1,j,k), 2 (i+1,j+1,k), 3 (i,j+1,k), 4-7 the same at k+1; the two mirror
+# splittings alternate with the parity of i + j + k so that neighbouring hexes share their face
+# diagonals.  The table and the mid-edge order above must be the reference's for the same mesh.
+_HEX5 = np.array([[(0, 1, 3, 4), (1, 2, 3, 6), (1, 4, 5, 6), (3, 4, 6, 7), (1, 3, 4, 6)],
+                  [(0, 1, 2, 5), (0, 2, 3, 7), (0, 4, 5, 7), (2, 5, 6, 7), (0, 2, 5, 7)]], dtype=np.int64)
+
+
+def generate_c3d10_structured_block(length: float = 10.0, width: float = 1.0, height: float = 1.0, nx: int = 40,
+                                    ny: int = 4, nz: int = 4, E: float = 2.1e11, nu: float = 0.3,
+                                    tip_load_total: float = 10000.0):
+    """The reference's structured C3D10 cantilever (wnfea/mesh/solid_generator.py:21-213), the
+    same mesh node for node: an (nx, ny, nz) hex grid of the box [0, length] x [0, width] x
+    [0, height], each hex cut into 5 tets (parity-alternating splitting), corners numbered
+    i (ny+1)(nz+1) + j (nz+1) + k, a tet of negative volume with its 2nd and 3rd corners swapped,
+    mid-edge nodes numbered after the corners in order of first use (element by element, edges
+    1-2, 2-3, 3-1, 1-4, 2-4, 3-4); the face x = 0 clamped, ``tip_load_total`` shared equally as
+    +y forces by the nodes of the face x = length.  Vectorised (no per-element Python loop).
+    Returns (model, meta) with the reference's meta keys."""
+    import time
+
+    t0 = time.perf_counter()
+    xs, ys, zs = np.linspace(0.0, length, nx + 1), np.linspace(0.0, width, ny + 1), np.linspace(0.0, height, nz + 1)
+    X, Y, Z = np.meshgrid(xs, ys, zs, indexing="ij")
+    corners = np.column_stack([X.ravel(), Y.ravel(), Z.ravel()])
+    n_corner = len(corners)
+    sj, si = nz + 1, (ny + 1) * (nz + 1)
+    I, J, K = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    base = (I * si + J * sj + K).ravel()
+    hexc = base[:, None] + np.array([0, si, si + sj, sj, 1, si + 1, si + sj + 1, sj + 1], dtype=np.int64)[None, :]
+    parity = ((I + J + K) % 2).ravel()
+    tets = np.take_along_axis(hexc[:, None, :], _HEX5[parity].reshape(len(base), 5 * 4)[:, None, :], axis=2)
+    tets = tets.reshape(-1, 4)
+    neg = _signed_volume6(corners[tets]) < 0.0
+    tets[neg, 1], tets[neg, 2] = tets[neg, 2].copy(), tets[neg, 1].copy()
+    n_el = len(tets)
+    # mid-edge nodes in order of first use
+    a = np.stack([tets[:, e0] for e0, _ in _EDGES], axis=1).ravel()
+    b = np.stack([tets[:, e1] for _, e1 in _EDGES], axis=1).ravel()
+    key = np.minimum(a, b) * n_corner + np.maximum(a, b)
+    uniq, first, inv = np.unique(key, return_index=True, return_inverse=True)
+    order = np.argsort(first, kind="stable")
+    rank = np.empty(len(uniq), dtype=np.int64)
+    rank[order] = np.arange(len(uniq))
+    conn = np.empty((n_el, 10), dtype=np.int32)
+    conn[:, :4] = tets
+    conn[:, 4:] = (n_corner + rank[inv]).reshape(n_el, 6)
+    fa, fb = a[first[order]], b[first[order]]
+    coords = np.vstack([corners, 0.5 * (corners[fa] + corners[fb])])
+    tol = 1e-6 * length
+    root = coords[:, 0] <= tol
+    tip = coords[:, 0] >= length - tol
+    model = _finish_model(coords, conn, E, nu, root, tip, (0.0, tip_load_total, 0.0))
+    model.solid_materials = {i: "Steel" for i in range(n_el)}
+    meta = {"length": length, "width": width, "height": height, "grid": (nx, ny, nz), "n_nodes": len(coords),
+            "n_elements": n_el, "n_dofs": 3 * len(coords), "root_nodes_fixed": int(root.sum()),
+            "tip_nodes_loaded": int(tip.sum()), "build_time_sec": time.perf_counter() - t0}
+    return model, meta
+
+
 def generate_c3d10_kuhn_block(
     length: float = 1.0,
     width: float = 0.1,
