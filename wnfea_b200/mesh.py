@@ -1,10 +1,10 @@
 """Structured C3D10 mesh generators for the solve path's workloads.
 
-The reference's structured generator (wnfea/mesh/solid_generator.py:21-213) cuts each hex
-into 5 tets and builds mid-edge nodes through a Python dict; its I-beam generator
-(solid_generator.py:284-412) needs Gmsh.  The workloads here want a 6-tet (Kuhn) split and
-a structured I-beam with seeded jitter, so these generators are new.  They keep the
-reference's conventions:
+``generate_c3d10_structured_block`` is the reference's structured generator
+(wnfea/mesh/solid_generator.py:21-213; 5 tets per hex) with the same arguments and the same
+mesh node for node, vectorised.  The reference's I-beam generator (solid_generator.py:284-412)
+needs Gmsh; the workloads here want a 6-tet (Kuhn) split and a structured I-beam with seeded
+jitter, so those generators are new.  All keep the reference's conventions:
 
 * C3D10 node order: 4 corners, then mid-edges 1-2, 2-3, 3-1, 1-4, 2-4, 3-4
   (c3d10.py:52-58 and the edge list at solid_generator.py:131-138);
