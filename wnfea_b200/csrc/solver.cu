@@ -884,14 +884,14 @@ static StreamView stream_view(const StreamMat& m) {
 
 // Launched with programmatic stream serialisation (launch_pdl): the first tiles of the matrix
 // are in flight before the predecessor has finished.
-template <typename T, int BR, int BC, typename XF, typename EPI>
-__global__ void __launch_bounds__(kStreamThreads, (StreamDefault<T, BR, BC>::kCtasPerSm))
+template <typename T, int BR, int BC, typename XF, typename EPI, typename SHAPE = StreamDefault<T, BR, BC>>
+__global__ void __launch_bounds__(kStreamThreads, (SHAPE::kCtasPerSm))
     k_stream_rows(StreamView m, XF xf, EPI epi, double* __restrict__ part, PcgScalars* __restrict__ S) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ double sh[kStreamThreads / 32];
   pdl_trigger();
   bool skipped = false;
-  const double dot = stream_rows<T, BR, BC, typename StreamDefault<T, BR, BC>::type>(
+  const double dot = stream_rows<T, BR, BC, typename SHAPE::type>(
       m.tiles, m.n_tiles, m.pack, xf, epi, smem, &S->status, &S->done, m.ctl, &skipped);
   if (part && !skipped) write_part(dot, part, sh);
 }
@@ -989,11 +989,11 @@ static int stream_grid(K kern, int n_tiles) {
 
 // launch a streamed row kernel on matrix m (BR x BC blocks); false (nothing launched) when m
 // has no current pack of that shape or the kernel cannot be configured
-template <typename T, int BR, int BC, typename XF, typename EPI>
+template <typename T, int BR, int BC, typename XF, typename EPI, typename SHAPE = StreamDefault<T, BR, BC>>
 static bool launch_stream_rows(const StreamMat& m, XF xf, EPI epi, double* part, PcgScalars* S, cudaStream_t st,
                                int* grid_out) {
   if (!m.packed || m.br != BR || m.bc != BC) return false;
-  auto kern = k_stream_rows<T, BR, BC, XF, EPI>;
+  auto kern = k_stream_rows<T, BR, BC, XF, EPI, SHAPE>;
   const int g = stream_grid<T, BR, BC>(kern, m.n_tiles);
   if (g == 0) return false;
   if (launch_pdl(kern, g, kStreamThreads, stream_smem_bytes<T, BR, BC>(), st, stream_view<T>(m), xf, epi, part, S) !=
@@ -1010,6 +1010,15 @@ static bool launch_stream_rows(const StreamMat& m, XF xf, EPI epi, double* part,
 template <int BR, int BC, typename T>
 static void level_spmv(const DevBsr& M, const StreamMat& Ms, const T* vals, const T* x, T* y, int accumulate,
                        PcgScalars* S, cudaStream_t st) {
+  if constexpr (BR == 6 && BC == 6) {  // short rows (the prolongations): 8 lanes per row
+    if (M.nnzb < 16 * M.n_rows) {
+      if (launch_stream_rows<T, 6, 6, XLoad<T, T>, EpiLevel<T>, StreamShort66<T>>(
+              Ms, XLoad<T, T>{x}, EpiLevel<T>{y, accumulate}, nullptr, S, st, nullptr))
+        return;
+      level_spmv_rows<BR, BC, T>(M, vals, x, y, accumulate, S, st);
+      return;
+    }
+  }
   if (launch_stream_rows<T, BR, BC>(Ms, XLoad<T, T>{x}, EpiLevel<T>{y, accumulate}, nullptr, S, st, nullptr)) return;
   level_spmv_rows<BR, BC, T>(M, vals, x, y, accumulate, S, st);
 }

@@ -119,6 +119,17 @@ struct StreamDefault<T, 6, 6> {
   using type = StreamCfg<256, kStreamRowCap, 8, 32, 2, 1>;
   static constexpr int kCtasPerSm = sizeof(T) == 4 ? 2 : 1;
 };
+// 6x6 operators with short rows (the level-1 and level-2 prolongations: ~5-8 blocks per row):
+// 8 lanes per row, 4 rows per warp, on the same tiles and packs as the default 6x6 shape
+template <typename T>
+struct StreamShort66 {
+  using type = StreamCfg<256, kStreamRowCap, 8, 8, 2, 1>;
+  static constexpr int kCtasPerSm = sizeof(T) == 4 ? 2 : 1;
+  static_assert(type::kCap == StreamDefault<T, 6, 6>::type::kCap &&
+                    type::kRowCap == StreamDefault<T, 6, 6>::type::kRowCap &&
+                    type::kStages == StreamDefault<T, 6, 6>::type::kStages,
+                "the short-row shape streams the default 6x6 tiles");
+};
 template <typename T>
 struct StreamDefault<T, 6, 3> {
   using type = StreamCfg<512, kStreamRowCap, 8, 32, 2, 2>;
