@@ -896,31 +896,6 @@ __global__ void __launch_bounds__(kStreamThreads, (SHAPE::kCtasPerSm))
   if (part && !skipped) write_part(dot, part, sh);
 }
 
-// p_new = z + beta p_old with beta read from shared memory (set after the programmatic wait)
-template <typename TK, typename TM>
-struct XPNewS {
-  const TM* __restrict__ z;
-  const TK* __restrict__ p;
-  const double* beta;
-  __device__ __forceinline__ TK operator()(int64_t j) const { return (TK)z[j] + (TK)*beta * p[j]; }
-};
-template <typename TK, typename TM>
-struct EpiSpmvDotS {
-  const TM* __restrict__ z;
-  const TK* __restrict__ p_old;
-  const double* beta;
-  TK* __restrict__ p_new;
-  TK* __restrict__ q;
-  struct Pre {
-    TK pi;
-  };
-  __device__ __forceinline__ Pre load(int64_t i) const { return {(TK)z[i] + (TK)*beta * p_old[i]}; }
-  __device__ __forceinline__ double store(int64_t i, const Pre& p, TK t) const {
-    p_new[i] = p.pi;
-    q[i] = t;
-    return (double)p.pi * (double)t;
-  }
-};
 // rz = sum(partA) and beta = rz / rz_prev (0 on the first iteration), into shared memory
 struct BetaHook {
   const double* partA;
@@ -938,25 +913,53 @@ struct BetaHook {
   }
 };
 
-// k_spmv_dot with the matrix streamed: beta from the partials of r . z, p_new = z + beta p_old,
-// q = A p_new, partials of p_new . q
-template <int BS, typename TK, typename TM>
+// The streamed PCG product in two launches: k_pnew forms p_new = z + beta p_old once (beta from
+// the partials of r . z, reduced by every CTA as BetaHook does; block 0 records rz for the next
+// beta), then k_stream_spmv_dot_p gathers p_new like a plain SpMV -- one vector per gathered
+// DOF instead of z and p_old, the same values.
+template <typename TK, typename TM>
+__global__ void __launch_bounds__(kThreads) k_pnew(int64_t n, const TM* __restrict__ z, const TK* __restrict__ p_old,
+                                                   TK* __restrict__ p_new, const double* __restrict__ partA,
+                                                   int nparts, int first, int par, PcgScalars* __restrict__ S) {
+  __shared__ double sh[kThreads / 32];
+  __shared__ double rz_beta[2];
+  pdl_trigger();
+  pdl_wait();
+  if (*(volatile int*)&S->done) return;
+  BetaHook{partA, nparts, first, par, S, sh, rz_beta}();
+  const double* beta = rz_beta + 1;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p_new[i] = (TK)z[i] + (TK)*beta * p_old[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0) S->rz[par] = rz_beta[0];
+}
+
+template <typename TK>
+struct EpiSpmvDotP {  // q = A p_new; dot: p_new . q (p_new already written)
+  const TK* __restrict__ p_new;
+  TK* __restrict__ q;
+  struct Pre {
+    TK pi;
+  };
+  __device__ __forceinline__ Pre load(int64_t i) const { return {p_new[i]}; }
+  __device__ __forceinline__ double store(int64_t i, const Pre& p, TK t) const {
+    q[i] = t;
+    return (double)p.pi * (double)t;
+  }
+};
+
+template <int BS, typename TK>
 __global__ void __launch_bounds__(kStreamThreads, (StreamDefault<TK, BS, BS>::kCtasPerSm))
-    k_stream_spmv_dot(StreamView m, const TM* __restrict__ z, const TK* __restrict__ p_old, TK* __restrict__ p_new,
-                      TK* __restrict__ q, const double* __restrict__ partA, double* __restrict__ partB, int nparts,
-                      int first, int par, PcgScalars* __restrict__ S) {
+    k_stream_spmv_dot_p(StreamView m, const TK* __restrict__ p_new, TK* __restrict__ q, double* __restrict__ partB,
+                        PcgScalars* __restrict__ S) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ double sh[kStreamThreads / 32];
-  __shared__ double rz_beta[2];
   pdl_trigger();
   bool skipped = false;
   const double dot = stream_rows<TK, BS, BS, typename StreamDefault<TK, BS, BS>::type>(
-      m.tiles, m.n_tiles, m.pack, XPNewS<TK, TM>{z, p_old, rz_beta + 1},
-      EpiSpmvDotS<TK, TM>{z, p_old, rz_beta + 1, p_new, q}, smem, &S->status, &S->done, m.ctl, &skipped,
-      BetaHook{partA, nparts, first, par, S, sh, rz_beta});
+      m.tiles, m.n_tiles, m.pack, XLoad<TK, TK>{p_new}, EpiSpmvDotP<TK>{p_new, q}, smem, &S->status, &S->done,
+      m.ctl, &skipped);
   if (skipped) return;
   write_part(dot, partB, sh);
-  if (blockIdx.x == 0 && threadIdx.x == 0) S->rz[par] = rz_beta[0];
 }
 
 // launch with programmatic stream serialisation: the kernel may begin (and start streaming its
@@ -1304,15 +1307,20 @@ static int pcg_iteration(Solid* s, SolverWork& W, int precond, int k, PcgScalars
   auto spmv_dot = [&](auto bs_tag) {
     constexpr int BS = decltype(bs_tag)::value;
     if (s->fine.packed && s->fine.br == BS) {  // the fine matrix streamed through shared memory
-      auto kern = k_stream_spmv_dot<BS, TK, TM>;
+      auto kern = k_stream_spmv_dot_p<BS, TK>;
       const int g = stream_grid<TK, BS, BS>(kern, s->fine.n_tiles);
+      const int gp = resident_grid(k_pnew<TK, TM>, kThreads, (W.n + kThreads - 1) / kThreads);
       if (g > 0) {
-        const cudaError_t e =
-            launch_pdl(kern, g, kStreamThreads, stream_smem_bytes<TK, BS, BS>(), st, stream_view<TK>(s->fine),
-                       (const TM*)B.z, (const TK*)p_old, p_new, B.q, (const double*)W.partA.p, W.partB.p, W.npA,
-                       (int)(k == 0), par, S);
-        if (e == cudaSuccess) return g;
-        cudaGetLastError();
+        cudaError_t e = launch_pdl(k_pnew<TK, TM>, gp, kThreads, 0, st, W.n, (const TM*)B.z, (const TK*)p_old, p_new,
+                                   (const double*)W.partA.p, W.npA, (int)(k == 0), par, S);
+        if (e == cudaSuccess) {
+          note(W, st, "pcg_pnew", -1, (double)W.n * (sizeof(TM) + 2 * sizeof(TK)));
+          W.launches++;
+          e = launch_pdl(kern, g, kStreamThreads, stream_smem_bytes<TK, BS, BS>(), st, stream_view<TK>(s->fine),
+                         (const TK*)p_new, B.q, W.partB.p, S);
+          if (e == cudaSuccess) return -g;  // negative: the product's bytes are those of a plain SpMV
+        }
+        return 0;  // a failed launch: reported by the error check below
       }
     }
     const int g = resident_grid(k_spmv_dot<BS, TK, TM>, kThreads, (s->n_nodes * 32 + kThreads - 1) / kThreads);
@@ -1321,9 +1329,15 @@ static int pcg_iteration(Solid* s, SolverWork& W, int precond, int k, PcgScalars
     return g;
   };
   const double b_start = W.bytes;
-  const int gsd = s->bs == 3 ? spmv_dot(std::integral_constant<int, 3>{}) : spmv_dot(std::integral_constant<int, 6>{});
+  int gsd = s->bs == 3 ? spmv_dot(std::integral_constant<int, 3>{}) : spmv_dot(std::integral_constant<int, 6>{});
   const double nK = (double)W.n * sizeof(TK), nM = (double)W.n * sizeof(TM);
-  note(W, st, "pcg_spmv_dot", -1, mat_bytes(s->nnzb, s->bs, s->bs, s->n_nodes, sizeof(TK)) + nM + 3 * nK);
+  // the fused product reads z and p_old and writes p_new and q; the split one reads p_new and
+  // writes q (k_pnew counted its own bytes)
+  note(W, st, "pcg_spmv_dot", -1,
+       mat_bytes(s->nnzb, s->bs, s->bs, s->n_nodes, sizeof(TK)) + (gsd < 0 ? 2 * nK : nM + 3 * nK));
+  gsd = gsd < 0 ? -gsd : gsd;
+  WN_CUDA(cudaGetLastError());
+  WN_REQUIRE(gsd > 0, WN_ESTATE, "PCG product: launch failed");
   W.npB = gsd;
   // with the AMG preconditioner, the update also writes the fine level's first smoothing input
   const bool pre_input = precond == 2 && !s->amg->levels.empty();
