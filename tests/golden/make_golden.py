@@ -25,11 +25,19 @@ functions, so both sides see identical inputs.  Fixtures:
                              solid_generator.py:21-213) with the arguments of its test
                              (tests/test_solid_bench.py:18-26): nodes, connectivity, clamped and
                              loaded nodes with their loads, and on that mesh the reference's
-                             F, direct solution and stress field.
+                             F, direct solution and stress field;
+* ``bc_cases.npz``       -- the reference's assembly, direct solve and stresses on a model with
+                             the boundary-condition cases its code distinguishes
+                             (solid_solver.py:67-127): roller supports (one FIXED DOF per node on
+                             three symmetry faces), a fully clamped corner, a duplicated support,
+                             a PRESCRIBED DOF (not applied by the solid path), repeated loads on one
+                             node, a load on a fixed DOF, two materials and elements left on the
+                             default material.
 
     python tests/golden/make_golden.py /path/to/reference structured_block
+    python tests/golden/make_golden.py /path/to/reference bc_cases
 
-makes only the last one.
+make only those.
 """
 
 from __future__ import annotations
@@ -68,6 +76,58 @@ def structured_block(ref: str) -> None:
                          meta["tip_nodes_loaded"]], dtype=np.int64),
         F=F, fixed=np.asarray(fixed, dtype=np.int64), u=u, cell_sig=cell_sig, cell_vm=cell_vm, nodal_vm=nodal_vm)
     print("structured block", meta["n_elements"], "elements,", meta["n_dofs"], "DOFs")
+
+
+def bc_case_model(wnfea, block):
+    """The boundary-condition model on the mesh of ``block`` (a FEAModel of this repository),
+    built with the reference's classes (and mirrored by tests/test_oracle_golden.py)."""
+    from wnfea.boundary.conditions import DOFConstraint, DOFType, SupportDef
+
+    X = block.mesh_nodes
+    rm = wnfea.FEAModel()
+    rm.mesh_nodes = X
+    rm.solid_elements = block.solid_elements
+    rm.materials["Steel"] = wnfea.MaterialDef("Steel", 2.1e11, 0.3, 2.5e8)
+    rm.materials["Alu"] = wnfea.MaterialDef("Alu", 7.0e10, 0.33, 1.0e8)
+    n_el = len(block.solid_elements)
+    rm.solid_materials = {e: "Alu" for e in range(0, n_el, 3)}  # the rest: the default (first) material
+    fixed = lambda: DOFConstraint(DOFType.FIXED)  # noqa: E731
+    for axis, name in ((0, "ux"), (1, "uy"), (2, "uz")):
+        for nid in np.flatnonzero(X[:, axis] <= 1e-12):
+            rm.supports.append(SupportDef(node_id=int(nid), is_geometry_node=False, **{name: fixed()}))
+    corner = int(np.argmin(np.abs(X - X.max(axis=0)).sum(axis=1)))
+    rm.supports.append(wnfea.create_fixed_support(corner, is_geometry_node=False))
+    rm.supports.append(wnfea.create_fixed_support(corner, is_geometry_node=False))  # duplicated
+    mid = int(np.argmin(np.abs(X - 0.5 * X.max(axis=0)).sum(axis=1)))
+    rm.supports.append(SupportDef(node_id=mid, is_geometry_node=False,
+                                  uz=DOFConstraint(DOFType.PRESCRIBED, value=1e-3)))
+    top = np.flatnonzero(X[:, 2] >= X[:, 2].max() - 1e-12)
+    for k, nid in enumerate(top):
+        rm.loads.append(wnfea.LoadDef(node_id=int(nid), is_geometry_node=False, fx=100.0 + k, fz=-500.0))
+    rm.loads.append(wnfea.LoadDef(node_id=int(top[0]), is_geometry_node=False, fy=250.0))  # repeated node
+    rm.loads.append(wnfea.LoadDef(node_id=corner, is_geometry_node=False, fx=1e6))  # on fixed DOFs
+    return rm
+
+
+def bc_cases(ref: str) -> None:
+    builtins.Path = pathlib.Path
+    sys.path.insert(0, ref)
+    sys.path.insert(0, str(ROOT))
+    import wnfea
+    from scipy.sparse.linalg import spsolve
+    from wnfea.solver.solid_solver import assemble_c3d10_sparse_3dof, compute_c3d10_stress_field
+
+    from wnfea_b200.mesh import generate_c3d10_kuhn_block
+
+    block, _ = generate_c3d10_kuhn_block(length=0.3, width=0.2, height=0.1, nx=3, ny=2, nz=2)
+    rm = bc_case_model(wnfea, block)
+    K, F, fixed = assemble_c3d10_sparse_3dof(rm)
+    u = spsolve(K.tocsc(), F)
+    cell_sig, cell_vm, nodal_vm = compute_c3d10_stress_field(rm, u)
+    np.savez_compressed(HERE / "bc_cases.npz", nodes=block.mesh_nodes, conn=block.solid_elements,
+                        K_data=K.data, K_indices=K.indices, K_indptr=K.indptr, F=F,
+                        fixed=np.asarray(fixed, dtype=np.int64), u=u, cell_vm=cell_vm, nodal_vm=nodal_vm)
+    print("bc cases", len(block.solid_elements), "elements,", len(fixed), "fixed DOFs")
 
 
 def main(ref: str) -> None:
@@ -207,6 +267,9 @@ if __name__ == "__main__":
     ref_dir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     if len(sys.argv) > 2 and sys.argv[2] == "structured_block":
         structured_block(ref_dir)
+    elif len(sys.argv) > 2 and sys.argv[2] == "bc_cases":
+        bc_cases(ref_dir)
     else:
         main(ref_dir)
         structured_block(ref_dir)
+        bc_cases(ref_dir)
