@@ -315,6 +315,12 @@ int wn_spmv_bsr_f64(int br, int bc, int64_t n_rows, int64_t n_cols, int64_t nnzb
  * coords (n_el x 10 x 3) and props (n_el x 2) -- host buffers.  Batched form of
  * element_stiffness_c3d10 (c3d10.py:219-249).  WN_EMESH on det J <= 0. */
 int wn_c3d10_element_stiffness(int64_t n_el, const double* coords, const double* props, double* Ke);
+/* Gauss-point Cauchy stresses gp_sig (n_el x 4 x 6: sxx, syy, szz, sxy, syz, szx) and von Mises
+ * gp_vm (n_el x 4) of elements given by coordinates coords (n_el x 10 x 3), props (n_el x 2)
+ * and element displacements u_e (n_el x 30, node-major) -- host buffers.  Batched form of
+ * element_stresses_c3d10 (c3d10.py:286-318). */
+int wn_c3d10_element_stresses(int64_t n_el, const double* coords, const double* props, const double* u_e,
+                              double* gp_sig, double* gp_vm);
 
 /* Element stiffness for callers that must not allocate device memory (no counterpart in the
  * reference).  Code whose device memory belongs to another allocator -- a framework's caching

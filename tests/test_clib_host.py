@@ -223,3 +223,14 @@ def test_assembly_work_items_cover_every_block(which):
         assert y == NH
     if which == "ibeam60":
         assert n_split_blocks > 0 and clen == 6
+
+
+def test_element_api_rejects_bad_shapes():
+    import wnfea_b200 as wn
+
+    with pytest.raises(ValueError):
+        wn.element_stiffness_c3d10(np.zeros((9, 3)), 2e11, 0.3)
+    with pytest.raises(ValueError):
+        wn.element_internal_forces_c3d10(np.zeros((10, 3)), np.zeros(29), 2e11, 0.3)
+    with pytest.raises(ValueError):
+        wn.element_stresses_c3d10(np.zeros((2, 10, 3)), np.zeros(30), 2e11, 0.3)

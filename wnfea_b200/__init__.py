@@ -34,6 +34,7 @@ from .rcm import (
 )
 from .vtu import VTUExporter, export_vtu
 from .mesh import generate_c3d10_structured_block
+from .elements import element_internal_forces_c3d10, element_stiffness_c3d10, element_stresses_c3d10
 from .mixed_precision import FULL_FP64, MIXED_FP32, TRI_PRECISION, PrecisionConfig
 from .solid_solver import (
     assemble_c3d10_sparse_3dof,
@@ -53,4 +54,5 @@ __all__ = [
     "BeamFrame", "ComplianceProblem", "Compliance",
     "apply_rcm_to_model", "compute_matrix_bandwidth", "compute_node_adjacency_matrix", "compute_rcm_order",
     "permute_solution_to_original", "VTUExporter", "export_vtu", "generate_c3d10_structured_block",
+    "element_stiffness_c3d10", "element_internal_forces_c3d10", "element_stresses_c3d10",
 ]

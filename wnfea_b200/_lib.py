@@ -103,6 +103,7 @@ SIGNATURES: dict[str, tuple] = {
     "wn_spmv_bsr_f32_device": (_I, [_I, _I, _I64, _P, _P, _P, _P, _P, _F, _F, _U]),
     "wn_spmv_bsr_f64": (_I, [_I, _I, _I64, _I64, _I64, _P, _P, _P, _P, _P, _D, _D]),
     "wn_c3d10_element_stiffness": (_I, [_I64, _P, _P, _P]),
+    "wn_c3d10_element_stresses": (_I, [_I64, _P, _P, _P, _P, _P]),
     "wn_c3d10_element_stiffness_noalloc": (_I, [_I64, _I64, _P, _P, _P, _P, _U]),
     "wn_c3d10_internal_forces": (_I, [_P, _P, _P, _P, _P, _I, _I]),
     "wn_fint_c3d10_device": (_I, [_P, _P, _P, _U]),

@@ -561,9 +561,12 @@ __global__ void node_gather_kernel(int64_t n_nodes, const int64_t* __restrict__ 
 
 // Cell stresses: mean of the 4 Gauss-point stresses [sxx, syy, szz, sxy, syz, szx] and the
 // mean Gauss-point von Mises (solid_solver.py:341-350, c3d10.py:286-318).
+// Also, when gp_sig / gp_vm are given, the stresses and von Mises of every Gauss point
+// (element_stresses_c3d10, c3d10.py:286-318): gp_sig[(e * 4 + g) * 6 + k], gp_vm[e * 4 + g].
 __global__ void stress_kernel(int64_t n_el, const double* __restrict__ nodes, const int32_t* __restrict__ conn,
                               const double* __restrict__ props, const double* __restrict__ u,
-                              double* __restrict__ cell_sig, double* __restrict__ cell_vm) {
+                              double* __restrict__ cell_sig, double* __restrict__ cell_vm, double* __restrict__ gp_sig,
+                              double* __restrict__ gp_vm) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n_el; e += (int64_t)gridDim.x * blockDim.x) {
     double X[10][3], ue[10][3];
     load_coords(nodes, conn, e, X);
@@ -598,11 +601,19 @@ __global__ void stress_kernel(int64_t n_el, const double* __restrict__ nodes, co
 #pragma unroll
       for (int k = 0; k < 6; ++k) ssum[k] += s[k];
       const double a0 = s[0] - s[1], a1 = s[1] - s[2], a2 = s[2] - s[0];
-      vmsum += sqrt(0.5 * (a0 * a0 + a1 * a1 + a2 * a2 + 6.0 * (s[3] * s[3] + s[4] * s[4] + s[5] * s[5])));
-    }
+      const double vm = sqrt(0.5 * (a0 * a0 + a1 * a1 + a2 * a2 + 6.0 * (s[3] * s[3] + s[4] * s[4] + s[5] * s[5])));
+      vmsum += vm;
+      if (gp_sig) {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) cell_sig[e * 6 + k] = ssum[k] / 4.0;
-    cell_vm[e] = vmsum / 4.0;
+        for (int k = 0; k < 6; ++k) gp_sig[(e * 4 + g) * 6 + k] = s[k];
+        gp_vm[e * 4 + g] = vm;
+      }
+    }
+    if (cell_sig) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) cell_sig[e * 6 + k] = ssum[k] / 4.0;
+      cell_vm[e] = vmsum / 4.0;
+    }
   }
 }
 
@@ -817,7 +828,7 @@ int launch_stress(int64_t n_el, int64_t n_nodes, const double* nodes, const int3
                   double* nodal_vm, cudaStream_t st) {
   if (n_el > 0) {
     const int grid = grid_for(n_el, 1, 128, 16);
-    stress_kernel<<<grid, 128, 0, st>>>(n_el, nodes, conn, props, u, cell_sig, cell_vm);
+    stress_kernel<<<grid, 128, 0, st>>>(n_el, nodes, conn, props, u, cell_sig, cell_vm, nullptr, nullptr);
     WN_CUDA(cudaGetLastError());
   }
   if (n_nodes > 0) {
@@ -825,6 +836,15 @@ int launch_stress(int64_t n_el, int64_t n_nodes, const double* nodes, const int3
     nodal_average_kernel<<<grid, 256, 0, st>>>(n_nodes, inc_ptr, inc_ea, cell_vm, nodal_vm);
     WN_CUDA(cudaGetLastError());
   }
+  return 0;
+}
+
+int launch_gp_stress(int64_t n_el, const double* nodes, const int32_t* conn, const double* props, const double* u,
+                     double* gp_sig, double* gp_vm, cudaStream_t st) {
+  if (n_el == 0) return 0;
+  const int grid = grid_for(n_el, 1, 128, 16);
+  stress_kernel<<<grid, 128, 0, st>>>(n_el, nodes, conn, props, u, nullptr, nullptr, gp_sig, gp_vm);
+  WN_CUDA(cudaGetLastError());
   return 0;
 }
 

@@ -641,6 +641,28 @@ int wn_spmv_bsr_f64(int br, int bc, int64_t n_rows, int64_t n_cols, int64_t nnzb
   return 0;
 }
 
+int wn_c3d10_element_stresses(int64_t n_el, const double* coords, const double* props, const double* u_e,
+                               double* gp_sig, double* gp_vm) {
+  WN_REQUIRE(n_el >= 0 && (n_el == 0 || (coords && props && u_e && gp_sig && gp_vm)), WN_EINVAL,
+             "wn_c3d10_element_stresses: null argument");
+  if (n_el == 0) return 0;
+  // each element gets its own 10 nodes: nodes = coords, conn[e][a] = 10 e + a, u = u_e
+  std::vector<int32_t> conn(n_el * 10);
+  for (int64_t k = 0; k < n_el * 10; ++k) conn[k] = (int32_t)k;
+  DArray<double> dn, dp, du, ds, dv;
+  DArray<int32_t> dc;
+  WN_CHECK(dn.upload(coords, n_el * 30));
+  WN_CHECK(dp.upload(props, n_el * 2));
+  WN_CHECK(du.upload(u_e, n_el * 30));
+  WN_CHECK(dc.upload(conn));
+  WN_CHECK(ds.alloc(n_el * 24));
+  WN_CHECK(dv.alloc(n_el * 4));
+  WN_CHECK(launch_gp_stress(n_el, dn.p, dc.p, dp.p, du.p, ds.p, dv.p, 0));
+  WN_CUDA(cudaMemcpy(gp_sig, ds.p, ds.bytes(), cudaMemcpyDeviceToHost));
+  WN_CUDA(cudaMemcpy(gp_vm, dv.p, dv.bytes(), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
 int wn_c3d10_element_stiffness(int64_t n_el, const double* coords, const double* props, double* Ke) {
   WN_REQUIRE(n_el >= 0 && (n_el == 0 || (coords && props && Ke)), WN_EINVAL,
              "wn_c3d10_element_stiffness: null argument");

@@ -53,6 +53,9 @@ int launch_node_gather(int64_t n_nodes, const int64_t* inc_ptr, const int32_t* i
 // ceil(nn / 1024) + 1 int64 scratch; flags[0] is set when a node index is out of range.
 int launch_build_incidence(int64_t nn, int64_t ne, const int32_t* conn, int32_t* counts, int64_t* inc_ptr,
                            int32_t* inc, int64_t* scan, int* flags, cudaStream_t st);
+// Gauss-point stresses gp_sig (n_el x 4 x 6) and von Mises gp_vm (n_el x 4), u at 3 DOFs per node
+int launch_gp_stress(int64_t n_el, const double* nodes, const int32_t* conn, const double* props, const double* u,
+                     double* gp_sig, double* gp_vm, cudaStream_t st);
 int launch_stress(int64_t n_el, int64_t n_nodes, const double* nodes, const int32_t* conn, const double* props,
                   const double* u, const int64_t* inc_ptr, const int32_t* inc_ea, double* cell_sig, double* cell_vm,
                   double* nodal_vm, cudaStream_t st);
