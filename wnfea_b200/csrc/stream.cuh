@@ -19,8 +19,8 @@
 //     signals completion through an mbarrier per stage (expect_tx bytes); the producer warp
 //     holds the next 32 tile descriptors, one per lane, so no copy waits on a descriptor load;
 //   * consumer warps wait on the stage, compute their rows from shared memory (G lanes per
-//     block row, lane l taking the row's blocks l, l + G, ... -- the assignment and summation
-//     order of the register kernels in spmv.cuh -- with U blocks' gathers in flight per lane),
+//     block row, lane l taking the row's blocks l, l + G, ... -- the assignment of the register
+//     kernels in spmv.cuh, with the shape's own G -- with U blocks' gathers in flight per lane),
 //     and release the stage through a second mbarrier;
 //   * CTAs are persistent and take fixed runs of tiles, so the per-CTA dot partials come out in
 //     a fixed order (deterministic two-stage dots);
@@ -96,22 +96,27 @@ struct StreamCfg {
 
 // The shapes the library launches, per value type and block shape (all 8 consumer warps + 1
 // producer warp: kStreamThreads threads).  3x3 (fine level; measured on the 1M-DOF I-beam,
-// 17,125 tiles: FP32 SpMV 64 us with 8 consumer warps, 3 stages of 20.7 KB and 3 CTAs per SM,
-// against 72-90 us for 12-16 warps at 2 CTAs or 4-8 stages at 1 CTA; FP64 104 us with 2 stages
-// of 39 KB and 2 CTAs per SM).  6x6 (AMG level 1, rows of ~54 blocks) and 6x3 (restriction,
-// rows of ~105 blocks): a warp per row; 3x6 (prolongation, rows of ~5.5 blocks): 4 lanes per
-// row, two blocks in flight per lane.
+// 17,125 tiles of ~20 rows of ~25 blocks: FP32 SpMV 63 us with 8 consumer warps, 3 stages of
+// 20.7 KB and 3 CTAs per SM, against 72-90 us for 12-16 warps at 2 CTAs or 4-8 stages at 1 CTA;
+// in FP32, 8 lanes per row with 4 blocks in flight each (four rows per warp: a tile in one pass
+// of the 8 warps, three shuffle levels) ran the fused V-cycle passes 12-16 % faster than 16
+// lanes x 2 blocks (0.74 vs 0.62 of HBM for the Chebyshev step; 4 x 8 and two rows per group
+// were slower); FP64 104 us with 2 stages of 39 KB and 2 CTAs per SM, 8 lanes x 4 blocks
+// as well: 3 % off the FP64 solve against 16 x 2).  6x6 (AMG level 1, rows
+// of ~54 blocks) and 6x3 (restriction, rows of ~105 blocks): a warp per row (16 lanes with one
+// or two blocks each were slower); 3x6 (prolongation, rows of ~5.5 blocks): 4 lanes per row,
+// two blocks in flight per lane, two rows per lane group (5 % faster than one).
 constexpr int kStreamThreads = 9 * 32;
 template <typename T, int BR, int BC>
 struct StreamDefault;
 template <>
 struct StreamDefault<float, 3, 3> {
-  using type = StreamCfg<kStreamCap, kStreamRowCap, 8, 16, 3, 2>;
+  using type = StreamCfg<kStreamCap, kStreamRowCap, 8, 8, 3, 4>;
   static constexpr int kCtasPerSm = 3;
 };
 template <>
 struct StreamDefault<double, 3, 3> {
-  using type = StreamCfg<kStreamCap, kStreamRowCap, 8, 16, 2, 2>;
+  using type = StreamCfg<kStreamCap, kStreamRowCap, 8, 8, 2, 4>;
   static constexpr int kCtasPerSm = 2;
 };
 template <typename T>
@@ -137,7 +142,7 @@ struct StreamDefault<T, 6, 3> {
 };
 template <typename T>
 struct StreamDefault<T, 3, 6> {
-  using type = StreamCfg<512, kStreamRowCap, 8, 4, 2, 2>;
+  using type = StreamCfg<512, kStreamRowCap, 8, 4, 2, 2, 2>;
   static constexpr int kCtasPerSm = sizeof(T) == 4 ? 2 : 1;
 };
 
