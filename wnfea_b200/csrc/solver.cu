@@ -981,11 +981,11 @@ static cudaError_t launch_pdl(void (*kern)(KArgs...), int grid, int threads, siz
   return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
-// grid of a streamed kernel (one persistent wave), 0 if it cannot run on this device
-template <typename T, int BR, int BC, typename K>
+// grid of a streamed kernel of shape CFG (one persistent wave), 0 if it cannot run on this device
+template <typename T, int BR, int BC, typename CFG = typename StreamDefault<T, BR, BC>::type, typename K>
 static int stream_grid(K kern, int n_tiles) {
   const int per_sm =
-      stream_ctas_per_sm(reinterpret_cast<const void*>(kern), kStreamThreads, stream_smem_bytes<T, BR, BC>());
+      stream_ctas_per_sm(reinterpret_cast<const void*>(kern), kStreamThreads, stream_smem_bytes<T, BR, BC, CFG>());
   if (per_sm < 1) return 0;
   return std::max(1, std::min(n_tiles, kNumSMs * per_sm));
 }
@@ -996,11 +996,12 @@ template <typename T, int BR, int BC, typename XF, typename EPI, typename SHAPE 
 static bool launch_stream_rows(const StreamMat& m, XF xf, EPI epi, double* part, PcgScalars* S, cudaStream_t st,
                                int* grid_out) {
   if (!m.packed || m.br != BR || m.bc != BC) return false;
+  using CFG = typename SHAPE::type;
   auto kern = k_stream_rows<T, BR, BC, XF, EPI, SHAPE>;
-  const int g = stream_grid<T, BR, BC>(kern, m.n_tiles);
+  const int g = stream_grid<T, BR, BC, CFG>(kern, m.n_tiles);
   if (g == 0) return false;
-  if (launch_pdl(kern, g, kStreamThreads, stream_smem_bytes<T, BR, BC>(), st, stream_view<T>(m), xf, epi, part, S) !=
-      cudaSuccess) {
+  if (launch_pdl(kern, g, kStreamThreads, stream_smem_bytes<T, BR, BC, CFG>(), st, stream_view<T>(m), xf, epi, part,
+                 S) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }

@@ -131,8 +131,7 @@ struct StreamShort66 {
   using type = StreamCfg<256, kStreamRowCap, 8, 8, 2, 1>;
   static constexpr int kCtasPerSm = sizeof(T) == 4 ? 2 : 1;
   static_assert(type::kCap == StreamDefault<T, 6, 6>::type::kCap &&
-                    type::kRowCap == StreamDefault<T, 6, 6>::type::kRowCap &&
-                    type::kStages == StreamDefault<T, 6, 6>::type::kStages,
+                    type::kRowCap == StreamDefault<T, 6, 6>::type::kRowCap,
                 "the short-row shape streams the default 6x6 tiles");
 };
 template <typename T>
