@@ -775,16 +775,19 @@ def run_ours(args):
         K2.system.close()
         del m2, K2, u2
 
-    # the other modes on the same I-beam, each solved once (after one warm-up for the graphs)
+    # the other modes on the same I-beam, each solved once (after one warm-up for the graphs); the
+    # FP32 refinement gets up to 40 outer passes (the reference's loop stops at 10): each pass
+    # contracts the FP64 residual by only about cond(K) x FP32 rounding on this beam
     modes = {}
-    for name, precision, precond, max_iter in (("fp32_ir", 2, 2, 5000), ("jacobi_fp64", 0, 1, 200000),
-                                               ("block_jacobi_fp64", 0, 3, 200000)):
+    for name, precision, precond, max_iter, max_outer in (("fp32_ir", 2, 2, 20000, 40),
+                                                          ("jacobi_fp64", 0, 1, 200000, 10),
+                                                          ("block_jacobi_fp64", 0, 3, 200000, 10)):
         if rank != 0 or (args.skip_jacobi and precond != 2):
             continue
-        solve(precision, precond, max_iter)
+        solve(precision, precond, max_iter, max_outer)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        st = solve(precision, precond, max_iter)
+        st = solve(precision, precond, max_iter, max_outer)
         e1.record(stream)
         torch.cuda.synchronize()
         modes[name] = {"ms": e0.elapsed_time(e1), "its": st.iterations, "outer": st.outer_iterations,

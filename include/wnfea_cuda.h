@@ -158,8 +158,8 @@ typedef struct wn_amg_params {
   double strength_theta;   /* strong if |A_ij|_F >= theta sqrt(|A_ii|_F |A_jj|_F)      (0.08) */
   int max_levels;          /* including the coarsest                                   (10)   */
   int coarse_size;         /* stop coarsening at <= this many scalar DOFs               (1500) */
-  int smoother_degree;     /* Chebyshev degree per pre-/post-smoothing                  (2)    */
-  double cheb_lower;       /* lambda_min = cheb_lower * lambda_max                      (1/30) */
+  int smoother_degree;     /* Chebyshev degree per pre-/post-smoothing                  (1)    */
+  double cheb_lower;       /* lambda_min = cheb_lower * lambda_max                      (1/16) */
   double cheb_safety;      /* lambda_max = cheb_safety * rho(D^-1 A) estimate          (1.1)  */
   double prolong_omega;    /* P = (I - prolong_omega / rho * D^-1 A) P_tent             (4/3)  */
   int smooth_prolongator;  /* 1 = smoothed aggregation, 0 = plain (tentative) aggregation      */

@@ -19,7 +19,7 @@ from __future__ import annotations
 import numpy as np
 
 
-def cheb_coefficients(rho, degree, lower=1.0 / 30.0, safety=1.1):
+def cheb_coefficients(rho, degree, lower=1.0 / 16.0, safety=1.1):
     lmax = safety * rho
     lmin = lower * lmax
     theta, delta = 0.5 * (lmax + lmin), 0.5 * (lmax - lmin)
@@ -45,7 +45,7 @@ def _cheb(A, dinv, b, x, inv_theta, c1, c2):
     return x
 
 
-def vcycle(K0, hier, b, degree=2, level=0, dtype=np.float64, lower=1.0 / 30.0, safety=1.1):
+def vcycle(K0, hier, b, degree=1, level=0, dtype=np.float64, lower=1.0 / 16.0, safety=1.1):
     """z = M^-1 b for the exported hierarchy; all arithmetic in ``dtype``."""
     if level == len(hier.levels):
         return (hier.coarse_inv @ b.astype(np.float64)).astype(dtype)

@@ -32,17 +32,19 @@ def _oracle_K(m):
 
 
 @pytest.mark.parametrize("which", ["c1", "ibeam"])
-def test_vcycle_matches_oracle(which):
+@pytest.mark.parametrize("degree", [1, 2, 3])
+def test_vcycle_matches_oracle(which, degree):
     import torch
 
     m = generate_c3d10_kuhn_block()[0] if which == "c1" else _ibeam()
     K, F, fixed = assemble_c3d10_sparse_3dof(m)
     s = K.system
-    s.amg_setup(AMGParams(coarse_size=300))
+    prm = AMGParams(coarse_size=300, smoother_degree=degree, cheb_lower=1.0 / 16.0 if degree == 1 else 1.0 / 30.0)
+    s.amg_setup(prm)
     H = export_system_hierarchy(s)
     Kfull = K.to_bsr().tocsr()  # with explicit zeros, as the GPU sees it
     r = np.random.default_rng(1).standard_normal(K.shape[0])
-    z_ref = oamg.vcycle(Kfull, H, r)
+    z_ref = oamg.vcycle(Kfull, H, r, degree=degree, lower=prm.cheb_lower, safety=prm.cheb_safety)
     dr = torch.from_numpy(r).cuda()
     dz = torch.empty_like(dr)
     _lib.call("wn_amg_vcycle_device", s.handle, 0, dr.data_ptr(), dz.data_ptr(), 0)
@@ -256,8 +258,8 @@ def test_profiled_solve_accounts_every_kernel():
     m = _ibeam(12, seed=4)
     K, F, _ = assemble_c3d10_sparse_3dof(m)
     s = K.system
-    s.amg_setup()
-    for precision in (0, 1):
+    for degree, precision in ((1, 0), (1, 1), (2, 0), (2, 1)):
+        s.amg_setup(AMGParams(smoother_degree=degree))
         u0, st0 = s.solve(F, rtol=1e-8, precision=precision)
         u1, st1 = s.solve(F, rtol=1e-8, precision=precision, profile=True)
         assert st0["status"] == 0 and st1["status"] == 0
@@ -265,8 +267,13 @@ def test_profiled_solve_accounts_every_kernel():
         assert st0["algorithmic_bytes"] > 0 and abs(st1["algorithmic_bytes"] - st0["algorithmic_bytes"]) <= (
             1e-12 * st0["algorithmic_bytes"])
         prof = s.profile_table()
-        for name in ("pcg_spmv_dot", "pcg_update", "l0.pre_smooth", "l0.residual", "l0.restrict", "l0.prolong",
-                     "l0.post_smooth", "l0.post_cheb", "coarse", "outer_residual"):
+        names = ["pcg_spmv_dot", "pcg_update", "l0.pre_smooth", "l0.restrict", "l0.prolong", "l0.post_smooth", "coarse",
+                 "outer_residual"]
+        if degree >= 2:  # the residual after the pre-smoother and the second post-smoothing step
+            names += ["l0.residual", "l0.post_cheb"]
+        else:
+            assert "l0.residual" not in prof and "l0.post_cheb" not in prof
+        for name in names:
             assert name in prof, (name, sorted(prof))
         its = st1["iterations"]
         assert prof["pcg_spmv_dot"][0] == its and prof["pcg_update"][0] == its

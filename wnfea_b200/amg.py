@@ -6,7 +6,9 @@ exposes its knobs (``AMGParams`` = ``wn_amg_params``) and reads a hierarchy back
 matrices, for inspection and for the parity tests.  The reference's counterpart is the
 beam-only ``BlockBeamAMGPreconditioner`` (wnfea/solver/amg_preconditioner.py:147-661);
 its parameters map as: ``max_levels`` (:159), ``coarse_size`` (:159, in DOFs), the
-Jacobi weight 0.67 (:449) is replaced by a Chebyshev smoother of ``smoother_degree``.
+Jacobi weight 0.67 (:449) is replaced by a Chebyshev smoother of ``smoother_degree`` (by default
+degree 1: one Jacobi step before and one after the coarse correction, as the reference's V-cycle
+takes (:504-536), weighted 1 / theta for the smoothing interval [lmax / 16, lmax]).
 """
 
 from __future__ import annotations
@@ -26,8 +28,8 @@ class AMGParams:
     strength_theta: float = 0.08
     max_levels: int = 10
     coarse_size: int = 1500
-    smoother_degree: int = 2
-    cheb_lower: float = 1.0 / 30.0
+    smoother_degree: int = 1
+    cheb_lower: float = 1.0 / 16.0
     cheb_safety: float = 1.1
     prolong_omega: float = 4.0 / 3.0
     smooth_prolongator: int = 1

@@ -36,8 +36,8 @@ wn_amg_params amg_default_params() {
   p.strength_theta = 0.08;
   p.max_levels = 10;
   p.coarse_size = 1500;
-  p.smoother_degree = 2;
-  p.cheb_lower = 1.0 / 30.0;
+  p.smoother_degree = 1;
+  p.cheb_lower = 1.0 / 16.0;
   p.cheb_safety = 1.1;
   p.prolong_omega = 4.0 / 3.0;
   p.smooth_prolongator = 1;
