@@ -779,7 +779,8 @@ def run_ours(args):
     # FP32 refinement gets up to 40 outer passes (the reference's loop stops at 10): each pass
     # contracts the FP64 residual by only about cond(K) x FP32 rounding on this beam
     modes = {}
-    for name, precision, precond, max_iter, max_outer in (("fp32_ir", 2, 2, 20000, 40),
+    for name, precision, precond, max_iter, max_outer in (("fp16_vcycle", 3, 2, 2000, 10),
+                                                          ("fp32_ir", 2, 2, 20000, 40),
                                                           ("jacobi_fp64", 0, 1, 200000, 10),
                                                           ("block_jacobi_fp64", 0, 3, 200000, 10)):
         if rank != 0 or (args.skip_jacobi and precond != 2):

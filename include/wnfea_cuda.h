@@ -179,7 +179,8 @@ int wn_amg_default_params(wn_amg_params* out);
  * FP64 and FP32 copies).  params NULL = defaults.  Re-run after every re-assembly. */
 int wn_amg_setup(void* h, const wn_amg_params* params);
 
-/* One V-cycle z = M^-1 r at the finest level (precision 0: double r/z, 1: float r/z).
+/* One V-cycle z = M^-1 r at the finest level (precision 0: double r/z, 1: float r/z, 3: float
+ * r/z through the FP16 fine level of solve precision 3).
  * Device pointers (the preconditioner apply of hip_amg_apply_vcycle_device,
  * hip_kernels.cpp:2080-2340). */
 int wn_amg_vcycle_device(void* h, int precision, const void* d_r, void* d_z, uintptr_t stream);
@@ -225,7 +226,13 @@ typedef struct wn_solve_params {
                            FP32 (AMG: FP32 V-cycle values, vectors and accumulation, FP64
                            coarsest inverse), inside the FP64 true-residual loop;
                          2 FP32 PCG (FP32 SpMV and preconditioner, FP64 dots) inside FP64
-                           iterative refinement (the scheme of solid_solver.py:271-300) */
+                           iterative refinement (the scheme of solid_solver.py:271-300);
+                         3 as 1, with the V-cycle's fine level on the equilibrated matrix
+                           S K S, S = diag(K)^-1/2, stored in FP16 (FP32 arithmetic and
+                           vectors; the FP16 preconditioner of the reference's TRI_PRECISION,
+                           mixed_precision.py:96-103, used on every iteration).  AMG on a
+                           C3D10 system with the streamed fine level only (else WN_EINVAL /
+                           WN_ESTATE)                                                   */
   double inner_rtol;  /* mixed: inner relative tolerance (<= 0: max(1e-4, rtol))      */
   int max_outer;      /* mixed: refinement steps (<= 0: 10)                           */
   int chunk;          /* iterations per CUDA-graph replay / host convergence check    */

@@ -234,3 +234,11 @@ def test_element_api_rejects_bad_shapes():
         wn.element_internal_forces_c3d10(np.zeros((10, 3)), np.zeros(29), 2e11, 0.3)
     with pytest.raises(ValueError):
         wn.element_stresses_c3d10(np.zeros((2, 10, 3)), np.zeros(30), 2e11, 0.3)
+
+
+def test_precision_presets_select_solver_modes():
+    import wnfea_b200 as wn
+
+    assert wn.MIXED_FP32.solver_precision == "mixed_fp32"
+    assert wn.FULL_FP64.solver_precision == "fp64"
+    assert wn.TRI_PRECISION.solver_precision == "mixed_fp16"  # the FP16 V-cycle (solve precision 3)

@@ -139,9 +139,14 @@ struct SolverWork {
   DArray<float> binv32;
   PcgVecs<double> p64;
   PcgVecs<float> p32;
-  // captured chunk graphs: [mode 0 fp64 / 1 mixed / 2 fp32]
+  // the FP16 V-cycle (solve precision 3): set for the solve's duration; s = diag(K)^-1/2 of the
+  // current matrix (FP64 for the FP16 pack, FP32 for the vectors) and q = 1 / s
+  bool half = false;
+  DArray<double> s64;
+  DArray<float> s32, q32;
+  // captured chunk graphs: [mode 0 fp64 / 1 mixed / 2 fp32 / 3 mixed with the FP16 V-cycle]
   //                        [preconditioner 0 none / 1 jacobi / 2 amg / 3 block jacobi]
-  GraphCache graphs[3][4];
+  GraphCache graphs[4][4];
   int64_t launches = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaStream_t own = nullptr;  // used when the caller passes the legacy default stream

@@ -133,6 +133,7 @@ int make_bsr6_system(int64_t n, const int32_t* rp, const int32_t* ci, const doub
   WN_CHECK(s->fine.make_plan(rp, n, 6, 6));
   WN_CHECK(s->fine.pack(s->row_ptr.p, s->col_idx.p, s->k32.p, s->k64.p, 0, 0));
   WN_CUDA(cudaDeviceSynchronize());
+  ++s->values_version;
   s->assembled = true;
   s->bcs_applied = fixed != nullptr;
   *out = s.release();
@@ -458,6 +459,7 @@ int wn_assemble_c3d10_device(void* h, const double* d_props, int apply_bcs, uint
     // tile-major copies for the streamed fine-level kernels
     if (s->stream_fine) WN_CHECK(s->fine.pack(s->row_ptr.p, s->col_idx.p, s->k32.p, s->k64.p, s->nnzb, st));
   }
+  ++s->values_version;
   int flag = 0;
   WN_CHECK(read_flag(s, st, &flag));
   WN_REQUIRE(flag == 0, WN_EMESH, "wn_assemble_c3d10: non-positive Jacobian determinant in a C3D10 element");

@@ -62,7 +62,8 @@ int wn_amg_setup(void* h, const wn_amg_params* params) {
 }
 
 int wn_amg_vcycle_device(void* h, int precision, const void* d_r, void* d_z, uintptr_t stream) {
-  WN_REQUIRE(h && d_r && d_z && (precision == 0 || precision == 1), WN_EINVAL, "wn_amg_vcycle_device: bad argument");
+  WN_REQUIRE(h && d_r && d_z && (precision == 0 || precision == 1 || precision == 3), WN_EINVAL,
+             "wn_amg_vcycle_device: bad argument");
   Solid* s = reinterpret_cast<Solid*>(h);
   WN_CUDA(cudaSetDevice(s->device));
   return amg_vcycle(s, precision, d_r, d_z, (cudaStream_t)stream);

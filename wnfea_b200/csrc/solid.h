@@ -59,6 +59,7 @@ struct Solid {
   bool batch_stage_x = false;   // wn_solid_set_batch_staging: batched fine level with x staged per tile
   bool assembled = false;
   bool bcs_applied = false;
+  uint64_t values_version = 0;  // bumped whenever the matrix values change (the FP16 pack's tag)
   std::unique_ptr<AmgHierarchy> amg;
   std::unique_ptr<SolverWork> work;
   std::unique_ptr<BlockWork> bwork;

@@ -73,6 +73,12 @@ struct XD0 {  // d0_j = dinv_j b_j / theta   (first Chebyshev step from a zero g
   __device__ __forceinline__ T operator()(int64_t j) const { return dinv[j] * b[j] * inv_theta; }
 };
 template <typename T>
+struct XD0U {  // the same with a unit diagonal (the FP16 V-cycle's equilibrated fine level)
+  const T* __restrict__ b;
+  T inv_theta;
+  __device__ __forceinline__ T operator()(int64_t j) const { return b[j] * inv_theta; }
+};
+template <typename T>
 struct XPNew {  // p_j = z_j + beta p_old_j
   const T* __restrict__ z;
   const T* __restrict__ p;
@@ -212,13 +218,14 @@ __global__ void __launch_bounds__(kThreads, (BS == 3) ? kMinBlocks : 1) k_residu
 }
 
 // y = A x (accumulate = 0) or y += A x (accumulate = 1) for a BR x BC block-contiguous
-// matrix; G lanes per block row (32 / G rows per warp) so that short rows (the prolongators)
-// still fill the warp.
+// matrix, (A x)_i scaled by ys_i when ys is given; G lanes per block row (32 / G rows per
+// warp) so that short rows (the prolongators) still fill the warp.
 template <int BR, int BC, int G, typename T>
 __global__ void __launch_bounds__(kThreads) k_level_spmv(int64_t n_rows, const int32_t* __restrict__ rp,
                                                          const int32_t* __restrict__ ci, const T* __restrict__ av,
                                                          const T* __restrict__ x, T* __restrict__ y, int accumulate,
-                                                         const PcgScalars* __restrict__ S) {
+                                                         const PcgScalars* __restrict__ S,
+                                                         const T* __restrict__ ys = nullptr) {
   pdl_trigger();  // dependents launched programmatically may start their prologue
   if (S->done) return;
   constexpr int RPW = 32 / G;
@@ -233,7 +240,7 @@ __global__ void __launch_bounds__(kThreads) k_level_spmv(int64_t n_rows, const i
     group_block_row<BR, BC, G, kAoS, T, T>(rp, ci, av, 0, row, active, XLoad<T, T>{x}, acc, gl);
     if (active && gl < BR) {
       const int64_t i = row * BR + gl;
-      const T v = pick<BR>(acc, gl);
+      const T v = (ys ? ys[i] : T(1)) * pick<BR>(acc, gl);
       y[i] = accumulate ? y[i] + v : v;
     }
   }
@@ -242,20 +249,20 @@ __global__ void __launch_bounds__(kThreads) k_level_spmv(int64_t n_rows, const i
 // launch k_level_spmv with a group size matched to the mean row length
 template <int BR, int BC, typename T>
 static void level_spmv_rows(const DevBsr& M, const T* vals, const T* x, T* y, int accumulate, const PcgScalars* S,
-                            cudaStream_t st) {
+                            cudaStream_t st, const T* ys = nullptr) {
   const double avg = M.n_rows ? (double)M.nnzb / (double)M.n_rows : 0.0;
   if (avg >= 24.0) {
     auto k = k_level_spmv<BR, BC, 32, T>;
     k<<<resident_grid(k, kThreads, (M.n_rows * 32 + kThreads - 1) / kThreads), kThreads, 0, st>>>(
-        M.n_rows, M.rp.p, M.ci.p, vals, x, y, accumulate, S);
+        M.n_rows, M.rp.p, M.ci.p, vals, x, y, accumulate, S, ys);
   } else if (avg >= 12.0) {
     auto k = k_level_spmv<BR, BC, 16, T>;
     k<<<resident_grid(k, kThreads, (M.n_rows * 16 + kThreads - 1) / kThreads), kThreads, 0, st>>>(
-        M.n_rows, M.rp.p, M.ci.p, vals, x, y, accumulate, S);
+        M.n_rows, M.rp.p, M.ci.p, vals, x, y, accumulate, S, ys);
   } else {
     auto k = k_level_spmv<BR, BC, 8, T>;
     k<<<resident_grid(k, kThreads, (M.n_rows * 8 + kThreads - 1) / kThreads), kThreads, 0, st>>>(
-        M.n_rows, M.rp.p, M.ci.p, vals, x, y, accumulate, S);
+        M.n_rows, M.rp.p, M.ci.p, vals, x, y, accumulate, S, ys);
   }
 }
 
@@ -330,11 +337,12 @@ __global__ void __launch_bounds__(kThreads) k_coarse(int64_t n, const double* __
 // PCG kernels
 // ---------------------------------------------------------------------------------------
 
-// r = b, x = 0, rm = (TM) b (if rm != null), partC = b . b (zero-RHS handling in k_init_scalars)
+// r = b, x = 0, rm = (TM) b (if rm != null; times rsc_i when rsc is given: the FP16 V-cycle's
+// scaled input), partC = b . b (zero-RHS handling in k_init_scalars)
 template <typename TK, typename TM>
 __global__ void __launch_bounds__(kThreads) k_init_vecs(int64_t n, const TK* __restrict__ b, TK* __restrict__ x,
                                                         TK* __restrict__ r, TM* __restrict__ rm,
-                                                        double* __restrict__ partC) {
+                                                        double* __restrict__ partC, const TM* __restrict__ rsc) {
   pdl_trigger();  // dependents launched programmatically may start their prologue
   __shared__ double sh[kThreads / 32];
   double s = 0.0;
@@ -342,10 +350,27 @@ __global__ void __launch_bounds__(kThreads) k_init_vecs(int64_t n, const TK* __r
     const TK v = b[i];
     r[i] = v;
     x[i] = TK(0);
-    if (rm) rm[i] = (TM)v;
+    if (rm) rm[i] = rsc ? rsc[i] * (TM)v : (TM)v;
     s += (double)v * (double)v;
   }
   write_part(s, partC, sh);
+}
+
+// The equilibration of the FP16 V-cycle from the fine matrix's diagonal: s = diag(K)^-1/2
+// (1 where the diagonal is not positive), q = 1 / s.
+__global__ void k_fill_scale(int64_t n_rows, int64_t nnzb, const int32_t* __restrict__ diag_block,
+                             const double* __restrict__ k64, double* __restrict__ s64, float* __restrict__ s32,
+                             float* __restrict__ q32) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_rows * 3;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = t / 3;
+    const int c = (int)(t - row * 3);
+    const double dv = k64[(int64_t)(c * 4) * nnzb + diag_block[row]];
+    const double q = dv > 0.0 ? sqrt(dv) : 1.0;
+    s64[t] = 1.0 / q;
+    s32[t] = (float)(1.0 / q);
+    q32[t] = (float)q;
+  }
 }
 
 __global__ void k_init_scalars(PcgScalars* S, const double* __restrict__ partC, int nparts, double rtol,
@@ -541,7 +566,8 @@ __global__ void __launch_bounds__(kThreads) k_update(int64_t n, TK* __restrict__
                                                      const TK* __restrict__ q, const double* __restrict__ partB,
                                                      double* __restrict__ partC, int nparts, int par,
                                                      PcgScalars* __restrict__ S, TM* __restrict__ d0,
-                                                     const TM* __restrict__ dinv, TM inv_theta) {
+                                                     const TM* __restrict__ dinv, TM inv_theta,
+                                                     const TM* __restrict__ rsc) {
   pdl_trigger();  // dependents launched programmatically may start their prologue
   __shared__ double sh[kThreads / 32];
   if (S->done) return;
@@ -560,7 +586,8 @@ __global__ void __launch_bounds__(kThreads) k_update(int64_t n, TK* __restrict__
     x[i] += a * p[i];
     const TK ri = r[i] - a * q[i];
     r[i] = ri;
-    if (rm) rm[i] = (TM)ri;
+    // rsc: the FP16 V-cycle's input is S r (and its first smoothing input S r / theta, dinv = S)
+    if (rm) rm[i] = rsc ? rsc[i] * (TM)ri : (TM)ri;
     // the next V-cycle's first smoothing input (x_j = D^-1 b_j / theta with b = r in the
     // preconditioner's precision), so that its streamed kernel gathers one vector, not two
     if (d0) d0[i] = dinv[i] * (TM)ri * inv_theta;
@@ -735,8 +762,28 @@ __global__ void k_fill_dinv(int64_t n_rows, int bs, int64_t nnzb, const int32_t*
 // k_post_first / k_spmv_dot on the 3x3 fine matrix, with the matrix streamed through shared
 // memory by bulk async copies (stream.cuh).  Each epilogue loads the row's own operands
 // before the row product (load) and writes its results after it (store).
+// With SC (the FP16 V-cycle) the fine level runs on the equilibrated matrix S A S (unit
+// diagonal: dinv is not read) with its vectors in the scaled space (x^ = S^-1 x, b^ = S b);
+// the epilogues then map back where the fine level hands a vector on: the residual to the
+// restriction (rs = S^-1), the V-cycle's output (os = S); a null scale pointer is 1.
+// Without SC the scale pointers are not read.
 // ---------------------------------------------------------------------------------------
-template <typename T>
+template <bool SC, typename T>
+__device__ __forceinline__ T scale_or_one(const T* __restrict__ s, int64_t i) {
+  if constexpr (SC)
+    return s ? s[i] : T(1);
+  else
+    return T(1);
+}
+template <bool SC, typename T>
+__device__ __forceinline__ T diag_inv(const T* __restrict__ dinv, int64_t i) {
+  if constexpr (SC)
+    return T(1);
+  else
+    return dinv[i];
+}
+
+template <typename T, bool SC = false>
 struct EpiPreFirst {
   const T* __restrict__ b;
   const T* __restrict__ dinv;
@@ -747,15 +794,18 @@ struct EpiPreFirst {
   T* __restrict__ r;
   T* __restrict__ d;
   T* __restrict__ res;
+  const T* __restrict__ rs = nullptr;  // residual scale (deg 1)
   struct Pre {
-    T bi, di;
+    T bi, di, si;
   };
-  __device__ __forceinline__ Pre load(int64_t i) const { return {b[i], dinv[i]}; }
+  __device__ __forceinline__ Pre load(int64_t i) const {
+    return {b[i], diag_inv<SC>(dinv, i), scale_or_one<SC>(rs, i)};
+  }
   __device__ __forceinline__ double store(int64_t i, const Pre& p, T t) const {
     const T d0 = p.di * p.bi * inv_theta;
     if (deg == 1) {
       x[i] = d0;
-      res[i] = p.bi - t;
+      res[i] = SC ? p.si * (p.bi - t) : p.bi - t;
     } else {
       const T r1 = p.di * p.bi - p.di * t;
       const T d1 = c1 * d0 + c2 * r1;
@@ -767,7 +817,7 @@ struct EpiPreFirst {
   }
 };
 
-template <typename T>
+template <typename T, bool SC = false>
 struct EpiCheb {
   const T* __restrict__ dinv;
   const T* __restrict__ d_in;
@@ -777,12 +827,13 @@ struct EpiCheb {
   T c1, c2;
   const T* __restrict__ b;
   int want_dot;
+  const T* __restrict__ os = nullptr;  // scale of the x written (the V-cycle's last step)
   struct Pre {
-    T di, dd, ri, xi, bi;
+    T di, dd, ri, xi, bi, si;
   };
   // b_i (for the dot) is loaded with the other operands, before the row product
   __device__ __forceinline__ Pre load(int64_t i) const {
-    return {dinv[i], d_in[i], r[i], x[i], want_dot ? b[i] : T(0)};
+    return {diag_inv<SC>(dinv, i), d_in[i], r[i], x[i], want_dot ? b[i] : T(0), scale_or_one<SC>(os, i)};
   }
   __device__ __forceinline__ double store(int64_t i, const Pre& p, T t) const {
     const T ri = p.ri - p.di * t;
@@ -790,26 +841,27 @@ struct EpiCheb {
     const T xn = p.xi + dn;
     r[i] = ri;
     d_out[i] = dn;
-    x[i] = xn;
-    return want_dot ? (double)p.bi * (double)xn : 0.0;
+    x[i] = SC ? p.si * xn : xn;
+    return want_dot ? (double)p.bi * (double)xn : 0.0;  // b^ . x^ = b . x in the scaled space
   }
 };
 
-template <typename T>
+template <typename T, bool SC = false>
 struct EpiResidual {
   const T* __restrict__ b;
   T* __restrict__ res;
+  const T* __restrict__ rs = nullptr;  // residual scale
   struct Pre {
-    T bi;
+    T bi, si;
   };
-  __device__ __forceinline__ Pre load(int64_t i) const { return {b[i]}; }
+  __device__ __forceinline__ Pre load(int64_t i) const { return {b[i], scale_or_one<SC>(rs, i)}; }
   __device__ __forceinline__ double store(int64_t i, const Pre& p, T t) const {
-    res[i] = p.bi - t;
+    res[i] = SC ? p.si * (p.bi - t) : p.bi - t;
     return 0.0;
   }
 };
 
-template <typename T>
+template <typename T, bool SC = false>
 struct EpiPostFirst {
   const T* __restrict__ b;
   const T* __restrict__ dinv;
@@ -819,17 +871,20 @@ struct EpiPostFirst {
   T* __restrict__ r;
   T* __restrict__ d;
   int want_dot;
+  const T* __restrict__ os = nullptr;  // scale of x2 (when this is the V-cycle's last step)
   struct Pre {
-    T di, bi, xi;
+    T di, bi, xi, si;
   };
-  __device__ __forceinline__ Pre load(int64_t i) const { return {dinv[i], b[i], x[i]}; }
+  __device__ __forceinline__ Pre load(int64_t i) const {
+    return {diag_inv<SC>(dinv, i), b[i], x[i], scale_or_one<SC>(os, i)};
+  }
   __device__ __forceinline__ double store(int64_t i, const Pre& p, T t) const {
     const T r0 = p.di * (p.bi - t);
     const T d0 = r0 * inv_theta;
     const T xn = p.xi + d0;
     r[i] = r0;
     d[i] = d0;
-    x2[i] = xn;
+    x2[i] = SC ? p.si * xn : xn;
     return want_dot ? (double)p.bi * (double)xn : 0.0;
   }
 };
@@ -852,16 +907,20 @@ struct EpiSpmvDot {
   }
 };
 
-template <typename T>
-struct EpiLevel {  // y = A x (accumulate = 0) or y += A x (the transfer operators)
+template <typename T, bool SC = false>
+struct EpiLevel {  // y = A x (accumulate = 0) or y += A x (the transfer operators); SC: row scale ys
   T* __restrict__ y;
   int accumulate;
+  const T* __restrict__ ys = nullptr;
   struct Pre {
-    T yi;
+    T yi, si;
   };
-  __device__ __forceinline__ Pre load(int64_t i) const { return {accumulate ? y[i] : T(0)}; }
+  __device__ __forceinline__ Pre load(int64_t i) const {
+    return {accumulate ? y[i] : T(0), scale_or_one<SC>(ys, i)};
+  }
   __device__ __forceinline__ double store(int64_t i, const Pre& p, T t) const {
-    y[i] = accumulate ? p.yi + t : t;
+    const T v = SC ? p.si * t : t;
+    y[i] = accumulate ? p.yi + v : v;
     return 0.0;
   }
 };
@@ -876,7 +935,9 @@ struct StreamView {
 
 template <typename T>
 static StreamView stream_view(const StreamMat& m) {
-  if constexpr (sizeof(T) == 4)
+  if constexpr (std::is_same<T, __half>::value)
+    return {m.d16.p, m.n_tiles, m.p16.p, m.ctl};
+  else if constexpr (sizeof(T) == 4)
     return {m.d32.p, m.n_tiles, m.p32.p, m.ctl};
   else
     return {m.d64.p, m.n_tiles, m.p64.p, m.ctl};
@@ -891,7 +952,7 @@ __global__ void __launch_bounds__(kStreamThreads, (SHAPE::kCtasPerSm))
   __shared__ double sh[kStreamThreads / 32];
   pdl_trigger();
   bool skipped = false;
-  const double dot = stream_rows<T, BR, BC, typename SHAPE::type>(
+  const double dot = stream_rows_v<T, typename ShapeValue<SHAPE, T>::type, BR, BC, typename SHAPE::type>(
       m.tiles, m.n_tiles, m.pack, xf, epi, smem, &S->status, &S->done, m.ctl, &skipped);
   if (part && !skipped) write_part(dot, part, sh);
 }
@@ -991,16 +1052,19 @@ static int stream_grid(K kern, int n_tiles) {
 }
 
 // launch a streamed row kernel on matrix m (BR x BC blocks); false (nothing launched) when m
-// has no current pack of that shape or the kernel cannot be configured
+// has no current pack of that shape or the kernel cannot be configured.  A shape with FP16
+// values streams the FP16 pack (its currency is the caller's to check).
 template <typename T, int BR, int BC, typename XF, typename EPI, typename SHAPE = StreamDefault<T, BR, BC>>
 static bool launch_stream_rows(const StreamMat& m, XF xf, EPI epi, double* part, PcgScalars* S, cudaStream_t st,
                                int* grid_out) {
-  if (!m.packed || m.br != BR || m.bc != BC) return false;
+  using TV = typename ShapeValue<SHAPE, T>::type;
+  constexpr bool kHalf = std::is_same<TV, __half>::value;
+  if (m.br != BR || m.bc != BC || (kHalf ? !m.p16.p : !m.packed)) return false;
   using CFG = typename SHAPE::type;
   auto kern = k_stream_rows<T, BR, BC, XF, EPI, SHAPE>;
-  const int g = stream_grid<T, BR, BC, CFG>(kern, m.n_tiles);
+  const int g = stream_grid<TV, BR, BC, CFG>(kern, m.n_tiles);
   if (g == 0) return false;
-  if (launch_pdl(kern, g, kStreamThreads, stream_smem_bytes<T, BR, BC, CFG>(), st, stream_view<T>(m), xf, epi, part,
+  if (launch_pdl(kern, g, kStreamThreads, stream_smem_bytes<TV, BR, BC, CFG>(), st, stream_view<TV>(m), xf, epi, part,
                  S) != cudaSuccess) {
     cudaGetLastError();
     return false;
@@ -1011,20 +1075,22 @@ static bool launch_stream_rows(const StreamMat& m, XF xf, EPI epi, double* part,
 
 // y = M x or y += M x for a transfer operator: streamed from its pack when it has one, else the
 // register row kernel
-template <int BR, int BC, typename T>
+// (SC: (M x)_i scaled by ys_i -- the FP16 V-cycle's prolongation into its scaled fine level)
+template <int BR, int BC, typename T, bool SC = false>
 static void level_spmv(const DevBsr& M, const StreamMat& Ms, const T* vals, const T* x, T* y, int accumulate,
-                       PcgScalars* S, cudaStream_t st) {
+                       PcgScalars* S, cudaStream_t st, const T* ys = nullptr) {
   if constexpr (BR == 6 && BC == 6) {  // short rows (the prolongations): 8 lanes per row
     if (M.nnzb < 16 * M.n_rows) {
-      if (launch_stream_rows<T, 6, 6, XLoad<T, T>, EpiLevel<T>, StreamShort66<T>>(
-              Ms, XLoad<T, T>{x}, EpiLevel<T>{y, accumulate}, nullptr, S, st, nullptr))
+      if (launch_stream_rows<T, 6, 6, XLoad<T, T>, EpiLevel<T, SC>, StreamShort66<T>>(
+              Ms, XLoad<T, T>{x}, EpiLevel<T, SC>{y, accumulate, ys}, nullptr, S, st, nullptr))
         return;
-      level_spmv_rows<BR, BC, T>(M, vals, x, y, accumulate, S, st);
+      level_spmv_rows<BR, BC, T>(M, vals, x, y, accumulate, S, st, SC ? ys : nullptr);
       return;
     }
   }
-  if (launch_stream_rows<T, BR, BC>(Ms, XLoad<T, T>{x}, EpiLevel<T>{y, accumulate}, nullptr, S, st, nullptr)) return;
-  level_spmv_rows<BR, BC, T>(M, vals, x, y, accumulate, S, st);
+  if (launch_stream_rows<T, BR, BC>(Ms, XLoad<T, T>{x}, EpiLevel<T, SC>{y, accumulate, ys}, nullptr, S, st, nullptr))
+    return;
+  level_spmv_rows<BR, BC, T>(M, vals, x, y, accumulate, S, st, SC ? ys : nullptr);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1124,22 +1190,37 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
   DevLevel& L = H.levels[lvl];
   LevelVecs<T>& V = Prec<T>::vecs(L);
   const int64_t nr = L.n_nodes;
+  // the FP16 V-cycle (W.half): level 0 streams the equilibrated matrix S A S from its FP16 pack
+  // with the level's vectors in the scaled space (unit diagonal, no dinv); qs = S^-1 maps the
+  // residual and the prolongated correction, os = S the output
+  const bool half0 = lvl == 0 && W.half;
+  const T* qs = nullptr;
+  const T* os = nullptr;
+  if constexpr (std::is_same<T, float>::value) {
+    if (half0) {
+      qs = W.q32.p;
+      os = W.s32.p;
+    }
+  }
   // level 0: 1/diag of the current matrix (refreshed per solve), so a hierarchy kept across
   // re-assemblies still smooths with the right diagonal
-  const T* dinv = (lvl == 0) ? Prec<T>::fine_dinv(W) : Prec<T>::dinv(L);
+  const T* dinv = half0 ? nullptr : (lvl == 0) ? Prec<T>::fine_dinv(W) : Prec<T>::dinv(L);
   const int deg = H.degree;
   const T it = (T)L.inv_theta;
   const int64_t sd = (lvl == 0) ? s->nnzb : 0;  // component stride of the fine matrix
   const int64_t work = (nr * 32 + kThreads - 1) / kThreads;
   // algorithmic bytes: the level matrix, one level vector, the transfer operators
   const double Vb = (double)nr * L.bs * sizeof(T);
-  const double Ab = mat_bytes(lvl == 0 ? s->nnzb : L.A.nnzb, L.bs, L.bs, nr, sizeof(T));
+  const double Ab = half0 ? mat_bytes(s->nnzb, 3, 3, nr, 2)
+                          : mat_bytes(lvl == 0 ? s->nnzb : L.A.nnzb, L.bs, L.bs, nr, sizeof(T));
   const int64_t nc_dofs = (lvl + 1 < nlev) ? H.levels[lvl + 1].n_nodes * H.levels[lvl + 1].bs : H.n_coarse;
   const double Vc = (double)nc_dofs * sizeof(T);
   const double Rb = mat_bytes(L.R.nnzb, L.R.br, L.R.bc, L.R.n_rows, sizeof(T));
   const double Pb = mat_bytes(L.P.nnzb, L.P.br, L.P.bc, L.P.n_rows, sizeof(T));
-  auto run = [&](auto bs_tag) -> int {
+  auto run = [&](auto bs_tag, auto sc_tag) -> int {
     constexpr int BS = decltype(bs_tag)::value;
+    constexpr bool SC = decltype(sc_tag)::value;  // the FP16 V-cycle's level 0 (3x3, FP32 only)
+    static_assert(!SC || (BS == 3 && std::is_same<T, float>::value), "FP16 level: 3x3 blocks, FP32 arithmetic");
     auto rg = [&](auto kern) { return resident_grid(kern, kThreads, work); };
     const int32_t* rp;
     const int32_t* ci;
@@ -1147,15 +1228,32 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
     level_A<BS, T>(s, L, lvl, rp, ci, av);
     // pre-smoothing (+ residual).  A level whose matrix has a current tile-major pack (the fine
     // level; coarse levels too large for L2) streams it through shared memory (stream.cuh);
-    // the others use the register row kernels
+    // the others use the register row kernels.  The FP16 level 0 has no register form: a
+    // launch that fails there is an error.
     const StreamMat& Am = (lvl == 0) ? s->fine : L.As;
     const bool stream = Am.packed;
+    bool half_failed = false;
+    auto rows = [&](auto xf, auto epi, double* prt, int* gout) -> bool {
+      if constexpr (SC) {
+        const bool ok = launch_stream_rows<T, 3, 3, decltype(xf), decltype(epi), StreamHalf33>(Am, xf, epi, prt, S,
+                                                                                               st, gout);
+        half_failed = half_failed || !ok;
+        return true;
+      } else {
+        return stream && launch_stream_rows<T, BS, BS>(Am, xf, epi, prt, S, st, gout);
+      }
+    };
     const T c1 = deg >= 2 ? (T)L.c1[0] : T(0), c2 = deg >= 2 ? (T)L.c2[0] : T(0);
     // d0 (level 0, from the PCG update): the first step's input D^-1 b / theta precomputed
-    const EpiPreFirst<T> epi_pre{b, dinv, it, deg, c1, c2, V.x.p, V.r.p, V.d.p, V.res.p};
-    const bool pre_streamed =
-        stream && (d0 ? launch_stream_rows<T, BS, BS>(Am, XLoad<T, T>{d0}, epi_pre, nullptr, S, st, nullptr)
-                      : launch_stream_rows<T, BS, BS>(Am, XD0<T>{b, dinv, it}, epi_pre, nullptr, S, st, nullptr));
+    EpiPreFirst<T, SC> epi_pre{b, dinv, it, deg, c1, c2, V.x.p, V.r.p, V.d.p, V.res.p};
+    epi_pre.rs = qs;
+    bool pre_streamed;
+    if (d0)
+      pre_streamed = rows(XLoad<T, T>{d0}, epi_pre, nullptr, nullptr);
+    else if constexpr (SC)
+      pre_streamed = rows(XD0U<T>{b, it}, epi_pre, nullptr, nullptr);
+    else
+      pre_streamed = rows(XD0<T>{b, dinv, it}, epi_pre, nullptr, nullptr);
     if (!pre_streamed)
       k_pre_first<BS, T><<<rg(k_pre_first<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, deg, c1, c2,
                                                                       V.x.p, V.r.p, V.d.p, V.res.p, S);
@@ -1165,9 +1263,7 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
     T* dout = V.d2.p;
     for (int k = 2; k < deg; ++k) {
       const T ck1 = (T)L.c1[k - 1], ck2 = (T)L.c2[k - 1];
-      if (!(stream && launch_stream_rows<T, BS, BS>(Am, XLoad<T, T>{din},
-                                            EpiCheb<T>{dinv, din, dout, V.r.p, V.x.p, ck1, ck2, b, 0}, nullptr, S,
-                                            st, nullptr)))
+      if (!rows(XLoad<T, T>{din}, EpiCheb<T, SC>{dinv, din, dout, V.r.p, V.x.p, ck1, ck2, b, 0}, nullptr, nullptr))
         k_cheb_step<BS, T><<<rg(k_cheb_step<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout, V.r.p,
                                                                         V.x.p, ck1, ck2, b, nullptr, S);
       W.launches++;
@@ -1175,8 +1271,9 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
       std::swap(din, dout);
     }
     if (deg >= 2) {
-      if (!(stream && launch_stream_rows<T, BS, BS>(Am, XLoad<T, T>{V.x.p}, EpiResidual<T>{b, V.res.p}, nullptr, S, st,
-                                            nullptr)))
+      EpiResidual<T, SC> epi_res{b, V.res.p};
+      epi_res.rs = qs;
+      if (!rows(XLoad<T, T>{V.x.p}, epi_res, nullptr, nullptr))
         k_residual<BS, T><<<rg(k_residual<BS, T>), kThreads, 0, st>>>(nr, rp, ci, av, sd, b, V.x.p, V.res.p, S);
       W.launches++;
       note(W, st, "residual", lvl, Ab + 3 * Vb);
@@ -1189,16 +1286,16 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
     W.launches++;
     note(W, st, "restrict", lvl, Rb + Vb + Vc);
     WN_CHECK(vcycle<T>(s, H, W, lvl + 1, bc, xc, nullptr, S, st));
-    // prolongation x += P x_c
-    level_spmv<BS, 6, T>(L.P, L.Ps, Prec<T>::Pv(L), xc, V.x.p, 1, S, st);
+    // prolongation x += P x_c (x^ += S^-1 P x_c in the scaled space)
+    level_spmv<BS, 6, T, SC>(L.P, L.Ps, Prec<T>::Pv(L), xc, V.x.p, 1, S, st, qs);
     W.launches++;
     note(W, st, "prolong", lvl, Pb + Vc + 2 * Vb);
     // post-smoothing: result in `out`
     double* part_last = (deg == 1) ? part : nullptr;
     int gpf = 0;
-    if (!(stream && launch_stream_rows<T, BS, BS>(Am, XLoad<T, T>{V.x.p},
-                                          EpiPostFirst<T>{b, dinv, it, V.x.p, out, V.r.p, V.d.p, part_last != nullptr},
-                                          part_last, S, st, &gpf))) {
+    EpiPostFirst<T, SC> epi_post{b, dinv, it, V.x.p, out, V.r.p, V.d.p, part_last != nullptr};
+    epi_post.os = deg == 1 ? os : nullptr;
+    if (!rows(XLoad<T, T>{V.x.p}, epi_post, part_last, &gpf)) {
       gpf = rg(k_post_first<BS, T>);
       k_post_first<BS, T><<<gpf, kThreads, 0, st>>>(nr, rp, ci, av, sd, b, dinv, it, V.x.p, out, V.r.p, V.d.p,
                                                      part_last, S);
@@ -1212,9 +1309,9 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
       double* pk = (k == deg - 1) ? part : nullptr;
       const T ck1 = (T)L.c1[k - 1], ck2 = (T)L.c2[k - 1];
       int gcs = 0;
-      if (!(stream && launch_stream_rows<T, BS, BS>(Am, XLoad<T, T>{din},
-                                            EpiCheb<T>{dinv, din, dout, V.r.p, out, ck1, ck2, b, pk != nullptr}, pk, S,
-                                            st, &gcs))) {
+      EpiCheb<T, SC> epi_cheb{dinv, din, dout, V.r.p, out, ck1, ck2, b, pk != nullptr};
+      epi_cheb.os = (k == deg - 1) ? os : nullptr;
+      if (!rows(XLoad<T, T>{din}, epi_cheb, pk, &gcs)) {
         gcs = rg(k_cheb_step<BS, T>);
         k_cheb_step<BS, T><<<gcs, kThreads, 0, st>>>(nr, rp, ci, av, sd, dinv, din, dout, V.r.p, out, ck1, ck2, b, pk,
                                                      S);
@@ -1224,13 +1321,20 @@ static int vcycle(Solid* s, AmgHierarchy& H, SolverWork& W, int lvl, const T* b,
       note(W, st, "post_cheb", lvl, Ab + (pk ? 8 : 7) * Vb);
       std::swap(din, dout);
     }
+    WN_REQUIRE(!half_failed, WN_ESTATE, "FP16 V-cycle: the streamed fine-level kernel could not be launched");
     return 0;
   };
   int rc;
-  if (L.bs == 3)
-    rc = run(std::integral_constant<int, 3>{});
-  else
-    rc = run(std::integral_constant<int, 6>{});
+  if (half0) {
+    if constexpr (std::is_same<T, float>::value)
+      rc = run(std::integral_constant<int, 3>{}, std::true_type{});
+    else
+      rc = WN_ESTATE;
+  } else if (L.bs == 3) {
+    rc = run(std::integral_constant<int, 3>{}, std::false_type{});
+  } else {
+    rc = run(std::integral_constant<int, 6>{}, std::false_type{});
+  }
   WN_CHECK(rc);
   WN_CUDA(cudaGetLastError());
   return 0;
@@ -1264,6 +1368,15 @@ static int apply_prec(Solid* s, SolverWork& W, int precond, const T* r, T* z, Pc
   note(W, st, precond == 1 ? "jacobi" : "copy", -1, (precond == 1 ? 3.0 : 2.0) * W.n * sizeof(T));
   WN_CUDA(cudaGetLastError());
   return 0;
+}
+
+// the FP16 V-cycle's input scale S (null otherwise)
+template <typename TM>
+static const TM* half_scale(const SolverWork& W) {
+  if constexpr (std::is_same<TM, float>::value)
+    return W.half ? W.s32.p : nullptr;
+  else
+    return nullptr;
 }
 
 // PCG buffers of one precision pairing: Krylov vectors / matrix in TK, preconditioner in TM
@@ -1345,7 +1458,8 @@ static int pcg_iteration(Solid* s, SolverWork& W, int precond, int k, PcgScalars
   TM* d0 = pre_input ? Prec<TM>::pcg(W).d0.p : nullptr;
   const TM it0 = pre_input ? (TM)s->amg->levels[0].inv_theta : TM(0);
   k_update<TK, TM><<<gup, kThreads, 0, st>>>(W.n, B.x, B.r, B.rm, p_new, B.q, W.partB.p, W.partC.p, W.npB, par, S, d0,
-                                             Prec<TM>::fine_dinv(W), it0);
+                                             W.half ? half_scale<TM>(W) : Prec<TM>::fine_dinv(W), it0,
+                                             half_scale<TM>(W));
   note(W, st, "pcg_update", -1, 6 * nK + (B.rm ? nM : 0.0) + (d0 ? 2 * nM : 0.0));
   W.npC = gup;
   k_check<<<1, kThreads, 0, st>>>(S, W.partC.p, W.npC);
@@ -1373,7 +1487,7 @@ static int pcg_solve(Solid* s, SolverWork& W, int mode, const TK* b, double rtol
   const size_t note0 = W.notes.size();
   W.cur_iter = -1;
   W.npC = resident_grid(k_init_vecs<TK, TM>, kThreads, (W.n + kThreads - 1) / kThreads);
-  k_init_vecs<TK, TM><<<W.npC, kThreads, 0, st>>>(W.n, b, B.x, B.r, B.rm, W.partC.p);
+  k_init_vecs<TK, TM><<<W.npC, kThreads, 0, st>>>(W.n, b, B.x, B.r, B.rm, W.partC.p, half_scale<TM>(W));
   note(W, st, "pcg_init", -1, 3.0 * W.n * sizeof(TK) + (B.rm ? (double)W.n * sizeof(TM) : 0.0));
   k_init_scalars<<<1, kThreads, 0, st>>>(S, W.partC.p, W.npC, rtol, max_iter);
   note(W, st, "pcg_check", -1, 0.0);
@@ -1618,6 +1732,40 @@ static int true_residual(Solid* s, SolverWork& W, const double* F, float* r32, c
   return 0;
 }
 
+// out = s * in, elementwise
+__global__ void k_scale_copy(int64_t n, const float* __restrict__ s, const float* __restrict__ in,
+                             float* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = s[i] * in[i];
+}
+
+// The FP16 V-cycle's inputs for the current matrix: the equilibration S = diag(K)^-1/2 (every
+// solve) and the FP16 pack of S K S (rebuilt when the values changed since it was made).  It
+// needs a C3D10 system with the streamed fine level and an AMG hierarchy.
+static int prepare_half(Solid* s, SolverWork& W, cudaStream_t st) {
+  WN_REQUIRE(s->bs == 3 && s->amg, WN_EINVAL, "FP16 V-cycle: needs a C3D10 (3x3) system with the AMG preconditioner");
+  WN_REQUIRE(s->stream_fine && s->fine.n_tiles > 0 && s->fine.size16 > 0 && s->fine.packed, WN_ESTATE,
+             "FP16 V-cycle: needs the streamed fine level (wn_solid_set_stream(h, 1))");
+  WN_REQUIRE(!s->amg->levels.empty(), WN_ESTATE, "FP16 V-cycle: the hierarchy has no fine level to smooth");
+  if (W.s32.n != W.n) {
+    WN_CHECK(W.s64.alloc(W.n));
+    WN_CHECK(W.s32.alloc(W.n));
+    WN_CHECK(W.q32.alloc(W.n));
+  }
+  k_fill_scale<<<vec_grid(W.n), kThreads, 0, st>>>(s->n_nodes, s->nnzb, s->diag_block.p, s->k64.p, W.s64.p, W.s32.p,
+                                                   W.q32.p);
+  WN_CUDA(cudaGetLastError());
+  note(W, st, "fill_scale", -1, 28.0 * W.n);
+  W.launches++;
+  if (s->fine.version16 != s->values_version) {
+    WN_CHECK(s->fine.pack_half33(s->row_ptr.p, s->col_idx.p, s->block_row.p, s->k64.p, s->nnzb, W.s64.p,
+                                 s->values_version, st));
+    note(W, st, "pack_half", -1, mat_bytes(s->nnzb, 3, 3, s->n_nodes, 8) + mat_bytes(s->nnzb, 3, 3, s->n_nodes, 2));
+    W.launches++;
+  }
+  return 0;
+}
+
 // Outer loop common to all modes: u = 0; r = F - K u; while ||r|| > rtol ||F||: solve K d = r
 // approximately with the inner PCG, u += d, recompute the residual.  u is kept as a
 // double-double pair and r is evaluated with compensated products and sums, so the test
@@ -1628,6 +1776,9 @@ static int true_residual(Solid* s, SolverWork& W, const double* F, float* r32, c
 //                   accumulation; FP64 coarsest inverse), same target
 //   mode 2 (fp32 IR): inner PCG entirely FP32 (FP32 K SpMV) to max(inner_rtol, target);
 //                   the classic iterative refinement of solid_solver.py:271-300
+//   mode 3 (mixed, FP16 V-cycle): mode 1 with the fine level of the V-cycle on the
+//                   equilibrated matrix S K S in FP16 (FP32 arithmetic and vectors); the
+//                   reference's tri-precision preconditioner (mixed_precision.py:96-103)
 // FP64 dot products everywhere.  The FP64 loop makes the stopping test the true residual.
 template <typename TK, typename TM>
 static int outer_loop(Solid* s, SolverWork& W, int mode, const double* F, double fnorm, const wn_solve_params& prm,
@@ -1691,8 +1842,11 @@ int solver_solve(Solid* s, const double* F, double* u, const wn_solve_params& pr
   WN_REQUIRE(s->assembled, WN_ESTATE, "solve: matrix not assembled");
   WN_REQUIRE(prm.precond >= 0 && prm.precond <= 3, WN_EINVAL,
              "solve: precond must be 0 (none), 1 (jacobi), 2 (amg) or 3 (block jacobi)");
-  WN_REQUIRE(prm.precision >= 0 && prm.precision <= 2, WN_EINVAL,
-             "solve: precision must be 0 (fp64), 1 (mixed: fp32 AMG in fp64 PCG) or 2 (fp32 PCG in fp64 refinement)");
+  WN_REQUIRE(prm.precision >= 0 && prm.precision <= 3, WN_EINVAL,
+             "solve: precision must be 0 (fp64), 1 (mixed: fp32 AMG in fp64 PCG), 2 (fp32 PCG in fp64 refinement) "
+             "or 3 (mixed with the fp16 fine-level V-cycle)");
+  WN_REQUIRE(prm.precision != 3 || prm.precond == 2, WN_EINVAL,
+             "solve: precision 3 (fp16 V-cycle) needs precond 2 (amg)");
   WN_REQUIRE(prm.max_iter > 0 && prm.rtol > 0.0, WN_EINVAL, "solve: max_iter > 0 and rtol > 0 required");
   if (prm.precond == 2 && !s->amg) WN_CHECK(solver_setup(s, amg_default_params()));
   WN_CHECK(ensure_work(s));
@@ -1759,7 +1913,13 @@ int solver_solve(Solid* s, const double* F, double* u, const wn_solve_params& pr
       WN_CHECK((outer_loop<double, double>(s, W, 0, F, fnorm, prm, chunk, st, &total_iters, &outer, &status, &rr)));
     else if (prm.precision == 1)
       WN_CHECK((outer_loop<double, float>(s, W, 1, F, fnorm, prm, chunk, st, &total_iters, &outer, &status, &rr)));
-    else
+    else if (prm.precision == 3) {
+      WN_CHECK(prepare_half(s, W, st));
+      W.half = true;
+      const int rc = outer_loop<double, float>(s, W, 3, F, fnorm, prm, chunk, st, &total_iters, &outer, &status, &rr);
+      W.half = false;
+      WN_CHECK(rc);
+    } else
       WN_CHECK((outer_loop<float, float>(s, W, 2, F, fnorm, prm, chunk, st, &total_iters, &outer, &status, &rr)));
     WN_CUDA(cudaMemcpyAsync(u, W.u64.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
   }
@@ -1827,6 +1987,15 @@ int amg_vcycle(Solid* s, int precision, const void* r, void* z, cudaStream_t st)
   WN_CUDA(cudaMemsetAsync(W.scal.p, 0, sizeof(PcgScalars), st));  // done = 0
   if (precision == 0)
     return vcycle<double>(s, *s->amg, W, 0, (const double*)r, (double*)z, nullptr, W.scal.p, st);
+  if (precision == 3) {  // the FP16 V-cycle: input S r, output unscaled by its last step
+    WN_CHECK(prepare_half(s, W, st));
+    k_scale_copy<<<vec_grid(W.n), kThreads, 0, st>>>(W.n, W.s32.p, (const float*)r, W.r32.p);
+    WN_CUDA(cudaGetLastError());
+    W.half = true;
+    const int rc = vcycle<float>(s, *s->amg, W, 0, W.r32.p, (float*)z, nullptr, W.scal.p, st);
+    W.half = false;
+    return rc;
+  }
   return vcycle<float>(s, *s->amg, W, 0, (const float*)r, (float*)z, nullptr, W.scal.p, st);
 }
 

@@ -20,6 +20,14 @@ static int plan_shape(StreamMat& m, const int32_t* h_rp, int64_t n_rows) {
   const int64_t b32 = build_pack_tiles<float, BR * BC>(plan, d32);
   const int64_t b64 = build_pack_tiles<double, BR * BC>(plan, d64);
   if (b32 <= 0 || b64 <= 0) return 0;
+  if constexpr (BR == 3 && BC == 3) {
+    std::vector<PackTile> d16;
+    const int64_t b16 = build_pack_tiles<__half, 9>(plan, d16);
+    if (b16 > 0) {
+      WN_CHECK(m.d16.upload(d16));
+      m.size16 = b16;
+    }
+  }
   WN_CHECK(m.plan.upload(plan));
   WN_CHECK(m.d32.upload(d32));
   WN_CHECK(m.d64.upload(d64));
@@ -39,7 +47,23 @@ void StreamMat::clear() {
   d64.release();
   p32.release();
   p64.release();
-  size32 = size64 = 0;
+  d16.release();
+  p16.release();
+  size32 = size64 = size16 = 0;
+  version16 = ~0ull;
+}
+
+int StreamMat::pack_half33(const int32_t* rp, const int32_t* ci, const int32_t* block_row, const double* v64,
+                           int64_t stride, const double* scale, uint64_t version, cudaStream_t st) {
+  WN_REQUIRE(br == 3 && bc == 3 && n_tiles > 0 && size16 > 0, WN_ESTATE, "FP16 pack: no 3x3 tile plan");
+  const unsigned char* old = p16.p;
+  WN_CHECK(p16.alloc(size16));
+  if (p16.p != old) ++epoch;
+  const int grid = std::min(n_tiles, kNumSMs * 8);
+  k_pack_half33<<<grid, 256, 0, st>>>(n_tiles, plan.p, d16.p, rp, ci, block_row, v64, stride, scale, p16.p);
+  WN_CUDA(cudaGetLastError());
+  version16 = version;
+  return 0;
 }
 
 int StreamMat::make_plan(const int32_t* h_rp, int64_t n_rows, int br_, int bc_) {

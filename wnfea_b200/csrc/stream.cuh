@@ -32,9 +32,11 @@
 // flight and returns.
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
 #include <vector>
 
 #include "wnfea_cuda.h"
@@ -144,6 +146,26 @@ struct StreamDefault<T, 3, 6> {
   using type = StreamCfg<512, kStreamRowCap, 8, 4, 2, 2, 2>;
   static constexpr int kCtasPerSm = sizeof(T) == 4 ? 2 : 1;
 };
+// The fine 3x3 level with FP16 values (the equilibrated matrix S A S of the FP16 V-cycle) and
+// FP32 arithmetic: the tiles of the FP32 / FP64 packs, stages of half the bytes, so four of them
+// per CTA at three CTAs per SM.
+struct StreamHalf33 {
+  using type = StreamCfg<kStreamCap, kStreamRowCap, 8, 8, 4, 4>;
+  using value = __half;
+  static constexpr int kCtasPerSm = 3;
+  static_assert(type::kCap == StreamDefault<float, 3, 3>::type::kCap &&
+                    type::kRowCap == StreamDefault<float, 3, 3>::type::kRowCap,
+                "the FP16 shape streams the default 3x3 tiles");
+};
+// storage type of a shape's matrix values: SHAPE::value when the shape names one, else T
+template <typename SHAPE, typename T, typename = void>
+struct ShapeValue {
+  using type = T;
+};
+template <typename SHAPE, typename T>
+struct ShapeValue<SHAPE, T, std::void_t<typename SHAPE::value>> {
+  using type = typename SHAPE::value;
+};
 
 template <typename T, int BR, int BC, typename Cfg = typename StreamDefault<T, BR, BC>::type>
 constexpr size_t stream_smem_bytes() {
@@ -211,6 +233,42 @@ __global__ void __launch_bounds__(256) k_pack_tiles(int n_tiles, const StreamTil
     for (int b = threadIdx.x; b < cntp; b += blockDim.x) sc[b] = b < cnt ? ci[p.b0 + b] : 0;
     uint16_t* sr = reinterpret_cast<uint16_t*>(seg + pack_row_off<T, NV>(cntp));
     const int slots = (int)(pack_bytes<T, NV>(cntp, nr) - pack_row_off<T, NV>(cntp)) / 2;
+    for (int i = threadIdx.x; i < slots; i += blockDim.x) sr[i] = (uint16_t)(i <= nr ? rp[p.r0 + i] - p.b0 : 0);
+  }
+}
+
+// The FP16 pack of the equilibrated 3x3 matrix S A S, S = diag(scale): component k = 3 r + c of
+// block b (row br, column bc) is v[k stride + b] scale[3 br + r] scale[3 bc + c], formed in FP64
+// and rounded to FP16 once.  With scale = diag(A)^-1/2 the matrix has a unit diagonal and, A
+// being symmetric positive (semi)definite, entries of magnitude <= 1.  Same tiles and layout as
+// k_pack_tiles<__half, 9>.
+static __global__ void __launch_bounds__(256) k_pack_half33(int n_tiles, const StreamTile* __restrict__ plan,
+                                                     const PackTile* __restrict__ desc, const int32_t* __restrict__ rp,
+                                                     const int32_t* __restrict__ ci,
+                                                     const int32_t* __restrict__ block_row,
+                                                     const double* __restrict__ v, int64_t stride,
+                                                     const double* __restrict__ scale, unsigned char* __restrict__ pack) {
+  for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    const StreamTile p = plan[t];
+    const PackTile d = desc[t];
+    const int cnt = p.b1 - p.b0, cntp = d.cntp, nr = p.r1 - p.r0;
+    unsigned char* seg = pack + (size_t)d.seg * 128;
+    __half* sv = reinterpret_cast<__half*>(seg);
+    for (int k = 0; k < 9; ++k) {
+      const int r = k / 3, c = k - 3 * (k / 3);
+      for (int b = threadIdx.x; b < cntp; b += blockDim.x) {
+        double a = 0.0;
+        if (b < cnt) {
+          const int64_t q = p.b0 + b;
+          a = v[(int64_t)k * stride + q] * scale[(int64_t)block_row[q] * 3 + r] * scale[(int64_t)ci[q] * 3 + c];
+        }
+        sv[k * cntp + b] = __double2half(a);
+      }
+    }
+    int32_t* sc = reinterpret_cast<int32_t*>(seg + pack_col_off<__half, 9>(cntp));
+    for (int b = threadIdx.x; b < cntp; b += blockDim.x) sc[b] = b < cnt ? ci[p.b0 + b] : 0;
+    uint16_t* sr = reinterpret_cast<uint16_t*>(seg + pack_row_off<__half, 9>(cntp));
+    const int slots = (int)(pack_bytes<__half, 9>(cntp, nr) - pack_row_off<__half, 9>(cntp)) / 2;
     for (int i = threadIdx.x; i < slots; i += blockDim.x) sr[i] = (uint16_t)(i <= nr ? rp[p.r0 + i] - p.b0 : 0);
   }
 }
@@ -459,16 +517,26 @@ __device__ __forceinline__ double stream_pipeline(const PackTile* __restrict__ t
   return dot;
 }
 
+// a stored matrix value in the arithmetic type
+template <typename T, typename TV>
+__device__ __forceinline__ T value_as(TV v) {
+  if constexpr (std::is_same<TV, __half>::value)
+    return (T)__half2float(v);
+  else
+    return (T)v;
+}
+
 // The row engine: y-rows of A x with G lanes per block row (lane l taking the row's blocks
 // l, l + G, ...; U blocks in flight per lane, R rows per lane group), for every row DOF
 // i = BR row + c of the CTA's tiles the owning lane (c < BR <= G) calls pre = epi.load(i) before
 // the row product and dot += epi.store(i, pre, (A x)_i) after it, with x_j = xf(j)
-// (j = BC col + c).  Returns the thread's dot sum (0 for the producer).
-template <typename T, int BR, int BC, typename Cfg, typename XF, typename EPI, typename HOOK = NoHook>
-__device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles, int n_tiles,
-                                              const unsigned char* __restrict__ pack, const XF& xf, const EPI& epi,
-                                              unsigned char* smem, int* status, int* done, const StreamCtl ctl,
-                                              bool* skipped = nullptr, const HOOK& hook = HOOK{}) {
+// (j = BC col + c).  Returns the thread's dot sum (0 for the producer).  The pack stores its
+// values as TV (T, or FP16 for an FP32 product), the arithmetic is T.
+template <typename T, typename TV, int BR, int BC, typename Cfg, typename XF, typename EPI, typename HOOK = NoHook>
+__device__ __forceinline__ double stream_rows_v(const PackTile* __restrict__ tiles, int n_tiles,
+                                                const unsigned char* __restrict__ pack, const XF& xf, const EPI& epi,
+                                                unsigned char* smem, int* status, int* done, const StreamCtl ctl,
+                                                bool* skipped = nullptr, const HOOK& hook = HOOK{}) {
   constexpr int NV = BR * BC;
   constexpr int G = Cfg::kG;
   constexpr int U = Cfg::kUnroll;
@@ -480,9 +548,9 @@ __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles
   const int gl = lane % G, grp = lane / G;
   auto body = [&](int jc, const unsigned char* st, const int4 d, double& dot) {
     const int r0 = d.x, nr = d.y - d.x, cntp = d.w;
-    const T* sv = reinterpret_cast<const T*>(st);
-    const int32_t* scol = reinterpret_cast<const int32_t*>(st + pack_col_off<T, NV>(cntp));
-    const uint16_t* srp = reinterpret_cast<const uint16_t*>(st + pack_row_off<T, NV>(cntp));
+    const TV* sv = reinterpret_cast<const TV*>(st);
+    const int32_t* scol = reinterpret_cast<const int32_t*>(st + pack_col_off<TV, NV>(cntp));
+    const uint16_t* srp = reinterpret_cast<const uint16_t*>(st + pack_row_off<TV, NV>(cntp));
     // warps take the tile's rows round-robin in passes of GPW * R rows (group g of a pass owns
     // rows base + q GPW + g, q < R), starting from a warp that rotates per tile
     const int wslot = (warp + jc) % NCW;
@@ -528,7 +596,8 @@ __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles
 #pragma unroll
               for (int r = 0; r < BR; ++r)
 #pragma unroll
-                for (int c = 0; c < BC; ++c) acc[q][r] = fma(sv[(r * BC + c) * cntp + b], xv[q][u][c], acc[q][r]);
+                for (int c = 0; c < BC; ++c)
+                  acc[q][r] = fma(value_as<T>(sv[(r * BC + c) * cntp + b]), xv[q][u][c], acc[q][r]);
             }
           }
       }
@@ -546,7 +615,14 @@ __device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles
       }
     }
   };
-  return stream_pipeline<T, NV, Cfg>(tiles, n_tiles, pack, smem, status, done, ctl, skipped, hook, body);
+  return stream_pipeline<TV, NV, Cfg>(tiles, n_tiles, pack, smem, status, done, ctl, skipped, hook, body);
+}
+template <typename T, int BR, int BC, typename Cfg, typename XF, typename EPI, typename HOOK = NoHook>
+__device__ __forceinline__ double stream_rows(const PackTile* __restrict__ tiles, int n_tiles,
+                                              const unsigned char* __restrict__ pack, const XF& xf, const EPI& epi,
+                                              unsigned char* smem, int* status, int* done, const StreamCtl ctl,
+                                              bool* skipped = nullptr, const HOOK& hook = HOOK{}) {
+  return stream_rows_v<T, T, BR, BC, Cfg>(tiles, n_tiles, pack, xf, epi, smem, status, done, ctl, skipped, hook);
 }
 
 #endif  // __CUDACC__

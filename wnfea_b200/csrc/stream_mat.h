@@ -1,5 +1,6 @@
 // A block-sparse matrix prepared for the streamed kernels (stream.cuh): its tile plan, the
-// segment descriptors of its FP32 and FP64 tile-major packs, and the packs themselves.  The
+// segment descriptors of its FP32 and FP64 tile-major packs (and, for 3x3 blocks, of an FP16
+// pack of the equilibrated matrix), and the packs themselves.  The
 // plan depends on the pattern only (made once); the packs are refreshed whenever the values
 // change.
 #pragma once
@@ -32,6 +33,14 @@ struct StreamMat {
   // stride == 0) into both packs; a no-op without a plan.
   int pack(const int32_t* rp, const int32_t* ci, const float* v32, const double* v64, int64_t stride,
            cudaStream_t st);
+  // 3x3 matrices: the FP16 pack of the equilibrated matrix S A S (k_pack_half33) for the FP16
+  // V-cycle, built on demand and tagged with the values version it was built from
+  DArray<PackTile> d16;
+  DArray<unsigned char> p16;
+  int64_t size16 = 0;
+  uint64_t version16 = ~0ull;
+  int pack_half33(const int32_t* rp, const int32_t* ci, const int32_t* block_row, const double* v64, int64_t stride,
+                  const double* scale, uint64_t version, cudaStream_t st);
   // drop the plan and packs (the matrix is then run by the register kernels)
   void clear();
 };

@@ -55,7 +55,7 @@ def assemble_c3d10_sparse_3dof(model: FEAModel, apply_bcs: bool = True):
 
 
 _PRECOND = {"none": 0, "jacobi": 1, "amg": 2, "block_jacobi": 3}
-_PRECISION = {"fp64": 0, "mixed_fp32": 1, "mixed_fp32_ir": 2}
+_PRECISION = {"fp64": 0, "mixed_fp32": 1, "mixed_fp32_ir": 2, "mixed_fp16": 3}
 
 
 def solve_c3d10_pcg(
@@ -84,7 +84,12 @@ def solve_c3d10_pcg(
                          SpMV, FP32 preconditioner, FP64 dots) inside FP64 iterative
                          refinement.  Converges slowly once cond(K) * 6e-8 approaches 1 (an
                          FP32 SpMV cannot resolve smooth displacement fields: K u cancels ~8
-                         digits per row); fine for small meshes.
+                         digits per row); fine for small meshes;
+    * "mixed_fp16"    -- "mixed_fp32" with the V-cycle's fine level on the equilibrated matrix
+                         S K S (S = diag(K)^-1/2, entries in [-1, 1]) stored in FP16, FP32
+                         arithmetic and vectors: the FP16 preconditioner of the reference's
+                         TRI_PRECISION (mixed_precision.py:96-103), on every iteration.  "amg"
+                         only.
 
     All modes stop on the true FP64 residual ||F - K u|| <= rtol ||F||.  The returned
     iteration count is the real one (the reference stores scipy's ``info`` there,
@@ -94,6 +99,8 @@ def solve_c3d10_pcg(
         raise ValueError(f"preconditioner must be one of {sorted(_PRECOND)}, got {preconditioner!r}")
     if precision not in _PRECISION:
         raise ValueError(f"precision must be one of {sorted(_PRECISION)}, got {precision!r}")
+    if precision == "mixed_fp16" and preconditioner != "amg":
+        raise ValueError("precision 'mixed_fp16' (FP16 V-cycle) needs preconditioner='amg'")
     t0 = time.perf_counter()
     system = K.system
     if preconditioner == "amg" and (amg_params is not None or not system.amg_ready):
