@@ -18,6 +18,7 @@
 #include "amg_setup.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -525,20 +526,65 @@ int dense_coarse(int64_t n, int bs, const int32_t* rp, const int32_t* ci, const 
     for (int64_t j = 0; j < nc && !any; ++j) any = D[(size_t)i * nc + j] != 0.0;
     if (!any) D[(size_t)i * nc + i] = 1.0;
   }
-  // Cholesky A = L L^T (left-looking; row-major L, the dot products run over contiguous rows)
+  // Cholesky A = L L^T (left-looking; row-major L, the dot products run over contiguous rows).
+  // Column j: the pivot L_jj from row j, then L_ij for every i > j, each from rows i and j only.
+  // A team of host threads owns the rows (row i on thread i mod T) and meets once per column;
+  // the owner of row j + 1 forms the next pivot right after its L_{j+1,j}.  Every entry is the
+  // same fixed-order dot product whatever T is, so L does not depend on the thread count.
   std::vector<double> Lf(D);
-  for (int64_t j = 0; j < nc; ++j) {
+  const int nth = (int)std::min<int64_t>(host_threads(), std::max<int64_t>(1, nc / 64));
+  std::atomic<int64_t> bad{-1};
+  auto pivot = [&](int64_t j) {
     const double* lj = &Lf[(size_t)j * nc];
     const double s = Lf[(size_t)j * nc + j] - dot_fixed(lj, lj, j);
-    WN_REQUIRE(s > 0.0 && std::isfinite(s), WN_ENOTSPD, "amg_build: coarsest matrix not SPD (pivot %lld)",
-               (long long)j);
-    const double ljj = std::sqrt(s);
-    Lf[(size_t)j * nc + j] = ljj;
-    for (int64_t i = j + 1; i < nc; ++i) {
+    if (!(s > 0.0 && std::isfinite(s))) {
+      int64_t none = -1;
+      bad.compare_exchange_strong(none, j);
+      return;
+    }
+    Lf[(size_t)j * nc + j] = std::sqrt(s);
+  };
+  auto column = [&](int64_t j, int t, int T) {  // L_ij for the rows i > j of thread t
+    const double* lj = &Lf[(size_t)j * nc];
+    const double ljj = lj[j];
+    int64_t i = j + 1 + ((t - (j + 1)) % T + T) % T;
+    for (; i < nc; i += T) {
       double* li = &Lf[(size_t)i * nc];
       li[j] = (li[j] - dot_fixed(li, lj, j)) / ljj;
+      if (i == j + 1) pivot(i);
     }
+  };
+  if (nc > 0) pivot(0);
+  if (nth <= 1) {
+    for (int64_t j = 0; j < nc && bad.load() < 0; ++j) column(j, 0, 1);
+  } else if (bad.load() < 0) {
+    // sense-counting barrier of the team: a generation counter bumped by the last arrival
+    std::atomic<int> arrived{0}, generation{0};
+    auto meet = [&]() {
+      const int g = generation.load(std::memory_order_acquire);
+      if (arrived.fetch_add(1, std::memory_order_acq_rel) + 1 == nth) {
+        arrived.store(0, std::memory_order_relaxed);
+        generation.fetch_add(1, std::memory_order_acq_rel);
+      } else {
+        while (generation.load(std::memory_order_acquire) == g) std::this_thread::yield();
+      }
+    };
+    // a failed pivot p is recorded during column p - 1; after the meet that ends column j every
+    // thread has seen each failure with p <= j + 1 and stops there, while a failure a faster
+    // thread already met in column j + 1 (p = j + 2) is acted on one meet later by all alike
+    std::vector<std::thread> team;
+    for (int t = 0; t < nth; ++t)
+      team.emplace_back([&, t]() {
+        for (int64_t j = 0; j < nc; ++j) {
+          column(j, t, nth);
+          meet();
+          const int64_t p = bad.load(std::memory_order_acquire);
+          if (p >= 0 && p <= j + 1) break;
+        }
+      });
+    for (auto& x : team) x.join();
   }
+  WN_REQUIRE(bad.load() < 0, WN_ENOTSPD, "amg_build: coarsest matrix not SPD (pivot %lld)", (long long)bad.load());
   // Wt = (L^-1)^T, upper triangular, row c = column c of L^-1 (forward substitution on e_c);
   // rows are independent and split over the host threads (interleaved: the work per row falls
   // with c)

@@ -1,11 +1,18 @@
-// Owning device allocation (cudaMalloc / cudaFree) with size bookkeeping.  Every allocation
-// carries kTailSlack bytes beyond its n elements, so a 16-byte-granular bulk copy of a range
-// that ends at the last element (rounded up to 16 bytes) stays inside the allocation.
+// Owning device allocation with size bookkeeping.  Every allocation carries kTailSlack bytes
+// beyond its n elements, so a 16-byte-granular bulk copy of a range that ends at the last
+// element (rounded up to 16 bytes) stays inside the allocation.
+//
+// Allocations come from the device's default stream-ordered memory pool, which keeps up to
+// kPoolKeepBytes of freed memory mapped for reuse: plain cudaMalloc / cudaFree of the large
+// hierarchy and pack buffers map and unmap memory each time, and single calls of the AMG setup
+// took 0.1-0.9 s that way.  release() waits for the device before it frees, as cudaFree does,
+// so no stream can still be using a buffer when it returns to the pool.
 #pragma once
 
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <utility>
 #include <vector>
 
@@ -14,6 +21,20 @@
 namespace wn {
 
 constexpr size_t kTailSlack = 16;
+constexpr uint64_t kPoolKeepBytes = 4ull << 30;
+
+// once per device: the default pool keeps kPoolKeepBytes of freed memory instead of unmapping it
+inline void pool_keep_memory() {
+  static std::atomic<uint64_t> done{0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || (done.load() >> dev) & 1ull) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = kPoolKeepBytes;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  done.fetch_or(1ull << dev);
+}
 
 template <typename T>
 struct DArray {
@@ -38,7 +59,10 @@ struct DArray {
   }
   ~DArray() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      cudaDeviceSynchronize();
+      cudaFreeAsync(p, 0);
+    }
     p = nullptr;
     n = 0;
   }
@@ -46,7 +70,8 @@ struct DArray {
     if (count == n && p) return 0;
     release();
     if (count <= 0) return 0;
-    WN_CUDA(cudaMalloc((void**)&p, sizeof(T) * (size_t)count + kTailSlack));
+    pool_keep_memory();
+    WN_CUDA(cudaMallocAsync((void**)&p, sizeof(T) * (size_t)count + kTailSlack, 0));
     n = count;
     return 0;
   }

@@ -25,6 +25,8 @@
 #include <string>
 #include <type_traits>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "amg.h"
@@ -1625,6 +1627,16 @@ int solver_setup(Solid* s, const wn_amg_params& prm) {
   WN_REQUIRE(prm.smoother_degree >= 1 && prm.smoother_degree <= 8, WN_EINVAL, "AMG setup: smoother_degree in [1, 8]");
   WN_REQUIRE(prm.max_levels >= 1 && prm.max_levels <= 16, WN_EINVAL, "AMG setup: max_levels in [1, 16]");
   const auto t0 = std::chrono::steady_clock::now();
+  // WN_AMG_TRACE=1: the steps around the hierarchy build on stderr too
+  const bool trace = std::getenv("WN_AMG_TRACE") != nullptr;
+  auto tmark = t0;
+  auto step = [&](const char* what) {
+    if (!trace) return;
+    cudaDeviceSynchronize();
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "solver_setup: %-24s %8.3f s\n", what, std::chrono::duration<double>(now - tmark).count());
+    tmark = now;
+  };
   std::unique_ptr<AmgHierarchy> H(new AmgHierarchy());
   // device setup first (1 = a row beyond its shared-memory capacities: the host builder then)
   int dev_rc = 1;
@@ -1649,6 +1661,7 @@ int solver_setup(Solid* s, const wn_amg_params& prm) {
                        s->h_nodes.data(), fixed, H->host));
     H->levels.resize(H->host.levels.size());
   }
+  step("hierarchy build");
   H->degree = prm.smoother_degree;
   static uint64_t next_id = 0;
   H->id = ++next_id;
@@ -1690,6 +1703,7 @@ int solver_setup(Solid* s, const wn_amg_params& prm) {
     WN_CHECK(L.v64.alloc(h.n_nodes * h.bs));
     WN_CHECK(L.v32.alloc(h.n_nodes * h.bs));
   }
+  step("level packs and vectors");
   H->n_coarse = H->host.n_coarse;
   WN_CHECK(H->coarse_inv.upload(H->host.coarse_inv));
   WN_CHECK(H->cb64.alloc(H->n_coarse));
@@ -1697,11 +1711,14 @@ int solver_setup(Solid* s, const wn_amg_params& prm) {
   WN_CHECK(H->cb32.alloc(H->n_coarse));
   WN_CHECK(H->cx32.alloc(H->n_coarse));
   WN_CUDA(cudaDeviceSynchronize());
+  step("coarse upload");
   H->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  s->amg = std::move(H);
+  s->amg = std::move(H);  // frees the previous hierarchy
+  step("previous hierarchy freed");
   WN_CHECK(ensure_work(s));
   for (auto& a : s->work->graphs)
     for (auto& g : a) g.reset();
+  step("graphs reset");
   return 0;
 }
 
