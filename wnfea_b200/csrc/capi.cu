@@ -822,5 +822,7 @@ int wn_adjoint_compliance(void* h, const double* u, double* grad_E, double* grad
 }  // extern "C"
 
 namespace wn {
-Solid::~Solid() = default;
+Solid::~Solid() {
+  for (cudaEvent_t e : io_ev) cudaEventDestroy(e);
+}
 }

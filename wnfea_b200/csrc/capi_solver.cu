@@ -1,5 +1,7 @@
 // extern "C" boundary of the AMG setup and the PCG / mixed-precision solver.
+#include <algorithm>
 #include <cstring>
+#include <thread>
 
 #include "amg.h"
 #include "amg_device.h"
@@ -180,15 +182,50 @@ int wn_solve(void* h, const double* F, double* u, const wn_solve_params* params,
   WN_CUDA(cudaSetDevice(s->device));
   const int64_t n = s->n_nodes * s->bs;
   // staged through page-locked memory: a device copy from / into pageable memory (a freshly
-  // allocated result array in particular) runs at a fraction of the link's speed
+  // allocated result array in particular) runs at a fraction of the link's speed.  The copies
+  // go in chunks so that each host copy overlaps the DMA of its neighbour: F chunk k + 1 is
+  // copied into the staging buffer while chunk k uploads, u chunk k is copied out while chunk
+  // k + 1 downloads (on the legacy stream, which the solve's stream is ordered with).
+  constexpr int64_t kChunk = 1 << 17;  // doubles (1 MB)
+  const int nch = (int)((n + kChunk - 1) / kChunk);
   WN_CHECK(s->io_f.alloc(n));
   WN_CHECK(s->io_u.alloc(n));
   WN_CHECK(s->io_pin.at_least(2 * n));
-  std::memcpy(s->io_pin.p, F, n * sizeof(double));
-  WN_CUDA(cudaMemcpy(s->io_f.p, s->io_pin.p, n * sizeof(double), cudaMemcpyHostToDevice));
+  while ((int)s->io_ev.size() < nch) {
+    cudaEvent_t e = nullptr;
+    WN_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    s->io_ev.push_back(e);
+  }
+  for (int c = 0; c < nch; ++c) {
+    const int64_t a = c * kChunk, len = std::min(kChunk, n - a);
+    std::memcpy(s->io_pin.p + a, F + a, len * sizeof(double));
+    WN_CUDA(cudaMemcpyAsync(s->io_f.p + a, s->io_pin.p + a, len * sizeof(double), cudaMemcpyHostToDevice, 0));
+  }
+  // while the GPU solves, a helper thread touches every page of u (F is staged already, so u may
+  // alias it): a freshly allocated result array otherwise takes its page faults in the final copy
+  struct Toucher {
+    std::thread t;
+    ~Toucher() {
+      if (t.joinable()) t.join();
+    }
+  } touch;
+  touch.t = std::thread([u, n]() {
+    volatile double* v = u;
+    for (int64_t i = 0; i < n; i += 512) v[i] = 0.0;
+    if (n > 0) v[n - 1] = 0.0;
+  });
   WN_CHECK(solver_solve(s, s->io_f.p, s->io_u.p, *params, stats, 0));
-  WN_CUDA(cudaMemcpy(s->io_pin.p + n, s->io_u.p, n * sizeof(double), cudaMemcpyDeviceToHost));
-  std::memcpy(u, s->io_pin.p + n, n * sizeof(double));
+  touch.t.join();
+  for (int c = 0; c < nch; ++c) {
+    const int64_t a = c * kChunk, len = std::min(kChunk, n - a);
+    WN_CUDA(cudaMemcpyAsync(s->io_pin.p + n + a, s->io_u.p + a, len * sizeof(double), cudaMemcpyDeviceToHost, 0));
+    WN_CUDA(cudaEventRecord(s->io_ev[c], 0));
+  }
+  for (int c = 0; c < nch; ++c) {
+    const int64_t a = c * kChunk, len = std::min(kChunk, n - a);
+    WN_CUDA(cudaEventSynchronize(s->io_ev[c]));
+    std::memcpy(u + a, s->io_pin.p + n + a, len * sizeof(double));
+  }
   return 0;
 }
 

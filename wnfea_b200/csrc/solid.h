@@ -64,9 +64,11 @@ struct Solid {
   std::unique_ptr<SolverWork> work;
   std::unique_ptr<BlockWork> bwork;
   // host-buffer solve: device copies of F / u and a page-locked staging buffer (2 n), kept
-  // between calls so that a call neither allocates nor copies from pageable memory
+  // between calls so that a call neither allocates nor copies from pageable memory; one event
+  // per staged chunk of the result (its copy out of the staging buffer waits for that chunk only)
   DArray<double> io_f, io_u;
   PinnedArray<double> io_pin;
+  std::vector<cudaEvent_t> io_ev;
   ~Solid();
 };
 
