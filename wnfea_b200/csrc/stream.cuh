@@ -374,14 +374,6 @@ struct NoHook {
   __device__ __forceinline__ void operator()() const {}
 };
 
-template <int N, typename T>
-__device__ __forceinline__ T pick_lane(const T (&a)[N], int l) {
-  T v = a[0];
-#pragma unroll
-  for (int k = 1; k < N; ++k)
-    if (l == k) v = a[k];
-  return v;
-}
 
 // The tile pipeline.  Every thread of a CTA of Cfg::kThreads threads calls it once (dynamic
 // shared memory of stream_smem_bytes<T, BR, BC, Cfg>()); the pack was built from a plan with
@@ -517,6 +509,40 @@ __device__ __forceinline__ double stream_pipeline(const PackTile* __restrict__ t
   return dot;
 }
 
+__host__ __device__ constexpr int pow2_ceil(int v) { return v <= 1 ? 1 : 2 * pow2_ceil((v + 1) / 2); }
+__host__ __device__ constexpr int ilog2(int v) { return v <= 1 ? 0 : 1 + ilog2(v / 2); }
+
+// Sum of a[0 .. BR) over the G lanes of a row group, transposed: with P = BR rounded up to a
+// power of two, each of the first log2 P butterfly levels halves the values a lane holds -- it
+// keeps one half and trades the other with its partner -- and the remaining levels are plain
+// butterflies.  Lane gl ends with the whole sum of value gl >> (log2 G - log2 P): log2 P + P - 1
+// shuffles instead of BR log2 G (9 instead of 30 for 6 values over 32 lanes).
+template <int BR, int G, typename T>
+__device__ __forceinline__ T group_sum_transposed(const T (&a)[BR], int gl) {
+  constexpr int P = pow2_ceil(BR), LG = ilog2(G), LP = ilog2(P);
+  static_assert(G >= P && (1 << LG) == G, "a power-of-two group of at least P lanes");
+  T v[P];
+#pragma unroll
+  for (int r = 0; r < P; ++r) v[r] = r < BR ? a[r] : T(0);
+#pragma unroll
+  for (int k = 0; k < LG; ++k) {
+    const int o = G >> (k + 1);
+    if (k < LP) {
+      const int h = P >> (k + 1);
+      const bool up = (gl & o) != 0;
+#pragma unroll
+      for (int j = 0; j < h; ++j) {
+        const T send = up ? v[j] : v[j + h];
+        const T keep = up ? v[j + h] : v[j];
+        v[j] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+      }
+    } else {
+      v[0] += __shfl_xor_sync(0xffffffffu, v[0], o);
+    }
+  }
+  return v[0];
+}
+
 // a stored matrix value in the arithmetic type
 template <typename T, typename TV>
 __device__ __forceinline__ T value_as(TV v) {
@@ -546,6 +572,11 @@ __device__ __forceinline__ double stream_rows_v(const PackTile* __restrict__ til
   static_assert(BR <= G, "a lane per row DOF");
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gl = lane % G, grp = lane / G;
+  // after group_sum_transposed, row DOF r's sum is in lanes r << SH .. ((r + 1) << SH) - 1; the
+  // first of them loads the DOF's epilogue operands and stores its result
+  constexpr int SH = ilog2(G) - ilog2(pow2_ceil(BR));
+  const int my_r = gl >> SH;
+  const bool owner = (gl & ((1 << SH) - 1)) == 0 && my_r < BR;
   auto body = [&](int jc, const unsigned char* st, const int4 d, double& dot) {
     const int r0 = d.x, nr = d.y - d.x, cntp = d.w;
     const TV* sv = reinterpret_cast<const TV*>(st);
@@ -567,7 +598,7 @@ __device__ __forceinline__ double stream_rows_v(const PackTile* __restrict__ til
         re[q] = active ? srp[lr + 1] : 0;
         len = max(len, re[q] - rs[q]);
         pre[q] = typename EPI::Pre{};
-        if (active && gl < BR) pre[q] = epi.load((int64_t)(r0 + lr) * BR + gl);
+        if (active && owner) pre[q] = epi.load((int64_t)(r0 + lr) * BR + my_r);
 #pragma unroll
         for (int r = 0; r < BR; ++r) acc[q][r] = T(0);
       }
@@ -603,15 +634,9 @@ __device__ __forceinline__ double stream_rows_v(const PackTile* __restrict__ til
       }
 #pragma unroll
       for (int q = 0; q < R; ++q) {
-#pragma unroll
-        for (int r = 0; r < BR; ++r) {
-          T v = acc[q][r];
-#pragma unroll
-          for (int o2 = G / 2; o2 > 0; o2 >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o2);
-          acc[q][r] = v;
-        }
+        const T sum = group_sum_transposed<BR, G>(acc[q], gl);
         const int lr = base + q * GPW + grp;
-        if (lr < nr && gl < BR) dot += epi.store((int64_t)(r0 + lr) * BR + gl, pre[q], pick_lane<BR>(acc[q], gl));
+        if (lr < nr && owner) dot += epi.store((int64_t)(r0 + lr) * BR + my_r, pre[q], sum);
       }
     }
   };
