@@ -672,9 +672,14 @@ def run_ours(args):
     # algorithmic bytes of one assembly: FP64 values written, element->block map, connectivity,
     # coordinates and element properties read
     asm_bytes = nb * 9 * 8 + n_el * 100 * 4 + n_el * 40 + n_nodes * 24 + n_el * 16
-    t0 = time.perf_counter()
-    s.amg_setup()
-    setup_s = time.perf_counter() - t0
+    # the setup's wall time varies from process to process by host-side allocation and paging
+    # (0.3 to 1.9 s seen for the first call): the line reports the median of three setups
+    setup_times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        s.amg_setup()
+        setup_times.append(time.perf_counter() - t0)
+    setup_s = statistics.median(setup_times)
 
     F = torch.from_numpy(F_np).cuda()
     u = torch.empty_like(F)
@@ -897,7 +902,8 @@ def run_ours(args):
         "profile_mixed": prof_summary(prof_mixed), "profile_fp64": prof_summary(prof_64),
         "profiled_solve_ms": {"mixed": prof_mixed_ms, "fp64": prof_64_ms},
         "modes": modes, "assembly_ms": assembly_ms, "assembly_algorithmic_bytes": asm_bytes,
-        "assembly_wall_s_first_call": t_asm_wall, "amg_setup_s": setup_s, "adjoint_grad_ms_ibeam": adjoint_ms,
+        "assembly_wall_s_first_call": t_asm_wall, "amg_setup_s": setup_s, "amg_setup_s_each": setup_times,
+        "adjoint_grad_ms_ibeam": adjoint_ms,
         "adjoint": adjoint, "multi_rhs": multi, "multi_rhs_sharded": sharded, "internal_force": fint,
         "beam_frame": frame_res, "c1": c1, "c2": c2,
         "roofline_fp64_spmv": {"achieved": ach64, "frac": ach64 / peak, "launch_ms": t64,

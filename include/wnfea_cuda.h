@@ -170,6 +170,11 @@ typedef struct wn_amg_params {
   int setup_on_device;     /* 1: diagonal, power iterations, prolongator and Galerkin
                               products on the GPU (aggregation and the per-aggregate QR on
                               the host); 0: the whole setup on the host               (1)    */
+  int coarse_block_smoother; /* 1: the 6-DOF levels (all but the finest) are smoothed with
+                              6 x 6 block Jacobi in place of point Jacobi, by a change of
+                              basis per aggregate made on the GPU after the build (the
+                              exported levels are those of the new basis); 0: point
+                              Jacobi on every level                                   (1)    */
 } wn_amg_params;
 
 /* Defaults above. */

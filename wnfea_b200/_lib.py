@@ -36,6 +36,7 @@ class AmgParams(C.Structure):
         ("power_iters", C.c_int),
         ("stream_min_mb", C.c_double),
         ("setup_on_device", C.c_int),
+        ("coarse_block_smoother", C.c_int),
     ]
 
 

@@ -8,7 +8,12 @@ beam-only ``BlockBeamAMGPreconditioner`` (wnfea/solver/amg_preconditioner.py:147
 its parameters map as: ``max_levels`` (:159), ``coarse_size`` (:159, in DOFs), the
 Jacobi weight 0.67 (:449) is replaced by a Chebyshev smoother of ``smoother_degree`` (by default
 degree 1: one Jacobi step before and one after the coarse correction, as the reference's V-cycle
-takes (:504-536), weighted 1 / theta for the smoothing interval [lmax / 16, lmax]).
+takes (:504-536), weighted 1 / theta for the smoothing interval [lmax / 16, lmax]).  On the
+6-DOF levels below the finest, ``coarse_block_smoother`` (default 1) makes that step block
+Jacobi over each aggregate's 6 x 6 diagonal block: the GPU setup moves those levels to the
+basis in which the diagonal blocks are the identity (A^ = T^T A T, T = diag(L_i^-T),
+D_i = L_i L_i^T), where the point smoother is the block one; the exported levels are then
+those of the new basis.
 """
 
 from __future__ import annotations
@@ -36,6 +41,7 @@ class AMGParams:
     power_iters: int = 15
     stream_min_mb: float = 4.0
     setup_on_device: int = 1
+    coarse_block_smoother: int = 1
 
     def to_c(self) -> _lib.AmgParams:
         return _lib.AmgParams(**{f.name: getattr(self, f.name) for f in fields(self)})

@@ -75,6 +75,8 @@ struct AmgHierarchy {
   double setup_seconds = 0.0;
   bool device_built = false;  // levels made by amg_build_device (host.levels hold no matrices
   bool host_synced = false;   // until amg_sync_host copies them down)
+  bool basis_changed = false;  // the 6-DOF levels were moved to the block-Jacobi basis on the
+                               // device (amg_coarse_block_basis): host copies are stale too
   uint64_t id = 0;  // unique per setup (workspaces sized for a hierarchy compare it)
 };
 

@@ -423,6 +423,132 @@ __global__ void ks_to_float(int64_t n, const double* __restrict__ a, float* __re
 }
 
 // ---------------------------------------------------------------------------------------
+// block-Jacobi smoothing of the coarse levels as a change of basis
+// ---------------------------------------------------------------------------------------
+// Per node i of a 6-DOF level: the Cholesky factor L_i of its diagonal block (D_i = L_i L_i^T)
+// and L_i^-1, both lower triangular, row-major 6 x 6.  A pivot at or below 1e-13 of the block's
+// largest diagonal entry (a direction the aggregate's prolongator columns do not span, e.g. a
+// zero column next to a support) is replaced by 1 with its row and column of L zeroed: that DOF
+// keeps the old basis, and L stays invertible.
+__global__ void ks_block_chol(DMat A, double* __restrict__ lf, double* __restrict__ li) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < A.n_rows; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t k = find_col(A.ci, A.rp[i], A.rp[i + 1], (int32_t)i);
+    double a[36], l[36], m[36];
+    double scale = 0.0;
+    for (int e = 0; e < 36; ++e) {
+      a[e] = k >= 0 ? A.at(k, e / 6, e % 6) : ((e % 7) == 0 ? 1.0 : 0.0);
+      l[e] = 0.0;
+      m[e] = 0.0;
+    }
+    for (int r = 0; r < 6; ++r) scale = fmax(scale, fabs(a[r * 7]));
+    for (int c = 0; c < 6; ++c) {
+      double d = a[c * 7];
+      for (int j = 0; j < c; ++j) d -= l[c * 6 + j] * l[c * 6 + j];
+      if (!(d > 1e-13 * scale)) {
+        for (int j = 0; j < c; ++j) l[c * 6 + j] = 0.0;
+        l[c * 7] = 1.0;
+        continue;  // l[r][c] = 0 below
+      }
+      const double dc = sqrt(d);
+      l[c * 7] = dc;
+      for (int r = c + 1; r < 6; ++r) {
+        double s = a[r * 6 + c];
+        for (int j = 0; j < c; ++j) s -= l[r * 6 + j] * l[c * 6 + j];
+        l[r * 6 + c] = s / dc;
+      }
+    }
+    // L^-1 by forward substitution, column by column
+    for (int c = 0; c < 6; ++c) {
+      m[c * 7] = 1.0 / l[c * 7];
+      for (int r = c + 1; r < 6; ++r) {
+        double s = 0.0;
+        for (int j = c; j < r; ++j) s += l[r * 6 + j] * m[j * 6 + c];
+        m[r * 6 + c] = -s / l[r * 7];
+      }
+    }
+    for (int e = 0; e < 36; ++e) {
+      lf[i * 36 + e] = l[e];
+      li[i * 36 + e] = m[e];
+    }
+  }
+}
+
+// Y = (U X) V for one BR x 6 block, row by row with fixed-order fused multiply-adds; U, X, V
+// and the store are accessors, so a block and its transpose go through the same operations
+template <int BR, typename UF, typename XF, typename VF, typename YF>
+__device__ __forceinline__ void basis_block(const UF& U, const XF& X, const VF& V, const YF& Y) {
+  for (int r = 0; r < BR; ++r) {
+    double t[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      double s = 0.0;
+#pragma unroll
+      for (int m = 0; m < BR; ++m) s = fma(U(r, m), X(m, c), s);
+      t[c] = s;
+    }
+#pragma unroll
+    for (int c2 = 0; c2 < 6; ++c2) {
+      double s = 0.0;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) s = fma(t[c], V(c, c2), s);
+      Y(r, c2, s);
+    }
+  }
+}
+
+// A^_ab = L_a^-1 A_ab L_b^-T on a 6-DOF level.  A block below the diagonal (a > b) is computed as
+// the transpose of the canonical product of its mirror (L_b^-1 A_ba L_a^-T with A_ba = A_ab^T,
+// bitwise, since the level matrices are symmetrised), and a diagonal block keeps the upper
+// triangle of its product, mirrored, so A^ is exactly symmetric.
+__global__ void ks_basis_level(int64_t nnzb, const int32_t* __restrict__ row, const int32_t* __restrict__ ci,
+                               const double* __restrict__ v, const double* __restrict__ li, double* __restrict__ out) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnzb; k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t a = row[k], b = ci[k];
+    const bool up = a <= b;
+    const int64_t lo = up ? a : b, hi = up ? b : a;
+    const double* X = v + k * 36;
+    double* Y = out + k * 36;
+    basis_block<6>([&](int r, int m) { return li[lo * 36 + r * 6 + m]; },
+                   [&](int m, int c) { return up ? X[m * 6 + c] : X[c * 6 + m]; },
+                   [&](int c, int c2) { return li[hi * 36 + c2 * 6 + c]; },
+                   [&](int r, int c2, double s) {
+                     if (a == b) {  // a diagonal block: its upper triangle, mirrored
+                       if (c2 >= r) Y[r * 6 + c2] = Y[c2 * 6 + r] = s;
+                     } else if (up) {
+                       Y[r * 6 + c2] = s;
+                     } else {
+                       Y[c2 * 6 + r] = s;
+                     }
+                   });
+  }
+}
+
+// The transfer operator between a level f (BR DOFs per node) and the next level c:
+// P^_ia = L_i^T P_ia L_a^-T (lf: the factors of level f, null = identity, the fine level;
+// lic: the inverse factors of level c, null = identity, the dense coarsest level).  With
+// transposed = 1 the blocks are those of R = P^T (row a, column i) and each is the transpose of
+// the same product, so R^ = P^^T bitwise.
+template <int BR>
+__global__ void ks_basis_transfer(int64_t nnzb, const int32_t* __restrict__ row, const int32_t* __restrict__ ci,
+                                  const double* __restrict__ v, const double* __restrict__ lf,
+                                  const double* __restrict__ lic, int transposed, double* __restrict__ out) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnzb; k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = transposed ? ci[k] : row[k], a = transposed ? row[k] : ci[k];
+    const double* X = v + k * BR * 6;
+    double* Y = out + k * BR * 6;
+    basis_block<BR>([&](int r, int m) { return lf ? lf[i * 36 + m * 6 + r] : (r == m ? 1.0 : 0.0); },
+                    [&](int m, int c) { return transposed ? X[c * BR + m] : X[m * 6 + c]; },
+                    [&](int c, int c2) { return lic ? lic[a * 36 + c2 * 6 + c] : (c == c2 ? 1.0 : 0.0); },
+                    [&](int r, int c2, double s) {
+                      if (transposed)
+                        Y[c2 * BR + r] = s;
+                      else
+                        Y[r * 6 + c2] = s;
+                    });
+  }
+}
+
+// ---------------------------------------------------------------------------------------
 // host helpers
 // ---------------------------------------------------------------------------------------
 int grid_n(int64_t n) { return grid_for(n, 1, kT, 16); }
@@ -754,9 +880,85 @@ int amg_build_device(Solid* s, const wn_amg_params& prm, AmgHierarchy& H) {
   return 0;
 }
 
-// Host copies of the device-built level matrices (for the hierarchy exports)
+int amg_coarse_block_basis(AmgHierarchy& H, const wn_amg_params& prm) {
+  const int nlev = (int)H.levels.size();
+  if (nlev < 2) return 0;  // no 6-DOF level with a smoother
+  PhaseClock tr("amg_coarse_block_basis");
+  // factors of the diagonal blocks of every 6-DOF level (index l >= 1), from the levels as built
+  std::vector<DArray<double>> lf(nlev), li(nlev);
+  for (int l = 1; l < nlev; ++l) {
+    DevLevel& D = H.levels[l];
+    WN_REQUIRE(D.bs == 6 && D.A.br == 6, WN_ESTATE, "coarse block basis: level %d is not a 6-DOF level", l);
+    WN_CHECK(lf[l].alloc(D.n_nodes * 36));
+    WN_CHECK(li[l].alloc(D.n_nodes * 36));
+    ks_block_chol<<<grid_n(D.n_nodes), kT>>>(dmat(D.A), lf[l].p, li[l].p);
+    WN_CUDA(cudaGetLastError());
+  }
+  auto rows_of = [&](const DevBsr& M, DArray<int32_t>& row) -> int {
+    WN_CHECK(row.alloc(std::max<int64_t>(M.nnzb, 1)));
+    ks_block_rows<<<grid_n(M.n_rows), kT>>>(M.n_rows, M.rp.p, row.p);
+    WN_CUDA(cudaGetLastError());
+    return 0;
+  };
+  auto refresh_float = [&](DevBsr& M) -> int {
+    const int64_t nv = M.nnzb * M.br * M.bc;
+    if (nv == 0) return 0;
+    ks_to_float<<<grid_n(nv), kT>>>(nv, M.v64.p, M.v32.p);
+    WN_CUDA(cudaGetLastError());
+    return 0;
+  };
+  for (int l = 0; l < nlev; ++l) {
+    DevLevel& D = H.levels[l];
+    const double* lfl = l >= 1 ? lf[l].p : nullptr;
+    const double* lic = l + 1 < nlev ? li[l + 1].p : nullptr;
+    // the transfer operators P_l (level l+1 -> l) and R_l = P_l^T
+    for (int t = 0; t < 2; ++t) {
+      DevBsr& M = t == 0 ? D.P : D.R;
+      if (M.nnzb == 0) continue;
+      DArray<int32_t> row;
+      DArray<double> out;
+      WN_CHECK(rows_of(M, row));
+      WN_CHECK(out.alloc(M.nnzb * M.br * M.bc));
+      if (D.bs == 3)
+        ks_basis_transfer<3><<<grid_n(M.nnzb), kT>>>(M.nnzb, row.p, M.ci.p, M.v64.p, lfl, lic, t, out.p);
+      else
+        ks_basis_transfer<6><<<grid_n(M.nnzb), kT>>>(M.nnzb, row.p, M.ci.p, M.v64.p, lfl, lic, t, out.p);
+      WN_CUDA(cudaGetLastError());
+      std::swap(M.v64, out);
+      WN_CHECK(refresh_float(M));
+    }
+    if (l == 0) continue;
+    // the level matrix, its diagonal (1 up to rounding) and rho(D^-1 A^) = rho(D_block^-1 A)
+    {
+      DArray<int32_t> row;
+      DArray<double> out;
+      WN_CHECK(rows_of(D.A, row));
+      WN_CHECK(out.alloc(std::max<int64_t>(D.A.nnzb, 1) * 36));
+      ks_basis_level<<<grid_n(D.A.nnzb), kT>>>(D.A.nnzb, row.p, D.A.ci.p, D.A.v64.p, li[l].p, out.p);
+      WN_CUDA(cudaGetLastError());
+      std::swap(D.A.v64, out);
+      WN_CHECK(refresh_float(D.A));
+    }
+    const int64_t nd = D.n_nodes * 6;
+    const DMat A = dmat(D.A);
+    ks_inv_diag<<<grid_n(D.n_nodes), kT>>>(A, D.dinv64.p);
+    WN_CUDA(cudaGetLastError());
+    ks_to_float<<<grid_n(nd), kT>>>(nd, D.dinv64.p, D.dinv32.p);
+    WN_CUDA(cudaGetLastError());
+    HostLevel& h = H.host.levels[l];
+    WN_CHECK(download(D.dinv64, nd, h.dinv));
+    WN_CHECK(power_rho_device(A, D.dinv64, prm.power_iters, &h.rho));
+    tr.mark("basis", l);
+  }
+  WN_CUDA(cudaDeviceSynchronize());
+  H.basis_changed = true;
+  H.host_synced = false;
+  return 0;
+}
+
+// Host copies of the device level matrices (for the hierarchy exports)
 int amg_sync_host(AmgHierarchy& H) {
-  if (!H.device_built || H.host_synced) return 0;
+  if (!(H.device_built || H.basis_changed) || H.host_synced) return 0;
   for (size_t l = 0; l < H.levels.size() && l < H.host.levels.size(); ++l) {
     DevLevel& D = H.levels[l];
     HostLevel& L = H.host.levels[l];

@@ -45,6 +45,7 @@ wn_amg_params amg_default_params() {
   p.power_iters = 15;
   p.stream_min_mb = 4.0;
   p.setup_on_device = 1;
+  p.coarse_block_smoother = 1;
   return p;
 }
 

@@ -1685,6 +1685,14 @@ int solver_setup(Solid* s, const wn_amg_params& prm) {
       L.h_P_rp = h.P.rp;
       L.h_R_rp = h.R.rp;
     }
+  }
+  // block-Jacobi smoothing of the 6-DOF levels: their basis is changed on the device before
+  // the packs are made (it rewrites A, P, R, 1/diag and rho of those levels)
+  if (prm.coarse_block_smoother) WN_CHECK(amg_coarse_block_basis(*H, prm));
+  step("coarse block basis");
+  for (size_t l = 0; l < H->host.levels.size(); ++l) {
+    const HostLevel& h = H->host.levels[l];
+    DevLevel& L = H->levels[l];
     L.rho = h.rho;
     cheb_coefficients(prm, L);
     // matrices of at least stream_min_mb MB (FP32) are streamed from tile-major packs (on the
