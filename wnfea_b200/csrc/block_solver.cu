@@ -1254,6 +1254,69 @@ __global__ void __launch_bounds__(kThreads) kb_spmv_dot(int64_t n_rows, const in
   write_case_parts<double>(dot, partB);
 }
 
+// The mixed batch (FP32 V-cycle) keeps its search directions in FP32: p = z + beta p is formed
+// once per iteration in FP64 and rounded (kb_pnew32), and the product gathers those FP32
+// values (12 bytes per column DOF and case pair instead of the 8-byte p and 4-byte z of the
+// fused kb_spmv_dot) into FP64 sums with the FP64 matrix.  x is updated with the same rounded p
+// whose product gave q, so r = b - A x still holds to FP64 rounding; only the A-conjugacy of the
+// directions carries the FP32 rounding (on the I-beam the iteration counts did not change).
+template <typename TM>
+__global__ void __launch_bounds__(kThreads) kb_pnew32(int64_t n, const TM* __restrict__ z, float* __restrict__ p,
+                                                      const BlockScalars* __restrict__ S) {
+  if (S->done) return;
+  const int l0 = threadIdx.x & 7;
+  const C4<double> b = case_scalars<float>(S->beta, l0);
+  BATCH_DOF_LOOP(n) {
+    const int64_t o = i * kBatch;
+    const C4<double> zz = cvt4<double>(ldc<float>(z + o, l));
+    const C4<float> pp = ldc<float>(p + o, l);
+    C4<float> pn;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) pn.v[k] = (float)(zz.v[k] + b.v[k] * (double)pp.v[k]);
+    stc<float>(p + o, l, pn);
+  }
+}
+
+struct BLoadWide {  // FP32 case rows with the double case map, widened to FP64
+  const float* __restrict__ x;
+  __device__ __forceinline__ C4<double> operator()(int64_t i, int l) const {
+    return cvt4<double>(ldc<double>(x + i * kBatch, l));
+  }
+};
+
+// q = A p (fine matrix, component-major FP64; p FP32); partB = p . q
+__global__ void __launch_bounds__(kThreads) kb_spmv_dot32(int64_t n_rows, const int32_t* __restrict__ rp,
+                                                          const int32_t* __restrict__ ci,
+                                                          const double* __restrict__ av, int64_t stride,
+                                                          const float* __restrict__ p, double* __restrict__ q,
+                                                          double* __restrict__ partB,
+                                                          const BlockScalars* __restrict__ S) {
+  if (S->done) return;
+  double dot[4] = {0.0, 0.0, 0.0, 0.0};
+  {
+    BATCH_ROW_LOOP(n_rows) {
+      const BLoadWide pf{p};
+      double acc[3][4];
+      batch_row_staged<3, 3, kSoA, Tpg<double>::value, 1, double>(rp, ci, av, stride, row, row < n_rows, l, pf,
+                                                               FmaAcc<3, double>(acc));
+      if (row >= n_rows) continue;
+#pragma unroll
+      for (int rr = 0; rr < 3; ++rr) {
+        const int64_t i = row * 3 + rr;
+        const C4<double> pv = pf(i, l);
+        C4<double> qv;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          qv.v[k] = acc[rr][k];
+          dot[k] += pv.v[k] * qv.v[k];
+        }
+        stc<double>(q + i * kBatch, l, qv);
+      }
+    }
+  }
+  write_case_parts<double>(dot, partB);
+}
+
 // alpha = rz / (p . q) for the running cases; a non-positive curvature ends that case
 __global__ void kb_alpha(BlockScalars* S, const double* __restrict__ partB, int nparts) {
   if (S->done) return;
@@ -1273,10 +1336,11 @@ __global__ void kb_alpha(BlockScalars* S, const double* __restrict__ partB, int 
   }
 }
 
-// x += alpha p; r -= alpha q; rm = (TM) r (if rm); partC = r . r per case
-template <typename TM>
+// x += alpha p; r -= alpha q; rm = (TM) r (if rm); partC = r . r per case (p: FP64, or the mixed
+// batch's FP32 search directions, widened)
+template <typename TM, typename TP = double>
 __global__ void __launch_bounds__(kThreads) kb_update(int64_t n, double* __restrict__ x, double* __restrict__ r,
-                                                      TM* __restrict__ rm, const double* __restrict__ p,
+                                                      TM* __restrict__ rm, const TP* __restrict__ p,
                                                       const double* __restrict__ q, double* __restrict__ partC,
                                                       const BlockScalars* __restrict__ S, TM* __restrict__ d0,
                                                       const TM* __restrict__ dinv, TM inv_theta) {
@@ -1288,7 +1352,7 @@ __global__ void __launch_bounds__(kThreads) kb_update(int64_t n, double* __restr
     BATCH_DOF_LOOP(n) {
       const int64_t o = i * kBatch;
       C4<double> xv = ldc<double>(x + o, l), rv = ldc<double>(r + o, l);
-      const C4<double> pv = ldc<double>(p + o, l), qv = ldc<double>(q + o, l);
+      const C4<double> pv = cvt4<double>(ldc<double>(p + o, l)), qv = ldc<double>(q + o, l);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         if (a.v[k] != 0.0) {  // finished cases keep x and r exactly (their p may be anything)
@@ -1705,20 +1769,35 @@ const TM* prec_input(BlockWork& W) {
     return W.r32.p;
 }
 
+// FP32 search directions (kb_pnew32 / kb_spmv_dot32): the mixed batch on the register fine
+// level; the FP64 batch and the streamed fine level keep FP64 directions
+template <typename TM>
+bool fp32_directions(const Solid* s) {
+  return std::is_same<TM, float>::value && !s->stream_batched;
+}
+
 // one batched PCG iteration (parity k & 1 selects the p buffers)
 template <typename TM>
 int batch_iteration(Solid* s, BlockWork& W, int precond, int k, BlockScalars* S, cudaStream_t st) {
   const int par = k & 1;
   double* p_new = par ? W.p1.p : W.p0.p;
   double* p_old = par ? W.p0.p : W.p1.p;
+  const bool p32 = fp32_directions<TM>(s);
+  float* p_f = reinterpret_cast<float*>(W.p0.p);  // the FP32 directions, in place
   // the fine FP64 matrix streamed from its pack when batched streaming is on, else the
   // register kernel
-  int gsd = s->stream_batched ? launch_bs<double>(kbs_spmv_dot<TM>, s->fine, st, bview<double>(s->fine),
-                                                  (const TM*)BPrec<TM>::z(W), (const double*)p_old, p_new, W.q.p,
-                                                  W.partB.p, S)
-                              : 0;
-
-  if (gsd == 0) {
+  int gsd = (s->stream_batched && !p32)
+                ? launch_bs<double>(kbs_spmv_dot<TM>, s->fine, st, bview<double>(s->fine),
+                                    (const TM*)BPrec<TM>::z(W), (const double*)p_old, p_new, W.q.p, W.partB.p, S)
+                : 0;
+  if (p32) {
+    kb_pnew32<TM><<<resident_grid(kb_pnew32<TM>, kThreads, quads_work(W.n)), kThreads, 0, st>>>(
+        W.n, BPrec<TM>::z(W), p_f, S);
+    gsd = resident_grid(kb_spmv_dot32, kThreads, rows_work(s->n_nodes));
+    kb_spmv_dot32<<<gsd, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, s->nnzb, p_f, W.q.p,
+                                            W.partB.p, S);
+    W.launches++;
+  } else if (gsd == 0) {
     gsd = resident_grid(kb_spmv_dot<TM>, kThreads, rows_work(s->n_nodes));
     kb_spmv_dot<TM><<<gsd, kThreads, 0, st>>>(s->n_nodes, s->row_ptr.p, s->col_idx.p, s->k64.p, s->nnzb,
                                               BPrec<TM>::z(W), p_old, p_new, W.q.p, W.partB.p, S);
@@ -1729,8 +1808,12 @@ int batch_iteration(Solid* s, BlockWork& W, int precond, int k, BlockScalars* S,
   TM* d0 = (precond == 2 && s->amg && !s->amg->levels.empty()) ? BPrec<TM>::d0(W) : nullptr;
   const TM it0 = d0 ? (TM)s->amg->levels[0].inv_theta : TM(0);
   const int gup = resident_grid(kb_update<TM>, kThreads, quads_work(W.n));
-  kb_update<TM><<<gup, kThreads, 0, st>>>(W.n, W.x.p, W.r.p, BPrec<TM>::rm(W), p_new, W.q.p, W.partC.p, S, d0,
-                                          BPrec<TM>::fine_dinv(W), it0);
+  if (p32)
+    kb_update<TM, float><<<gup, kThreads, 0, st>>>(W.n, W.x.p, W.r.p, BPrec<TM>::rm(W), p_f, W.q.p, W.partC.p, S,
+                                                   d0, BPrec<TM>::fine_dinv(W), it0);
+  else
+    kb_update<TM><<<gup, kThreads, 0, st>>>(W.n, W.x.p, W.r.p, BPrec<TM>::rm(W), p_new, W.q.p, W.partC.p, S, d0,
+                                            BPrec<TM>::fine_dinv(W), it0);
   W.npC = gup;
   kb_check<<<1, kThreads, 0, st>>>(S, W.partC.p, W.npC);
   W.launches += 4;
