@@ -215,16 +215,34 @@ __global__ void beam_dense_kernel(int64_t n_nodes, const int32_t* __restrict__ r
   }
 }
 
-// In-place LU with partial pivoting and solve of A x = b on one CTA (x overwrites b).
-// status: 0 ok, 1 singular.  Every loop is bounded by n.
-__global__ void __launch_bounds__(1024) beam_dense_lu_solve_kernel(int n, double* __restrict__ A,
-                                                                   double* __restrict__ b, int* __restrict__ status) {
+// Blocked right-looking LU with partial pivoting and the solve of A x = b (x overwrites b),
+// in panels of kLuPanel columns: per panel
+//   beam_lu_panel_kernel   (one CTA)   pivots, row swaps, multipliers and rank-1 updates inside
+//                                      the panel's columns, and the forward elimination of b;
+//   beam_lu_swap_trsm_kernel (a thread per trailing column) the panel's row swaps and
+//                                      U12 = L11^-1 A12 on the columns right of the panel;
+//   beam_lu_update_kernel  (32 x 32 tiles) A22 -= L21 U12, each element subtracting the
+//                                      panel's terms in column order;
+// then beam_lu_backsub_kernel (one CTA).  Every element sees the unblocked algorithm's
+// operations in its order (fused multiply-adds), so the factors and x do not depend on the
+// panel width.  The multipliers of earlier panels are never read again (b is eliminated as
+// the panels go), so row swaps touch the panel, the trailing columns and b only.
+// status: 0 ok, 1 singular (a zero pivot column; the later kernels then see status != 0 and
+// return).  Every loop is bounded by n.
+constexpr int kLuPanel = 32;
+
+__global__ void __launch_bounds__(1024) beam_lu_panel_kernel(int n, int k0, double* __restrict__ A,
+                                                             double* __restrict__ b, int* __restrict__ piv,
+                                                             int* __restrict__ status) {
   __shared__ double sv[32];
   __shared__ int si[32];
   __shared__ int s_piv;
   __shared__ double s_pv;
+  if (status[0] != 0) return;
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int k = 0; k < n; ++k) {
+  const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  const int k1 = min(n, k0 + kLuPanel);
+  for (int k = k0; k < k1; ++k) {
     // pivot: argmax |A[i][k]|, i >= k (ties -> smallest i)
     double best = -1.0;
     int bi = k;
@@ -243,30 +261,29 @@ __global__ void __launch_bounds__(1024) beam_dense_lu_solve_kernel(int n, double
         bi = oi;
       }
     }
-    if ((tid & 31) == 0) {
-      sv[tid >> 5] = best;
-      si[tid >> 5] = bi;
+    if (lane == 0) {
+      sv[warp] = best;
+      si[warp] = bi;
     }
     __syncthreads();
     if (tid == 0) {
       double bb = sv[0];
       int ii = si[0];
-      for (int w = 1; w < (nt + 31) / 32; ++w)
+      for (int w = 1; w < nw; ++w)
         if (sv[w] > bb || (sv[w] == bb && si[w] < ii)) {
           bb = sv[w];
           ii = si[w];
         }
       s_piv = ii;
       s_pv = bb;
+      piv[k - k0] = ii;
+      if (!(bb > 0.0)) status[0] = 1;
     }
     __syncthreads();
-    if (!(s_pv > 0.0)) {
-      if (tid == 0) status[0] = 1;
-      return;
-    }
+    if (!(s_pv > 0.0)) return;
     const int p = s_piv;
-    if (p != k) {
-      for (int j = tid; j < n; j += nt) {
+    if (p != k) {  // the panel's columns and b
+      for (int j = k0 + tid; j < k1; j += nt) {
         const double t = A[(int64_t)k * n + j];
         A[(int64_t)k * n + j] = A[(int64_t)p * n + j];
         A[(int64_t)p * n + j] = t;
@@ -278,31 +295,87 @@ __global__ void __launch_bounds__(1024) beam_dense_lu_solve_kernel(int n, double
       }
     }
     __syncthreads();
-    const double piv = A[(int64_t)k * n + k];
-    const int m = n - k - 1;
-    // eliminate below the pivot: rows k+1..n-1, columns k..n-1 (column k keeps the multiplier)
-    for (int64_t t = tid; t < (int64_t)m * (m + 1); t += nt) {
-      const int i = k + 1 + (int)(t / (m + 1));
-      const int j = k + (int)(t % (m + 1));
-      const double l = A[(int64_t)i * n + k] / piv;
-      if (j > k) A[(int64_t)i * n + j] -= l * A[(int64_t)k * n + j];
+    const double pv = A[(int64_t)k * n + k];
+    for (int i = k + 1 + tid; i < n; i += nt) {
+      const double l = A[(int64_t)i * n + k] / pv;
+      A[(int64_t)i * n + k] = l;
+      b[i] = fma(-l, b[k], b[i]);
     }
     __syncthreads();
-    for (int i = k + 1 + tid; i < n; i += nt) {
-      const double l = A[(int64_t)i * n + k] / piv;
-      b[i] -= l * b[k];
+    // rank-1 update of the panel's remaining columns: a warp per row
+    const double* __restrict__ pk = A + (int64_t)k * n;
+    for (int i = k + 1 + warp; i < n; i += nw) {
+      double* __restrict__ ai = A + (int64_t)i * n;
+      const double l = ai[k];
+      for (int j = k + 1 + lane; j < k1; j += 32) ai[j] = fma(-l, pk[j], ai[j]);
     }
     __syncthreads();
   }
-  // back substitution, column oriented
+}
+
+// columns j >= k0 + kLuPanel: the panel's row swaps in order, then U12 = L11^-1 A12 (unit lower
+// L11), one thread per column
+__global__ void beam_lu_swap_trsm_kernel(int n, int k0, double* __restrict__ A, const int* __restrict__ piv,
+                                         const int* __restrict__ status) {
+  if (status[0] != 0) return;
+  const int k1 = min(n, k0 + kLuPanel);
+  for (int j = k1 + blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    for (int k = k0; k < k1; ++k) {
+      const int p = piv[k - k0];
+      if (p != k) {
+        const double t = A[(int64_t)k * n + j];
+        A[(int64_t)k * n + j] = A[(int64_t)p * n + j];
+        A[(int64_t)p * n + j] = t;
+      }
+    }
+    for (int k = k0; k < k1; ++k) {
+      const double ukj = A[(int64_t)k * n + j];
+      for (int i = k + 1; i < k1; ++i) A[(int64_t)i * n + j] = fma(-A[(int64_t)i * n + k], ukj, A[(int64_t)i * n + j]);
+    }
+  }
+}
+
+// A22 -= L21 U12 for rows and columns >= k0 + kLuPanel: a 32 x 32 tile per CTA (32 x 8 threads,
+// four rows each), L21 and U12 tiles staged in shared memory
+__global__ void __launch_bounds__(256) beam_lu_update_kernel(int n, int k0, double* __restrict__ A,
+                                                             const int* __restrict__ status) {
+  __shared__ double sl[32][kLuPanel + 1];
+  __shared__ double su[kLuPanel][32 + 1];
+  if (status[0] != 0) return;
+  const int k1 = min(n, k0 + kLuPanel), w = k1 - k0;
+  const int r0 = k1 + blockIdx.y * 32, c0 = k1 + blockIdx.x * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int e = threadIdx.x; e < 32 * kLuPanel; e += 256) {
+    const int r = e / kLuPanel, c = e % kLuPanel;
+    sl[r][c] = (r0 + r < n && c < w) ? A[(int64_t)(r0 + r) * n + k0 + c] : 0.0;
+    const int kr = e / 32, cc = e % 32;
+    su[kr][cc] = (kr < w && c0 + cc < n) ? A[(int64_t)(k0 + kr) * n + c0 + cc] : 0.0;
+  }
+  __syncthreads();
+  const int j = c0 + tx;
+  if (j >= n) return;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int r = ty + 8 * q, i = r0 + r;
+    if (i >= n) continue;
+    double a = A[(int64_t)i * n + j];
+    for (int k = 0; k < w; ++k) a = fma(-sl[r][k], su[k][tx], a);
+    A[(int64_t)i * n + j] = a;
+  }
+}
+
+// back substitution with the upper factor, column oriented
+__global__ void __launch_bounds__(1024) beam_lu_backsub_kernel(int n, const double* __restrict__ A,
+                                                               double* __restrict__ b, const int* __restrict__ status) {
+  if (status[0] != 0) return;
+  const int tid = threadIdx.x, nt = blockDim.x;
   for (int k = n - 1; k >= 0; --k) {
     if (tid == 0) b[k] /= A[(int64_t)k * n + k];
     __syncthreads();
     const double xk = b[k];
-    for (int i = tid; i < k; i += nt) b[i] -= A[(int64_t)i * n + k] * xk;
+    for (int i = tid; i < k; i += nt) b[i] = fma(-A[(int64_t)i * n + k], xk, b[i]);
     __syncthreads();
   }
-  if (tid == 0) status[0] = 0;
 }
 
 }  // namespace wn
@@ -614,11 +687,23 @@ int wn_beam_solve_device(void* h, const double* d_b, double* d_x, int method, do
     WN_REQUIRE(n <= WN_BEAM_DENSE_MAX, WN_ETOOBIG, "wn_beam_solve_device: dense LU limited to %d DOFs",
                WN_BEAM_DENSE_MAX);
     WN_CHECK(b->dense.alloc(n * n));
-    WN_CHECK(b->dstat.alloc(1));
+    WN_CHECK(b->dstat.alloc(1 + kLuPanel));  // [0] status, [1..] the current panel's pivots
     WN_CUDA(cudaMemsetAsync(b->dense.p, 0, n * n * sizeof(double), st));
+    WN_CUDA(cudaMemsetAsync(b->dstat.p, 0, sizeof(int), st));
     beam_dense_kernel<<<grid_for(n, 1, 256, 8), 256, 0, st>>>(b->n_nodes, b->rp.p, b->ci.p, b->K.p, b->dense.p);
     WN_CUDA(cudaMemcpyAsync(d_x, d_b, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    beam_dense_lu_solve_kernel<<<1, 1024, 0, st>>>((int)n, b->dense.p, d_x, b->dstat.p);
+    const int ni = (int)n;
+    int* piv = b->dstat.p + 1;
+    for (int k0 = 0; k0 < ni; k0 += kLuPanel) {
+      beam_lu_panel_kernel<<<1, 1024, 0, st>>>(ni, k0, b->dense.p, d_x, piv, b->dstat.p);
+      const int rest = ni - std::min(ni, k0 + kLuPanel);
+      if (rest > 0) {
+        beam_lu_swap_trsm_kernel<<<(rest + 127) / 128, 128, 0, st>>>(ni, k0, b->dense.p, piv, b->dstat.p);
+        const unsigned tiles = (unsigned)((rest + 31) / 32);
+        beam_lu_update_kernel<<<dim3(tiles, tiles), 256, 0, st>>>(ni, k0, b->dense.p, b->dstat.p);
+      }
+    }
+    beam_lu_backsub_kernel<<<1, 1024, 0, st>>>(ni, b->dense.p, d_x, b->dstat.p);
     WN_CUDA(cudaGetLastError());
     int stat = 0;
     WN_CUDA(cudaMemcpyAsync(&stat, b->dstat.p, sizeof(int), cudaMemcpyDeviceToHost, st));
