@@ -414,8 +414,8 @@ int wn_beam_evaluate_device(void* h, const double* d_U, double* d_fint, int asse
 int wn_beam_evaluate(void* h, const double* U, double* fint, int assemble_tangent, int apply_bcs);
 /* Host copy of the tangent values: nnzb x 36, row-major 6x6 blocks. */
 int wn_beam_get_tangent(void* h, double* values);
-/* Solve K_t x = b (K_t is not symmetric away from U = 0).  method 1: dense LU with partial
- * pivoting on one CTA (frames up to WN_BEAM_DENSE_MAX DOFs); 2: BiCGStab preconditioned by
+/* Solve K_t x = b (K_t is not symmetric away from U = 0).  method 1: dense blocked LU with
+ * partial pivoting (frames up to WN_BEAM_DENSE_MAX DOFs); 2: BiCGStab preconditioned by
  * the inverse 6x6 diagonal blocks (rtol, max_iter); 0: dense when it fits, else BiCGStab.
  * Returns WN_ENOCONV / WN_EBREAKDOWN (singular) as status; rel_res = ||b - K x|| / ||b||. */
 #define WN_BEAM_DENSE_MAX 3072
