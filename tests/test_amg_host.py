@@ -84,6 +84,39 @@ def test_oracle_pcg_with_hierarchy_converges(case):
     assert np.linalg.norm(x - u_ref) / np.linalg.norm(u_ref) < 1e-8
 
 
+def test_oracle_block_smoother_helpers_and_vcycle(case):
+    """The oracle's block-Jacobi pieces behind the coarse-level change of basis: the block
+    Cholesky (with its rule for a direction a block does not span), the block-diagonal inverse,
+    and PCG with block smoothing on the 6-DOF levels reaching the direct solution."""
+    m, K, F, mask, H = case
+    rng = np.random.default_rng(4)
+    M = rng.standard_normal((3, 6, 6))
+    D = M @ np.transpose(M, (0, 2, 1)) + 6.0 * np.eye(6)
+    D[1] = 0.0
+    D[1, :3, :3] = 2.0 * np.eye(3)  # spans three of the six directions
+    L = oamg.block_cholesky(D)
+    for k in (0, 2):
+        np.testing.assert_allclose(L[k] @ L[k].T, D[k], rtol=0, atol=1e-12 * np.abs(D[k]).max())
+    np.testing.assert_allclose(L[1][:3, :3], np.sqrt(2.0) * np.eye(3))
+    np.testing.assert_array_equal(L[1][3:, 3:], np.eye(3))
+    A = sp.bsr_matrix((D, np.arange(3), np.arange(4)), shape=(18, 18)).tocsr()
+    B = oamg.block_diag_inverse(A, 6).toarray()
+    np.testing.assert_allclose(B[:6, :6] @ D[0], np.eye(6), atol=1e-12)
+    if len(H.levels) < 2:
+        return
+    rhos = [None]
+    for lv in range(1, len(H.levels)):
+        Al = sp.csr_matrix(H.levels[lv].A)
+        Li = np.linalg.inv(oamg.block_cholesky(oamg.diag_blocks(Al, 6)))
+        n = Li.shape[0]
+        T = sp.bsr_matrix((np.transpose(Li, (0, 2, 1)), np.arange(n), np.arange(n + 1)), shape=Al.shape)
+        rhos.append(float(np.abs(np.linalg.eigvalsh((T.T @ Al @ T).toarray())).max()))
+    u_ref = spsolve(K.tocsc(), F)
+    x, its = oamg.pcg(K, F, lambda r: oamg.vcycle(K, H, r, block_rho=rhos), rtol=1e-10, max_iter=300)
+    assert its < 80, its
+    assert np.linalg.norm(x - u_ref) / np.linalg.norm(u_ref) < 1e-8
+
+
 def test_setup_is_deterministic():
     m, K, F, mask = _system("c1")
     Kb = sp.bsr_matrix(K, blocksize=(3, 3))
