@@ -921,7 +921,7 @@ def run_ours(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64 PCG/SpMV/dots + f32 AMG V-cycle + f64 coarsest inverse",
+        "dtype": "f64 PCG/SpMV/dots (f32 search directions) + f32 AMG V-cycle + f64 coarsest inverse",
         "data": "synthetic",
         "config": {
             "workload": f"C3D10 I-beam {n_el} el / {ndof} DOFs, FP64 PCG + FP32 SA-AMG V-cycle to true rel.res 1e-8",

@@ -227,9 +227,11 @@ typedef struct wn_solve_params {
                          3 block Jacobi: pseudo-inverses of the diagonal node blocks
                          (solid_solver.py:237-258)                                    */
   int precision;      /* 0 FP64 throughout;
-                         1 FP64 PCG (FP64 SpMV, vectors, dots) with the preconditioner in
-                           FP32 (AMG: FP32 V-cycle values, vectors and accumulation, FP64
-                           coarsest inverse), inside the FP64 true-residual loop;
+                         1 FP64 PCG (FP64 SpMV, x, r, q and dots; on the streamed fine level
+                           the search directions p are rounded to FP32 once formed) with the
+                           preconditioner in FP32 (AMG: FP32 V-cycle values, vectors and
+                           accumulation, FP64 coarsest inverse), inside the FP64
+                           true-residual loop;
                          2 FP32 PCG (FP32 SpMV and preconditioner, FP64 dots) inside FP64
                            iterative refinement (the scheme of solid_solver.py:271-300);
                          3 as 1, with the V-cycle's fine level on the equilibrated matrix

@@ -15,7 +15,8 @@
 //   * the iterations are captured once into a CUDA graph (a chunk of iterations whose
 //     kernels return early once the device-side convergence flag is set); the host reads
 //     the flag once per chunk instead of once per iteration (hip_kernels.cpp:2465-2476);
-//   * precision modes: FP64 throughout; "mixed" = FP64 PCG (FP64 SpMV, vectors, dots) with
+//   * precision modes: FP64 throughout; "mixed" = FP64 PCG (FP64 SpMV, x, r, q, dots; FP32
+//     search directions p on the streamed fine level) with
 //     an FP32 preconditioner (the V-cycle's values, vectors and accumulation in FP32, FP64
 //     coarsest inverse); "fp32 IR" = FP32 PCG (FP32 SpMV) inside FP64 iterative refinement.
 //     Every mode runs inside an FP64 refinement loop whose residual r = F - K u uses the FP64
@@ -562,9 +563,9 @@ __global__ void __launch_bounds__(kThreads, (BS == 3) ? (sizeof(TK) == 4 ? kMinB
 }
 
 // alpha = rz / (p . q); x += alpha p; r -= alpha q; rm = (TM) r (if rm != null); partC = r . r
-template <typename TK, typename TM>
+template <typename TK, typename TM, typename TP = TK>
 __global__ void __launch_bounds__(kThreads) k_update(int64_t n, TK* __restrict__ x, TK* __restrict__ r,
-                                                     TM* __restrict__ rm, const TK* __restrict__ p,
+                                                     TM* __restrict__ rm, const TP* __restrict__ p,
                                                      const TK* __restrict__ q, const double* __restrict__ partB,
                                                      double* __restrict__ partC, int nparts, int par,
                                                      PcgScalars* __restrict__ S, TM* __restrict__ d0,
@@ -585,7 +586,7 @@ __global__ void __launch_bounds__(kThreads) k_update(int64_t n, TK* __restrict__
   const TK a = (TK)alpha;
   double s = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    x[i] += a * p[i];
+    x[i] += a * (TK)p[i];
     const TK ri = r[i] - a * q[i];
     r[i] = ri;
     // rsc: the FP16 V-cycle's input is S r (and its first smoothing input S r / theta, dinv = S)
@@ -980,9 +981,9 @@ struct BetaHook {
 // the partials of r . z, reduced by every CTA as BetaHook does; block 0 records rz for the next
 // beta), then k_stream_spmv_dot_p gathers p_new like a plain SpMV -- one vector per gathered
 // DOF instead of z and p_old, the same values.
-template <typename TK, typename TM>
-__global__ void __launch_bounds__(kThreads) k_pnew(int64_t n, const TM* __restrict__ z, const TK* __restrict__ p_old,
-                                                   TK* __restrict__ p_new, const double* __restrict__ partA,
+template <typename TK, typename TM, typename TP = TK>
+__global__ void __launch_bounds__(kThreads) k_pnew(int64_t n, const TM* __restrict__ z, const TP* __restrict__ p_old,
+                                                   TP* __restrict__ p_new, const double* __restrict__ partA,
                                                    int nparts, int first, int par, PcgScalars* __restrict__ S) {
   __shared__ double sh[kThreads / 32];
   __shared__ double rz_beta[2];
@@ -992,34 +993,34 @@ __global__ void __launch_bounds__(kThreads) k_pnew(int64_t n, const TM* __restri
   BetaHook{partA, nparts, first, par, S, sh, rz_beta}();
   const double* beta = rz_beta + 1;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    p_new[i] = (TK)z[i] + (TK)*beta * p_old[i];
+    p_new[i] = (TP)((TK)z[i] + (TK)*beta * (TK)p_old[i]);
   if (blockIdx.x == 0 && threadIdx.x == 0) S->rz[par] = rz_beta[0];
 }
 
-template <typename TK>
+template <typename TK, typename TP = TK>
 struct EpiSpmvDotP {  // q = A p_new; dot: p_new . q (p_new already written)
-  const TK* __restrict__ p_new;
+  const TP* __restrict__ p_new;
   TK* __restrict__ q;
   struct Pre {
     TK pi;
   };
-  __device__ __forceinline__ Pre load(int64_t i) const { return {p_new[i]}; }
+  __device__ __forceinline__ Pre load(int64_t i) const { return {(TK)p_new[i]}; }
   __device__ __forceinline__ double store(int64_t i, const Pre& p, TK t) const {
     q[i] = t;
     return (double)p.pi * (double)t;
   }
 };
 
-template <int BS, typename TK>
+template <int BS, typename TK, typename TP = TK>
 __global__ void __launch_bounds__(kStreamThreads, (StreamDefault<TK, BS, BS>::kCtasPerSm))
-    k_stream_spmv_dot_p(StreamView m, const TK* __restrict__ p_new, TK* __restrict__ q, double* __restrict__ partB,
+    k_stream_spmv_dot_p(StreamView m, const TP* __restrict__ p_new, TK* __restrict__ q, double* __restrict__ partB,
                         PcgScalars* __restrict__ S) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ double sh[kStreamThreads / 32];
   pdl_trigger();
   bool skipped = false;
   const double dot = stream_rows<TK, BS, BS, typename StreamDefault<TK, BS, BS>::type>(
-      m.tiles, m.n_tiles, m.pack, XLoad<TK, TK>{p_new}, EpiSpmvDotP<TK>{p_new, q}, smem, &S->status, &S->done,
+      m.tiles, m.n_tiles, m.pack, XLoad<TP, TK>{p_new}, EpiSpmvDotP<TK, TP>{p_new, q}, smem, &S->status, &S->done,
       m.ctl, &skipped);
   if (skipped) return;
   write_part(dot, partB, sh);
@@ -1420,20 +1421,30 @@ static int pcg_iteration(Solid* s, SolverWork& W, int precond, int k, PcgScalars
   TK* p_new = par ? B.p1 : B.p0;
   TK* p_old = par ? B.p0 : B.p1;
   const int gup = resident_grid(k_update<TK, TM>, kThreads, (W.n + kThreads - 1) / kThreads);
+  // The mixed modes on the streamed fine level keep the search directions in FP32: p = z + beta p
+  // is formed in FP64 and rounded once, and the product and the update read that same rounded p,
+  // so q = A p and r = b - A x stay consistent in FP64; the gathers and the vector passes move
+  // half the bytes.  (FP64 everywhere else: the matrix, q, x, r and the dots.)
+  constexpr bool kMixed = std::is_same<TK, double>::value && std::is_same<TM, float>::value;
+  using TPf = typename std::conditional<kMixed, float, TK>::type;
+  bool p32 = false;
   auto spmv_dot = [&](auto bs_tag) {
     constexpr int BS = decltype(bs_tag)::value;
     if (s->fine.packed && s->fine.br == BS) {  // the fine matrix streamed through shared memory
-      auto kern = k_stream_spmv_dot_p<BS, TK>;
+      auto kern = k_stream_spmv_dot_p<BS, TK, TPf>;
       const int g = stream_grid<TK, BS, BS>(kern, s->fine.n_tiles);
-      const int gp = resident_grid(k_pnew<TK, TM>, kThreads, (W.n + kThreads - 1) / kThreads);
+      const int gp = resident_grid(k_pnew<TK, TM, TPf>, kThreads, (W.n + kThreads - 1) / kThreads);
       if (g > 0) {
-        cudaError_t e = launch_pdl(k_pnew<TK, TM>, gp, kThreads, 0, st, W.n, (const TM*)B.z, (const TK*)p_old, p_new,
-                                   (const double*)W.partA.p, W.npA, (int)(k == 0), par, S);
+        p32 = kMixed;
+        TPf* pn = reinterpret_cast<TPf*>(p_new);
+        cudaError_t e = launch_pdl(k_pnew<TK, TM, TPf>, gp, kThreads, 0, st, W.n, (const TM*)B.z,
+                                   (const TPf*)reinterpret_cast<TPf*>(p_old), pn, (const double*)W.partA.p, W.npA,
+                                   (int)(k == 0), par, S);
         if (e == cudaSuccess) {
-          note(W, st, "pcg_pnew", -1, (double)W.n * (sizeof(TM) + 2 * sizeof(TK)));
+          note(W, st, "pcg_pnew", -1, (double)W.n * (sizeof(TM) + 2 * sizeof(TPf)));
           W.launches++;
           e = launch_pdl(kern, g, kStreamThreads, stream_smem_bytes<TK, BS, BS>(), st, stream_view<TK>(s->fine),
-                         (const TK*)p_new, B.q, W.partB.p, S);
+                         (const TPf*)pn, B.q, W.partB.p, S);
           if (e == cudaSuccess) return -g;  // negative: the product's bytes are those of a plain SpMV
         }
         return 0;  // a failed launch: reported by the error check below
@@ -1450,7 +1461,8 @@ static int pcg_iteration(Solid* s, SolverWork& W, int precond, int k, PcgScalars
   // the fused product reads z and p_old and writes p_new and q; the split one reads p_new and
   // writes q (k_pnew counted its own bytes)
   note(W, st, "pcg_spmv_dot", -1,
-       mat_bytes(s->nnzb, s->bs, s->bs, s->n_nodes, sizeof(TK)) + (gsd < 0 ? 2 * nK : nM + 3 * nK));
+       mat_bytes(s->nnzb, s->bs, s->bs, s->n_nodes, sizeof(TK)) +
+           (gsd < 0 ? (p32 ? nM + nK : 2 * nK) : nM + 3 * nK));
   gsd = gsd < 0 ? -gsd : gsd;
   WN_CUDA(cudaGetLastError());
   WN_REQUIRE(gsd > 0, WN_ESTATE, "PCG product: launch failed");
@@ -1459,10 +1471,16 @@ static int pcg_iteration(Solid* s, SolverWork& W, int precond, int k, PcgScalars
   const bool pre_input = precond == 2 && !s->amg->levels.empty();
   TM* d0 = pre_input ? Prec<TM>::pcg(W).d0.p : nullptr;
   const TM it0 = pre_input ? (TM)s->amg->levels[0].inv_theta : TM(0);
-  k_update<TK, TM><<<gup, kThreads, 0, st>>>(W.n, B.x, B.r, B.rm, p_new, B.q, W.partB.p, W.partC.p, W.npB, par, S, d0,
-                                             W.half ? half_scale<TM>(W) : Prec<TM>::fine_dinv(W), it0,
-                                             half_scale<TM>(W));
-  note(W, st, "pcg_update", -1, 6 * nK + (B.rm ? nM : 0.0) + (d0 ? 2 * nM : 0.0));
+  if (p32)
+    k_update<TK, TM, TPf><<<gup, kThreads, 0, st>>>(W.n, B.x, B.r, B.rm, reinterpret_cast<const TPf*>(p_new), B.q,
+                                                    W.partB.p, W.partC.p, W.npB, par, S, d0,
+                                                    W.half ? half_scale<TM>(W) : Prec<TM>::fine_dinv(W), it0,
+                                                    half_scale<TM>(W));
+  else
+    k_update<TK, TM><<<gup, kThreads, 0, st>>>(W.n, B.x, B.r, B.rm, p_new, B.q, W.partB.p, W.partC.p, W.npB, par, S,
+                                               d0, W.half ? half_scale<TM>(W) : Prec<TM>::fine_dinv(W), it0,
+                                               half_scale<TM>(W));
+  note(W, st, "pcg_update", -1, (p32 ? 5 * nK + nM : 6 * nK) + (B.rm ? nM : 0.0) + (d0 ? 2 * nM : 0.0));
   W.npC = gup;
   k_check<<<1, kThreads, 0, st>>>(S, W.partC.p, W.npC);
   note(W, st, "pcg_check", -1, 0.0);

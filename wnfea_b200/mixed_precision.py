@@ -4,8 +4,8 @@
 On this path a configuration selects the solver's ``precision`` argument
 (``solver_precision``):
 
-* ``enabled`` with ``inner_dtype = float32`` -> ``"mixed_fp32"``: FP64 PCG (FP64 SpMV, vectors
-  and dot products) preconditioned in FP32 (the AMG V-cycle with FP32 values, vectors and
+* ``enabled`` with ``inner_dtype = float32`` -> ``"mixed_fp32"``: FP64 PCG (FP64 SpMV, x, r, q
+  and dot products; FP32 search directions on the streamed fine level) preconditioned in FP32 (the AMG V-cycle with FP32 values, vectors and
   accumulation and an FP64 coarsest inverse), inside the FP64 true-residual loop;
 * otherwise (``FULL_FP64``) -> ``"fp64"``.
 

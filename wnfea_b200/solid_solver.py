@@ -77,7 +77,8 @@ def solve_c3d10_pcg(
     reference counterpart for solids, and the fast choice for large meshes).  ``precision``:
 
     * "fp64"          -- FP64 matrix, vectors, dots and preconditioner;
-    * "mixed_fp32"    -- FP64 PCG (FP64 SpMV, vectors and dots) with the preconditioner in FP32
+    * "mixed_fp32"    -- FP64 PCG (FP64 SpMV, x, r, q and dots; FP32 search directions on the
+                         streamed fine level) with the preconditioner in FP32
                          (for "amg": FP32 V-cycle values, vectors and accumulation, FP64
                          coarsest inverse), inside the FP64 true-residual loop;
     * "mixed_fp32_ir" -- the scheme of the reference's mixed mode (:271-300): FP32 PCG (FP32
