@@ -672,14 +672,15 @@ def run_ours(args):
     # algorithmic bytes of one assembly: FP64 values written, element->block map, connectivity,
     # coordinates and element properties read
     asm_bytes = nb * 9 * 8 + n_el * 100 * 4 + n_el * 40 + n_nodes * 24 + n_el * 16
-    # the setup's wall time varies from process to process by host-side allocation and paging
-    # (0.3 to 1.9 s seen for the first call): the line reports the median of three setups
+    # the line reports the first setup of this matrix (what a new mesh pays); the two repeats
+    # rebuild while the previous hierarchy is still held and grow the device memory pool, which
+    # took from 0.3 to 1.4 s on different boxes: all three are in amg_setup_s_each
     setup_times = []
     for _ in range(3):
         t0 = time.perf_counter()
         s.amg_setup()
         setup_times.append(time.perf_counter() - t0)
-    setup_s = statistics.median(setup_times)
+    setup_s = setup_times[0]
 
     F = torch.from_numpy(F_np).cuda()
     u = torch.empty_like(F)
